@@ -1,0 +1,173 @@
+/*
+ * qxmd_b200 -- C ABI of the B200 (sm_100a) Kohn-Sham hot path of QXMD.
+ *
+ * Plain C: opaque context, host or device pointers and sizes, int status.
+ * Layouts are those of the Fortran arrays the reference subroutines take:
+ * a wavefunction block gdcr(nplwex, nband) is column-major real*8 with
+ * nplwex = 2*(nplw+1) (Re, Im of c(G) on the Gamma-point half sphere); the
+ * FFT grid index is n1 + (n2 + n3*k2)*k1 with n1 fastest.
+ *
+ * Two precisions per context: QX_PREC_FP64 (the plain drop-in) keeps every
+ * device array in FP64; QX_PREC_MIXED keeps wavefunctions, FFTs and the band
+ * contractions in FP32 and the nband x nband Cholesky / eigen-decomposition,
+ * energies and density in FP64.  Host transfer functions always take real*8.
+ *
+ * Every function returns QX_OK (0) or an error code; qx_last_error() gives
+ * the message.  Nothing here falls back to the CPU.
+ */
+#ifndef QXMD_B200_H
+#define QXMD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QX_OK 0
+#define QX_ERR_ARG 1       /* bad argument or unsupported size          */
+#define QX_ERR_CUDA 2      /* CUDA runtime error                        */
+#define QX_ERR_NOTPD 3     /* <psi_i|psi_j> not positive definite       */
+#define QX_ERR_EIG 4       /* subspace eigen-decomposition not converged */
+#define QX_ERR_STATE 5     /* call order (e.g. untryt before hmatrix)   */
+
+#define QX_PREC_FP64 0
+#define QX_PREC_MIXED 1
+
+#define QX_NL_NONE 0
+#define QX_NL_GSPACE 1     /* KB projectors in G space (lking = .false.) */
+#define QX_NL_RSPACE 2     /* KB projectors in real space (lking = .true.) */
+
+/* qx_hpsi flags */
+#define QX_HPSI_KINETIC 1
+#define QX_HPSI_NONLOCAL 2
+#define QX_HPSI_ACCUMULATE 4
+
+typedef struct qx_ctx qx_ctx;
+
+/* Convergence controls of the CG band update; defaults of
+ * modules.f90:171-182 (toleig, roughfeig, roughfzan, threinn, wdinner,
+ * itermx, iteremx) and noband (number of occupied bands). */
+typedef struct {
+  int itermx, iteremx, noband;
+  double tolera, roughfzan, roughfeig, threinn, wdinner;
+  int ccreal4;   /* FP64 contexts: round the lower-band snapshot to real*4 */
+} qx_cgparm;
+
+/* Result of one SCF iteration (energies in Ry). */
+typedef struct {
+  double etot;       /* band energy - E_H + E_xc - int V_xc rho + E_ion   */
+  double eband;      /* sum occ * eigenvalue (after subspace rotation)  */
+  double ehartree;
+  double exc;
+  double evxc;
+  double resid;      /* int (rho_out - rho_in)^2                         */
+  double zmax;       /* max band residual before the CG (gradres)        */
+  int ncg_hpsi;      /* H|psi> band applications spent in the CG        */
+  int jacobi_sweeps;
+} qx_scf_out;
+
+const char *qx_last_error(void);
+int qx_version(void);
+
+/* ---- set-up (module state of the reference, uploaded once per geometry) -- */
+
+/* Grid and G sphere: the outputs of reclat/set_rciprl (reclat.f90:167-475,
+ * modules.f90:1402-1603).  ijkgd: 2*nplw+1 zero-based grid indices of G index
+ * -nplw..nplw (ijkgd(-nplw:nplw) of reclat.f90:256-274 minus one);
+ * dkgnrm: |G|^2 per real component, 2*(nplw+1).  stream: cudaStream_t or 0. */
+int qx_create(qx_ctx **ctx, int precision, int kfft1, int kfft2, int kfft3, int nplw, const int *ijkgd,
+              const double *dkgnrm, int nband, void *stream);
+int qx_destroy(qx_ctx *ctx);
+
+/* glocal(kfft0): total local potential on the FFT grid (pwlda.f90:1984-2024). */
+int qx_set_glocal(qx_ctx *ctx, const double *glocal);
+/* G-space KB tables, eqlmr_(nplwex, nproj) and vclalp(nproj)
+ * (setbgq nlkbpp.f90:2135-2187, setnlc_g nlkbpp.f90:1236-1279). */
+int qx_set_kb_g(qx_ctx *ctx, int nproj, const double *eqlmr, const double *vclalp);
+/* Real-space KB tables (setnlc nlkbppr.f90:1010-1768, used by calnlc
+ * nlkbppr.f90:1773-1900): atom a owns points off[a]..off[a+1]-1 with
+ * zero-based grid index mesh[] and projector values vnl[point*lmx + l];
+ * clalp(lmx) = clalp_ncr; rdelv = volume per grid point.  lmx must be 4. */
+int qx_set_kb_r(qx_ctx *ctx, int natom, int lmx, const int *off, const int *mesh, const double *vnl,
+                const double *clalp, double rdelv);
+int qx_set_nlmode(qx_ctx *ctx, int mode);
+/* occ(nband) and the cell volume (softchg weights occ/rvol, chgdns.f90:421). */
+int qx_set_occ(qx_ctx *ctx, const double *occ, double rvol);
+
+/* ---- host <-> device (real*8 host arrays) ------------------------------ */
+int qx_put_psi(qx_ctx *ctx, const double *gdcr);
+int qx_get_psi(qx_ctx *ctx, double *gdcr);
+int qx_put_hpsi(qx_ctx *ctx, const double *rhcr);
+int qx_get_hpsi(qx_ctx *ctx, double *rhcr);
+int qx_get_eig(qx_ctx *ctx, double *eig);
+int qx_get_rho(qx_ctx *ctx, double *rho);
+int qx_put_rho(qx_ctx *ctx, const double *rho);
+int qx_get_glocal(qx_ctx *ctx, double *glocal);
+/* Device pointers of the resident arrays: 0 psi, 1 hpsi, 2 rho_in (double),
+ * 3 rho_out (double), 4 eig (double).  psi/hpsi are double or float by
+ * precision. */
+void *qx_dev_ptr(qx_ctx *ctx, int which);
+int qx_sync(qx_ctx *ctx);
+
+/* ---- hot path on device-resident data ---------------------------------- */
+
+/* hc = [hc +] T c + V_loc c [+ V_NL c] for nb bands of device array c
+ * (leading dimension nplwex, the context's precision): hcnonloc
+ * (engrad.f90:411-606) with the kinetic term (eigen.f90:335) and KB part
+ * (hckbpp_ib_g nlkbpp.f90:1623-1721 or calnlc) chosen by flags. */
+int qx_hpsi(qx_ctx *ctx, const void *c, void *hc, int nb, int flags);
+/* ekinetic2 (engrad.f90:75-127): ekib(b) = 2 <psi_b|T|psi_b>; *ekin = sum occ <T>. */
+int qx_ekinetic(qx_ctx *ctx, double *ekin, double *ekib);
+/* enonloc2 + ekinetic2 HC products for all bands: hpsi = H psi. */
+int qx_enonloc(qx_ctx *ctx);
+/* hmatrix2 (engrad.f90:845-956): H_sub = <psi|H|psi>, eig = diag. */
+int qx_hmatrix(qx_ctx *ctx, double *hsub);
+/* gradresnv (engrad.f90:1013-1067). */
+int qx_gradres(qx_ctx *ctx, double *prod, double *zmax, double *zsum);
+/* untryt2 (eigen.f90:1171-1331): diagonalise the last H_sub, psi <- psi U;
+ * eigenvalues ascending into ev (nullable). */
+int qx_untryt(qx_ctx *ctx, double *ev);
+/* untryhc2 (eigen.f90:1383-1451): hpsi <- hpsi U with the same U. */
+int qx_untryhc(qx_ctx *ctx);
+/* eigen_BKL (eigen.f90:199-938) for all bands; needs hpsi = H psi and the
+ * ekib of the last qx_ekinetic.  nriter (nullable): iterations per band. */
+int qx_eigen(qx_ctx *ctx, const qx_cgparm *p, int *nriter, int *nhpsi);
+/* schmidt2 (schmidt.f90:117-378): psi <- psi L^-T. */
+int qx_schmidt(qx_ctx *ctx);
+/* softchg (chgdns.f90:388-454): rho_out(r) = sum occ/Omega psi(r)^2. */
+int qx_softchg(qx_ctx *ctx);
+
+/* ---- one SCF iteration (pwlda.f90:1628-3700 order) --------------------- */
+/* vloc(kfft0): local pseudopotential on the grid; cross: 2*pi*reciprocal
+ * vectors, column-major 3x3; eion: ion-ion energy added to etot. */
+int qx_scf_init(qx_ctx *ctx, const double *vloc, const double *cross, double ecutdens, double eion, double mixbeta,
+                double kerker_q0);
+/* rho_in <- rho_out of the current psi (start of an SCF run). */
+int qx_scf_rho_from_psi(qx_ctx *ctx);
+int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
+
+/* ---- drop-in shims with the reference's host-array arguments ----------- */
+/* hcnonloc: rhcr(nplwex, nb) += local (+ real-space KB) H products of cgjr. */
+int qxgpu_hcnonloc(qx_ctx *ctx, const double *cgjr, double *rhcr, int nb);
+/* hckbpp_g (nlkbpp.f90:1284-1393): rhcr += G-space KB products of cgjr. */
+int qxgpu_hckbpp_g(qx_ctx *ctx, const double *cgjr, double *rhcr, int nb);
+/* ekinetic + enonloc: rhcr = H cgjr for all nband bands; ekib(nband). */
+int qxgpu_enonloc(qx_ctx *ctx, const double *cgjr, double *rhcr, double *ekib);
+/* eigen (eigen.f90:52): gdcr, rhcr updated in place; eig out. */
+int qxgpu_eigen(qx_ctx *ctx, double *gdcr, double *rhcr, const double *ekib, double *eig, const qx_cgparm *p);
+/* schmidt (schmidt.f90:71): cgjr orthonormalised in place. */
+int qxgpu_schmidt(qx_ctx *ctx, double *cgjr);
+/* hmatrix (engrad.f90:804): dmtrxr(nband, nband) and eig from cgjr, rhcr. */
+int qxgpu_hmatrix(qx_ctx *ctx, const double *cgjr, const double *rhcr, double *dmtrxr, double *eig);
+/* untryt + untryhc (eigen.f90:1118, 1336) after qxgpu_hmatrix: gdcr, rhcr rotated in place. */
+int qxgpu_untryt(qx_ctx *ctx, double *gdcr, double *rhcr, double *ev);
+/* softchg: glocal(kfft0) = sum occ/rvol |psi(r)|^2 of cgjr. */
+int qxgpu_softchg(qx_ctx *ctx, const double *cgjr, double *rho);
+/* rfft3 (fft3.f90:113-232) on the full grid: key = 1 forward real -> complex
+ * scaled 1/kfft0 (fft3x = Re, fft3y = Im on the full grid), key = 2 backward
+ * complex -> real (fft3x out, fft3y zeroed). */
+int qxgpu_rfft3(qx_ctx *ctx, int key, double *fft3x, double *fft3y);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1037 @@
+// C ABI of the hot path: context, plan construction and the entry points that
+// mirror the reference subroutines (see include/qxmd_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/qxmd_b200.h"
+#include "qx_cg.h"
+#include "qx_internal.h"
+#include "qx_scf.h"
+
+namespace qx {
+static thread_local char g_err[512] = "";
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+}  // namespace qx
+
+using namespace qx;
+
+#define CK(x)                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = (x);                                                              \
+    if (e_ != cudaSuccess) {                                                           \
+      set_error("%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e_));       \
+      return QX_ERR_CUDA;                                                              \
+    }                                                                                  \
+  } while (0)
+
+#define CKL()                                                                          \
+  do {                                                                                 \
+    cudaError_t e_ = cudaGetLastError();                                               \
+    if (e_ != cudaSuccess) {                                                           \
+      set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_));       \
+      return QX_ERR_CUDA;                                                              \
+    }                                                                                  \
+  } while (0)
+
+#define TRY(x)                   \
+  do {                           \
+    int r_ = (x);                \
+    if (r_) return r_;           \
+  } while (0)
+
+struct qx_ctx {
+  int prec = 0;
+  cudaStream_t st = 0;
+  Plan pl;
+  int nb = 0, ne = 0, npair_all = 0;
+  int nlmode = 0;
+  double rvol = 0.0;
+  bool have_occ = false, have_glocal = false, have_hsub = false, have_u = false, have_kbg = false, have_kbr = false;
+  // FP64 small arrays
+  double *d_dk = nullptr, *d_occ = nullptr, *d_wocc = nullptr, *d_eig = nullptr, *d_ekib = nullptr, *d_w = nullptr;
+  double *d_hsub = nullptr, *d_mat = nullptr, *d_V = nullptr;   // nb*nb, nb*nb, 2*nb*nb
+  double *d_prod = nullptr;
+  int *d_info = nullptr;
+  int *d_allpairs = nullptr;
+  // state arrays in the context precision
+  void *psi = nullptr, *hpsi = nullptr, *g = nullptr, *h = nullptr, *gh = nullptr, *snap = nullptr, *tmp = nullptr;
+  void *mat_t = nullptr;   // nb*nb in T
+  void *proj = nullptr;    // nproj*nb in T
+  CgState cg;
+  // density side
+  double *d_rho_in = nullptr, *d_rho_out = nullptr, *d_vloc = nullptr, *d_glocal = nullptr, *d_g2 = nullptr;
+  double2 *d_zg = nullptr;
+  double *d_part = nullptr, *d_sc = nullptr;
+  double eion = 0.0, mixbeta = 0.3, q02 = 1.0;
+  bool scf_ready = false;
+  std::vector<void *> allocs;
+  size_t tsize() const { return prec == QX_PREC_FP64 ? sizeof(double) : sizeof(float); }
+};
+
+static int dalloc(qx_ctx *c, void **p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  CK(cudaMalloc(p, bytes));
+  c->allocs.push_back(*p);
+  return 0;
+}
+template <typename P>
+static int dalloc(qx_ctx *c, P **p, size_t bytes) {
+  void *v = nullptr;
+  TRY(dalloc(c, &v, bytes));
+  *p = (P *)v;
+  return 0;
+}
+
+extern "C" const char *qx_last_error(void) { return g_err; }
+extern "C" int qx_version(void) { return 1; }
+
+// ---------------------------------------------------------------------------
+static bool factor_len(int n, FftLen &L) {
+  L.n = n;
+  L.nstage = 0;
+  int m = n;
+  const int rad[5] = {4, 2, 3, 5, 7};
+  for (int r : rad) {
+    while (m % r == 0) {
+      if (L.nstage >= 8) return false;
+      L.radix[L.nstage++] = r;
+      m /= r;
+    }
+  }
+  if (m != 1) return false;
+  if (n == 1) { L.radix[0] = 1; }
+  return true;
+}
+
+template <typename T>
+static int upload_tw(qx_ctx *c) {
+  typedef typename c2t<T>::type C;
+  Plan &pl = c->pl;
+  const int tot = pl.k1 + pl.k2 + pl.k3;
+  std::vector<C> h(tot);
+  const int ns[3] = {pl.k1, pl.k2, pl.k3};
+  const double tp = 2.0 * std::acos(-1.0);
+  for (int d = 0; d < 3; ++d)
+    for (int t = 0; t < ns[d]; ++t) {
+      h[pl.tw_off[d] + t].x = (T)std::cos(tp * t / ns[d]);
+      h[pl.tw_off[d] + t].y = (T)-std::sin(tp * t / ns[d]);
+    }
+  C *dp = nullptr;
+  TRY(dalloc(c, &dp, sizeof(C) * tot));
+  CK(cudaMemcpy(dp, h.data(), sizeof(C) * tot, cudaMemcpyHostToDevice));
+  pl.bufs<T>().tw = dp;
+  return 0;
+}
+
+template <typename T>
+static int alloc_pipe(qx_ctx *c) {
+  typedef typename c2t<T>::type C;
+  Plan &pl = c->pl;
+  Bufs<T> &b = pl.bufs<T>();
+  const long per_pair = (long)pl.k3 * pl.P2 * pl.P1 + (long)pl.k3 * pl.k2 * pl.P1 + (long)(pl.nplw + 1) * 2;
+  const char *env = getenv("QX_CHUNK_MB");
+  const double mb = env ? atof(env) : 64.0;
+  long ch = (long)(mb * 1048576.0 / (sizeof(C) * (double)per_pair));
+  ch = std::max(1L, std::min(ch, (long)c->npair_all));
+  pl.chunk = (int)ch;
+  TRY(dalloc(c, &b.bufA, sizeof(C) * ch * pl.k3 * pl.P2 * pl.P1));
+  TRY(dalloc(c, &b.bufB, sizeof(C) * ch * pl.k3 * pl.k2 * pl.P1));
+  TRY(dalloc(c, &b.zsph, sizeof(C) * ch * (pl.nplw + 1) * 2));
+  TRY(dalloc(c, &b.vloc, sizeof(T) * pl.n));
+  CK(cudaMemset(b.vloc, 0, sizeof(T) * pl.n));
+  TRY(upload_tw<T>(c));
+  // shared-memory opt-in for the largest launch of this plan
+  const size_t cs = sizeof(C);
+  size_t need = 0;
+  auto fs = [&](int n, int ld) { return cs * (n + 2 * (size_t)n * ld); };
+  need = std::max(need, fs(pl.k3, pl.P1 | 1));
+  need = std::max(need, fs(pl.k2, pl.P1));
+  need = std::max(need, fs(pl.k1, pl.xlines<T>() | 1));
+  need = std::max(need, fs(pl.k1, pl.rholines | 1) + sizeof(double) * pl.rholines * pl.k1);
+  need = std::max(need, fs(pl.k3, 17));
+  need = std::max(need, fs(pl.k2, 17));
+  if (need > 227 * 1024) {
+    set_error("FFT tile needs %zu bytes of shared memory (> 227 KB)", need);
+    return QX_ERR_ARG;
+  }
+  set_fft_smem_limits<T>(need);
+  CKL();
+  return 0;
+}
+
+extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, int nplw, const int *ijkgd,
+                         const double *dkgnrm, int nband, void *stream) {
+  if (!out || !ijkgd || !dkgnrm || k1 <= 0 || k2 <= 0 || k3 <= 0 || nplw < 0 || nband <= 0 ||
+      (precision != QX_PREC_FP64 && precision != QX_PREC_MIXED)) {
+    set_error("qx_create: bad arguments");
+    return QX_ERR_ARG;
+  }
+  qx_ctx *c = new qx_ctx();
+  *out = nullptr;
+  c->prec = precision;
+  c->st = (cudaStream_t)stream;
+  c->nb = nband;
+  c->ne = 2 * (nplw + 1);
+  c->npair_all = (nband + 1) / 2;
+  Plan &pl = c->pl;
+  pl.k1 = k1; pl.k2 = k2; pl.k3 = k3;
+  pl.n = (long)k1 * k2 * k3;
+  pl.nplw = nplw;
+  pl.nplwex = c->ne;
+  if (!factor_len(k1, pl.L[0]) || !factor_len(k2, pl.L[1]) || !factor_len(k3, pl.L[2])) {
+    set_error("qx_create: FFT sizes must be products of 2,3,5,7 (got %d %d %d)", k1, k2, k3);
+    delete c;
+    return QX_ERR_ARG;
+  }
+  pl.tw_off[0] = 0; pl.tw_off[1] = k1; pl.tw_off[2] = k1 + k2;
+  // sphere geometry from ijkgd
+  std::vector<int> n1(nplw + 1), n2(nplw + 1), i3v(nplw + 1);
+  int m1 = 0, m2 = 0, m3 = 0;
+  for (int ig = 0; ig <= nplw; ++ig) {
+    const long ijk = ijkgd[nplw + ig];
+    if (ijk < 0 || ijk >= pl.n) { set_error("qx_create: ijkgd out of range"); delete c; return QX_ERR_ARG; }
+    const int a = (int)(ijk % k1), b = (int)((ijk / k1) % k2), d = (int)(ijk / ((long)k1 * k2));
+    n1[ig] = a <= k1 / 2 ? a : a - k1;
+    n2[ig] = b <= k2 / 2 ? b : b - k2;
+    const int n3 = d <= k3 / 2 ? d : d - k3;
+    i3v[ig] = d;
+    m1 = std::max(m1, std::abs(n1[ig]));
+    m2 = std::max(m2, std::abs(n2[ig]));
+    m3 = std::max(m3, std::abs(n3));
+    // -G must sit at the mirrored index
+    const long ijm = ijkgd[nplw - ig];
+    const int am = (int)(ijm % k1), bm = (int)((ijm / k1) % k2), dm = (int)(ijm / ((long)k1 * k2));
+    if (am != (k1 - a) % k1 || bm != (k2 - b) % k2 || dm != (k3 - d) % k3) {
+      set_error("qx_create: ijkgd(-G) is not the mirror of ijkgd(G) at G index %d", ig);
+      delete c;
+      return QX_ERR_ARG;
+    }
+  }
+  if (2 * m1 + 1 > k1 || 2 * m2 + 1 > k2 || 2 * m3 + 1 > k3) {
+    set_error("qx_create: wavefunction sphere does not fit the grid");
+    delete c;
+    return QX_ERR_ARG;
+  }
+  pl.m1 = m1; pl.m2 = m2; pl.m3 = m3;
+  pl.P1 = 2 * m1 + 1; pl.P2 = 2 * m2 + 1;
+  // row CSR of the +G and -G positions
+  struct Ent { int j2, a, i3, ig, sgn; };
+  std::vector<Ent> ents;
+  ents.reserve(2 * nplw + 1);
+  for (int ig = 0; ig <= nplw; ++ig) {
+    ents.push_back({n2[ig] + m2, n1[ig] + m1, i3v[ig], ig, +1});
+    if (ig) ents.push_back({-n2[ig] + m2, -n1[ig] + m1, (k3 - i3v[ig]) % k3, ig, -1});
+  }
+  std::vector<int> lo(pl.P2, 1 << 30), hi(pl.P2, -1), cnt(pl.P2 + 1, 0);
+  for (auto &e : ents) {
+    lo[e.j2] = std::min(lo[e.j2], e.a);
+    hi[e.j2] = std::max(hi[e.j2], e.a);
+    cnt[e.j2 + 1]++;
+  }
+  for (int j = 0; j < pl.P2; ++j) {
+    if (hi[j] < 0) { lo[j] = 1; hi[j] = 0; }
+    cnt[j + 1] += cnt[j];
+  }
+  std::vector<int4> rent(ents.size());
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  for (auto &e : ents) rent[fill[e.j2]++] = make_int4(e.a - lo[e.j2], e.i3, e.ig, e.sgn);
+  int rc = 0;
+#define FAIL(x) do { rc = (x); if (rc) { qx_destroy(c); return rc; } } while (0)
+  FAIL(dalloc(c, &pl.d_row_lo, sizeof(int) * pl.P2));
+  FAIL(dalloc(c, &pl.d_row_hi, sizeof(int) * pl.P2));
+  FAIL(dalloc(c, &pl.d_row_off, sizeof(int) * (pl.P2 + 1)));
+  FAIL(dalloc(c, &pl.d_row_ent, sizeof(int4) * rent.size()));
+  if (cudaMemcpy(pl.d_row_lo, lo.data(), sizeof(int) * pl.P2, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(pl.d_row_hi, hi.data(), sizeof(int) * pl.P2, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(pl.d_row_off, cnt.data(), sizeof(int) * (pl.P2 + 1), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(pl.d_row_ent, rent.data(), sizeof(int4) * rent.size(), cudaMemcpyHostToDevice)) {
+    set_error("qx_create: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+    qx_destroy(c);
+    return QX_ERR_CUDA;
+  }
+  // small FP64 arrays
+  const int nb = nband, ne = c->ne;
+  FAIL(dalloc(c, &c->d_dk, sizeof(double) * ne));
+  if (cudaMemcpy(c->d_dk, dkgnrm, sizeof(double) * ne, cudaMemcpyHostToDevice)) { qx_destroy(c); return QX_ERR_CUDA; }
+  FAIL(dalloc(c, &c->d_occ, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_wocc, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_eig, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_ekib, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_w, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_prod, sizeof(double) * nb));
+  FAIL(dalloc(c, &c->d_hsub, sizeof(double) * nb * nb));
+  FAIL(dalloc(c, &c->d_mat, sizeof(double) * nb * nb));
+  FAIL(dalloc(c, &c->d_V, sizeof(double) * 2 * nb * nb));
+  FAIL(dalloc(c, &c->d_info, sizeof(int) * 4));
+  std::vector<int> pairs(2 * c->npair_all);
+  for (int p = 0; p < c->npair_all; ++p) {
+    pairs[2 * p] = 2 * p;
+    pairs[2 * p + 1] = (2 * p + 1 < nb) ? 2 * p + 1 : -1;
+  }
+  FAIL(dalloc(c, &c->d_allpairs, sizeof(int) * pairs.size()));
+  cudaMemcpy(c->d_allpairs, pairs.data(), sizeof(int) * pairs.size(), cudaMemcpyHostToDevice);
+  // state arrays
+  const size_t ts = c->tsize(), blk = ts * (size_t)nb * ne;
+  FAIL(dalloc(c, &c->psi, blk));
+  FAIL(dalloc(c, &c->hpsi, blk));
+  FAIL(dalloc(c, &c->g, blk));
+  FAIL(dalloc(c, &c->h, blk));
+  FAIL(dalloc(c, &c->gh, blk));
+  FAIL(dalloc(c, &c->snap, blk));
+  FAIL(dalloc(c, &c->tmp, blk));
+  FAIL(dalloc(c, &c->mat_t, ts * nb * nb));
+  cudaMemset(c->psi, 0, blk);
+  cudaMemset(c->hpsi, 0, blk);
+  // CG state
+  CgState &s = c->cg;
+  double **dd[] = {&s.eig, &s.zansa, &s.zansab, &s.z000re, &s.x000re, &s.eigb, &s.betk, &s.dinnerx, &s.cai};
+  for (auto p : dd) FAIL(dalloc(c, p, sizeof(double) * nb));
+  s.ekib = c->d_ekib;
+  int **ii[] = {&s.iter, &s.izcnt, &s.lreset, &s.active, &s.list};
+  for (auto p : ii) FAIL(dalloc(c, p, sizeof(int) * nb));
+  FAIL(dalloc(c, &s.pairs, sizeof(int) * 2 * c->npair_all));
+  FAIL(dalloc(c, &s.nact, sizeof(int)));
+  FAIL(dalloc(c, &s.npair, sizeof(int)));
+  // pipeline buffers for the context precision (FP64 density FFTs always)
+  if (c->prec == QX_PREC_FP64) {
+    FAIL(alloc_pipe<double>(c));
+  } else {
+    FAIL(alloc_pipe<float>(c));
+    TRY(upload_tw<double>(c));
+    set_fft_smem_limits<double>(227 * 1024);
+  }
+  if (cudaGetLastError() != cudaSuccess) { set_error("qx_create: CUDA error during set-up"); qx_destroy(c); return QX_ERR_CUDA; }
+#undef FAIL
+  *out = c;
+  return QX_OK;
+}
+
+extern "C" int qx_destroy(qx_ctx *c) {
+  if (!c) return QX_OK;
+  cudaStreamSynchronize(c->st);
+  for (void *p : c->allocs) cudaFree(p);
+  delete c;
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+static int upload_conv(qx_ctx *c, T *dst, const double *src, long n) {
+  if (sizeof(T) == sizeof(double)) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    return 0;
+  }
+  double *tmp = nullptr;
+  CK(cudaMallocAsync((void **)&tmp, sizeof(double) * n, c->st));
+  CK(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  convert<double, T>(tmp, dst, n, c->st);
+  CK(cudaFreeAsync(tmp, c->st));
+  CKL();
+  return 0;
+}
+
+template <typename T>
+static int download_conv(qx_ctx *c, double *dst, const T *src, long n) {
+  if (sizeof(T) == sizeof(double)) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  double *tmp = nullptr;
+  CK(cudaMallocAsync((void **)&tmp, sizeof(double) * n, c->st));
+  convert<T, double>(src, tmp, n, c->st);
+  CK(cudaMemcpyAsync(dst, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(tmp, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+static int up(qx_ctx *c, void *dst, const double *src, long n) {
+  return c->prec == QX_PREC_FP64 ? upload_conv<double>(c, (double *)dst, src, n)
+                                 : upload_conv<float>(c, (float *)dst, src, n);
+}
+static int down(qx_ctx *c, double *dst, const void *src, long n) {
+  return c->prec == QX_PREC_FP64 ? download_conv<double>(c, dst, (const double *)src, n)
+                                 : download_conv<float>(c, dst, (const float *)src, n);
+}
+
+extern "C" int qx_set_glocal(qx_ctx *c, const double *glocal) {
+  if (!c || !glocal) { set_error("qx_set_glocal: null"); return QX_ERR_ARG; }
+  if (!c->d_glocal) TRY(dalloc(c, &c->d_glocal, sizeof(double) * c->pl.n));
+  CK(cudaMemcpyAsync(c->d_glocal, glocal, sizeof(double) * c->pl.n, cudaMemcpyHostToDevice, c->st));
+  if (c->prec == QX_PREC_FP64)
+    convert<double, double>(c->d_glocal, c->pl.b64.vloc, c->pl.n, c->st);
+  else
+    convert<double, float>(c->d_glocal, c->pl.b32.vloc, c->pl.n, c->st);
+  CKL();
+  c->have_glocal = true;
+  return QX_OK;
+}
+
+extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const double *vclalp) {
+  if (!c || nproj <= 0 || !eqlmr || !vclalp) { set_error("qx_set_kb_g: bad arguments"); return QX_ERR_ARG; }
+  const size_t ts = c->tsize();
+  void *kbg = nullptr, *vcl = nullptr, *proj = nullptr;
+  TRY(dalloc(c, &kbg, ts * (size_t)nproj * c->ne));
+  TRY(dalloc(c, &vcl, ts * nproj));
+  TRY(dalloc(c, &proj, ts * (size_t)nproj * c->nb));
+  TRY(up(c, kbg, eqlmr, (long)nproj * c->ne));
+  TRY(up(c, vcl, vclalp, nproj));
+  c->pl.nproj = nproj;
+  if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
+  else { c->pl.b32.kbg = (float *)kbg; c->pl.b32.vclalp = (float *)vcl; }
+  c->proj = proj;
+  c->have_kbg = true;
+  return QX_OK;
+}
+
+extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const int *mesh, const double *vnl,
+                           const double *clalp, double rdelv) {
+  if (!c || natom <= 0 || lmx != 4 || !off || !mesh || !vnl || !clalp) {
+    set_error("qx_set_kb_r: bad arguments (lmx must be 4)");
+    return QX_ERR_ARG;
+  }
+  Plan &pl = c->pl;
+  const int npts = off[natom];
+  for (int a = 0; a < natom; ++a)
+    if (off[a + 1] < off[a]) { set_error("qx_set_kb_r: off not ascending"); return QX_ERR_ARG; }
+  for (int i = 0; i < npts; ++i)
+    if (mesh[i] < 0 || mesh[i] >= pl.n) { set_error("qx_set_kb_r: mesh index out of range"); return QX_ERR_ARG; }
+  // line CSR: the projector points that fall on each x line (i3*k2 + i2)
+  const long nlines = (long)pl.k2 * pl.k3;
+  std::vector<int> loff(nlines + 1, 0);
+  for (int i = 0; i < npts; ++i) loff[mesh[i] / pl.k1 + 1]++;
+  for (long l = 0; l < nlines; ++l) loff[l + 1] += loff[l];
+  std::vector<int4> lent(std::max(npts, 1));
+  std::vector<int> fill(loff.begin(), loff.end() - 1);
+  for (int a = 0; a < natom; ++a)
+    for (int i = off[a]; i < off[a + 1]; ++i) lent[fill[mesh[i] / pl.k1]++] = make_int4(mesh[i] % pl.k1, i, a, 0);
+  TRY(dalloc(c, &pl.d_kb_off, sizeof(int) * (natom + 1)));
+  TRY(dalloc(c, &pl.d_kb_mesh, sizeof(int) * std::max(npts, 1)));
+  TRY(dalloc(c, &pl.d_kb_clalp, sizeof(double) * lmx));
+  TRY(dalloc(c, &pl.d_line_off, sizeof(int) * (nlines + 1)));
+  TRY(dalloc(c, &pl.d_line_ent, sizeof(int4) * lent.size()));
+  CK(cudaMemcpy(pl.d_kb_off, off, sizeof(int) * (natom + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pl.d_kb_mesh, mesh, sizeof(int) * npts, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pl.d_kb_clalp, clalp, sizeof(double) * lmx, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pl.d_line_off, loff.data(), sizeof(int) * (nlines + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(pl.d_line_ent, lent.data(), sizeof(int4) * lent.size(), cudaMemcpyHostToDevice));
+  void *v = nullptr;
+  TRY(dalloc(c, &v, c->tsize() * (size_t)npts * 4));
+  TRY(up(c, v, vnl, (long)npts * 4));
+  pl.natom = natom;
+  pl.npts = npts;
+  pl.rdelv = rdelv;
+  // real-space line buffer and projection sums, per chunk
+  const long ch = pl.chunk;
+  if (c->prec == QX_PREC_FP64) {
+    pl.b64.kb_vnl = (double *)v;
+    TRY(dalloc(c, &pl.b64.bufR, sizeof(double2) * ch * pl.n));
+    TRY(dalloc(c, &pl.b64.sumr, sizeof(double2) * ch * natom * 4));
+  } else {
+    pl.b32.kb_vnl = (float *)v;
+    TRY(dalloc(c, &pl.b32.bufR, sizeof(float2) * ch * pl.n));
+    TRY(dalloc(c, &pl.b32.sumr, sizeof(float2) * ch * natom * 4));
+  }
+  c->have_kbr = true;
+  return QX_OK;
+}
+
+extern "C" int qx_set_nlmode(qx_ctx *c, int mode) {
+  if (!c || mode < 0 || mode > 2) { set_error("qx_set_nlmode: bad mode"); return QX_ERR_ARG; }
+  if (mode == QX_NL_GSPACE && !c->have_kbg) { set_error("qx_set_nlmode: G-space tables not set"); return QX_ERR_STATE; }
+  if (mode == QX_NL_RSPACE && !c->have_kbr) { set_error("qx_set_nlmode: real-space tables not set"); return QX_ERR_STATE; }
+  c->nlmode = mode;
+  return QX_OK;
+}
+
+__global__ void k_wocc(const double *occ, double *w, int n, double rv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w[i] = occ[i] / rv;
+}
+
+extern "C" int qx_set_occ(qx_ctx *c, const double *occ, double rvol) {
+  if (!c || !occ || rvol <= 0) { set_error("qx_set_occ: bad arguments"); return QX_ERR_ARG; }
+  CK(cudaMemcpyAsync(c->d_occ, occ, sizeof(double) * c->nb, cudaMemcpyHostToDevice, c->st));
+  k_wocc<<<(c->nb + 127) / 128, 128, 0, c->st>>>(c->d_occ, c->d_wocc, c->nb, rvol);
+  CKL();
+  c->rvol = rvol;
+  c->have_occ = true;
+  return QX_OK;
+}
+
+extern "C" int qx_put_psi(qx_ctx *c, const double *x) { return c && x ? up(c, c->psi, x, (long)c->nb * c->ne) : QX_ERR_ARG; }
+extern "C" int qx_get_psi(qx_ctx *c, double *x) { return c && x ? down(c, x, c->psi, (long)c->nb * c->ne) : QX_ERR_ARG; }
+extern "C" int qx_put_hpsi(qx_ctx *c, const double *x) { return c && x ? up(c, c->hpsi, x, (long)c->nb * c->ne) : QX_ERR_ARG; }
+extern "C" int qx_get_hpsi(qx_ctx *c, double *x) { return c && x ? down(c, x, c->hpsi, (long)c->nb * c->ne) : QX_ERR_ARG; }
+extern "C" int qx_get_eig(qx_ctx *c, double *x) {
+  if (!c || !x) return QX_ERR_ARG;
+  CK(cudaMemcpyAsync(x, c->d_eig, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return QX_OK;
+}
+
+static int ensure_rho(qx_ctx *c) {
+  if (!c->d_rho_out) {
+    TRY(dalloc(c, &c->d_rho_out, sizeof(double) * c->pl.n));
+    TRY(dalloc(c, &c->d_rho_in, sizeof(double) * c->pl.n));
+    CK(cudaMemset(c->d_rho_in, 0, sizeof(double) * c->pl.n));
+  }
+  return 0;
+}
+extern "C" int qx_get_rho(qx_ctx *c, double *x) {
+  if (!c || !x || !c->d_rho_out) { set_error("qx_get_rho: no density"); return QX_ERR_STATE; }
+  CK(cudaMemcpyAsync(x, c->d_rho_out, sizeof(double) * c->pl.n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return QX_OK;
+}
+extern "C" int qx_put_rho(qx_ctx *c, const double *x) {
+  if (!c || !x) return QX_ERR_ARG;
+  TRY(ensure_rho(c));
+  CK(cudaMemcpyAsync(c->d_rho_in, x, sizeof(double) * c->pl.n, cudaMemcpyHostToDevice, c->st));
+  return QX_OK;
+}
+extern "C" int qx_get_glocal(qx_ctx *c, double *x) {
+  if (!c || !x || !c->d_glocal) return QX_ERR_STATE;
+  CK(cudaMemcpyAsync(x, c->d_glocal, sizeof(double) * c->pl.n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return QX_OK;
+}
+extern "C" void *qx_dev_ptr(qx_ctx *c, int which) {
+  if (!c) return nullptr;
+  switch (which) {
+    case 0: return c->psi;
+    case 1: return c->hpsi;
+    case 2: return c->d_rho_in;
+    case 3: return c->d_rho_out;
+    case 4: return c->d_eig;
+    default: return nullptr;
+  }
+}
+extern "C" int qx_sync(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  CKL();
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+static PipeParams base_params(const qx_ctx *c) {
+  const Plan &pl = c->pl;
+  PipeParams P;
+  P.k1 = pl.k1; P.k2 = pl.k2; P.k3 = pl.k3;
+  P.m1 = pl.m1; P.m2 = pl.m2; P.P1 = pl.P1; P.P2 = pl.P2;
+  P.nplw = pl.nplw;
+  P.L1 = pl.L[0]; P.L2 = pl.L[1]; P.L3 = pl.L[2];
+  P.row_lo = pl.d_row_lo; P.row_hi = pl.d_row_hi; P.row_off = pl.d_row_off; P.row_ent = pl.d_row_ent;
+  P.pairs = c->d_allpairs;
+  P.npair_dev = nullptr;
+  P.npair = c->npair_all;
+  P.pair0 = 0;
+  P.inv_n = 1.0 / (double)pl.n;
+  return P;
+}
+
+// H|c> for the bands listed in `pairs` (device, 2 per pair).  npair_dev
+// (device count) bounds the pairs; npair_max is the host bound.  colmap /
+// ncol_dev list the same bands for the G-space KB GEMMs.
+template <typename T>
+static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const int *npair_dev, int npair_max,
+                     const int *colmap, const int *ncol_dev, int ncol_max, int flags) {
+  if (!c->have_glocal) { set_error("hpsi: glocal not set"); return QX_ERR_STATE; }
+  const Plan &pl = c->pl;
+  PipeParams P = base_params(c);
+  P.pairs = pairs;
+  P.npair_dev = npair_dev;
+  const int nlm = (flags & QX_HPSI_NONLOCAL) ? c->nlmode : 0;
+  const double *dk = (flags & QX_HPSI_KINETIC) ? c->d_dk : nullptr;
+  const int acc = (flags & QX_HPSI_ACCUMULATE) ? 1 : 0;
+  for (int p0 = 0; p0 < npair_max; p0 += pl.chunk) {
+    P.pair0 = p0;
+    const int npl = std::min(pl.chunk, npair_max - p0);
+    P.npair = npair_max;
+    TRY(launch_hpsi_chunk<T>(pl, P, npl, cin, c->ne, out, c->ne, dk, acc, nlm == QX_NL_RSPACE ? 2 : 0, c->st));
+    CKL();
+  }
+  if (nlm == QX_NL_GSPACE) {
+    Bufs<T> &b = pl.bufs<T>();
+    T *proj = (T *)c->proj;
+    const int np = pl.nproj;
+    TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, colmap,
+                ncol_dev, c->st));
+    scale_rows<T>(np, ncol_max, proj, np, b.vclalp, colmap, ncol_dev, c->st);
+    TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, colmap,
+                ncol_dev, c->st));
+    CKL();
+  }
+  return 0;
+}
+
+template <typename T>
+static int hpsi_all(qx_ctx *c, const T *cin, T *out, int nb, int flags) {
+  const int npair = (nb + 1) / 2;
+  // the all-bands pair list covers nband; fewer bands use its prefix, which
+  // is consecutive, except for an odd tail handled by the count bound
+  if (nb > c->nb) { set_error("hpsi: nb > nband"); return QX_ERR_ARG; }
+  if (nb % 2 && nb != c->nb) {
+    std::vector<int> pr(2 * npair);
+    for (int p = 0; p < npair; ++p) { pr[2 * p] = 2 * p; pr[2 * p + 1] = (2 * p + 1 < nb) ? 2 * p + 1 : -1; }
+    int *dp = (int *)c->cg.pairs;
+    CK(cudaMemcpyAsync(dp, pr.data(), sizeof(int) * pr.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return hpsi_impl<T>(c, cin, out, dp, nullptr, npair, nullptr, nullptr, nb, flags);
+  }
+  return hpsi_impl<T>(c, cin, out, c->d_allpairs, nullptr, npair, nullptr, nullptr, nb, flags);
+}
+
+extern "C" int qx_hpsi(qx_ctx *c, const void *cin, void *out, int nb, int flags) {
+  if (!c || !cin || !out || nb <= 0) { set_error("qx_hpsi: bad arguments"); return QX_ERR_ARG; }
+  if (c->prec == QX_PREC_FP64) return hpsi_all<double>(c, (const double *)cin, (double *)out, nb, flags);
+  return hpsi_all<float>(c, (const float *)cin, (float *)out, nb, flags);
+}
+
+template <typename T>
+static int ekinetic_impl(qx_ctx *c, double *ekin_sum, double *ekib) {
+  qx::ekin<T>(c->nb, c->ne, c->ne, (const T *)c->psi, c->d_dk, c->d_ekib, c->st);
+  CKL();
+  if (ekin_sum || ekib) {
+    std::vector<double> e(c->nb), o(c->nb);
+    CK(cudaMemcpyAsync(e.data(), c->d_ekib, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(o.data(), c->d_occ, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (ekib) memcpy(ekib, e.data(), sizeof(double) * c->nb);
+    if (ekin_sum) {
+      double s = 0.0;
+      for (int b = 0; b < c->nb; ++b) s += (c->have_occ ? o[b] : 0.0) * 0.5 * e[b];
+      *ekin_sum = s;
+    }
+  }
+  return 0;
+}
+
+extern "C" int qx_ekinetic(qx_ctx *c, double *ekin_out, double *ekib) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? ekinetic_impl<double>(c, ekin_out, ekib) : ekinetic_impl<float>(c, ekin_out, ekib);
+}
+
+extern "C" int qx_enonloc(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_ekinetic(c, nullptr, nullptr));
+  return qx_hpsi(c, c->psi, c->hpsi, c->nb, QX_HPSI_KINETIC | QX_HPSI_NONLOCAL);
+}
+
+template <typename T>
+static int hmatrix_impl(qx_ctx *c, double *hsub) {
+  const int nb = c->nb;
+  T *m = (T *)c->mat_t;
+  // m(j, i) = <psi_j | hpsi_i>
+  TRY(gemm<T>(true, false, nb, nb, c->ne, (T)1, (const T *)c->psi, c->ne, (const T *)c->hpsi, c->ne, (T)0, m, nb, 1,
+              nullptr, nullptr, c->st));
+  symmetrize_lower<T>(m, c->d_hsub, c->d_eig, nb, c->st);
+  CKL();
+  c->have_hsub = true;
+  if (hsub) {
+    CK(cudaMemcpyAsync(hsub, c->d_hsub, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return 0;
+}
+extern "C" int qx_hmatrix(qx_ctx *c, double *hsub) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? hmatrix_impl<double>(c, hsub) : hmatrix_impl<float>(c, hsub);
+}
+
+template <typename T>
+static int gradres_impl(qx_ctx *c, double *prod, double *zmax, double *zsum) {
+  gradres<T>(c->nb, c->ne, c->ne, (const T *)c->psi, (const T *)c->hpsi, c->d_eig, c->d_prod, c->st);
+  CKL();
+  std::vector<double> p(c->nb), o(c->nb, 0.0);
+  CK(cudaMemcpyAsync(p.data(), c->d_prod, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+  if (c->have_occ) CK(cudaMemcpyAsync(o.data(), c->d_occ, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double m = 0.0, s = 0.0;
+  for (int b = 0; b < c->nb; ++b) { m = std::max(m, p[b]); s += p[b] * o[b]; }
+  if (prod) memcpy(prod, p.data(), sizeof(double) * c->nb);
+  if (zmax) *zmax = m;
+  if (zsum) *zsum = s;
+  return 0;
+}
+extern "C" int qx_gradres(qx_ctx *c, double *prod, double *zmax, double *zsum) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? gradres_impl<double>(c, prod, zmax, zsum) : gradres_impl<float>(c, prod, zmax, zsum);
+}
+
+template <typename T>
+static int rotate(qx_ctx *c, void *&arr) {
+  const int nb = c->nb;
+  const T *U = (const T *)c->mat_t;
+  TRY(gemm<T>(false, false, c->ne, nb, nb, (T)1, (const T *)arr, c->ne, U, nb, (T)0, (T *)c->tmp, c->ne, 0, nullptr,
+              nullptr, c->st));
+  CKL();
+  std::swap(arr, c->tmp);
+  return 0;
+}
+
+template <typename T>
+static int untryt_impl(qx_ctx *c, double *ev, int *sweeps) {
+  if (!c->have_hsub) { set_error("untryt: call hmatrix first"); return QX_ERR_STATE; }
+  const int nb = c->nb;
+  CK(cudaMemcpyAsync(c->d_mat, c->d_hsub, sizeof(double) * nb * nb, cudaMemcpyDeviceToDevice, c->st));
+  TRY(jacobi(c->d_mat, nb, c->d_w, c->d_V, 60, c->d_info, c->st));
+  CKL();
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  // U in the working precision for the GEMMs
+  convert<double, T>(c->d_V, (T *)c->mat_t, (long)nb * nb, c->st);
+  CKL();
+  TRY(rotate<T>(c, c->psi));
+  CK(cudaStreamSynchronize(c->st));
+  if (info < 0) { set_error("untryt: Jacobi did not converge in 60 sweeps"); return QX_ERR_EIG; }
+  if (sweeps) *sweeps = info;
+  c->have_u = true;
+  c->have_hsub = false;
+  if (ev) CK(cudaMemcpy(ev, c->d_w, sizeof(double) * nb, cudaMemcpyDeviceToHost));
+  return 0;
+}
+extern "C" int qx_untryt(qx_ctx *c, double *ev) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? untryt_impl<double>(c, ev, nullptr) : untryt_impl<float>(c, ev, nullptr);
+}
+extern "C" int qx_untryhc(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_u) { set_error("untryhc: call untryt first"); return QX_ERR_STATE; }
+  return c->prec == QX_PREC_FP64 ? rotate<double>(c, c->hpsi) : rotate<float>(c, c->hpsi);
+}
+
+template <typename T>
+static int eigen_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out) {
+  const int nb = c->nb, ne = c->ne;
+  CgParm pm{p->itermx, p->iteremx, p->noband, p->tolera, p->roughfzan, p->roughfeig, p->threinn, p->wdinner};
+  T *x = (T *)c->psi, *hx = (T *)c->hpsi, *g = (T *)c->g, *h = (T *)c->h, *gh = (T *)c->gh, *snap = (T *)c->snap;
+  T *pm_t = (T *)c->mat_t;
+  const CgState &s = c->cg;
+  // lower-band snapshot (real*4 when requested in FP64 contexts)
+  if (sizeof(T) == sizeof(double) && p->ccreal4) {
+    convert<double, float>((const double *)x, (float *)c->tmp, (long)nb * ne, c->st);
+    convert<float, double>((const float *)c->tmp, (double *)snap, (long)nb * ne, c->st);
+  } else {
+    CK(cudaMemcpyAsync(snap, x, sizeof(T) * (size_t)nb * ne, cudaMemcpyDeviceToDevice, c->st));
+  }
+  cg_init<T>(nb, ne, ne, x, hx, g, s, c->st);
+  CKL();
+  const int maxit = std::max(p->itermx, p->iteremx);
+  int nh = 0;
+  for (int it = 0; it < maxit; ++it) {
+    cg_prec<T>(nb, ne, ne, g, h, c->d_dk, s, c->st);
+    // subgs3: Pm = snap^T h ; Pm masked to j < i, active i ; h -= snap * Pm
+    TRY(gemm<T>(true, false, nb, nb, ne, (T)1, snap, ne, h, ne, (T)0, pm_t, nb, 1, nullptr, nullptr, c->st));
+    cg_mask<T>(nb, pm_t, s, c->st);
+    TRY(gemm<T>(false, false, ne, nb, nb, (T)-1, snap, ne, pm_t, nb, (T)1, h, ne, 0, nullptr, nullptr, c->st));
+    cg_orth<T>(nb, ne, ne, x, hx, h, s, c->st);
+    cg_list(nb, s, c->st);
+    CKL();
+    TRY(hpsi_impl<T>(c, h, gh, s.pairs, s.npair, c->npair_all, s.list, s.nact, nb,
+                     QX_HPSI_KINETIC | QX_HPSI_NONLOCAL));
+    cg_update<T>(nb, ne, ne, x, hx, g, h, gh, s, pm, c->st);
+    CKL();
+  }
+  // eig and iteration counts
+  CK(cudaMemcpyAsync(c->d_eig, s.eig, sizeof(double) * nb, cudaMemcpyDeviceToDevice, c->st));
+  std::vector<int> iters(nb);
+  CK(cudaMemcpyAsync(iters.data(), s.iter, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int b = 0; b < nb; ++b) nh += iters[b];
+  if (nriter) memcpy(nriter, iters.data(), sizeof(int) * nb);
+  if (nhpsi_out) *nhpsi_out = nh;
+  c->have_hsub = false;
+  return 0;
+}
+extern "C" int qx_eigen(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi) {
+  if (!c || !p) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? eigen_impl<double>(c, p, nriter, nhpsi) : eigen_impl<float>(c, p, nriter, nhpsi);
+}
+
+template <typename T>
+static int schmidt_impl(qx_ctx *c) {
+  const int nb = c->nb, ne = c->ne;
+  T *m = (T *)c->mat_t;
+  TRY(gemm<T>(true, false, nb, nb, ne, (T)1, (const T *)c->psi, ne, (const T *)c->psi, ne, (T)0, m, nb, 1, nullptr,
+              nullptr, c->st));
+  convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
+  TRY(cholinv(c->d_mat, nb, c->d_info, c->st));
+  CKL();
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (info) { set_error("schmidt: <psi|psi> not positive definite at band %d", info - 1); return QX_ERR_NOTPD; }
+  convert<double, T>(c->d_mat, m, (long)nb * nb, c->st);
+  // psi <- psi * Linv^T
+  TRY(gemm<T>(false, true, ne, nb, nb, (T)1, (const T *)c->psi, ne, m, nb, (T)0, (T *)c->tmp, ne, 0, nullptr, nullptr,
+              c->st));
+  CKL();
+  std::swap(c->psi, c->tmp);
+  return 0;
+}
+extern "C" int qx_schmidt(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? schmidt_impl<double>(c) : schmidt_impl<float>(c);
+}
+
+template <typename T>
+static int softchg_impl(qx_ctx *c) {
+  if (!c->have_occ) { set_error("softchg: occupations not set"); return QX_ERR_STATE; }
+  TRY(ensure_rho(c));
+  const Plan &pl = c->pl;
+  PipeParams P = base_params(c);
+  for (int p0 = 0; p0 < c->npair_all; p0 += pl.chunk) {
+    // pairs p0 .. p0+npl-1: the kernels bound pairs by npair and k_xrho
+    // loops over npair - pair0 of them
+    P.pair0 = p0;
+    const int npl = std::min(pl.chunk, c->npair_all - p0);
+    P.npair = p0 + npl;
+    TRY(launch_rho_chunk<T>(pl, P, npl, (const T *)c->psi, c->ne, c->d_wocc, c->d_rho_out, p0 > 0, c->st));
+    CKL();
+  }
+  return 0;
+}
+extern "C" int qx_softchg(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  return c->prec == QX_PREC_FP64 ? softchg_impl<double>(c) : softchg_impl<float>(c);
+}
+
+// ---------------------------------------------------------------------------
+// SCF iteration
+extern "C" int qx_scf_init(qx_ctx *c, const double *vloc, const double *cross, double ecutdens, double eion,
+                           double mixbeta, double q0) {
+  if (!c || !vloc || !cross) return QX_ERR_ARG;
+  TRY(ensure_rho(c));
+  const long n = c->pl.n;
+  if (!c->d_vloc) {
+    TRY(dalloc(c, &c->d_vloc, sizeof(double) * n));
+    TRY(dalloc(c, &c->d_g2, sizeof(double) * n));
+    TRY(dalloc(c, &c->d_zg, sizeof(double2) * n));
+    TRY(dalloc(c, &c->d_part, sizeof(double) * 2 * SCF_NBLK));
+    TRY(dalloc(c, &c->d_sc, sizeof(double) * 16));
+    if (!c->d_glocal) TRY(dalloc(c, &c->d_glocal, sizeof(double) * n));
+  }
+  CK(cudaMemcpyAsync(c->d_vloc, vloc, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  grid_g2(c->pl.k1, c->pl.k2, c->pl.k3, cross, ecutdens, c->d_g2, c->st);
+  CKL();
+  c->eion = eion;
+  c->mixbeta = mixbeta;
+  c->q02 = q0 * q0;
+  c->scf_ready = true;
+  return QX_OK;
+}
+
+extern "C" int qx_scf_rho_from_psi(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_softchg(c));
+  CK(cudaMemcpyAsync(c->d_rho_in, c->d_rho_out, sizeof(double) * c->pl.n, cudaMemcpyDeviceToDevice, c->st));
+  return QX_OK;
+}
+
+// glocal = V_loc + V_H[rho_in] + V_xc[rho_in]; sc[0] = E_H, sc[1..2] = E_xc, int V_xc rho.
+static int scf_potential(qx_ctx *c) {
+  const long n = c->pl.n;
+  real_to_cplx(c->d_rho_in, nullptr, c->d_zg, n, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0 / (double)n, c->st));
+  hartree_g(c->d_zg, c->d_g2, n, 0.5 * c->rvol, c->d_part, c->d_sc + 0, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, +1, 1.0, c->st));
+  const double rdelv = c->rvol / (double)n;
+  if (c->prec == QX_PREC_FP64)
+    xc_glocal<double>(c->d_rho_in, c->d_vloc, c->d_zg, n, rdelv, c->d_glocal, c->pl.b64.vloc, c->d_part, c->d_sc + 1,
+                      c->st);
+  else
+    xc_glocal<float>(c->d_rho_in, c->d_vloc, c->d_zg, n, rdelv, c->d_glocal, c->pl.b32.vloc, c->d_part, c->d_sc + 1,
+                     c->st);
+  CKL();
+  c->have_glocal = true;
+  return 0;
+}
+
+static int scf_mix(qx_ctx *c) {
+  const long n = c->pl.n;
+  real_to_cplx(c->d_rho_out, c->d_rho_in, c->d_zg, n, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0 / (double)n, c->st));
+  kerker(c->d_zg, c->d_g2, n, c->q02, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, +1, 1.0, c->st));
+  mix(c->d_rho_in, c->d_rho_out, c->d_zg, n, c->mixbeta, c->rvol / (double)n, c->d_part, c->d_sc + 3, c->st);
+  CKL();
+  return 0;
+}
+
+extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
+  if (!c || !p) return QX_ERR_ARG;
+  if (!c->scf_ready || !c->have_occ) { set_error("qx_scf_iteration: call qx_scf_init and qx_set_occ first"); return QX_ERR_STATE; }
+  TRY(scf_potential(c));
+  TRY(qx_enonloc(c));
+  TRY(qx_hmatrix(c, nullptr));
+  double zmax = 0.0, zsum = 0.0;
+  if (out) TRY(qx_gradres(c, nullptr, &zmax, &zsum));
+  int sweeps = 0;
+  TRY(c->prec == QX_PREC_FP64 ? untryt_impl<double>(c, nullptr, &sweeps) : untryt_impl<float>(c, nullptr, &sweeps));
+  TRY(qx_untryhc(c));
+  band_energy(c->d_w, c->d_occ, c->nb, c->d_sc + 4, c->st);
+  int nh = 0;
+  TRY(qx_eigen(c, p, nullptr, &nh));
+  TRY(qx_schmidt(c));
+  TRY(qx_softchg(c));
+  TRY(scf_mix(c));
+  double sc[5];
+  CK(cudaMemcpyAsync(sc, c->d_sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (out) {
+    out->ehartree = sc[0];
+    out->exc = sc[1];
+    out->evxc = sc[2];
+    out->resid = sc[3];
+    out->eband = sc[4];
+    out->etot = sc[4] - sc[0] + sc[1] - sc[2] + c->eion;
+    out->zmax = zmax;
+    out->ncg_hpsi = nh;
+    out->jacobi_sweeps = sweeps;
+  }
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in shims on host arrays.
+extern "C" int qxgpu_hcnonloc(qx_ctx *c, const double *cgjr, double *rhcr, int nb) {
+  if (!c || nb > c->nb) return QX_ERR_ARG;
+  TRY(up(c, c->g, cgjr, (long)nb * c->ne));
+  TRY(up(c, c->gh, rhcr, (long)nb * c->ne));
+  const int save = c->nlmode;
+  if (c->nlmode == QX_NL_GSPACE) c->nlmode = QX_NL_NONE;
+  int r = qx_hpsi(c, c->g, c->gh, nb, QX_HPSI_ACCUMULATE | QX_HPSI_NONLOCAL);
+  c->nlmode = save;
+  TRY(r);
+  return down(c, rhcr, c->gh, (long)nb * c->ne);
+}
+
+template <typename T>
+static int kbg_only(qx_ctx *c, const T *cin, T *out, int nb) {
+  const Plan &pl = c->pl;
+  Bufs<T> &b = pl.bufs<T>();
+  const int np = pl.nproj;
+  T *proj = (T *)c->proj;
+  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st));
+  scale_rows<T>(np, nb, proj, np, b.vclalp, nullptr, nullptr, c->st);
+  TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st));
+  CKL();
+  return 0;
+}
+extern "C" int qxgpu_hckbpp_g(qx_ctx *c, const double *cgjr, double *rhcr, int nb) {
+  if (!c || nb > c->nb || !c->have_kbg) return QX_ERR_ARG;
+  TRY(up(c, c->g, cgjr, (long)nb * c->ne));
+  TRY(up(c, c->gh, rhcr, (long)nb * c->ne));
+  TRY(c->prec == QX_PREC_FP64 ? kbg_only<double>(c, (double *)c->g, (double *)c->gh, nb)
+                              : kbg_only<float>(c, (float *)c->g, (float *)c->gh, nb));
+  return down(c, rhcr, c->gh, (long)nb * c->ne);
+}
+
+extern "C" int qxgpu_enonloc(qx_ctx *c, const double *cgjr, double *rhcr, double *ekib) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, cgjr));
+  TRY(qx_enonloc(c));
+  if (ekib) TRY(qx_ekinetic(c, nullptr, ekib));
+  return qx_get_hpsi(c, rhcr);
+}
+
+extern "C" int qxgpu_eigen(qx_ctx *c, double *gdcr, double *rhcr, const double *ekib, double *eig, const qx_cgparm *p) {
+  if (!c || !p) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, gdcr));
+  TRY(qx_put_hpsi(c, rhcr));
+  if (ekib) CK(cudaMemcpyAsync(c->d_ekib, ekib, sizeof(double) * c->nb, cudaMemcpyHostToDevice, c->st));
+  else TRY(qx_ekinetic(c, nullptr, nullptr));
+  TRY(qx_eigen(c, p, nullptr, nullptr));
+  TRY(qx_get_psi(c, gdcr));
+  TRY(qx_get_hpsi(c, rhcr));
+  if (eig) TRY(qx_get_eig(c, eig));
+  return QX_OK;
+}
+
+extern "C" int qxgpu_schmidt(qx_ctx *c, double *cgjr) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, cgjr));
+  TRY(qx_schmidt(c));
+  return qx_get_psi(c, cgjr);
+}
+
+extern "C" int qxgpu_hmatrix(qx_ctx *c, const double *cgjr, const double *rhcr, double *dmtrxr, double *eig) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, cgjr));
+  TRY(qx_put_hpsi(c, rhcr));
+  TRY(qx_hmatrix(c, dmtrxr));
+  if (eig) TRY(qx_get_eig(c, eig));
+  return QX_OK;
+}
+
+extern "C" int qxgpu_untryt(qx_ctx *c, double *gdcr, double *rhcr, double *ev) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, gdcr));
+  TRY(qx_put_hpsi(c, rhcr));
+  TRY(qx_untryt(c, ev));
+  TRY(qx_untryhc(c));
+  TRY(qx_get_psi(c, gdcr));
+  return qx_get_hpsi(c, rhcr);
+}
+
+extern "C" int qxgpu_softchg(qx_ctx *c, const double *cgjr, double *rho) {
+  if (!c) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, cgjr));
+  TRY(qx_softchg(c));
+  return qx_get_rho(c, rho);
+}
+
+__global__ void k_split(const double2 *z, double *x, double *y, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    x[i] = z[i].x;
+    if (y) y[i] = z[i].y;
+  }
+}
+__global__ void k_join(const double *x, const double *y, double2 *z, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    z[i] = make_double2(x[i], y ? y[i] : 0.0);
+}
+
+extern "C" int qxgpu_rfft3(qx_ctx *c, int key, double *fft3x, double *fft3y) {
+  if (!c || !fft3x || !fft3y) return QX_ERR_ARG;
+  const long n = c->pl.n;
+  double2 *z = nullptr;
+  double *x = nullptr, *y = nullptr;
+  CK(cudaMallocAsync((void **)&z, sizeof(double2) * n, c->st));
+  CK(cudaMallocAsync((void **)&x, sizeof(double) * n, c->st));
+  CK(cudaMallocAsync((void **)&y, sizeof(double) * n, c->st));
+  CK(cudaMemcpyAsync(x, fft3x, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  if (key == 1) {
+    k_join<<<148 * 4, 256, 0, c->st>>>(x, nullptr, z, n);
+    TRY(launch_full_fft<double>(c->pl, z, -1, 1.0 / (double)n, c->st));
+  } else {
+    CK(cudaMemcpyAsync(y, fft3y, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    k_join<<<148 * 4, 256, 0, c->st>>>(x, y, z, n);
+    TRY(launch_full_fft<double>(c->pl, z, +1, 1.0, c->st));
+  }
+  k_split<<<148 * 4, 256, 0, c->st>>>(z, x, key == 1 ? y : nullptr, n);
+  CKL();
+  CK(cudaMemcpyAsync(fft3x, x, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  if (key == 1) CK(cudaMemcpyAsync(fft3y, y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(z, c->st));
+  CK(cudaFreeAsync(x, c->st));
+  CK(cudaFreeAsync(y, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (key != 1) memset(fft3y, 0, sizeof(double) * n);
+  return QX_OK;
+}

@@ -1,0 +1,315 @@
+// Batched BKL conjugate-gradient band update (eigen_BKL, eigen.f90:199-938,
+// preconditioner prpcg eigen.f90:1093-1113, subgs4 engrad.f90:1196-1248).
+// All bands iterate together; band ib is projected against the entry
+// snapshot of bands < ib (subgs3, done as two GEMMs by the caller), which is
+// the reference's result with one band per rank.  One CTA per band; every
+// reduction is accumulated in FP64.  Per-band state lives on the device, so a
+// CG sweep needs no host round trip.
+#include "qx_internal.h"
+#include "qx_cg.h"
+
+namespace qx {
+
+template <typename T>
+__device__ __forceinline__ double ld(const T *p, long i) { return (double)p[i]; }
+
+// Gamma-point inner product of two bands, block-wide.
+template <typename T>
+__device__ double bdot(const T *x, const T *y, int ne, double *red) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) s += ld(x, i) * ld(y, i);
+  s = block_sum(s, red);
+  return 2.0 * s - ld(x, 0) * ld(y, 0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_cg_init(int ne, long ldx, const T *__restrict__ x,
+                                                         const T *__restrict__ hx, T *__restrict__ g, CgState s) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  const T *xb = x + b * ldx, *hb = hx + b * ldx;
+  T *gb = g + b * ldx;
+  const double e = bdot(xb, hb, ne, red);
+  double z = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const T v = (T)e * xb[i] - hb[i];
+    gb[i] = v;
+    z += (double)v * (double)v;
+  }
+  z = block_sum(z, red);
+  z = 2.0 * z - ld(gb, 0) * ld(gb, 0);
+  if (threadIdx.x == 0) {
+    s.eig[b] = e;
+    s.zansa[b] = z;
+    s.zansab[b] = z;
+    s.z000re[b] = z;
+    s.x000re[b] = 1.0e10;
+    s.eigb[b] = e;
+    s.dinnerx[b] = 0.0;
+    s.betk[b] = 0.0;
+    s.izcnt[b] = 0;
+    s.lreset[b] = 1;
+    s.iter[b] = 0;
+    s.active[b] = 1;
+  }
+}
+
+// g <- prcd * g; zansap = <g|g>; h <- g + beta*h (h <- g on reset).
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_cg_prec(int ne, long ldx, T *__restrict__ g, T *__restrict__ h,
+                                                         const double *__restrict__ dk, CgState s) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  if (!s.active[b]) return;
+  T *gb = g + b * ldx, *hb = h + b * ldx;
+  const double e15 = 1.5 * s.ekib[b];
+  double z = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const double x = dk[i] / e15;
+    double t = 27.0 + x * (18.0 + x * (12.0 + 8.0 * x));
+    const double x2 = x * x, x4 = x2 * x2;
+    t = t / (t + 16.0 * x4);
+    const T v = (T)((double)gb[i] * (t * 2.0 / e15));
+    gb[i] = v;
+    z += (double)v * (double)v;
+  }
+  z = block_sum(z, red);
+  const double zansap = 2.0 * z - ld(gb, 0) * ld(gb, 0);
+  const int reset = s.lreset[b];
+  const double beta = reset ? 0.0 : zansap / s.betk[b];
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const T hv = reset ? (T)0 : hb[i];
+    hb[i] = gb[i] + (T)beta * hv;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.lreset[b] = 0;
+    s.betk[b] = zansap;
+    s.iter[b] += 1;
+  }
+}
+
+// Mask for subgs3: M(j,i) = P(j,i) if j < i and band i is active, else 0.
+template <typename T>
+__global__ void k_cg_mask(int nb, T *__restrict__ Pm, CgState s) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)nb * nb) return;
+  const int i = (int)(e / nb), j = (int)(e - (long)i * nb);
+  if (!(j < i && s.active[i])) Pm[e] = (T)0;
+}
+
+// subgs4: h -= <x|h> x; cai = <h|hx>.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_cg_orth(int ne, long ldx, const T *__restrict__ x,
+                                                         const T *__restrict__ hx, T *__restrict__ h, CgState s) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  if (!s.active[b]) return;
+  const T *xb = x + b * ldx, *hxb = hx + b * ldx;
+  T *hb = h + b * ldx;
+  const double hhx = bdot(xb, (const T *)hb, ne, red);
+  double c = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const T v = hb[i] - (T)hhx * xb[i];
+    hb[i] = v;
+    c += (double)v * (double)hxb[i];
+  }
+  c = block_sum(c, red);
+  if (threadIdx.x == 0) s.cai[b] = 2.0 * c - ld(hb, 0) * ld(hxb, 0);
+}
+
+// Active-band list and the band pairs of the FFT pipeline.
+__global__ void k_cg_list(int nb, CgState s) {
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int b = 0; b < nb; ++b)
+      if (s.active[b]) s.list[n++] = b;
+    for (int p = 0; p < (n + 1) / 2; ++p) {
+      s.pairs[2 * p] = s.list[2 * p];
+      s.pairs[2 * p + 1] = (2 * p + 1 < n) ? s.list[2 * p + 1] : -1;
+    }
+    *s.nact = n;
+    *s.npair = (n + 1) / 2;
+  }
+}
+
+// BKL 2x2 step (eigen.f90:593-622), line minimisation fallback (624-695),
+// x/hx update (698-709), residual and convergence test (731-764).
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
+                                                           T *__restrict__ g, const T *__restrict__ h,
+                                                           const T *__restrict__ gh, CgState s, CgParm pm) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  if (!s.active[b]) return;
+  T *xb = x + b * ldx, *hxb = hx + b * ldx, *gb = g + b * ldx;
+  const T *hb = h + b * ldx, *ghb = gh + b * ldx;
+  const double dinx = s.dinnerx[b];   // read before thread 0 may update it
+  double cb = 0.0, hh = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const double hv = (double)hb[i];
+    cb += hv * (double)ghb[i];
+    hh += hv * hv;
+  }
+  cb = block_sum(cb, red);
+  hh = block_sum(hh, red);
+  const double h0 = ld(hb, 0);
+  const double cbi = 2.0 * cb - h0 * ld(ghb, 0);
+  const double hhi = 2.0 * hh - h0 * h0;
+  const double cai = s.cai[b];
+  double e = s.eig[b];
+  double dtnew, alpsq;
+  if (hhi > 0.0) {
+    const double h11 = e, h12 = cai / sqrt(hhi), h21 = h12, h22 = cbi / hhi;
+    const double enew = 0.5 * (h11 + h22 - sqrt((h11 + h22) * (h11 + h22) - 4.0 * (h11 * h22 - h12 * h21)));
+    dtnew = (enew - h11) / h12 / sqrt(hhi);
+    const double alpsq2 = 1.0 / (1.0 + dtnew * (0.0 + dtnew * hhi));
+    alpsq = sqrt(alpsq2);
+    e = enew;
+  } else {
+    double hx2 = 0.0;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) hx2 += (double)hb[i] * (double)xb[i];
+    hx2 = block_sum(hx2, red);
+    const double hhx = 2.0 * hx2 - h0 * ld(xb, 0);
+    const double c0 = e, c1 = cai, c2 = cbi, c3 = hhi, c4 = 2.0 * hhx;
+    const double s0 = c0 * c4 - c1, s1 = c0 * c3 - c2, s2 = c1 * c3 - c2 * c4;
+    const double sr = s1 * s1 - s2 * s0;
+    dtnew = (sr > 0.0) ? (-s1 - sqrt(sr)) / s2 : -1.0;
+    if (dtnew > 0.0) {
+      const double dinner = sqrt(1.0 / (1.0 + dtnew * dtnew * hhi));
+      if (dinner < pm.threinn) dtnew = 0.0;
+      if (dinner < dinx * pm.wdinner) dtnew = 0.0;
+      if (threadIdx.x == 0 && dinner > dinx) s.dinnerx[b] = dinner;
+    }
+    const double d2 = dtnew * dtnew;
+    const double alpsq2 = 1.0 / (1.0 + dtnew * c4 + d2 * c3);
+    e = (c0 + dtnew * c1 + d2 * c2) * alpsq2;
+    alpsq = sqrt(alpsq2);
+  }
+  const T a = (T)alpsq, dt = (T)dtnew, et = (T)e;
+  double z = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const T xn = a * (xb[i] + dt * hb[i]);
+    const T hn = a * (hxb[i] + dt * ghb[i]);
+    xb[i] = xn;
+    hxb[i] = hn;
+    const T gv = et * xn - hn;
+    gb[i] = gv;
+    z += (double)gv * (double)gv;
+  }
+  z = block_sum(z, red);
+  const double zansa = 2.0 * z - ld(gb, 0) * ld(gb, 0);
+  if (threadIdx.x == 0) {
+    const int iter = s.iter[b];
+    const double eigb = s.eigb[b];
+    const double de = fabs(eigb - e);
+    const int stop = (b < pm.noband && iter >= pm.itermx) || (b >= pm.noband && iter >= pm.iteremx) ||
+                     zansa < pm.tolera || de < pm.tolera || zansa < s.z000re[b] * pm.roughfzan ||
+                     (iter > 1 && de < s.x000re[b] * pm.roughfeig);
+    s.eig[b] = e;
+    s.zansa[b] = zansa;
+    if (stop) {
+      s.active[b] = 0;
+    } else {
+      if (iter == 1) s.x000re[b] = de;
+      if (zansa > s.zansab[b]) {
+        if (++s.izcnt[b] > 20) { s.izcnt[b] = 0; s.lreset[b] = 1; }
+      }
+      s.zansab[b] = zansa;
+      s.eigb[b] = e;
+    }
+  }
+}
+
+// ekinetic2 (engrad.f90:75-127): ekib(b) = 2*<c|T|c>, and sum occ*<c|T|c>
+// into *ekin (one CTA per band writes its term; summed by k_sum_occ).
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_ekin(int ne, long ldx, const T *__restrict__ x,
+                                                      const double *__restrict__ dk, double *__restrict__ ekib) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  const T *xb = x + b * ldx;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) s += dk[i] * ld(xb, i) * ld(xb, i);
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) ekib[b] = 2.0 * (2.0 * s - dk[0] * ld(xb, 0) * ld(xb, 0));
+}
+
+// gradresnv (engrad.f90:1013-1067): per-band |eig*c - hc|^2 (Gamma metric).
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_gradres(int ne, long ldx, const T *__restrict__ x,
+                                                         const T *__restrict__ hx, const double *__restrict__ eig,
+                                                         double *__restrict__ prod) {
+  __shared__ double red[QX_THREADS / 32];
+  const int b = blockIdx.x;
+  const T *xb = x + b * ldx, *hb = hx + b * ldx;
+  const double e = eig[b];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+    const double r = e * ld(xb, i) - ld(hb, i);
+    s += r * r;
+  }
+  s = block_sum(s, red);
+  const double r0 = e * ld(xb, 0) - ld(hb, 0);
+  if (threadIdx.x == 0) prod[b] = 2.0 * s - r0 * r0;
+}
+
+// Row scaling of the projection matrix P (nproj x ncol, column-major, columns
+// through colmap): P(j, n) *= v(j).
+template <typename T>
+__global__ void k_scale_rows(int nproj, int ncol, T *__restrict__ P, long ldp, const T *__restrict__ v,
+                             const int *__restrict__ colmap, const int *__restrict__ ncol_dev) {
+  const int nc = ncol_dev ? min(ncol, *ncol_dev) : ncol;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)nproj * nc) return;
+  const int n = (int)(e / nproj), j = (int)(e - (long)n * nproj);
+  const long cn = colmap ? colmap[n] : n;
+  P[cn * ldp + j] *= v[j];
+}
+
+// ---- launchers -------------------------------------------------------------
+template <typename T> void cg_init(int nb, int ne, long ldx, const T *x, const T *hx, T *g, const CgState &s, cudaStream_t st) {
+  k_cg_init<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, s);
+}
+template <typename T> void cg_prec(int nb, int ne, long ldx, T *g, T *h, const double *dk, const CgState &s, cudaStream_t st) {
+  k_cg_prec<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, g, h, dk, s);
+}
+template <typename T> void cg_mask(int nb, T *Pm, const CgState &s, cudaStream_t st) {
+  const long nn = (long)nb * nb;
+  k_cg_mask<T><<<(int)((nn + 255) / 256), 256, 0, st>>>(nb, Pm, s);
+}
+template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T *hx, T *h, const CgState &s, cudaStream_t st) {
+  k_cg_orth<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, h, s);
+}
+void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); }
+template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
+                                     const CgState &s, const CgParm &pm, cudaStream_t st) {
+  k_cg_update<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm);
+}
+template <typename T> void ekin(int nb, int ne, long ldx, const T *x, const double *dk, double *ekib, cudaStream_t st) {
+  k_ekin<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, dk, ekib);
+}
+template <typename T> void gradres(int nb, int ne, long ldx, const T *x, const T *hx, const double *eig, double *prod,
+                                   cudaStream_t st) {
+  k_gradres<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, eig, prod);
+}
+template <typename T> void scale_rows(int nproj, int ncol, T *P, long ldp, const T *v, const int *colmap,
+                                      const int *ncol_dev, cudaStream_t st) {
+  const long n = (long)nproj * ncol;
+  k_scale_rows<T><<<(int)((n + 255) / 256), 256, 0, st>>>(nproj, ncol, P, ldp, v, colmap, ncol_dev);
+}
+
+#define QX_INST(T)                                                                                          \
+  template void cg_init<T>(int, int, long, const T *, const T *, T *, const CgState &, cudaStream_t);        \
+  template void cg_prec<T>(int, int, long, T *, T *, const double *, const CgState &, cudaStream_t);          \
+  template void cg_mask<T>(int, T *, const CgState &, cudaStream_t);                                         \
+  template void cg_orth<T>(int, int, long, const T *, const T *, T *, const CgState &, cudaStream_t);        \
+  template void cg_update<T>(int, int, long, T *, T *, T *, const T *, const T *, const CgState &,            \
+                             const CgParm &, cudaStream_t);                                                  \
+  template void ekin<T>(int, int, long, const T *, const double *, double *, cudaStream_t);                  \
+  template void gradres<T>(int, int, long, const T *, const T *, const double *, double *, cudaStream_t);    \
+  template void scale_rows<T>(int, int, T *, long, const T *, const int *, const int *, cudaStream_t);
+QX_INST(float)
+QX_INST(double)
+
+}  // namespace qx

@@ -1,0 +1,611 @@
+// Batched, sphere-pruned 3D FFT pipeline for the Gamma-point H|psi> product.
+//
+// Replaces wvg2r (engrad.f90:1492-1559), the V_loc multiply and real-space KB
+// add of hcnonloc (engrad.f90:484-530), rfft3 (fft3.f90:113-232), the gather
+// at ijkgd (engrad.f90:564-571) and the kinetic term (eigen.f90:335,516).
+//
+// Two real bands A, B share one complex transform: Z(G) = cA(G) + i cB(G).
+// Grid index n1 + (n2 + n3*k2)*k1.  The wavefunction sphere spans
+// |n1| <= m1, |n2| <= m2 (compact indices a = n1 + m1 < P1, j2 = n2 + m2 < P2),
+// so the pipeline keeps only what is non-zero between passes:
+//   zinv : gather sphere -> z-FFT backward, per grid row j2   -> bufA[p][i3][j2][a]
+//   y<+1>: y-FFT backward per (p, i3) plane                   -> bufB[p][i3][i2][a]
+//   xvx  : x-FFT backward, * V(r), x-FFT forward per line     -> bufB (in place)
+//   y<-1>: y-FFT forward                                      -> bufA rows j2
+//   zfwd : z-FFT forward, 1/N, pick +G and -G                 -> zsph[p][ig][2]
+//   unpack: split the two bands, add kinetic, write H|psi>
+// Real-space KB (calnlc, nlkbppr.f90:1773-1900) splits xvx into xinv_r,
+// nlproj and xfwd_r.  Density (softchg, chgdns.f90:388-454) uses zinv, y<+1>
+// and xrho.
+#include "qx_internal.h"
+
+__device__ __forceinline__ int pair_count(const PipeParams &P) {
+  return P.npair_dev ? *P.npair_dev : P.npair;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_tw(typename c2t<T>::type *dst, const typename c2t<T>::type *src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// --------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_zinv(PipeParams P, const T *__restrict__ cin, long ldc,
+                                                      typename c2t<T>::type *__restrict__ bufA,
+                                                      const typename c2t<T>::type *__restrict__ tw3) {
+  typedef typename c2t<T>::type C;
+  const int j2 = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int lo = P.row_lo[j2], hi = P.row_hi[j2];
+  if (lo > hi) return;
+  const int W = hi - lo + 1, ld = W | 1, k3 = P.k3;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k3;
+  C *t1 = t0 + k3 * ld;
+  load_tw<T>(tw, tw3, k3);
+  const C zero = mk2<T>(0, 0);
+  for (int i = threadIdx.x; i < k3 * ld; i += blockDim.x) t0[i] = zero;
+  __syncthreads();
+  const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+  const T *cA = cin + (long)bA * ldc;
+  const T *cB = bB >= 0 ? cin + (long)bB * ldc : nullptr;
+  for (int e = P.row_off[j2] + threadIdx.x; e < P.row_off[j2 + 1]; e += blockDim.x) {
+    const int4 en = P.row_ent[e];
+    const int ig = en.z;
+    T ra = cA[2 * ig], ia = ig ? cA[2 * ig + 1] : T(0);
+    T rb = cB ? cB[2 * ig] : T(0), ib = (cB && ig) ? cB[2 * ig + 1] : T(0);
+    C z;
+    if (en.w > 0) { z.x = ra - ib; z.y = ia + rb; }
+    else          { z.x = ra + ib; z.y = rb - ia; }
+    t0[en.y * ld + en.x] = z;
+  }
+  __syncthreads();
+  C *res = smem_fft<T, +1>(t0, t1, W, ld, P.L3, tw);
+  C *dst = bufA + ((long)pl * k3) * P.P2 * P.P1 + (long)j2 * P.P1 + lo;
+  for (int i = threadIdx.x; i < k3 * W; i += blockDim.x) {
+    const int i3 = i / W, l = i - i3 * W;
+    dst[(long)i3 * P.P2 * P.P1 + l] = res[i3 * ld + l];
+  }
+}
+
+// y pass.  SIGN=+1: bufA (rows j2, sphere ranges) -> bufB (all i2).
+//          SIGN=-1: bufB -> bufA (rows j2, sphere ranges).
+template <typename T, int SIGN>
+__global__ void __launch_bounds__(QX_THREADS) k_ypass(PipeParams P, typename c2t<T>::type *__restrict__ bufA,
+                                                       typename c2t<T>::type *__restrict__ bufB,
+                                                       const typename c2t<T>::type *__restrict__ tw2) {
+  typedef typename c2t<T>::type C;
+  const int i3 = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int k2 = P.k2, P1 = P.P1, P2 = P.P2, ld = P1;   // P1 is odd
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k2;
+  C *t1 = t0 + k2 * ld;
+  load_tw<T>(tw, tw2, k2);
+  C *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
+  C *B = bufB + ((long)pl * P.k3 + i3) * k2 * P1;
+  if (SIGN > 0) {
+    const C zero = mk2<T>(0, 0);
+    for (int i = threadIdx.x; i < k2 * ld; i += blockDim.x) t0[i] = zero;
+    __syncthreads();
+    for (int i = threadIdx.x; i < P2 * P1; i += blockDim.x) {
+      const int j2 = i / P1, a = i - j2 * P1;
+      if (a >= P.row_lo[j2] && a <= P.row_hi[j2]) {
+        int i2 = j2 - P.m2; if (i2 < 0) i2 += k2;
+        t0[i2 * ld + a] = A[i];
+      }
+    }
+    __syncthreads();
+    C *res = smem_fft<T, +1>(t0, t1, P1, ld, P.L2, tw);
+    for (int i = threadIdx.x; i < k2 * P1; i += blockDim.x) B[i] = res[i];
+  } else {
+    for (int i = threadIdx.x; i < k2 * P1; i += blockDim.x) t0[i] = B[i];
+    __syncthreads();
+    C *res = smem_fft<T, -1>(t0, t1, P1, ld, P.L2, tw);
+    for (int i = threadIdx.x; i < P2 * P1; i += blockDim.x) {
+      const int j2 = i / P1, a = i - j2 * P1;
+      if (a >= P.row_lo[j2] && a <= P.row_hi[j2]) {
+        int i2 = j2 - P.m2; if (i2 < 0) i2 += k2;
+        A[i] = res[i2 * ld + a];
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int a_to_i1(int a, int m1, int k1) {
+  int i1 = a - m1;
+  return i1 < 0 ? i1 + k1 : i1;
+}
+
+// x pass fused with the local potential: backward x-FFT of the pruned line,
+// multiply by V(r), forward x-FFT, keep the pruned part.  One CTA handles
+// `nlines` consecutive i2 lines of plane i3.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T>::type *__restrict__ bufB,
+                                                     const T *__restrict__ vloc, int nlines, int nchunk,
+                                                     const typename c2t<T>::type *__restrict__ tw1) {
+  typedef typename c2t<T>::type C;
+  const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
+  const int i20 = ch * nlines;
+  const int nl = min(nlines, k2 - i20);
+  const int ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k1;
+  C *t1 = t0 + k1 * ld;
+  load_tw<T>(tw, tw1, k1);
+  const C zero = mk2<T>(0, 0);
+  for (int i = threadIdx.x; i < k1 * ld; i += blockDim.x) t0[i] = zero;
+  __syncthreads();
+  C *B = bufB + (((long)pl * P.k3 + i3) * k2 + i20) * P1;
+  for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
+    const int l = i / P1, a = i - l * P1;
+    t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
+  }
+  __syncthreads();
+  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+  C *o = (r == t0) ? t1 : t0;
+  const T *V = vloc + ((long)i3 * k2 + i20) * k1;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+    const int l = i / k1, i1 = i - l * k1;
+    const T v = V[i];
+    C z = r[i1 * ld + l];
+    z.x *= v; z.y *= v;
+    r[i1 * ld + l] = z;
+  }
+  __syncthreads();
+  C *res = smem_fft<T, -1>(r, o, nl, ld, P.L1, tw);
+  for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
+    const int l = i / P1, a = i - l * P1;
+    B[i] = res[a_to_i1(a, P.m1, k1) * ld + l];
+  }
+}
+
+// z pass forward + pick: writes Z(+G) to slot 0 and Z(-G) to slot 1 of zsph.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_zfwd(PipeParams P, const typename c2t<T>::type *__restrict__ bufA,
+                                                      typename c2t<T>::type *__restrict__ zsph,
+                                                      const typename c2t<T>::type *__restrict__ tw3) {
+  typedef typename c2t<T>::type C;
+  const int j2 = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int lo = P.row_lo[j2], hi = P.row_hi[j2];
+  if (lo > hi) return;
+  const int W = hi - lo + 1, ld = W | 1, k3 = P.k3;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k3;
+  C *t1 = t0 + k3 * ld;
+  load_tw<T>(tw, tw3, k3);
+  const C *src = bufA + ((long)pl * k3) * P.P2 * P.P1 + (long)j2 * P.P1 + lo;
+  for (int i = threadIdx.x; i < k3 * W; i += blockDim.x) {
+    const int i3 = i / W, l = i - i3 * W;
+    t0[i3 * ld + l] = src[(long)i3 * P.P2 * P.P1 + l];
+  }
+  __syncthreads();
+  C *res = smem_fft<T, -1>(t0, t1, W, ld, P.L3, tw);
+  const T s = (T)P.inv_n;
+  C *Z = zsph + (long)pl * (P.nplw + 1) * 2;
+  for (int e = P.row_off[j2] + threadIdx.x; e < P.row_off[j2 + 1]; e += blockDim.x) {
+    const int4 en = P.row_ent[e];
+    C z = res[en.y * ld + en.x];
+    z.x *= s; z.y *= s;
+    if (en.w > 0) {
+      Z[2 * en.z] = z;
+      if (en.z == 0) Z[1] = z;
+    } else {
+      Z[2 * en.z + 1] = z;
+    }
+  }
+}
+
+// Split the two bands of each pair and write H|psi> = [acc ? out : 0]
+// + dkgnrm*c (if dk != null) + FFT part.  Component 2 (Im c(G=0)) gets the
+// exact 0 imaginary part of a real function's G=0 coefficient.
+template <typename T>
+__global__ void k_unpack(PipeParams P, const typename c2t<T>::type *__restrict__ zsph,
+                         const T *__restrict__ cin, long ldc, T *__restrict__ out, long ldo,
+                         const double *__restrict__ dk, int accumulate) {
+  typedef typename c2t<T>::type C;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int ig = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ig > P.nplw) return;
+  const C *Z = zsph + (long)pl * (P.nplw + 1) * 2;
+  const C zp = Z[2 * ig], zm = Z[2 * ig + 1];
+  const T h = (T)0.5;
+  T har = h * (zp.x + zm.x), hai = h * (zp.y - zm.y);
+  T hbr = h * (zp.y + zm.y), hbi = h * (zm.x - zp.x);
+  if (ig == 0) { hai = 0; hbi = 0; }
+  const int b[2] = {P.pairs[2 * p], P.pairs[2 * p + 1]};
+  const T hr[2] = {har, hbr}, hi[2] = {hai, hbi};
+  for (int s = 0; s < 2; ++s) {
+    if (b[s] < 0) continue;
+    T *o = out + (long)b[s] * ldo;
+    const T *c = cin + (long)b[s] * ldc;
+    T vr = hr[s], vi = hi[s];
+    if (dk) { vr += (T)dk[2 * ig] * c[2 * ig]; vi += (T)dk[2 * ig + 1] * c[2 * ig + 1]; }
+    if (accumulate) { vr += o[2 * ig]; vi += o[2 * ig + 1]; }
+    o[2 * ig] = vr;
+    o[2 * ig + 1] = vi;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Real-space KB variant of the x pass.
+
+// Backward x-FFT only: full real-space lines -> R[p][i3][i2][i1].
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typename c2t<T>::type *__restrict__ bufB,
+                                                        typename c2t<T>::type *__restrict__ R, int nlines,
+                                                        int nchunk, const typename c2t<T>::type *__restrict__ tw1) {
+  typedef typename c2t<T>::type C;
+  const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
+  const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k1;
+  C *t1 = t0 + k1 * ld;
+  load_tw<T>(tw, tw1, k1);
+  const C zero = mk2<T>(0, 0);
+  for (int i = threadIdx.x; i < k1 * ld; i += blockDim.x) t0[i] = zero;
+  __syncthreads();
+  const C *B = bufB + (((long)pl * P.k3 + i3) * k2 + i20) * P1;
+  for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
+    const int l = i / P1, a = i - l * P1;
+    t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
+  }
+  __syncthreads();
+  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+  C *dst = R + (((long)pl * P.k3 + i3) * k2 + i20) * k1;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+    const int l = i / k1, i1 = i - l * k1;
+    dst[i] = r[i1 * ld + l];
+  }
+}
+
+// sumr(l, atom) = rdelv * clalp_l * sum_points vnl_l * psi(point), both bands
+// of the pair at once (real part band A, imaginary part band B).
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_nlproj(PipeParams P, const typename c2t<T>::type *__restrict__ R,
+                                                        const int *__restrict__ off, const int *__restrict__ mesh,
+                                                        const T *__restrict__ vnl, const double *__restrict__ clalp,
+                                                        double rdelv, int natom,
+                                                        typename c2t<T>::type *__restrict__ sumr) {
+  typedef typename c2t<T>::type C;
+  const int at = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const long n = (long)P.k1 * P.k2 * P.k3;
+  const C *Rp = R + (long)pl * n;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int mm = off[at] + threadIdx.x; mm < off[at + 1]; mm += blockDim.x) {
+    const C z = Rp[mesh[mm]];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const double v = (double)vnl[(long)mm * 4 + l];
+      acc[2 * l] += v * (double)z.x;
+      acc[2 * l + 1] += v * (double)z.y;
+    }
+  }
+  __shared__ double red[QX_THREADS / 32];
+  for (int l = 0; l < 8; ++l) {
+    const double s = block_sum(acc[l], red);
+    if (threadIdx.x == 0) acc[l] = s;
+  }
+  if (threadIdx.x == 0) {
+    C *o = sumr + ((long)pl * natom + at) * 4;
+    for (int l = 0; l < 4; ++l) {
+      const double f = rdelv * clalp[l];
+      o[l] = mk2<T>((T)(acc[2 * l] * f), (T)(acc[2 * l + 1] * f));
+    }
+  }
+}
+
+// Forward x pass for the real-space KB mode: V*psi + sum vnl*sumr, forward
+// x-FFT, keep the pruned part.  Line CSR `loff/lent` lists the projector
+// points of each line (i3*k2 + i2): {i1, point index, atom}.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typename c2t<T>::type *__restrict__ R,
+                                                        typename c2t<T>::type *__restrict__ bufB,
+                                                        const T *__restrict__ vloc, const int *__restrict__ loff,
+                                                        const int4 *__restrict__ lent, const T *__restrict__ vnl,
+                                                        const typename c2t<T>::type *__restrict__ sumr, int natom,
+                                                        int nlines, int nchunk,
+                                                        const typename c2t<T>::type *__restrict__ tw1) {
+  typedef typename c2t<T>::type C;
+  const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
+  const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k1;
+  C *t1 = t0 + k1 * ld;
+  load_tw<T>(tw, tw1, k1);
+  const C *src = R + (((long)pl * P.k3 + i3) * k2 + i20) * k1;
+  const T *V = vloc + ((long)i3 * k2 + i20) * k1;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+    const int l = i / k1, i1 = i - l * k1;
+    C z = src[i];
+    const T v = V[i];
+    z.x *= v; z.y *= v;
+    t0[i1 * ld + l] = z;
+  }
+  __syncthreads();
+  const C *S = sumr + (long)pl * natom * 4;
+  const int line0 = i3 * k2 + i20;
+  for (int l = 0; l < nl; ++l) {
+    for (int e = loff[line0 + l] + threadIdx.x; e < loff[line0 + l + 1]; e += blockDim.x) {
+      const int4 en = lent[e];
+      const C *s = S + (long)en.z * 4;
+      const T *v = vnl + (long)en.y * 4;
+      T ar = 0, ai = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) { ar += v[q] * s[q].x; ai += v[q] * s[q].y; }
+      atomicAdd(&t0[en.x * ld + l].x, ar);
+      atomicAdd(&t0[en.x * ld + l].y, ai);
+    }
+  }
+  __syncthreads();
+  C *res = smem_fft<T, -1>(t0, t1, nl, ld, P.L1, tw);
+  C *B = bufB + (((long)pl * P.k3 + i3) * k2 + i20) * P1;
+  for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
+    const int l = i / P1, a = i - l * P1;
+    B[i] = res[a_to_i1(a, P.m1, k1) * ld + l];
+  }
+}
+
+// --------------------------------------------------------------------------
+// Density: rho(r) += occ_A/Omega * psiA(r)^2 + occ_B/Omega * psiB(r)^2 over
+// all pairs; one CTA owns `nlines` lines of a plane and loops over the pairs,
+// so the sum is deterministic and needs no atomics.  accumulate=0 overwrites.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_xrho(PipeParams P, const typename c2t<T>::type *__restrict__ bufB,
+                                                      const double *__restrict__ wocc, double *__restrict__ rho,
+                                                      int nlines, int nchunk, int accumulate,
+                                                      const typename c2t<T>::type *__restrict__ tw1) {
+  typedef typename c2t<T>::type C;
+  const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
+  const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
+  const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k1;
+  C *t1 = t0 + k1 * ld;
+  double *acc = reinterpret_cast<double *>(t1 + k1 * ld);
+  load_tw<T>(tw, tw1, k1);
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) acc[i] = 0.0;
+  const int np = min(pair_count(P) - P.pair0, P.npair);
+  const C zero = mk2<T>(0, 0);
+  for (int pl = 0; pl < np; ++pl) {
+    const int p = P.pair0 + pl;
+    for (int i = threadIdx.x; i < k1 * ld; i += blockDim.x) t0[i] = zero;
+    __syncthreads();
+    const C *B = bufB + (((long)pl * P.k3 + i3) * k2 + i20) * P1;
+    for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
+      const int l = i / P1, a = i - l * P1;
+      t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
+    }
+    __syncthreads();
+    C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+    const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+    const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
+    for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+      const int l = i / k1, i1 = i - l * k1;
+      const C z = r[i1 * ld + l];
+      acc[i] += fa * (double)z.x * (double)z.x + fb * (double)z.y * (double)z.y;
+    }
+    __syncthreads();
+  }
+  double *dst = rho + ((long)i3 * k2 + i20) * k1;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) dst[i] = accumulate ? dst[i] + acc[i] : acc[i];
+}
+
+// --------------------------------------------------------------------------
+// Full-grid complex 3D FFT passes (density side, rfft3/fft3 drop-in).
+template <typename T, int SIGN>
+__global__ void __launch_bounds__(QX_THREADS) k_full_z(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
+                                                        int tx, FftLen L3, const typename c2t<T>::type *__restrict__ tw3) {
+  typedef typename c2t<T>::type C;
+  const int nxc = (k1 + tx - 1) / tx;
+  const int i2 = blockIdx.x / nxc, i10 = (blockIdx.x - i2 * nxc) * tx;
+  const int nl = min(tx, k1 - i10), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k3;
+  C *t1 = t0 + k3 * ld;
+  load_tw<T>(tw, tw3, k3);
+  for (int i = threadIdx.x; i < k3 * nl; i += blockDim.x) {
+    const int i3 = i / nl, l = i - i3 * nl;
+    t0[i3 * ld + l] = g[((long)i3 * k2 + i2) * k1 + i10 + l];
+  }
+  __syncthreads();
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L3, tw);
+  for (int i = threadIdx.x; i < k3 * nl; i += blockDim.x) {
+    const int i3 = i / nl, l = i - i3 * nl;
+    g[((long)i3 * k2 + i2) * k1 + i10 + l] = r[i3 * ld + l];
+  }
+}
+
+template <typename T, int SIGN>
+__global__ void __launch_bounds__(QX_THREADS) k_full_y(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
+                                                        int tx, FftLen L2, const typename c2t<T>::type *__restrict__ tw2) {
+  typedef typename c2t<T>::type C;
+  const int nxc = (k1 + tx - 1) / tx;
+  const int i3 = blockIdx.x / nxc, i10 = (blockIdx.x - i3 * nxc) * tx;
+  const int nl = min(tx, k1 - i10), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k2;
+  C *t1 = t0 + k2 * ld;
+  load_tw<T>(tw, tw2, k2);
+  C *base = g + (long)i3 * k2 * k1 + i10;
+  for (int i = threadIdx.x; i < k2 * nl; i += blockDim.x) {
+    const int i2 = i / nl, l = i - i2 * nl;
+    t0[i2 * ld + l] = base[(long)i2 * k1 + l];
+  }
+  __syncthreads();
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L2, tw);
+  for (int i = threadIdx.x; i < k2 * nl; i += blockDim.x) {
+    const int i2 = i / nl, l = i - i2 * nl;
+    base[(long)i2 * k1 + l] = r[i2 * ld + l];
+  }
+}
+
+template <typename T, int SIGN>
+__global__ void __launch_bounds__(QX_THREADS) k_full_x(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
+                                                        int nlines, FftLen L1, const typename c2t<T>::type *__restrict__ tw1,
+                                                        double scale) {
+  typedef typename c2t<T>::type C;
+  const int nch = (k2 + nlines - 1) / nlines;
+  const int i3 = blockIdx.x / nch, i20 = (blockIdx.x - i3 * nch) * nlines;
+  const int nl = min(nlines, k2 - i20), ld = nl | 1;
+  extern __shared__ unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *t0 = tw + k1;
+  C *t1 = t0 + k1 * ld;
+  load_tw<T>(tw, tw1, k1);
+  C *base = g + ((long)i3 * k2 + i20) * k1;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+    const int l = i / k1, i1 = i - l * k1;
+    t0[i1 * ld + l] = base[i];
+  }
+  __syncthreads();
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L1, tw);
+  const T s = (T)scale;
+  for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
+    const int l = i / k1, i1 = i - l * k1;
+    C z = r[i1 * ld + l];
+    z.x *= s; z.y *= s;
+    base[i] = z;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Host-side launchers (called from qx_api.cu).
+
+namespace qx {
+
+static size_t fft_smem(int n, int ld, size_t csz) { return (size_t)csz * (n + 2 * (size_t)n * ld); }
+
+template <typename T>
+int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
+                      const double *dk, int accumulate, int nlmode, cudaStream_t st) {
+  typedef typename c2t<T>::type C;
+  const size_t cs = sizeof(C);
+  Bufs<T> &bf = pl.bufs<T>();
+  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  dim3 gz(P.P2, npl);
+  size_t smz = fft_smem(P.k3, (P.P1 | 1), cs);
+  k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, tw3);
+  dim3 gy(P.k3, npl);
+  size_t smy = fft_smem(P.k2, P.P1, cs);
+  k_ypass<T, +1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, tw2);
+  const int nlines = pl.xlines<T>();
+  const int nch = (P.k2 + nlines - 1) / nlines;
+  dim3 gx(P.k3 * nch, npl);
+  size_t smx = fft_smem(P.k1, nlines | 1, cs);
+  if (nlmode == 2) {
+    k_xinv_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.bufR, nlines, nch, tw1);
+    dim3 ga(pl.natom, npl);
+    k_nlproj<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, pl.d_kb_clalp,
+                                           pl.rdelv, pl.natom, bf.sumr);
+    k_xfwd_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufR, bf.bufB, bf.vloc, pl.d_line_off, pl.d_line_ent,
+                                             bf.kb_vnl, bf.sumr, pl.natom, nlines, nch, tw1);
+  } else {
+    k_xvx<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.vloc, nlines, nch, tw1);
+  }
+  k_ypass<T, -1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, tw2);
+  k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, tw3);
+  dim3 gu((P.nplw + 1 + 127) / 128, npl);
+  k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate);
+  return 0;
+}
+
+template <typename T>
+int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const double *wocc,
+                     double *rho, int accumulate, cudaStream_t st) {
+  typedef typename c2t<T>::type C;
+  const size_t cs = sizeof(C);
+  Bufs<T> &bf = pl.bufs<T>();
+  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  dim3 gz(P.P2, npl);
+  k_zinv<T><<<gz, QX_THREADS, fft_smem(P.k3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, tw3);
+  dim3 gy(P.k3, npl);
+  k_ypass<T, +1><<<gy, QX_THREADS, fft_smem(P.k2, P.P1, cs), st>>>(P, bf.bufA, bf.bufB, tw2);
+  const int nlines = pl.rholines;
+  const int nch = (P.k2 + nlines - 1) / nlines;
+  size_t sm = fft_smem(P.k1, nlines | 1, cs) + sizeof(double) * nlines * P.k1;
+  k_xrho<T><<<P.k3 * nch, QX_THREADS, sm, st>>>(P, bf.bufB, wocc, rho, nlines, nch, accumulate, tw1);
+  return 0;
+}
+
+template <typename T>
+int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st) {
+  typedef typename c2t<T>::type C;
+  const size_t cs = sizeof(C);
+  Bufs<T> &bf = pl.bufs<T>();
+  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  const int k1 = pl.k1, k2 = pl.k2, k3 = pl.k3;
+  const int tx = 16;
+  const int nxc = (k1 + tx - 1) / tx;
+  const int nlines = pl.xlines<T>();
+  const int nch = (k2 + nlines - 1) / nlines;
+  if (sign > 0) {
+    k_full_z<T, +1><<<k2 * nxc, QX_THREADS, fft_smem(k3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[2], tw3);
+    k_full_y<T, +1><<<k3 * nxc, QX_THREADS, fft_smem(k2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[1], tw2);
+    k_full_x<T, +1><<<k3 * nch, QX_THREADS, fft_smem(k1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, pl.L[0], tw1, scale);
+  } else {
+    k_full_z<T, -1><<<k2 * nxc, QX_THREADS, fft_smem(k3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[2], tw3);
+    k_full_y<T, -1><<<k3 * nxc, QX_THREADS, fft_smem(k2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[1], tw2);
+    k_full_x<T, -1><<<k3 * nch, QX_THREADS, fft_smem(k1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, pl.L[0], tw1, scale);
+  }
+  return 0;
+}
+
+// Opt every kernel above into the shared-memory size the largest plan needs.
+template <typename T>
+void set_fft_smem_limits(size_t bytes) {
+  cudaFuncSetAttribute(k_zinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_ypass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_ypass<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xvx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_zfwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xinv_r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xfwd_r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xrho<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_z<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_z<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_y<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_y<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_x<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_full_x<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template int launch_hpsi_chunk<float>(const Plan &, const PipeParams &, int, const float *, long, float *, long,
+                                      const double *, int, int, cudaStream_t);
+template int launch_hpsi_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, double *, long,
+                                       const double *, int, int, cudaStream_t);
+template int launch_rho_chunk<float>(const Plan &, const PipeParams &, int, const float *, long, const double *,
+                                     double *, int, cudaStream_t);
+template int launch_rho_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, const double *,
+                                      double *, int, cudaStream_t);
+template int launch_full_fft<float>(const Plan &, float2 *, int, double, cudaStream_t);
+template int launch_full_fft<double>(const Plan &, double2 *, int, double, cudaStream_t);
+template void set_fft_smem_limits<float>(size_t);
+template void set_fft_smem_limits<double>(size_t);
+
+}  // namespace qx

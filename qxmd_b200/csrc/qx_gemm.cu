@@ -1,0 +1,110 @@
+// Tiled CUDA-core GEMM for the band and projector contractions:
+// S = C^T C (schmidt.f90:190-237), H_sub = C^T HC (engrad.f90:869-895),
+// <beta|psi> and its back-application (nlkbpp.f90:1678-1713), subgs3
+// (engrad.f90:1122-1142), C*U (eigen.f90:1482-1510) and C*L^-T
+// (schmidt.f90:284-313).  The Gamma-point half-sphere metric
+// 2*sum - x(1)*y(1) is applied in the epilogue.
+#include "qx_internal.h"
+
+namespace qx {
+
+constexpr int BM = 64, BN = 64, BK = 16;
+
+template <typename T, bool TA, bool TB>
+__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, const T *__restrict__ A, long lda,
+                                              const T *__restrict__ B, long ldb, T beta, T *__restrict__ Cm, long ldc,
+                                              int gamma, const int *__restrict__ colmap, const int *__restrict__ ncol_dev) {
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+  const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (n0 >= Nact) return;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  T acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int e = tid + 256 * r;
+      int m, k;
+      if (TA) { k = e & 15; m = e >> 4; } else { m = e & 63; k = e >> 6; }
+      const int gm = m0 + m, gk = k0 + k;
+      T v = 0;
+      if (gm < M && gk < K) v = TA ? A[(long)gm * lda + gk] : A[(long)gk * lda + gm];
+      As[k][m] = v;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int e = tid + 256 * r;
+      int n, k;
+      if (!TB) { k = e & 15; n = e >> 4; } else { n = e & 63; k = e >> 6; }
+      const int gn = n0 + n, gk = k0 + k;
+      T v = 0;
+      if (gn < Nact && gk < K) {
+        const long cn = colmap ? colmap[gn] : gn;
+        v = TB ? B[(long)gk * ldb + cn] : B[cn * ldb + gk];
+      }
+      Bs[k][n] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BK; ++k) {
+      T a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx + 16 * j;
+      if (gn >= Nact) continue;
+      const long cn = colmap ? colmap[gn] : gn;
+      T v = acc[i][j];
+      if (gamma) {
+        const T a0 = TA ? A[(long)gm * lda] : A[gm];
+        const T b0 = TB ? B[cn] : B[cn * ldb];
+        v = (T)2 * v - a0 * b0;
+        if (gamma == 2) {
+          const T a1 = TA ? A[(long)gm * lda + 1] : A[lda + gm];
+          const T b1 = TB ? B[ldb + cn] : B[cn * ldb + 1];
+          v -= (T)2 * a1 * b1;
+        }
+      }
+      T *c = Cm + cn * ldc + gm;
+      *c = (beta == (T)0) ? alpha * v : alpha * v + beta * *c;
+    }
+  }
+}
+
+template <typename T>
+int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
+         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return 0;
+  dim3 g((M + BM - 1) / BM, (N + BN - 1) / BN);
+  if (ta && tb) k_gemm<T, true, true><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
+  else if (ta) k_gemm<T, true, false><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
+  else if (tb) k_gemm<T, false, true><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
+  else k_gemm<T, false, false><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
+  return 0;
+}
+
+template int gemm<float>(bool, bool, int, int, int, float, const float *, long, const float *, long, float, float *,
+                         long, int, const int *, const int *, cudaStream_t);
+template int gemm<double>(bool, bool, int, int, int, double, const double *, long, const double *, long, double,
+                          double *, long, int, const int *, const int *, cudaStream_t);
+
+}  // namespace qx

@@ -1,0 +1,108 @@
+// Internal structures shared by the kernel files and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "qx_common.cuh"
+
+// Parameters of one launch of the FFT pipeline (passed by value).
+struct PipeParams {
+  int k1, k2, k3;
+  int m1, m2, P1, P2;
+  int nplw;
+  FftLen L1, L2, L3;
+  const int *row_lo, *row_hi, *row_off;
+  const int4 *row_ent;      // {line = a - lo, i3, ig, sign(+1 : +G, -1 : -G)}
+  const int *pairs;         // band indices, 2 per pair, -1 = empty slot
+  const int *npair_dev;     // number of valid pairs (device), or null
+  int npair;                // pair bound when npair_dev is null
+  int pair0;                // first pair of this launch
+  double inv_n;             // 1 / kfft0
+};
+
+namespace qx {
+
+void set_error(const char *fmt, ...);
+
+// Per-precision device buffers of the FFT pipeline.
+template <typename T>
+struct Bufs {
+  typedef typename c2t<T>::type C;
+  C *tw = nullptr;         // twiddles of all three lengths
+  C *bufA = nullptr;       // [chunk][k3][P2][P1]
+  C *bufB = nullptr;       // [chunk][k3][k2][P1]
+  C *bufR = nullptr;       // [chunk][k3][k2][k1] (real-space KB mode)
+  C *zsph = nullptr;       // [chunk][nplw+1][2]
+  C *sumr = nullptr;       // [chunk][natom][4]
+  T *vloc = nullptr;       // glocal(kfft0)
+  T *kb_vnl = nullptr;     // real-space projector values [npts][4]
+  T *kbg = nullptr;        // G-space projectors [nproj][nplwex]
+  T *vclalp = nullptr;     // [nproj]
+};
+
+struct Plan {
+  int k1 = 0, k2 = 0, k3 = 0;
+  long n = 0;
+  int m1 = 0, m2 = 0, m3 = 0, P1 = 0, P2 = 0;
+  int nplw = 0, nplwex = 0;
+  FftLen L[3];
+  int tw_off[3];
+  int chunk = 0;           // pairs per pipeline launch
+  int rholines = 8;
+  int xl32 = 16, xl64 = 8; // lines per CTA of the x pass
+  // sphere rows
+  int *d_row_lo = nullptr, *d_row_hi = nullptr, *d_row_off = nullptr;
+  int4 *d_row_ent = nullptr;
+  // real-space KB
+  int natom = 0, npts = 0;
+  int *d_kb_off = nullptr, *d_kb_mesh = nullptr;
+  double *d_kb_clalp = nullptr;
+  double rdelv = 0.0;
+  int *d_line_off = nullptr;
+  int4 *d_line_ent = nullptr;
+  // G-space KB
+  int nproj = 0;
+  mutable Bufs<float> b32;
+  mutable Bufs<double> b64;
+  template <typename T> Bufs<T> &bufs() const;
+  template <typename T> int xlines() const;
+};
+
+template <> inline Bufs<float> &Plan::bufs<float>() const { return b32; }
+template <> inline Bufs<double> &Plan::bufs<double>() const { return b64; }
+template <> inline int Plan::xlines<float>() const { return xl32; }
+template <> inline int Plan::xlines<double>() const { return xl64; }
+
+// qx_fft.cu
+template <typename T>
+int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
+                      const double *dk, int accumulate, int nlmode, cudaStream_t st);
+template <typename T>
+int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const double *wocc,
+                     double *rho, int accumulate, cudaStream_t st);
+template <typename T>
+int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
+template <typename T> void set_fft_smem_limits(size_t bytes);
+
+// qx_gemm.cu: C(m,n) = alpha * op(A)(m,:) . op(B)(:,n) + beta * C(m,n), column-major.
+// TA: A stored K x M (A[m*lda + k]); TB: B stored N x K (B[k*ldb + n]).
+// gamma: 0 plain; 1 Gamma-point metric 2*sum - a0*b0; 2 KB projection
+// metric 2*sum - a0*b0 - 2*a1*b1.  colmap (device, optional) maps output
+// column n to stored column colmap[n] of B and C; ncol_dev (device,
+// optional) bounds the number of columns.
+template <typename T>
+int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
+         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st);
+
+// qx_dense.cu (FP64, nb x nb)
+int cholinv(double *S, int n, int *d_info, cudaStream_t st);
+int jacobi(double *A, int n, double *w, double *V, int maxsweep, int *d_info, cudaStream_t st);
+template <typename Tin, typename Tout>
+void convert(const Tin *in, Tout *out, long n, cudaStream_t st);
+template <typename T>
+void symmetrize_lower(const T *in, double *out, double *diag, int n, cudaStream_t st);
+
+}  // namespace qx

@@ -1,0 +1,139 @@
+"""Band-space routines through the C ABI against the oracle: schmidt2
+(schmidt.f90:117-378), hmatrix2 (engrad.f90:845-956), untryt2/untryhc2
+(eigen.f90:1171-1451), eigen_BKL (eigen.f90:199-938), softchg
+(chgdns.f90:388-454), gradresnv and rfft3 (fft3.f90:113-232).
+
+FP64 tolerances 1e-10 (eigenvector-dependent quantities 1e-8); mixed 1e-4."""
+import numpy as np
+import pytest
+
+import oracle
+from qxmd_b200 import cell
+from qxmd_b200.lib import CgParm, Context, QxError, QX_NL_GSPACE, QX_NL_RSPACE, QX_PREC_FP64, QX_PREC_MIXED
+
+from gpu_util import need_gpu, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def raw_psi(s, nb):
+    return cell.random_wavefunctions(s.gs.nplwex, nb)
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-11), (QX_PREC_MIXED, 1e-4)])
+def test_schmidt(si8, prec, tol):
+    need_gpu()
+    c = raw_psi(si8, 16)
+    ctx = Context(si8, prec, QX_NL_GSPACE)
+    q = ctx.schmidt_host(c)
+    ref, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    assert relerr(q, ref) < tol
+
+
+def test_schmidt_not_positive_definite(si8):
+    need_gpu()
+    c = raw_psi(si8, 16)
+    # A zero band gives a zero pivot; the reference's test is pivot <= 1e-30
+    # (schmidt.f90:256-267), which rounding noise of merely dependent bands
+    # does not reach.
+    c[5] = 0.0
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    with pytest.raises(QxError) as e:
+        ctx.schmidt_host(c)
+    assert e.value.code == 3
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-11), (QX_PREC_MIXED, 5e-5)])
+def test_hmatrix_untryt_untryhc(si8, si8_psi, prec, tol):
+    need_gpu()
+    h = oracle.Ham(si8, 1)
+    hc = h.hpsi(si8_psi)
+    ctx = Context(si8, prec, QX_NL_GSPACE)
+    ctx.put_psi(si8_psi)
+    ctx.put_hpsi(hc)
+    hm = ctx.hmatrix()
+    hm_ref, eig_ref = oracle.hmatrix(si8_psi, hc)
+    assert relerr(hm, hm_ref) < tol
+    assert relerr(ctx.get_eig(), eig_ref) < tol
+    ev = ctx.untryt()
+    ctx.untryhc()
+    w, u, _ = oracle.jacobi(hm_ref)
+    assert relerr(ev, w) < tol
+    psi_ref = oracle.rotate(si8_psi, u)
+    hc_ref = oracle.rotate(hc, u)
+    assert relerr(ctx.get_psi(), psi_ref) < tol * 1e3
+    assert relerr(ctx.get_hpsi(), hc_ref) < tol * 1e3
+
+
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+@pytest.mark.parametrize("nlmode", [QX_NL_GSPACE, QX_NL_RSPACE])
+def test_eigen_bkl(si8, si8_psi, prec, nlmode):
+    need_gpu()
+    h = oracle.Ham(si8, nlmode)
+    hc = h.hpsi(si8_psi)
+    _, ekib = h.ekinetic(si8_psi)
+    x_ref, hx_ref, eig_ref, _, nri_ref = h.eigen(si8_psi, hc, ekib, noband=16)
+    ctx = Context(si8, prec, nlmode)
+    p = CgParm.defaults(16)
+    x, hx, eig = ctx.eigen_host(si8_psi, hc, ekib, p)
+    if prec == QX_PREC_FP64:
+        assert relerr(eig, eig_ref) < 1e-10
+        assert relerr(x, x_ref) < 1e-8
+        assert relerr(hx, hx_ref) < 1e-8
+    else:
+        assert relerr(eig, eig_ref) < 1e-4
+        assert relerr(x, x_ref) < 1e-2
+
+
+def test_eigen_snapshot_semantics_real4(si8, si8_psi):
+    """CCREAL4: the lower-band snapshot is rounded to real*4 (eigen.f90:78-82)."""
+    need_gpu()
+    h = oracle.Ham(si8, 1)
+    hc = h.hpsi(si8_psi)
+    _, ekib = h.ekinetic(si8_psi)
+    ref = h.eigen(si8_psi, hc, ekib, noband=16, ccreal4=True)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    x, hx, eig = ctx.eigen_host(si8_psi, hc, ekib, CgParm.defaults(16, ccreal4=1))
+    assert relerr(eig, ref[2]) < 1e-10
+    assert relerr(x, ref[0]) < 1e-8
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-12), (QX_PREC_MIXED, 1e-5)])
+def test_softchg(si8, si8_psi, prec, tol):
+    need_gpu()
+    ctx = Context(si8, prec, QX_NL_GSPACE)
+    rho = ctx.softchg_host(si8_psi)
+    ref = oracle.Ham(si8, 1).softchg(si8_psi, si8.occ)
+    assert relerr(rho, ref) < tol
+    assert rho.sum() * si8.gs.rvol / si8.gs.kfft0 == pytest.approx(si8.cell.nel, rel=10 * tol)
+
+
+def test_gradres(si8, si8_psi):
+    need_gpu()
+    h = oracle.Ham(si8, 1)
+    hc = h.hpsi(si8_psi)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    ctx.put_psi(si8_psi)
+    ctx.put_hpsi(hc)
+    ctx.hmatrix()
+    prod, zmax, zsum = ctx.gradres()
+    _, eig = oracle.hmatrix(si8_psi, hc)
+    pref, zm, zs = oracle.gradres(si8_psi, hc, eig, si8.occ)
+    assert relerr(prod, pref) < 1e-10
+    assert zmax == pytest.approx(zm, rel=1e-10)
+
+
+def test_rfft3(si8):
+    need_gpu()
+    gs = si8.gs
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(gs.kfft0)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    fx, fy = ctx.rfft3_host(1, x, np.zeros_like(x))
+    k1, k2, k3 = gs.grid
+    ref = np.fft.fftn(x.reshape(k3, k2, k1)).ravel() / gs.kfft0
+    assert relerr(fx + 1j * fy, ref) < 1e-13
+    bx, by = ctx.rfft3_host(2, fx, fy)
+    assert relerr(bx, x) < 1e-13
+    assert np.all(by == 0.0)

@@ -1,0 +1,45 @@
+"""Whole SCF iterations (pwlda.f90:1628-3700 order) on the device against the
+oracle's iteration on the same inputs (Si8, G-space and real-space KB)."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle.scf import ScfState
+from qxmd_b200 import cell
+from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_NL_RSPACE, QX_PREC_FP64, QX_PREC_MIXED
+
+from gpu_util import need_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nlmode", [QX_NL_GSPACE, QX_NL_RSPACE])
+def test_scf_iterations_match_oracle_fp64(si8, si8_psi, nlmode):
+    need_gpu()
+    st = ScfState(si8, si8_psi, nlmode=nlmode)
+    ctx = Context(si8, QX_PREC_FP64, nlmode)
+    ctx.put_psi(si8_psi)
+    ctx.scf_init()
+    ctx.scf_rho_from_psi()
+    p = CgParm.defaults(16)
+    for it in range(4):
+        g = ctx.scf_iteration(p)
+        r = st.iteration(noband=16)
+        assert g["etot"] == pytest.approx(r["etot"], abs=1e-8 * max(1.0, abs(r["etot"])))
+        assert g["ncg_hpsi"] == r["ncg_hpsi"]
+        assert g["resid"] == pytest.approx(r["resid"], rel=1e-6)
+
+
+def test_scf_mixed_tracks_fp64(si8, si8_psi):
+    need_gpu()
+    p = CgParm.defaults(16)
+    e = {}
+    for prec in (QX_PREC_FP64, QX_PREC_MIXED):
+        ctx = Context(si8, prec, QX_NL_GSPACE)
+        ctx.put_psi(si8_psi)
+        ctx.scf_init()
+        ctx.scf_rho_from_psi()
+        e[prec] = [ctx.scf_iteration(p)["etot"] for _ in range(6)]
+    # same trajectory to FP32 accuracy over the first iterations
+    assert abs(e[QX_PREC_MIXED][0] - e[QX_PREC_FP64][0]) < 1e-3
+    assert abs(e[QX_PREC_MIXED][-1] - e[QX_PREC_FP64][-1]) < 5e-2
