@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the Kohn-Sham hot path: SCF iterations per second on Si64.
+
+Workload: Si64 2x2x2 diamond supercell, a = 20.52 bohr, seeded +-0.05 bohr
+displacements, Gamma point, Ecut 16 Ry with the norm-conserving density cutoff
+4*Ecut (54^3 FFT grid by the reference's chkftm rule), 160 bands (128
+occupied), G-space KB projectors (256), model pseudopotential, reference LCG
+initial wavefunctions.  One step = one SCF iteration in the reference's order
+(potential, H|psi> for all bands, H_sub, subspace rotation, BKL CG, Gram-
+Schmidt, density, mixing), mixed precision (FP32 FFTs and band contractions,
+FP64 Cholesky/eigen/density).  The FP64 drop-in path is timed beside it.
+
+Arms:
+  --impl ours       the CUDA library through its C ABI (default)
+  --impl reference  the CPU restatement of the reference algorithm (the
+                    oracle; QXMD itself needs gfortran+FFTW+MPI, absent on
+                    this image), all host cores, same metric.
+Multi-GPU: the single-cell path does not shard, so N ranks run N independent
+replicas ("replicas only"); value = all iterations / max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SCF iter/s"
+UNIT = "iter/s"
+WORKLOAD = "Si64 diamond 2x2x2, Gamma, Ecut 16 Ry / 64 Ry, 54^3 grid, 160 bands, G-space KB"
+# Average CG H|psi> band applications per SCF iteration of this workload after
+# the warm-up iterations (measured on the device path), used to scale the
+# reference arm's band-application rate to SCF iterations.
+CG_BAPPS_PER_ITER = 250
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_sample(sys_, nb_apps, nthreads=1):
+    """Oracle (CPU FP64 restatement) band-application rate and dense-part
+    time on this workload: returns (band-apps/s, dense seconds)."""
+    import oracle
+    from qxmd_b200 import cell
+    ham = oracle.Ham(sys_, 1)
+    c = cell.random_wavefunctions(sys_.gs.nplwex, nb_apps)
+    t = time.perf_counter()
+    ham.hpsi(c)
+    rate = nb_apps / (time.perf_counter() - t)
+    return rate
+
+
+def run_ours(args):
+    import torch
+
+    from qxmd_b200 import cell
+    from qxmd_b200.lib import (CgParm, Context, QX_HPSI_KINETIC, QX_NL_GSPACE, QX_PREC_FP64,
+                               QX_PREC_MIXED, launch_count)
+    ws, rank, local = dist_setup(args)
+    sys_ = cell.si64()
+    psi0 = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
+    noband = int(sys_.cell.nel // 2)
+    parm = CgParm.defaults(noband)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    K, W = args.steps, args.warmup
+    res = {}
+    clocks = Clocks(local)
+    for prec in (QX_PREC_MIXED, QX_PREC_FP64):
+        ctx = Context(sys_, prec, QX_NL_GSPACE)
+        ctx.put_psi(psi0)
+        ctx.schmidt()
+        ctx.scf_init()
+        ctx.scf_rho_from_psi()
+        for _ in range(W):
+            ctx.scf_iteration(parm)
+        barrier(ws)
+        if prec == QX_PREC_MIXED:
+            clocks.start()
+        n0 = launch_count()
+        tot_ms, outs = 0.0, []
+        for _ in range(K):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            outs.append(ctx.scf_iteration(parm))
+            e1.record()
+            torch.cuda.synchronize()
+            tot_ms += e0.elapsed_time(e1)
+        launches = launch_count() - n0
+        if prec == QX_PREC_MIXED:
+            clk = clocks.stop()
+        barrier(ws)
+        tmax = max_over_ranks(tot_ms, ws)
+        r = {"ms_per_step": tmax / K, "value": ws * K / (tmax / 1e3), "launches": launches,
+             "etot_last": outs[-1]["etot"], "cg_bapps_per_iter": float(np.mean([o["ncg_hpsi"] for o in outs])),
+             "eig_clusters": float(np.mean([o["eig_clusters"] for o in outs]))}
+        # H|psi> band applications per second (enonloc: kinetic + local + KB, all bands)
+        R = max(3, K)
+        ctx.enonloc()
+        t = 0.0
+        for _ in range(R):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.enonloc()
+            e1.record()
+            torch.cuda.synchronize()
+            t += e0.elapsed_time(e1)
+        r["hpsi_band_apps_per_s"] = ws * sys_.nband * R / (max_over_ranks(t, ws) / 1e3)
+        # FFT pipeline alone (kinetic + local potential): roofline unit
+        p_psi, p_h = ctx.dev_ptr(0), ctx.dev_ptr(1)
+        t = 0.0
+        for _ in range(R):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.hpsi_dev(p_psi, p_h, sys_.nband, QX_HPSI_KINETIC)
+            e1.record()
+            torch.cuda.synchronize()
+            t += e0.elapsed_time(e1)
+        r["fft_pipeline_ms"] = t / R
+        if prec == QX_PREC_MIXED:
+            # end to end through the host-array API: H2D psi (pinned), one
+            # iteration, D2H psi, rho, eigenvalues
+            hpsi = torch.empty((sys_.nband, sys_.gs.nplwex), dtype=torch.float64).pin_memory()
+            hrho = torch.empty(sys_.gs.kfft0, dtype=torch.float64).pin_memory()
+            heig = torch.empty(sys_.nband, dtype=torch.float64).pin_memory()
+            npsi, nrho, neig = hpsi.numpy(), hrho.numpy(), heig.numpy()
+            npsi[:] = ctx.get_psi()
+            t = 0.0
+            for _ in range(K):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                ctx.put_psi(npsi)
+                ctx.scf_iteration(parm)
+                ctx.L.qx_get_psi(ctx.h, npsi)
+                ctx.L.qx_get_rho(ctx.h, nrho)
+                ctx.L.qx_get_eig(ctx.h, neig)
+                e1.record()
+                torch.cuda.synchronize()
+                t += e0.elapsed_time(e1)
+            tm = max_over_ranks(t, ws)
+            r["e2e"] = {"value": ws * K / (tm / 1e3), "unit": UNIT,
+                        "h2d_bytes_per_step": int(npsi.nbytes),
+                        "d2h_bytes_per_step": int(npsi.nbytes + nrho.nbytes + neig.nbytes)}
+            r["clocks"] = clk
+        res[prec] = r
+        ctx.close()
+    mixed, fp64 = res[QX_PREC_MIXED], res[QX_PREC_FP64]
+    hbm, peak_kind = peaks()
+    N, ne = sys_.gs.kfft0, sys_.gs.nplwex
+    bytes_per_bapp = 4 * N * 4 + 2 * ne * 4
+    achieved = bytes_per_bapp * sys_.nband / (mixed["fft_pipeline_ms"] * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": mixed["value"], "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded Si64 cell, model pseudopotential)",
+        "config": {"workload": WORKLOAD, "bands": sys_.nband, "nplwex": ne, "grid": list(sys_.gs.grid),
+                   "precision": "mixed", "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "256 MB buffer written between timed iterations"},
+        "hpsi_band_apps_per_s": mixed["hpsi_band_apps_per_s"],
+        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"],
+                 "hpsi_band_apps_per_s": fp64["hpsi_band_apps_per_s"]},
+        "mixed_over_fp64": mixed["value"] / fp64["value"],
+        "cg_bapps_per_iter": mixed["cg_bapps_per_iter"],
+        "eig_clusters": mixed["eig_clusters"],
+        "e2e": mixed["e2e"],
+        "gpu_launches": mixed["launches"],
+        "roofline": {"kernel": "H|psi> FFT pipeline (zinv, y, xvx, y, zfwd, unpack), FP32",
+                     "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_band_app": bytes_per_bapp, "traffic": None},
+        "clocks": mixed["clocks"],
+    }
+    if ws == 1 and rank == 0:
+        rate = cpu_sample(sys_, 8)
+        bapps = sys_.nband + mixed["cg_bapps_per_iter"]
+        line["cpu_baseline"] = {"value": rate / bapps, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": f"8 H|psi> band-applications of this workload on the FP64 oracle "
+                                          f"({rate:.2f}/s, 1 thread) scaled by {bapps:.0f} band-applications "
+                                          f"per SCF iteration; dense band-space work not included"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def _ref_worker(args):
+    import oracle
+    from qxmd_b200 import cell
+    seed, nb = args
+    sys_ = cell.si64(with_ewald=False)
+    ham = oracle.Ham(sys_, 1)
+    c = cell.random_wavefunctions(sys_.gs.nplwex, nb, seed=25.0 + seed)
+    t = time.perf_counter()
+    ham.hpsi(c)
+    return nb, time.perf_counter() - t
+
+
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    ctxm = mp.get_context("spawn")
+    from qxmd_b200 import cell
+    sys_ = cell.si64(with_ewald=False)
+    bapps_iter = sys_.nband + CG_BAPPS_PER_ITER
+    times = []
+    with ctxm.Pool(ncores) as pool:
+        for step in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            out = pool.map(_ref_worker, [(step * ncores + i, 1) for i in range(ncores)])
+            dt = time.perf_counter() - t
+            if step >= args.warmup:
+                times.append((sum(o[0] for o in out), dt))
+    nb_done = sum(x[0] for x in times)
+    tt = sum(x[1] for x in times)
+    rate = nb_done / tt
+    v = rate / bapps_iter
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
+                             "sample": f"each step: {ncores} Si64 H|psi> band-applications in parallel on the "
+                                       f"FP64 oracle ({rate:.2f} band-apps/s), scaled by {bapps_iter} "
+                                       f"band-applications per SCF iteration"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -62,11 +62,13 @@ typedef struct {
   double resid;      /* int (rho_out - rho_in)^2                         */
   double zmax;       /* max band residual before the CG (gradres)        */
   int ncg_hpsi;      /* H|psi> band applications spent in the CG        */
-  int jacobi_sweeps;
+  int eig_clusters;     /* eigenvalue clusters of the subspace problem */
 } qx_scf_out;
 
 const char *qx_last_error(void);
 int qx_version(void);
+/* Number of kernels this library has launched in the process (all contexts). */
+long qx_launch_count(void);
 
 /* ---- set-up (module state of the reference, uploaded once per geometry) -- */
 

@@ -15,7 +15,11 @@
 #include "qx_internal.h"
 #include "qx_scf.h"
 
+#include <atomic>
+
 namespace qx {
+static std::atomic<long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 static thread_local char g_err[512] = "";
 void set_error(const char *fmt, ...) {
   va_list ap;
@@ -63,12 +67,15 @@ struct qx_ctx {
   double *d_dk = nullptr, *d_occ = nullptr, *d_wocc = nullptr, *d_eig = nullptr, *d_ekib = nullptr, *d_w = nullptr;
   double *d_hsub = nullptr, *d_mat = nullptr, *d_V = nullptr;   // nb*nb, nb*nb, 2*nb*nb
   double *d_prod = nullptr;
+  double *d_eigws = nullptr;   // eigensolver work, 8*nb*nb + 16*nb
   int *d_info = nullptr;
   int *d_allpairs = nullptr;
   // state arrays in the context precision
   void *psi = nullptr, *hpsi = nullptr, *g = nullptr, *h = nullptr, *gh = nullptr, *snap = nullptr, *tmp = nullptr;
   void *mat_t = nullptr;   // nb*nb in T
   void *proj = nullptr;    // nproj*nb in T
+  void *gws = nullptr;     // split-K GEMM workspace
+  size_t gws_bytes = 0;
   CgState cg;
   // density side
   double *d_rho_in = nullptr, *d_rho_out = nullptr, *d_vloc = nullptr, *d_glocal = nullptr, *d_g2 = nullptr;
@@ -96,42 +103,86 @@ static int dalloc(qx_ctx *c, P **p, size_t bytes) {
 
 extern "C" const char *qx_last_error(void) { return g_err; }
 extern "C" int qx_version(void) { return 1; }
+extern "C" long qx_launch_count(void) { return g_launches.load(); }
 
 // ---------------------------------------------------------------------------
 static bool factor_len(int n, FftLen &L) {
   L.n = n;
   L.nstage = 0;
   int m = n;
-  const int rad[5] = {4, 2, 3, 5, 7};
-  for (int r : rad) {
-    while (m % r == 0) {
-      if (L.nstage >= 8) return false;
-      L.radix[L.nstage++] = r;
-      m /= r;
-    }
+  // largest radices first: fewer passes through shared memory
+  const int rad[8] = {9, 8, 7, 6, 5, 4, 3, 2};
+  while (m > 1) {
+    int r = 0;
+    for (int c : rad)
+      if (m % c == 0) { r = c; break; }
+    if (!r || L.nstage >= 8) return false;
+    L.radix[L.nstage++] = r;
+    m /= r;
   }
-  if (m != 1) return false;
-  if (n == 1) { L.radix[0] = 1; }
+  // stage table layout
+  int ns = 1, st = 0, ob = 0;
+  for (int s = 0; s < L.nstage; ++s) {
+    const int R = L.radix[s], nr = n / R;
+    L.st_off[s] = st;
+    L.ob_off[s] = ob;
+    st += nr * (R - 1);
+    ob += nr;
+    ns *= R;
+  }
+  L.nst = st;
+  L.nob = ob;
   return true;
+}
+
+// Stage output bases (precision independent) of the three lengths.
+static void stage_bases(const FftLen &L, std::vector<int> &out) {
+  int ns = 1;
+  for (int s = 0; s < L.nstage; ++s) {
+    const int R = L.radix[s], nr = L.n / R;
+    for (int j = 0; j < nr; ++j) out.push_back((j / ns) * ns * R + j % ns);
+    ns *= R;
+  }
 }
 
 template <typename T>
 static int upload_tw(qx_ctx *c) {
   typedef typename c2t<T>::type C;
   Plan &pl = c->pl;
-  const int tot = pl.k1 + pl.k2 + pl.k3;
-  std::vector<C> h(tot);
-  const int ns[3] = {pl.k1, pl.k2, pl.k3};
   const double tp = 2.0 * std::acos(-1.0);
-  for (int d = 0; d < 3; ++d)
-    for (int t = 0; t < ns[d]; ++t) {
-      h[pl.tw_off[d] + t].x = (T)std::cos(tp * t / ns[d]);
-      h[pl.tw_off[d] + t].y = (T)-std::sin(tp * t / ns[d]);
+  std::vector<C> base, stg;
+  for (int d = 0; d < 3; ++d) {
+    const FftLen &L = pl.L[d];
+    const int n = L.n;
+    for (int t = 0; t < n; ++t) {
+      C w;
+      w.x = (T)std::cos(tp * t / n);
+      w.y = (T)-std::sin(tp * t / n);
+      base.push_back(w);
     }
-  C *dp = nullptr;
-  TRY(dalloc(c, &dp, sizeof(C) * tot));
-  CK(cudaMemcpy(dp, h.data(), sizeof(C) * tot, cudaMemcpyHostToDevice));
+    int ns = 1;
+    for (int s = 0; s < L.nstage; ++s) {
+      const int R = L.radix[s], nr = n / R, tstep = n / (ns * R);
+      for (int j = 0; j < nr; ++j) {
+        const int k = j % ns;
+        for (int r = 1; r < R; ++r) {
+          const long idx = ((long)k * r * tstep) % n;
+          C w;
+          w.x = (T)std::cos(tp * idx / n);
+          w.y = (T)-std::sin(tp * idx / n);
+          stg.push_back(w);
+        }
+      }
+      ns *= R;
+    }
+  }
+  C *dp = nullptr, *ds = nullptr;
+  TRY(dalloc(c, &dp, sizeof(C) * base.size()));
+  TRY(dalloc(c, &ds, sizeof(C) * std::max<size_t>(stg.size(), 1)));
+  CK(cudaMemcpy(dp, base.data(), sizeof(C) * base.size(), cudaMemcpyHostToDevice));
+  if (!stg.empty()) CK(cudaMemcpy(ds, stg.data(), sizeof(C) * stg.size(), cudaMemcpyHostToDevice));
   pl.bufs<T>().tw = dp;
+  pl.bufs<T>().stw = ds;
   return 0;
 }
 
@@ -153,15 +204,7 @@ static int alloc_pipe(qx_ctx *c) {
   CK(cudaMemset(b.vloc, 0, sizeof(T) * pl.n));
   TRY(upload_tw<T>(c));
   // shared-memory opt-in for the largest launch of this plan
-  const size_t cs = sizeof(C);
-  size_t need = 0;
-  auto fs = [&](int n, int ld) { return cs * (n + 2 * (size_t)n * ld); };
-  need = std::max(need, fs(pl.k3, pl.P1 | 1));
-  need = std::max(need, fs(pl.k2, pl.P1));
-  need = std::max(need, fs(pl.k1, pl.xlines<T>() | 1));
-  need = std::max(need, fs(pl.k1, pl.rholines | 1) + sizeof(double) * pl.rholines * pl.k1);
-  need = std::max(need, fs(pl.k3, 17));
-  need = std::max(need, fs(pl.k2, 17));
+  const size_t need = fft_smem_need<T>(pl);
   if (need > 227 * 1024) {
     set_error("FFT tile needs %zu bytes of shared memory (> 227 KB)", need);
     return QX_ERR_ARG;
@@ -195,7 +238,14 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
     delete c;
     return QX_ERR_ARG;
   }
+  if (init_fft_roots()) {
+    set_error("qx_create: cannot write FFT roots to the device: %s", cudaGetErrorString(cudaGetLastError()));
+    delete c;
+    return QX_ERR_CUDA;
+  }
   pl.tw_off[0] = 0; pl.tw_off[1] = k1; pl.tw_off[2] = k1 + k2;
+  pl.stw_off[0] = 0; pl.stw_off[1] = pl.L[0].nst; pl.stw_off[2] = pl.L[0].nst + pl.L[1].nst;
+  pl.sob_off[0] = 0; pl.sob_off[1] = pl.L[0].nob; pl.sob_off[2] = pl.L[0].nob + pl.L[1].nob;
   // sphere geometry from ijkgd
   std::vector<int> n1(nplw + 1), n2(nplw + 1), i3v(nplw + 1);
   int m1 = 0, m2 = 0, m3 = 0;
@@ -261,6 +311,15 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
     qx_destroy(c);
     return QX_ERR_CUDA;
   }
+  {
+    std::vector<int> sob;
+    for (int d = 0; d < 3; ++d) stage_bases(pl.L[d], sob);
+    FAIL(dalloc(c, &pl.d_sob, sizeof(int) * std::max<size_t>(sob.size(), 1)));
+    if (!sob.empty() && cudaMemcpy(pl.d_sob, sob.data(), sizeof(int) * sob.size(), cudaMemcpyHostToDevice)) {
+      qx_destroy(c);
+      return QX_ERR_CUDA;
+    }
+  }
   // small FP64 arrays
   const int nb = nband, ne = c->ne;
   FAIL(dalloc(c, &c->d_dk, sizeof(double) * ne));
@@ -274,6 +333,7 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   FAIL(dalloc(c, &c->d_hsub, sizeof(double) * nb * nb));
   FAIL(dalloc(c, &c->d_mat, sizeof(double) * nb * nb));
   FAIL(dalloc(c, &c->d_V, sizeof(double) * 2 * nb * nb));
+  FAIL(dalloc(c, &c->d_eigws, sizeof(double) * (8 * (size_t)nb * nb + 16 * nb)));
   FAIL(dalloc(c, &c->d_info, sizeof(int) * 4));
   std::vector<int> pairs(2 * c->npair_all);
   for (int p = 0; p < c->npair_all; ++p) {
@@ -292,6 +352,8 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   FAIL(dalloc(c, &c->snap, blk));
   FAIL(dalloc(c, &c->tmp, blk));
   FAIL(dalloc(c, &c->mat_t, ts * nb * nb));
+  c->gws_bytes = sizeof(double) * (size_t)64 * 1024 * 1024 / 8;   // 64 MB
+  FAIL(dalloc(c, &c->gws, c->gws_bytes));
   cudaMemset(c->psi, 0, blk);
   cudaMemset(c->hpsi, 0, blk);
   // CG state
@@ -465,7 +527,7 @@ __global__ void k_wocc(const double *occ, double *w, int n, double rv) {
 extern "C" int qx_set_occ(qx_ctx *c, const double *occ, double rvol) {
   if (!c || !occ || rvol <= 0) { set_error("qx_set_occ: bad arguments"); return QX_ERR_ARG; }
   CK(cudaMemcpyAsync(c->d_occ, occ, sizeof(double) * c->nb, cudaMemcpyHostToDevice, c->st));
-  k_wocc<<<(c->nb + 127) / 128, 128, 0, c->st>>>(c->d_occ, c->d_wocc, c->nb, rvol);
+  k_wocc<<<(c->nb + 127) / 128, 128, 0, c->st>>>(c->d_occ, c->d_wocc, c->nb, rvol); note_launch();
   CKL();
   c->rvol = rvol;
   c->have_occ = true;
@@ -570,7 +632,7 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
     T *proj = (T *)c->proj;
     const int np = pl.nproj;
     TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, colmap,
-                ncol_dev, c->st));
+                ncol_dev, c->st, c->gws, c->gws_bytes));
     scale_rows<T>(np, ncol_max, proj, np, b.vclalp, colmap, ncol_dev, c->st);
     TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, colmap,
                 ncol_dev, c->st));
@@ -638,7 +700,7 @@ static int hmatrix_impl(qx_ctx *c, double *hsub) {
   T *m = (T *)c->mat_t;
   // m(j, i) = <psi_j | hpsi_i>
   TRY(gemm<T>(true, false, nb, nb, c->ne, (T)1, (const T *)c->psi, c->ne, (const T *)c->hpsi, c->ne, (T)0, m, nb, 1,
-              nullptr, nullptr, c->st));
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
   symmetrize_lower<T>(m, c->d_hsub, c->d_eig, nb, c->st);
   CKL();
   c->have_hsub = true;
@@ -689,7 +751,7 @@ static int untryt_impl(qx_ctx *c, double *ev, int *sweeps) {
   if (!c->have_hsub) { set_error("untryt: call hmatrix first"); return QX_ERR_STATE; }
   const int nb = c->nb;
   CK(cudaMemcpyAsync(c->d_mat, c->d_hsub, sizeof(double) * nb * nb, cudaMemcpyDeviceToDevice, c->st));
-  TRY(jacobi(c->d_mat, nb, c->d_w, c->d_V, 60, c->d_info, c->st));
+  TRY(syev(c->d_mat, nb, c->d_w, c->d_V, c->d_eigws, c->d_info, c->st));
   CKL();
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -698,7 +760,7 @@ static int untryt_impl(qx_ctx *c, double *ev, int *sweeps) {
   CKL();
   TRY(rotate<T>(c, c->psi));
   CK(cudaStreamSynchronize(c->st));
-  if (info < 0) { set_error("untryt: Jacobi did not converge in 60 sweeps"); return QX_ERR_EIG; }
+  if (info <= 0) { set_error("untryt: eigen-decomposition produced no eigenvectors"); return QX_ERR_EIG; }
   if (sweeps) *sweeps = info;
   c->have_u = true;
   c->have_hsub = false;
@@ -736,7 +798,7 @@ static int eigen_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out
   for (int it = 0; it < maxit; ++it) {
     cg_prec<T>(nb, ne, ne, g, h, c->d_dk, s, c->st);
     // subgs3: Pm = snap^T h ; Pm masked to j < i, active i ; h -= snap * Pm
-    TRY(gemm<T>(true, false, nb, nb, ne, (T)1, snap, ne, h, ne, (T)0, pm_t, nb, 1, nullptr, nullptr, c->st));
+    TRY(gemm<T>(true, false, nb, nb, ne, (T)1, snap, ne, h, ne, (T)0, pm_t, nb, 1, nullptr, nullptr, c->st, c->gws, c->gws_bytes));
     cg_mask<T>(nb, pm_t, s, c->st);
     TRY(gemm<T>(false, false, ne, nb, nb, (T)-1, snap, ne, pm_t, nb, (T)1, h, ne, 0, nullptr, nullptr, c->st));
     cg_orth<T>(nb, ne, ne, x, hx, h, s, c->st);
@@ -768,7 +830,7 @@ static int schmidt_impl(qx_ctx *c) {
   const int nb = c->nb, ne = c->ne;
   T *m = (T *)c->mat_t;
   TRY(gemm<T>(true, false, nb, nb, ne, (T)1, (const T *)c->psi, ne, (const T *)c->psi, ne, (T)0, m, nb, 1, nullptr,
-              nullptr, c->st));
+              nullptr, c->st, c->gws, c->gws_bytes));
   convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
   TRY(cholinv(c->d_mat, nb, c->d_info, c->st));
   CKL();
@@ -902,7 +964,7 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
     out->etot = sc[4] - sc[0] + sc[1] - sc[2] + c->eion;
     out->zmax = zmax;
     out->ncg_hpsi = nh;
-    out->jacobi_sweeps = sweeps;
+    out->eig_clusters = sweeps;
   }
   return QX_OK;
 }
@@ -927,7 +989,7 @@ static int kbg_only(qx_ctx *c, const T *cin, T *out, int nb) {
   Bufs<T> &b = pl.bufs<T>();
   const int np = pl.nproj;
   T *proj = (T *)c->proj;
-  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st));
+  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st, c->gws, c->gws_bytes));
   scale_rows<T>(np, nb, proj, np, b.vclalp, nullptr, nullptr, c->st);
   TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st));
   CKL();
@@ -1017,14 +1079,14 @@ extern "C" int qxgpu_rfft3(qx_ctx *c, int key, double *fft3x, double *fft3y) {
   CK(cudaMallocAsync((void **)&y, sizeof(double) * n, c->st));
   CK(cudaMemcpyAsync(x, fft3x, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   if (key == 1) {
-    k_join<<<148 * 4, 256, 0, c->st>>>(x, nullptr, z, n);
+    k_join<<<148 * 4, 256, 0, c->st>>>(x, nullptr, z, n); note_launch();
     TRY(launch_full_fft<double>(c->pl, z, -1, 1.0 / (double)n, c->st));
   } else {
     CK(cudaMemcpyAsync(y, fft3y, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-    k_join<<<148 * 4, 256, 0, c->st>>>(x, y, z, n);
+    k_join<<<148 * 4, 256, 0, c->st>>>(x, y, z, n); note_launch();
     TRY(launch_full_fft<double>(c->pl, z, +1, 1.0, c->st));
   }
-  k_split<<<148 * 4, 256, 0, c->st>>>(z, x, key == 1 ? y : nullptr, n);
+  k_split<<<148 * 4, 256, 0, c->st>>>(z, x, key == 1 ? y : nullptr, n); note_launch();
   CKL();
   CK(cudaMemcpyAsync(fft3x, x, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
   if (key == 1) CK(cudaMemcpyAsync(fft3y, y, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));

@@ -269,34 +269,34 @@ __global__ void k_scale_rows(int nproj, int ncol, T *__restrict__ P, long ldp, c
 
 // ---- launchers -------------------------------------------------------------
 template <typename T> void cg_init(int nb, int ne, long ldx, const T *x, const T *hx, T *g, const CgState &s, cudaStream_t st) {
-  k_cg_init<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, s);
+  k_cg_init<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, s); note_launch();
 }
 template <typename T> void cg_prec(int nb, int ne, long ldx, T *g, T *h, const double *dk, const CgState &s, cudaStream_t st) {
-  k_cg_prec<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, g, h, dk, s);
+  k_cg_prec<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, g, h, dk, s); note_launch();
 }
 template <typename T> void cg_mask(int nb, T *Pm, const CgState &s, cudaStream_t st) {
   const long nn = (long)nb * nb;
-  k_cg_mask<T><<<(int)((nn + 255) / 256), 256, 0, st>>>(nb, Pm, s);
+  k_cg_mask<T><<<(int)((nn + 255) / 256), 256, 0, st>>>(nb, Pm, s); note_launch();
 }
 template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T *hx, T *h, const CgState &s, cudaStream_t st) {
-  k_cg_orth<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, h, s);
+  k_cg_orth<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, h, s); note_launch();
 }
-void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); }
+void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); note_launch(); }
 template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
                                      const CgState &s, const CgParm &pm, cudaStream_t st) {
-  k_cg_update<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm);
+  k_cg_update<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm); note_launch();
 }
 template <typename T> void ekin(int nb, int ne, long ldx, const T *x, const double *dk, double *ekib, cudaStream_t st) {
-  k_ekin<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, dk, ekib);
+  k_ekin<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, dk, ekib); note_launch();
 }
 template <typename T> void gradres(int nb, int ne, long ldx, const T *x, const T *hx, const double *eig, double *prod,
                                    cudaStream_t st) {
-  k_gradres<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, eig, prod);
+  k_gradres<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, eig, prod); note_launch();
 }
 template <typename T> void scale_rows(int nproj, int ncol, T *P, long ldp, const T *v, const int *colmap,
                                       const int *ncol_dev, cudaStream_t st) {
   const long n = (long)nproj * ncol;
-  k_scale_rows<T><<<(int)((n + 255) / 256), 256, 0, st>>>(nproj, ncol, P, ldp, v, colmap, ncol_dev);
+  k_scale_rows<T><<<(int)((n + 255) / 256), 256, 0, st>>>(nproj, ncol, P, ldp, v, colmap, ncol_dev); note_launch();
 }
 
 #define QX_INST(T)                                                                                          \

@@ -17,22 +17,224 @@
 // Real-space KB (calnlc, nlkbppr.f90:1773-1900) splits xvx into xinv_r,
 // nlproj and xfwd_r.  Density (softchg, chgdns.f90:388-454) uses zinv, y<+1>
 // and xrho.
+#include <algorithm>
+#include <cmath>
+
 #include "qx_internal.h"
+
+// --------------------------------------------------------------------------
+// Small DFTs in registers.  Roots of unity w_R^m = exp(-2 pi i m / R) for
+// R = 2..9 live in constant memory (row R, column m), written once per
+// device by init_fft_roots().  SIGN = -1 forward, +1 backward (conjugate roots).
+__constant__ float2 c_root32[10 * 16];
+__constant__ double2 c_root64[10 * 16];
+
+template <typename T> __device__ __forceinline__ typename c2t<T>::type root(int R, int m);
+template <> __device__ __forceinline__ float2 root<float>(int R, int m) { return c_root32[R * 16 + m]; }
+template <> __device__ __forceinline__ double2 root<double>(int R, int m) { return c_root64[R * 16 + m]; }
+
+template <typename T, int SIGN>
+__device__ __forceinline__ typename c2t<T>::type rootS(int R, int m) {
+  typename c2t<T>::type w = root<T>(R, m);
+  if (SIGN > 0) w.y = -w.y;
+  return w;
+}
+
+// multiply by SIGN * i
+template <int SIGN, typename C> __device__ __forceinline__ C mul_si(C d) {
+  C r;
+  if (SIGN < 0) { r.x = d.y; r.y = -d.x; } else { r.x = -d.y; r.y = d.x; }
+  return r;
+}
+
+template <typename T, int SIGN, int R>
+struct Dft;
+
+template <typename T, int SIGN> struct Dft<T, SIGN, 1> {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) { o[0] = v[0]; }
+};
+template <typename T, int SIGN> struct Dft<T, SIGN, 2> {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) {
+    const C a = v[0], b = v[sv];
+    o[0] = cadd(a, b);
+    o[so] = csub(a, b);
+  }
+};
+template <typename T, int SIGN> struct Dft<T, SIGN, 3> {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) {
+    const T hs = (T)0.86602540378443864676;   // sqrt(3)/2
+    const C v0 = v[0], t1 = cadd(v[sv], v[2 * sv]), d = csub(v[sv], v[2 * sv]);
+    C t2;
+    t2.x = v0.x - (T)0.5 * t1.x;
+    t2.y = v0.y - (T)0.5 * t1.y;
+    C hd; hd.x = hs * d.x; hd.y = hs * d.y;
+    const C jd = mul_si<SIGN>(hd);
+    o[0] = cadd(v0, t1);
+    o[so] = cadd(t2, jd);
+    o[2 * so] = csub(t2, jd);
+  }
+};
+template <typename T, int SIGN> struct Dft<T, SIGN, 4> {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) {
+    const C s0 = cadd(v[0], v[2 * sv]), d0 = csub(v[0], v[2 * sv]);
+    const C s1 = cadd(v[sv], v[3 * sv]), d1 = csub(v[sv], v[3 * sv]);
+    const C jd1 = mul_si<SIGN>(d1);
+    o[0] = cadd(s0, s1);
+    o[2 * so] = csub(s0, s1);
+    o[so] = cadd(d0, jd1);
+    o[3 * so] = csub(d0, jd1);
+  }
+};
+// Direct DFT for the prime radices 5 and 7.
+template <typename T, int SIGN, int R> struct DftDirect {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) {
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = v[r * sv];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      C acc = x[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) acc = cadd(acc, cmul(x[r], rootS<T, SIGN>(R, (r * q) % R)));
+      o[q * so] = acc;
+    }
+  }
+};
+template <typename T, int SIGN> struct Dft<T, SIGN, 5> : DftDirect<T, SIGN, 5> {};
+template <typename T, int SIGN> struct Dft<T, SIGN, 7> : DftDirect<T, SIGN, 7> {};
+// Two-factor radices R = P*Q: input r = a + P*c, output k = k1 + Q*k2:
+// X[k1 + Q k2] = sum_a w_R^{a k1} w_P^{a k2} sum_c v[a + P c] w_Q^{c k1}.
+template <typename T, int SIGN, int P, int Q> struct DftPQ {
+  typedef typename c2t<T>::type C;
+  static __device__ __forceinline__ void run(const C *v, int sv, C *o, int so) {
+    C t[P * Q];
+#pragma unroll
+    for (int a = 0; a < P; ++a) Dft<T, SIGN, Q>::run(v + a * sv, P * sv, t + a * Q, 1);
+#pragma unroll
+    for (int a = 1; a < P; ++a)
+#pragma unroll
+      for (int k1 = 1; k1 < Q; ++k1) t[a * Q + k1] = cmul(t[a * Q + k1], rootS<T, SIGN>(P * Q, a * k1));
+#pragma unroll
+    for (int k1 = 0; k1 < Q; ++k1) Dft<T, SIGN, P>::run(t + k1, Q, o + k1 * so, Q * so);
+  }
+};
+template <typename T, int SIGN> struct Dft<T, SIGN, 6> : DftPQ<T, SIGN, 2, 3> {};
+template <typename T, int SIGN> struct Dft<T, SIGN, 8> : DftPQ<T, SIGN, 2, 4> {};
+template <typename T, int SIGN> struct Dft<T, SIGN, 9> : DftPQ<T, SIGN, 3, 3> {};
+
+// One Stockham stage of radix R over `nl` lines (element-major layout).
+template <typename T, int SIGN, int R>
+__device__ __forceinline__ void fft_stage(const typename c2t<T>::type *a, typename c2t<T>::type *b, int nr, int ns,
+                                          int ld, int l, int j0, int jstep, const typename c2t<T>::type *st,
+                                          const int *ob) {
+  typedef typename c2t<T>::type C;
+  for (int j = j0; j < nr; j += jstep) {
+    C v[R], o[R];
+    v[0] = a[j * ld + l];
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      C t = st[j * (R - 1) + r - 1];
+      if (SIGN > 0) t.y = -t.y;
+      v[r] = cmul(a[(j + r * nr) * ld + l], t);
+    }
+    Dft<T, SIGN, R>::run(v, 1, o, 1);
+    const int base = ob[j];
+#pragma unroll
+    for (int q = 0; q < R; ++q) b[(base + q * ns) * ld + l] = o[q];
+  }
+}
+
+// Batched in-shared-memory Stockham FFT (decimation in time, natural order
+// in and out).  `nl` lines of length L.n, element-major: element e of line l
+// at buf[e * ld + l].  Ping-pongs between buf and tmp; returns the buffer
+// holding the result.  SIGN = -1 forward, +1 backward (unscaled).  stw/sob:
+// the stage tables in shared memory.  Thread t works on line t % nl (needs
+// nl <= blockDim.x).  Called by all threads; ends with a __syncthreads.
+template <typename T, int SIGN>
+__device__ typename c2t<T>::type *smem_fft(typename c2t<T>::type *buf, typename c2t<T>::type *tmp, int nl, int ld,
+                                           const FftLen &L, const typename c2t<T>::type *tw,
+                                           const typename c2t<T>::type *stw, const int *sob) {
+  typedef typename c2t<T>::type C;
+  (void)tw;
+  const int n = L.n;
+  const int l = threadIdx.x % nl;
+  const int j0 = threadIdx.x / nl;
+  const int jstep = blockDim.x / nl;
+  const bool act = threadIdx.x < jstep * nl;
+  int ns = 1;
+  C *a = buf, *b = tmp;
+  for (int s = 0; s < L.nstage; ++s) {
+    const int R = L.radix[s];
+    const int nr = n / R;
+    const C *st = stw + L.st_off[s];
+    const int *ob = sob + L.ob_off[s];
+    if (act) {
+      switch (R) {
+        case 2: fft_stage<T, SIGN, 2>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 3: fft_stage<T, SIGN, 3>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 4: fft_stage<T, SIGN, 4>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 5: fft_stage<T, SIGN, 5>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 6: fft_stage<T, SIGN, 6>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 7: fft_stage<T, SIGN, 7>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        case 8: fft_stage<T, SIGN, 8>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+        default: fft_stage<T, SIGN, 9>(a, b, nr, ns, ld, l, j0, jstep, st, ob); break;
+      }
+    }
+    __syncthreads();
+    C *t = a; a = b; b = t;
+    ns *= R;
+  }
+  return a;
+}
 
 __device__ __forceinline__ int pair_count(const PipeParams &P) {
   return P.npair_dev ? *P.npair_dev : P.npair;
 }
 
+// Device copies of one length's FFT tables (see FftLen).
 template <typename T>
-__device__ __forceinline__ void load_tw(typename c2t<T>::type *dst, const typename c2t<T>::type *src, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+struct FftTabs {
+  const typename c2t<T>::type *tw, *stw;
+  const int *sob;
+};
+
+// Shared-memory layout of a kernel: [tw | stw | sob | pad] then the tiles.
+template <typename T>
+struct SmTabs {
+  typename c2t<T>::type *tw, *stw;
+  int *sob;
+  typename c2t<T>::type *tiles;
+};
+
+__host__ __device__ __forceinline__ size_t tab_bytes(const FftLen &L, size_t cs) {
+  size_t b = (size_t)(L.n + L.nst) * cs + (size_t)L.nob * 4;
+  return (b + 15) & ~(size_t)15;
+}
+
+template <typename T>
+__device__ __forceinline__ SmTabs<T> load_tabs(unsigned char *sm, const FftLen &L, const FftTabs<T> &g) {
+  typedef typename c2t<T>::type C;
+  SmTabs<T> t;
+  t.tw = reinterpret_cast<C *>(sm);
+  t.stw = t.tw + L.n;
+  t.sob = reinterpret_cast<int *>(t.stw + L.nst);
+  t.tiles = reinterpret_cast<C *>(sm + tab_bytes(L, sizeof(C)));
+  for (int i = threadIdx.x; i < L.n; i += blockDim.x) t.tw[i] = g.tw[i];
+  for (int i = threadIdx.x; i < L.nst; i += blockDim.x) t.stw[i] = g.stw[i];
+  for (int i = threadIdx.x; i < L.nob; i += blockDim.x) t.sob[i] = g.sob[i];
+  return t;
 }
 
 // --------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(QX_THREADS) k_zinv(PipeParams P, const T *__restrict__ cin, long ldc,
                                                       typename c2t<T>::type *__restrict__ bufA,
-                                                      const typename c2t<T>::type *__restrict__ tw3) {
+                                                      FftTabs<T> gt3) {
   typedef typename c2t<T>::type C;
   const int j2 = blockIdx.x;
   const int pl = blockIdx.y, p = P.pair0 + pl;
@@ -41,10 +243,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_zinv(PipeParams P, const T *__re
   if (lo > hi) return;
   const int W = hi - lo + 1, ld = W | 1, k3 = P.k3;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k3;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L3, gt3);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k3 * ld;
-  load_tw<T>(tw, tw3, k3);
   const C zero = mk2<T>(0, 0);
   for (int i = threadIdx.x; i < k3 * ld; i += blockDim.x) t0[i] = zero;
   __syncthreads();
@@ -62,7 +263,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_zinv(PipeParams P, const T *__re
     t0[en.y * ld + en.x] = z;
   }
   __syncthreads();
-  C *res = smem_fft<T, +1>(t0, t1, W, ld, P.L3, tw);
+  C *res = smem_fft<T, +1>(t0, t1, W, ld, P.L3, tb.tw, tb.stw, tb.sob);
   C *dst = bufA + ((long)pl * k3) * P.P2 * P.P1 + (long)j2 * P.P1 + lo;
   for (int i = threadIdx.x; i < k3 * W; i += blockDim.x) {
     const int i3 = i / W, l = i - i3 * W;
@@ -75,17 +276,16 @@ __global__ void __launch_bounds__(QX_THREADS) k_zinv(PipeParams P, const T *__re
 template <typename T, int SIGN>
 __global__ void __launch_bounds__(QX_THREADS) k_ypass(PipeParams P, typename c2t<T>::type *__restrict__ bufA,
                                                        typename c2t<T>::type *__restrict__ bufB,
-                                                       const typename c2t<T>::type *__restrict__ tw2) {
+                                                       FftTabs<T> gt2) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x;
   const int pl = blockIdx.y, p = P.pair0 + pl;
   if (p >= pair_count(P)) return;
   const int k2 = P.k2, P1 = P.P1, P2 = P.P2, ld = P1;   // P1 is odd
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k2;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L2, gt2);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k2 * ld;
-  load_tw<T>(tw, tw2, k2);
   C *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
   C *B = bufB + ((long)pl * P.k3 + i3) * k2 * P1;
   if (SIGN > 0) {
@@ -100,12 +300,12 @@ __global__ void __launch_bounds__(QX_THREADS) k_ypass(PipeParams P, typename c2t
       }
     }
     __syncthreads();
-    C *res = smem_fft<T, +1>(t0, t1, P1, ld, P.L2, tw);
+    C *res = smem_fft<T, +1>(t0, t1, P1, ld, P.L2, tb.tw, tb.stw, tb.sob);
     for (int i = threadIdx.x; i < k2 * P1; i += blockDim.x) B[i] = res[i];
   } else {
     for (int i = threadIdx.x; i < k2 * P1; i += blockDim.x) t0[i] = B[i];
     __syncthreads();
-    C *res = smem_fft<T, -1>(t0, t1, P1, ld, P.L2, tw);
+    C *res = smem_fft<T, -1>(t0, t1, P1, ld, P.L2, tb.tw, tb.stw, tb.sob);
     for (int i = threadIdx.x; i < P2 * P1; i += blockDim.x) {
       const int j2 = i / P1, a = i - j2 * P1;
       if (a >= P.row_lo[j2] && a <= P.row_hi[j2]) {
@@ -127,7 +327,7 @@ __device__ __forceinline__ int a_to_i1(int a, int m1, int k1) {
 template <typename T>
 __global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T>::type *__restrict__ bufB,
                                                      const T *__restrict__ vloc, int nlines, int nchunk,
-                                                     const typename c2t<T>::type *__restrict__ tw1) {
+                                                     FftTabs<T> gt1) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
   const int pl = blockIdx.y, p = P.pair0 + pl;
@@ -137,10 +337,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T
   const int nl = min(nlines, k2 - i20);
   const int ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k1;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L1, gt1);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k1 * ld;
-  load_tw<T>(tw, tw1, k1);
   const C zero = mk2<T>(0, 0);
   for (int i = threadIdx.x; i < k1 * ld; i += blockDim.x) t0[i] = zero;
   __syncthreads();
@@ -150,7 +349,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T
     t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
   }
   __syncthreads();
-  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tb.tw, tb.stw, tb.sob);
   C *o = (r == t0) ? t1 : t0;
   const T *V = vloc + ((long)i3 * k2 + i20) * k1;
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
@@ -161,7 +360,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T
     r[i1 * ld + l] = z;
   }
   __syncthreads();
-  C *res = smem_fft<T, -1>(r, o, nl, ld, P.L1, tw);
+  C *res = smem_fft<T, -1>(r, o, nl, ld, P.L1, tb.tw, tb.stw, tb.sob);
   for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
     const int l = i / P1, a = i - l * P1;
     B[i] = res[a_to_i1(a, P.m1, k1) * ld + l];
@@ -172,7 +371,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xvx(PipeParams P, typename c2t<T
 template <typename T>
 __global__ void __launch_bounds__(QX_THREADS) k_zfwd(PipeParams P, const typename c2t<T>::type *__restrict__ bufA,
                                                       typename c2t<T>::type *__restrict__ zsph,
-                                                      const typename c2t<T>::type *__restrict__ tw3) {
+                                                      FftTabs<T> gt3) {
   typedef typename c2t<T>::type C;
   const int j2 = blockIdx.x;
   const int pl = blockIdx.y, p = P.pair0 + pl;
@@ -181,17 +380,16 @@ __global__ void __launch_bounds__(QX_THREADS) k_zfwd(PipeParams P, const typenam
   if (lo > hi) return;
   const int W = hi - lo + 1, ld = W | 1, k3 = P.k3;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k3;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L3, gt3);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k3 * ld;
-  load_tw<T>(tw, tw3, k3);
   const C *src = bufA + ((long)pl * k3) * P.P2 * P.P1 + (long)j2 * P.P1 + lo;
   for (int i = threadIdx.x; i < k3 * W; i += blockDim.x) {
     const int i3 = i / W, l = i - i3 * W;
     t0[i3 * ld + l] = src[(long)i3 * P.P2 * P.P1 + l];
   }
   __syncthreads();
-  C *res = smem_fft<T, -1>(t0, t1, W, ld, P.L3, tw);
+  C *res = smem_fft<T, -1>(t0, t1, W, ld, P.L3, tb.tw, tb.stw, tb.sob);
   const T s = (T)P.inv_n;
   C *Z = zsph + (long)pl * (P.nplw + 1) * 2;
   for (int e = P.row_off[j2] + threadIdx.x; e < P.row_off[j2 + 1]; e += blockDim.x) {
@@ -246,7 +444,7 @@ __global__ void k_unpack(PipeParams P, const typename c2t<T>::type *__restrict__
 template <typename T>
 __global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typename c2t<T>::type *__restrict__ bufB,
                                                         typename c2t<T>::type *__restrict__ R, int nlines,
-                                                        int nchunk, const typename c2t<T>::type *__restrict__ tw1) {
+                                                        int nchunk, FftTabs<T> gt1) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
   const int pl = blockIdx.y, p = P.pair0 + pl;
@@ -254,10 +452,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typen
   const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
   const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k1;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L1, gt1);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k1 * ld;
-  load_tw<T>(tw, tw1, k1);
   const C zero = mk2<T>(0, 0);
   for (int i = threadIdx.x; i < k1 * ld; i += blockDim.x) t0[i] = zero;
   __syncthreads();
@@ -267,7 +464,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typen
     t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
   }
   __syncthreads();
-  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+  C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tb.tw, tb.stw, tb.sob);
   C *dst = R + (((long)pl * P.k3 + i3) * k2 + i20) * k1;
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
     const int l = i / k1, i1 = i - l * k1;
@@ -323,7 +520,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typen
                                                         const int4 *__restrict__ lent, const T *__restrict__ vnl,
                                                         const typename c2t<T>::type *__restrict__ sumr, int natom,
                                                         int nlines, int nchunk,
-                                                        const typename c2t<T>::type *__restrict__ tw1) {
+                                                        FftTabs<T> gt1) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
   const int pl = blockIdx.y, p = P.pair0 + pl;
@@ -331,10 +528,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typen
   const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
   const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k1;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L1, gt1);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k1 * ld;
-  load_tw<T>(tw, tw1, k1);
   const C *src = R + (((long)pl * P.k3 + i3) * k2 + i20) * k1;
   const T *V = vloc + ((long)i3 * k2 + i20) * k1;
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
@@ -360,7 +556,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typen
     }
   }
   __syncthreads();
-  C *res = smem_fft<T, -1>(t0, t1, nl, ld, P.L1, tw);
+  C *res = smem_fft<T, -1>(t0, t1, nl, ld, P.L1, tb.tw, tb.stw, tb.sob);
   C *B = bufB + (((long)pl * P.k3 + i3) * k2 + i20) * P1;
   for (int i = threadIdx.x; i < nl * P1; i += blockDim.x) {
     const int l = i / P1, a = i - l * P1;
@@ -376,17 +572,16 @@ template <typename T>
 __global__ void __launch_bounds__(QX_THREADS) k_xrho(PipeParams P, const typename c2t<T>::type *__restrict__ bufB,
                                                       const double *__restrict__ wocc, double *__restrict__ rho,
                                                       int nlines, int nchunk, int accumulate,
-                                                      const typename c2t<T>::type *__restrict__ tw1) {
+                                                      FftTabs<T> gt1) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
   const int k1 = P.k1, k2 = P.k2, P1 = P.P1;
   const int i20 = ch * nlines, nl = min(nlines, k2 - i20), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k1;
+  SmTabs<T> tb = load_tabs<T>(smraw, P.L1, gt1);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k1 * ld;
   double *acc = reinterpret_cast<double *>(t1 + k1 * ld);
-  load_tw<T>(tw, tw1, k1);
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) acc[i] = 0.0;
   const int np = min(pair_count(P) - P.pair0, P.npair);
   const C zero = mk2<T>(0, 0);
@@ -400,7 +595,7 @@ __global__ void __launch_bounds__(QX_THREADS) k_xrho(PipeParams P, const typenam
       t0[a_to_i1(a, P.m1, k1) * ld + l] = B[i];
     }
     __syncthreads();
-    C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tw);
+    C *r = smem_fft<T, +1>(t0, t1, nl, ld, P.L1, tb.tw, tb.stw, tb.sob);
     const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
     const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
     for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
@@ -418,22 +613,21 @@ __global__ void __launch_bounds__(QX_THREADS) k_xrho(PipeParams P, const typenam
 // Full-grid complex 3D FFT passes (density side, rfft3/fft3 drop-in).
 template <typename T, int SIGN>
 __global__ void __launch_bounds__(QX_THREADS) k_full_z(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
-                                                        int tx, FftLen L3, const typename c2t<T>::type *__restrict__ tw3) {
+                                                        int tx, FftLen L3, FftTabs<T> gt3) {
   typedef typename c2t<T>::type C;
   const int nxc = (k1 + tx - 1) / tx;
   const int i2 = blockIdx.x / nxc, i10 = (blockIdx.x - i2 * nxc) * tx;
   const int nl = min(tx, k1 - i10), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k3;
+  SmTabs<T> tb = load_tabs<T>(smraw, L3, gt3);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k3 * ld;
-  load_tw<T>(tw, tw3, k3);
   for (int i = threadIdx.x; i < k3 * nl; i += blockDim.x) {
     const int i3 = i / nl, l = i - i3 * nl;
     t0[i3 * ld + l] = g[((long)i3 * k2 + i2) * k1 + i10 + l];
   }
   __syncthreads();
-  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L3, tw);
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L3, tb.tw, tb.stw, tb.sob);
   for (int i = threadIdx.x; i < k3 * nl; i += blockDim.x) {
     const int i3 = i / nl, l = i - i3 * nl;
     g[((long)i3 * k2 + i2) * k1 + i10 + l] = r[i3 * ld + l];
@@ -442,23 +636,22 @@ __global__ void __launch_bounds__(QX_THREADS) k_full_z(typename c2t<T>::type *__
 
 template <typename T, int SIGN>
 __global__ void __launch_bounds__(QX_THREADS) k_full_y(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
-                                                        int tx, FftLen L2, const typename c2t<T>::type *__restrict__ tw2) {
+                                                        int tx, FftLen L2, FftTabs<T> gt2) {
   typedef typename c2t<T>::type C;
   const int nxc = (k1 + tx - 1) / tx;
   const int i3 = blockIdx.x / nxc, i10 = (blockIdx.x - i3 * nxc) * tx;
   const int nl = min(tx, k1 - i10), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k2;
+  SmTabs<T> tb = load_tabs<T>(smraw, L2, gt2);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k2 * ld;
-  load_tw<T>(tw, tw2, k2);
   C *base = g + (long)i3 * k2 * k1 + i10;
   for (int i = threadIdx.x; i < k2 * nl; i += blockDim.x) {
     const int i2 = i / nl, l = i - i2 * nl;
     t0[i2 * ld + l] = base[(long)i2 * k1 + l];
   }
   __syncthreads();
-  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L2, tw);
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L2, tb.tw, tb.stw, tb.sob);
   for (int i = threadIdx.x; i < k2 * nl; i += blockDim.x) {
     const int i2 = i / nl, l = i - i2 * nl;
     base[(long)i2 * k1 + l] = r[i2 * ld + l];
@@ -467,24 +660,23 @@ __global__ void __launch_bounds__(QX_THREADS) k_full_y(typename c2t<T>::type *__
 
 template <typename T, int SIGN>
 __global__ void __launch_bounds__(QX_THREADS) k_full_x(typename c2t<T>::type *__restrict__ g, int k1, int k2, int k3,
-                                                        int nlines, FftLen L1, const typename c2t<T>::type *__restrict__ tw1,
+                                                        int nlines, FftLen L1, FftTabs<T> gt1,
                                                         double scale) {
   typedef typename c2t<T>::type C;
   const int nch = (k2 + nlines - 1) / nlines;
   const int i3 = blockIdx.x / nch, i20 = (blockIdx.x - i3 * nch) * nlines;
   const int nl = min(nlines, k2 - i20), ld = nl | 1;
   extern __shared__ unsigned char smraw[];
-  C *tw = reinterpret_cast<C *>(smraw);
-  C *t0 = tw + k1;
+  SmTabs<T> tb = load_tabs<T>(smraw, L1, gt1);
+  C *t0 = tb.tiles;
   C *t1 = t0 + k1 * ld;
-  load_tw<T>(tw, tw1, k1);
   C *base = g + ((long)i3 * k2 + i20) * k1;
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
     const int l = i / k1, i1 = i - l * k1;
     t0[i1 * ld + l] = base[i];
   }
   __syncthreads();
-  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L1, tw);
+  C *r = smem_fft<T, SIGN>(t0, t1, nl, ld, L1, tb.tw, tb.stw, tb.sob);
   const T s = (T)scale;
   for (int i = threadIdx.x; i < nl * k1; i += blockDim.x) {
     const int l = i / k1, i1 = i - l * k1;
@@ -499,7 +691,17 @@ __global__ void __launch_bounds__(QX_THREADS) k_full_x(typename c2t<T>::type *__
 
 namespace qx {
 
-static size_t fft_smem(int n, int ld, size_t csz) { return (size_t)csz * (n + 2 * (size_t)n * ld); }
+static size_t fft_smem(const FftLen &L, int ld, size_t cs) { return tab_bytes(L, cs) + 2 * (size_t)L.n * ld * cs; }
+
+template <typename T>
+static FftTabs<T> tabs(const Plan &pl, int d) {
+  Bufs<T> &bf = pl.bufs<T>();
+  FftTabs<T> t;
+  t.tw = bf.tw + pl.tw_off[d];
+  t.stw = bf.stw + pl.stw_off[d];
+  t.sob = pl.d_sob + pl.sob_off[d];
+  return t;
+}
 
 template <typename T>
 int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
@@ -507,31 +709,31 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   typedef typename c2t<T>::type C;
   const size_t cs = sizeof(C);
   Bufs<T> &bf = pl.bufs<T>();
-  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
-  size_t smz = fft_smem(P.k3, (P.P1 | 1), cs);
-  k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, tw3);
+  const size_t smz = fft_smem(P.L3, P.P1 | 1, cs);
+  k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
   dim3 gy(P.k3, npl);
-  size_t smy = fft_smem(P.k2, P.P1, cs);
-  k_ypass<T, +1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, tw2);
+  const size_t smy = fft_smem(P.L2, P.P1, cs);
+  k_ypass<T, +1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
   const int nlines = pl.xlines<T>();
   const int nch = (P.k2 + nlines - 1) / nlines;
   dim3 gx(P.k3 * nch, npl);
-  size_t smx = fft_smem(P.k1, nlines | 1, cs);
+  const size_t smx = fft_smem(P.L1, nlines | 1, cs);
   if (nlmode == 2) {
-    k_xinv_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.bufR, nlines, nch, tw1);
+    k_xinv_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.bufR, nlines, nch, g1); note_launch();
     dim3 ga(pl.natom, npl);
     k_nlproj<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, pl.d_kb_clalp,
-                                           pl.rdelv, pl.natom, bf.sumr);
+                                           pl.rdelv, pl.natom, bf.sumr); note_launch();
     k_xfwd_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufR, bf.bufB, bf.vloc, pl.d_line_off, pl.d_line_ent,
-                                             bf.kb_vnl, bf.sumr, pl.natom, nlines, nch, tw1);
+                                             bf.kb_vnl, bf.sumr, pl.natom, nlines, nch, g1); note_launch();
   } else {
-    k_xvx<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.vloc, nlines, nch, tw1);
+    k_xvx<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.vloc, nlines, nch, g1); note_launch();
   }
-  k_ypass<T, -1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, tw2);
-  k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, tw3);
+  k_ypass<T, -1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
+  k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
   dim3 gu((P.nplw + 1 + 127) / 128, npl);
-  k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate);
+  k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
   return 0;
 }
 
@@ -541,15 +743,15 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
   typedef typename c2t<T>::type C;
   const size_t cs = sizeof(C);
   Bufs<T> &bf = pl.bufs<T>();
-  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
-  k_zinv<T><<<gz, QX_THREADS, fft_smem(P.k3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, tw3);
+  k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
   dim3 gy(P.k3, npl);
-  k_ypass<T, +1><<<gy, QX_THREADS, fft_smem(P.k2, P.P1, cs), st>>>(P, bf.bufA, bf.bufB, tw2);
+  k_ypass<T, +1><<<gy, QX_THREADS, fft_smem(P.L2, P.P1, cs), st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
   const int nlines = pl.rholines;
   const int nch = (P.k2 + nlines - 1) / nlines;
-  size_t sm = fft_smem(P.k1, nlines | 1, cs) + sizeof(double) * nlines * P.k1;
-  k_xrho<T><<<P.k3 * nch, QX_THREADS, sm, st>>>(P, bf.bufB, wocc, rho, nlines, nch, accumulate, tw1);
+  const size_t sm = fft_smem(P.L1, nlines | 1, cs) + sizeof(double) * nlines * P.k1;
+  k_xrho<T><<<P.k3 * nch, QX_THREADS, sm, st>>>(P, bf.bufB, wocc, rho, nlines, nch, accumulate, g1); note_launch();
   return 0;
 }
 
@@ -557,24 +759,56 @@ template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st) {
   typedef typename c2t<T>::type C;
   const size_t cs = sizeof(C);
-  Bufs<T> &bf = pl.bufs<T>();
-  const C *tw1 = bf.tw + pl.tw_off[0], *tw2 = bf.tw + pl.tw_off[1], *tw3 = bf.tw + pl.tw_off[2];
+  const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   const int k1 = pl.k1, k2 = pl.k2, k3 = pl.k3;
   const int tx = 16;
   const int nxc = (k1 + tx - 1) / tx;
   const int nlines = pl.xlines<T>();
   const int nch = (k2 + nlines - 1) / nlines;
+  const FftLen &L1 = pl.L[0], &L2 = pl.L[1], &L3 = pl.L[2];
   if (sign > 0) {
-    k_full_z<T, +1><<<k2 * nxc, QX_THREADS, fft_smem(k3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[2], tw3);
-    k_full_y<T, +1><<<k3 * nxc, QX_THREADS, fft_smem(k2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[1], tw2);
-    k_full_x<T, +1><<<k3 * nch, QX_THREADS, fft_smem(k1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, pl.L[0], tw1, scale);
+    k_full_z<T, +1><<<k2 * nxc, QX_THREADS, fft_smem(L3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L3, g3); note_launch();
+    k_full_y<T, +1><<<k3 * nxc, QX_THREADS, fft_smem(L2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L2, g2); note_launch();
+    k_full_x<T, +1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch();
   } else {
-    k_full_z<T, -1><<<k2 * nxc, QX_THREADS, fft_smem(k3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[2], tw3);
-    k_full_y<T, -1><<<k3 * nxc, QX_THREADS, fft_smem(k2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, pl.L[1], tw2);
-    k_full_x<T, -1><<<k3 * nch, QX_THREADS, fft_smem(k1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, pl.L[0], tw1, scale);
+    k_full_z<T, -1><<<k2 * nxc, QX_THREADS, fft_smem(L3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L3, g3); note_launch();
+    k_full_y<T, -1><<<k3 * nxc, QX_THREADS, fft_smem(L2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L2, g2); note_launch();
+    k_full_x<T, -1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch();
   }
   return 0;
 }
+
+// Roots of unity of the register DFTs, on the current device.
+int init_fft_roots() {
+  float2 h32[10 * 16];
+  double2 h64[10 * 16];
+  const double tp = 2.0 * 3.14159265358979323846;
+  for (int R = 0; R < 10; ++R)
+    for (int m = 0; m < 16; ++m) {
+      const double ang = (R > 0 && m < R) ? tp * m / R : 0.0;
+      h64[R * 16 + m] = make_double2(std::cos(ang), -std::sin(ang));
+      h32[R * 16 + m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+    }
+  if (cudaMemcpyToSymbol(c_root32, h32, sizeof(h32)) != cudaSuccess) return 1;
+  if (cudaMemcpyToSymbol(c_root64, h64, sizeof(h64)) != cudaSuccess) return 1;
+  return 0;
+}
+
+// Largest dynamic shared memory any pipeline launch of this plan needs.
+template <typename T>
+size_t fft_smem_need(const Plan &pl) {
+  const size_t cs = sizeof(typename c2t<T>::type);
+  size_t need = 0;
+  need = std::max(need, fft_smem(pl.L[2], pl.P1 | 1, cs));
+  need = std::max(need, fft_smem(pl.L[1], pl.P1, cs));
+  need = std::max(need, fft_smem(pl.L[0], pl.xlines<T>() | 1, cs));
+  need = std::max(need, fft_smem(pl.L[0], pl.rholines | 1, cs) + sizeof(double) * pl.rholines * pl.k1);
+  need = std::max(need, fft_smem(pl.L[2], 17, cs));
+  need = std::max(need, fft_smem(pl.L[1], 17, cs));
+  return need;
+}
+template size_t fft_smem_need<float>(const Plan &);
+template size_t fft_smem_need<double>(const Plan &);
 
 // Opt every kernel above into the shared-memory size the largest plan needs.
 template <typename T>

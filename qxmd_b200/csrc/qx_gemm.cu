@@ -4,16 +4,21 @@
 // (engrad.f90:1122-1142), C*U (eigen.f90:1482-1510) and C*L^-T
 // (schmidt.f90:284-313).  The Gamma-point half-sphere metric
 // 2*sum - x(1)*y(1) is applied in the epilogue.
+#include <algorithm>
+
 #include "qx_internal.h"
 
 namespace qx {
 
 constexpr int BM = 64, BN = 64, BK = 16;
 
-template <typename T, bool TA, bool TB>
+// SPLIT: block z sums k in [z*kchunk, (z+1)*kchunk) and stores its raw
+// partial tile to W[z][n][m] (n = logical column); k_gemm_reduce finishes.
+template <typename T, bool TA, bool TB, bool SPLIT>
 __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, const T *__restrict__ A, long lda,
                                               const T *__restrict__ B, long ldb, T beta, T *__restrict__ Cm, long ldc,
-                                              int gamma, const int *__restrict__ colmap, const int *__restrict__ ncol_dev) {
+                                              int gamma, const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
+                                              int kchunk, T *__restrict__ W) {
   __shared__ T As[BK][BM + 1];
   __shared__ T Bs[BK][BN + 1];
   const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
@@ -25,7 +30,9 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0;
-  for (int k0 = 0; k0 < K; k0 += BK) {
+  const int kb = SPLIT ? blockIdx.z * kchunk : 0;
+  const int ke = SPLIT ? min(K, kb + kchunk) : K;
+  for (int k0 = kb; k0 < ke; k0 += BK) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const int e = tid + 256 * r;
@@ -33,7 +40,7 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
       if (TA) { k = e & 15; m = e >> 4; } else { m = e & 63; k = e >> 6; }
       const int gm = m0 + m, gk = k0 + k;
       T v = 0;
-      if (gm < M && gk < K) v = TA ? A[(long)gm * lda + gk] : A[(long)gk * lda + gm];
+      if (gm < M && gk < ke) v = TA ? A[(long)gm * lda + gk] : A[(long)gk * lda + gm];
       As[k][m] = v;
     }
 #pragma unroll
@@ -43,7 +50,7 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
       if (!TB) { k = e & 15; n = e >> 4; } else { n = e & 63; k = e >> 6; }
       const int gn = n0 + n, gk = k0 + k;
       T v = 0;
-      if (gn < Nact && gk < K) {
+      if (gn < Nact && gk < ke) {
         const long cn = colmap ? colmap[gn] : gn;
         v = TB ? B[(long)gk * ldb + cn] : B[cn * ldb + gk];
       }
@@ -72,6 +79,10 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
     for (int j = 0; j < 4; ++j) {
       const int gn = n0 + tx + 16 * j;
       if (gn >= Nact) continue;
+      if (SPLIT) {
+        W[((long)blockIdx.z * N + gn) * M + gm] = acc[i][j];
+        continue;
+      }
       const long cn = colmap ? colmap[gn] : gn;
       T v = acc[i][j];
       if (gamma) {
@@ -90,21 +101,87 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
   }
 }
 
+// Sum the split-K partials in a fixed order, apply the Gamma-metric
+// epilogue and alpha/beta, scatter through colmap.
+template <typename T, bool TA, bool TB>
+__global__ void k_gemm_reduce(int M, int N, int nsplit, T alpha, const T *__restrict__ A, long lda,
+                              const T *__restrict__ B, long ldb, T beta, T *__restrict__ Cm, long ldc, int gamma,
+                              const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
+                              const T *__restrict__ W) {
+  const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)M * Nact) return;
+  const int gn = (int)(e / M), gm = (int)(e - (long)gn * M);
+  T v = 0;
+  for (int z = 0; z < nsplit; ++z) v += W[((long)z * N + gn) * M + gm];
+  const long cn = colmap ? colmap[gn] : gn;
+  if (gamma) {
+    const T a0 = TA ? A[(long)gm * lda] : A[gm];
+    const T b0 = TB ? B[cn] : B[cn * ldb];
+    v = (T)2 * v - a0 * b0;
+    if (gamma == 2) {
+      const T a1 = TA ? A[(long)gm * lda + 1] : A[lda + gm];
+      const T b1 = TB ? B[ldb + cn] : B[cn * ldb + 1];
+      v -= (T)2 * a1 * b1;
+    }
+  }
+  T *c = Cm + cn * ldc + gm;
+  *c = (beta == (T)0) ? alpha * v : alpha * v + beta * *c;
+}
+
+template <typename T, bool TA, bool TB>
+static void launch(dim3 g, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
+                   long ldc, int gamma, const int *colmap, const int *ncol_dev, int nsplit, int kchunk, T *W,
+                   cudaStream_t st) {
+  if (nsplit <= 1) {
+    k_gemm<T, TA, TB, false><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap,
+                                               ncol_dev, 0, nullptr);
+    note_launch();
+    return;
+  }
+  g.z = nsplit;
+  k_gemm<T, TA, TB, true><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev,
+                                            kchunk, W);
+  note_launch();
+  const long mn = (long)M * N;
+  k_gemm_reduce<T, TA, TB><<<(int)((mn + 255) / 256), 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                     gamma, colmap, ncol_dev, W);
+  note_launch();
+}
+
+// Split K when the output has too few tiles to fill the GPU and the caller
+// provides a workspace of at least nsplit*M*N elements.
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
-         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st) {
+         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes) {
   if (M <= 0 || N <= 0) return 0;
   dim3 g((M + BM - 1) / BM, (N + BN - 1) / BN);
-  if (ta && tb) k_gemm<T, true, true><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
-  else if (ta) k_gemm<T, true, false><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
-  else if (tb) k_gemm<T, false, true><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
-  else k_gemm<T, false, false><<<g, 256, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev);
+  const long tiles = (long)g.x * g.y;
+  int nsplit = 1, kchunk = K;
+  if (ws && tiles < 2 * 148 && K >= 4 * 256) {
+    nsplit = (int)std::min<long>((2 * 148 + tiles - 1) / tiles, (K + 255) / 256);
+    kchunk = ((K + nsplit - 1) / nsplit + BK - 1) / BK * BK;
+    nsplit = (K + kchunk - 1) / kchunk;
+    if ((size_t)nsplit * M * N * sizeof(T) > ws_bytes) {
+      nsplit = (int)(ws_bytes / ((size_t)M * N * sizeof(T)));
+      if (nsplit < 2) nsplit = 1;
+      else {
+        kchunk = ((K + nsplit - 1) / nsplit + BK - 1) / BK * BK;
+        nsplit = (K + kchunk - 1) / kchunk;
+      }
+    }
+  }
+  T *W = (T *)ws;
+  if (ta && tb) launch<T, true, true>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
+  else if (ta) launch<T, true, false>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
+  else if (tb) launch<T, false, true>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
+  else launch<T, false, false>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
   return 0;
 }
 
 template int gemm<float>(bool, bool, int, int, int, float, const float *, long, const float *, long, float, float *,
-                         long, int, const int *, const int *, cudaStream_t);
+                         long, int, const int *, const int *, cudaStream_t, void *, size_t);
 template int gemm<double>(bool, bool, int, int, int, double, const double *, long, const double *, long, double,
-                          double *, long, int, const int *, const int *, cudaStream_t);
+                          double *, long, int, const int *, const int *, cudaStream_t, void *, size_t);
 
 }  // namespace qx

@@ -26,12 +26,15 @@ struct PipeParams {
 namespace qx {
 
 void set_error(const char *fmt, ...);
+// Count of kernels launched by this library (qx_launch_count()).
+void note_launch();
 
 // Per-precision device buffers of the FFT pipeline.
 template <typename T>
 struct Bufs {
   typedef typename c2t<T>::type C;
-  C *tw = nullptr;         // twiddles of all three lengths
+  C *tw = nullptr;         // base twiddles of the three lengths
+  C *stw = nullptr;        // stage twiddles of the three lengths
   C *bufA = nullptr;       // [chunk][k3][P2][P1]
   C *bufB = nullptr;       // [chunk][k3][k2][P1]
   C *bufR = nullptr;       // [chunk][k3][k2][k1] (real-space KB mode)
@@ -49,10 +52,11 @@ struct Plan {
   int m1 = 0, m2 = 0, m3 = 0, P1 = 0, P2 = 0;
   int nplw = 0, nplwex = 0;
   FftLen L[3];
-  int tw_off[3];
+  int tw_off[3], stw_off[3], sob_off[3];
+  int *d_sob = nullptr;    // stage output bases of the three lengths
   int chunk = 0;           // pairs per pipeline launch
   int rholines = 8;
-  int xl32 = 16, xl64 = 8; // lines per CTA of the x pass
+  int xl32 = 32, xl64 = 16; // lines per CTA of the x pass
   // sphere rows
   int *d_row_lo = nullptr, *d_row_hi = nullptr, *d_row_off = nullptr;
   int4 *d_row_ent = nullptr;
@@ -86,6 +90,8 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
 template <typename T> void set_fft_smem_limits(size_t bytes);
+template <typename T> size_t fft_smem_need(const Plan &pl);
+int init_fft_roots();
 
 // qx_gemm.cu: C(m,n) = alpha * op(A)(m,:) . op(B)(:,n) + beta * C(m,n), column-major.
 // TA: A stored K x M (A[m*lda + k]); TB: B stored N x K (B[k*ldb + n]).
@@ -93,13 +99,16 @@ template <typename T> void set_fft_smem_limits(size_t bytes);
 // metric 2*sum - a0*b0 - 2*a1*b1.  colmap (device, optional) maps output
 // column n to stored column colmap[n] of B and C; ncol_dev (device,
 // optional) bounds the number of columns.
+// ws/ws_bytes: optional split-K workspace (null: no split).
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
-         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st);
+         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws = nullptr,
+         size_t ws_bytes = 0);
 
 // qx_dense.cu (FP64, nb x nb)
 int cholinv(double *S, int n, int *d_info, cudaStream_t st);
-int jacobi(double *A, int n, double *w, double *V, int maxsweep, int *d_info, cudaStream_t st);
+// Symmetric eigen-decomposition; work >= 8*n*n + 16*n doubles.
+int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st);
 template <typename Tin, typename Tout>
 void convert(const Tin *in, Tout *out, long n, cudaStream_t st);
 template <typename T>

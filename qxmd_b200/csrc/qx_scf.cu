@@ -154,27 +154,27 @@ __global__ void k_band_energy(const double *__restrict__ w, const double *__rest
 // ---- launchers -------------------------------------------------------------
 void grid_g2(int k1, int k2, int k3, const double *cross, double ecutdens, double *g2, cudaStream_t st) {
   k_grid_g2<<<148 * 4, 256, 0, st>>>(k1, k2, k3, cross[0], cross[3], cross[6], cross[1], cross[4], cross[7],
-                                    cross[2], cross[5], cross[8], ecutdens, g2);
+                                    cross[2], cross[5], cross[8], ecutdens, g2); note_launch();
 }
 
 void real_to_cplx(const double *r, const double *r2, double2 *z, long n, cudaStream_t st) {
-  k_real_to_cplx<<<148 * 4, 256, 0, st>>>(r, r2, z, n);
+  k_real_to_cplx<<<148 * 4, 256, 0, st>>>(r, r2, z, n); note_launch();
 }
 
 void hartree_g(double2 *z, const double *g2, long n, double half_vol, double *part, double *out, cudaStream_t st) {
-  k_hartree<<<SCF_NBLK, RB, 0, st>>>(z, g2, n, half_vol, part);
-  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 1, 1, out);
+  k_hartree<<<SCF_NBLK, RB, 0, st>>>(z, g2, n, half_vol, part); note_launch();
+  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 1, 1, out); note_launch();
 }
 
 void kerker(double2 *z, const double *g2, long n, double q02, cudaStream_t st) {
-  k_kerker<<<148 * 4, 256, 0, st>>>(z, g2, n, q02);
+  k_kerker<<<148 * 4, 256, 0, st>>>(z, g2, n, q02); note_launch();
 }
 
 template <typename T>
 void xc_glocal(const double *rho, const double *vloc, const double2 *vh, long n, double rdelv, double *glocal,
                T *glocal_t, double *part, double *out2, cudaStream_t st) {
-  k_xc_glocal<T><<<SCF_NBLK, RB, 0, st>>>(rho, vloc, vh, n, rdelv, glocal, glocal_t, part);
-  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 2, 2, out2);
+  k_xc_glocal<T><<<SCF_NBLK, RB, 0, st>>>(rho, vloc, vh, n, rdelv, glocal, glocal_t, part); note_launch();
+  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 2, 2, out2); note_launch();
 }
 template void xc_glocal<float>(const double *, const double *, const double2 *, long, double, double *, float *,
                                double *, double *, cudaStream_t);
@@ -183,12 +183,12 @@ template void xc_glocal<double>(const double *, const double *, const double2 *,
 
 void mix(double *rho_in, const double *rho_out, const double2 *dfilt, long n, double beta, double rdelv, double *part,
          double *out, cudaStream_t st) {
-  k_mix<<<SCF_NBLK, RB, 0, st>>>(rho_in, rho_out, dfilt, n, beta, rdelv, part);
-  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 1, 1, out);
+  k_mix<<<SCF_NBLK, RB, 0, st>>>(rho_in, rho_out, dfilt, n, beta, rdelv, part); note_launch();
+  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 1, 1, out); note_launch();
 }
 
 void band_energy(const double *w, const double *occ, int nb, double *out, cudaStream_t st) {
-  k_band_energy<<<1, 32, 0, st>>>(w, occ, nb, out);
+  k_band_energy<<<1, 32, 0, st>>>(w, occ, nb, out); note_launch();
 }
 
 }  // namespace qx

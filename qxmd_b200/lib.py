@@ -23,7 +23,7 @@ QX_ERR = {1: "ARG", 2: "CUDA", 3: "NOTPD", 4: "EIG", 5: "STATE"}
 
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [
-    "qx_last_error", "qx_version", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
+    "qx_last_error", "qx_version", "qx_launch_count", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
@@ -56,7 +56,7 @@ class CgParm(C.Structure):
 class ScfOut(C.Structure):
     _fields_ = [("etot", C.c_double), ("eband", C.c_double), ("ehartree", C.c_double),
                 ("exc", C.c_double), ("evxc", C.c_double), ("resid", C.c_double),
-                ("zmax", C.c_double), ("ncg_hpsi", C.c_int), ("jacobi_sweeps", C.c_int)]
+                ("zmax", C.c_double), ("ncg_hpsi", C.c_int), ("eig_clusters", C.c_int)]
 
     def asdict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -82,6 +82,7 @@ def lib(build_if_missing: bool = True):
     sig = {
         "qx_last_error": ([], C.c_char_p),
         "qx_version": ([], C.c_int),
+        "qx_launch_count": ([], C.c_long),
         "qx_create": ([C.POINTER(_ctx), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip, _dp, C.c_int, _vp], C.c_int),
         "qx_destroy": ([_ctx], C.c_int),
         "qx_set_glocal": ([_ctx, _dp], C.c_int),
@@ -128,6 +129,10 @@ def lib(build_if_missing: bool = True):
         f.restype = res
     _lib = L
     return L
+
+
+def launch_count() -> int:
+    return int(lib().qx_launch_count())
 
 
 def last_error() -> str:
