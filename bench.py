@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-step", action="store_true",
+                    help="only the mixed-precision SCF iterations (warm-up, then --steps), no L2 flush, "
+                         "no extra arms: the launch sequence profiled under ncu")
     return ap.parse_args()
 
 
@@ -149,6 +152,36 @@ def cpu_sample(sys_, nb_apps, nthreads=1):
     ham.hpsi(c)
     rate = nb_apps / (time.perf_counter() - t)
     return rate
+
+
+def run_profile_step(args):
+    """W + K mixed-precision SCF iterations of the workload and nothing else,
+    printing the library's launch counts so that an ncu capture can skip the
+    set-up and warm-up launches (-s) and take exactly the timed ones (-c)."""
+    import torch
+
+    from qxmd_b200 import cell
+    from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_MIXED, launch_count
+    torch.cuda.set_device(0)
+    sys_ = cell.si64()
+    ctx = Context(sys_, QX_PREC_MIXED, QX_NL_GSPACE)
+    ctx.put_psi(cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband))
+    ctx.schmidt()
+    ctx.scf_init()
+    ctx.scf_rho_from_psi()
+    parm = CgParm.defaults(int(sys_.cell.nel // 2))
+    for _ in range(args.warmup):
+        ctx.scf_iteration(parm)
+    ctx.sync()
+    n0 = launch_count()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        out = ctx.scf_iteration(parm)
+    ctx.sync()
+    dt = time.perf_counter() - t
+    print(json.dumps({"profile_step": True, "launches_before": n0, "launches_per_step": (launch_count() - n0) / max(1, args.steps),
+                      "wall_ms_per_step": 1e3 * dt / max(1, args.steps), "etot": out["etot"]}), flush=True)
+    ctx.close()
 
 
 def run_ours(args):
@@ -339,6 +372,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.profile_step:
+        run_profile_step(args)
     else:
         run_ours(args)
 
