@@ -123,6 +123,27 @@ int qx_ekinetic(qx_ctx *ctx, double *ekin, double *ekib);
 int qx_enonloc(qx_ctx *ctx);
 /* hmatrix2 (engrad.f90:845-956): H_sub = <psi|H|psi>, eig = diag. */
 int qx_hmatrix(qx_ctx *ctx, double *hsub);
+/* Allocation-free band matrix.  No counterpart in the reference: an extra
+ * entry point for host programs that cannot call cudaMalloc once their run
+ * has started -- codes that carve all device memory out of one pool sized at
+ * start-up, or run where a further allocation could fail or stall the time
+ * step.  It computes what qx_hmatrix computes before symmetrising, on device
+ * arrays the caller owns and without a context:
+ *   hsub(j, i) = 2 sum_g c(g, j) hc(g, i) - c(1, j) hc(1, i)
+ * for all j, i < nb (FP64, column-major nb x nb, leading dimension nb; c and
+ * hc column-major nplwex x nb), as a split-K GEMM whose partial sums live in
+ * a 16 MiB file-scope device array (QX_HMATRIX_STATIC_SCRATCH_BYTES) that
+ * every GPU loading this library holds until exit.  Returns QX_ERR_ARG for
+ * nb > QX_HMATRIX_STATIC_MAX_NB (two nb x nb partials must fit).  The first
+ * call on each device looks up that array's device address (with the device
+ * current) and should come before any stream capture.  All calls share the
+ * one array and it keeps the last call's partials; each call writes every
+ * partial it reads, so nothing needs clearing, but calls that overlap on the
+ * GPU (other streams, other host threads) race on it.  Enqueued on `stream`
+ * (cudaStream_t or 0); the result is ready when that stream is. */
+#define QX_HMATRIX_STATIC_SCRATCH_BYTES 16777216
+#define QX_HMATRIX_STATIC_MAX_NB 1024
+int qx_hmatrix_static(const double *c, const double *hc, int nplwex, int nb, double *hsub, void *stream);
 /* gradresnv (engrad.f90:1013-1067). */
 int qx_gradres(qx_ctx *ctx, double *prod, double *zmax, double *zsum);
 /* untryt2 (eigen.f90:1171-1331): diagonalise the last H_sub, psi <- psi U;

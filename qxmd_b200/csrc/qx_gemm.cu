@@ -185,3 +185,88 @@ template int gemm<double>(bool, bool, int, int, int, double, const double *, lon
                           double *, long, int, const int *, const int *, cudaStream_t, void *, size_t);
 
 }  // namespace qx
+
+// ---------------------------------------------------------------------------
+// Allocation-free band matrix: the split-K GEMM above with its partial sums in
+// a fixed, file-scope device array instead of a caller- or context-owned
+// workspace.  For host programs that must not allocate device memory after
+// start-up (a memory pool sized once and locked, or a host code that owns all
+// device memory itself and forbids cudaMalloc in its time-step loop).
+#include <mutex>
+
+#include "../../include/qxmd_b200.h"
+
+// Split-K partials of qx_hmatrix_static: nsplit * nb * nb doubles.  Every
+// device that loads this library holds these 16 MiB until the process exits.
+static __device__ __align__(256) double g_hmat_scratch[QX_HMATRIX_STATIC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_hmat_scratch on the current device.  In host code the
+// symbol only names a host-side shadow; the address the kernels need comes
+// from cudaGetSymbolAddress, taken once per device with that device current.
+int scratch_address(double **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    qx::set_error("qx_hmatrix_static: cudaGetDevice: %s", cudaGetErrorString(e));
+    return QX_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    qx::set_error("qx_hmatrix_static: device ordinal %d beyond %d", dev, kMaxDevices);
+    return QX_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_hmat_scratch);
+    if (e != cudaSuccess || !p) {
+      qx::set_error("qx_hmatrix_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return QX_ERR_CUDA;
+    }
+    g_scratch_ptr[dev] = (double *)p;
+  }
+  *out = g_scratch_ptr[dev];
+  return QX_OK;
+}
+}  // namespace
+
+extern "C" int qx_hmatrix_static(const double *c, const double *hc, int nplwex, int nb, double *hsub, void *stream) {
+  if (!c || !hc || !hsub || nplwex <= 0 || nb <= 0) {
+    qx::set_error("qx_hmatrix_static: bad arguments");
+    return QX_ERR_ARG;
+  }
+  if (nb > QX_HMATRIX_STATIC_MAX_NB) {
+    qx::set_error("qx_hmatrix_static: nb = %d exceeds %d, the most whose two K-partials fit the %d-byte scratch",
+                  nb, QX_HMATRIX_STATIC_MAX_NB, QX_HMATRIX_STATIC_SCRATCH_BYTES);
+    return QX_ERR_ARG;
+  }
+  double *W = nullptr;
+  int rc = scratch_address(&W);
+  if (rc) return rc;
+  // Split K into at least two partials (so the scratch is always the
+  // reduction path), enough of them to give about two CTAs per SM, each at
+  // least 128 deep, as many as the scratch holds.
+  const int tiles_m = (nb + qx::BM - 1) / qx::BM;
+  const long tiles = (long)tiles_m * tiles_m;
+  const long cap = (long)(QX_HMATRIX_STATIC_SCRATCH_BYTES / (sizeof(double) * (size_t)nb * nb));
+  long want = std::max<long>(2, (2 * 148 + tiles - 1) / tiles);
+  want = std::min<long>(want, std::max<long>(2, (nplwex + 127) / 128));
+  want = std::min<long>(want, cap);
+  int kchunk = (int)(((nplwex + want - 1) / want + qx::BK - 1) / qx::BK * qx::BK);
+  const int nsplit = (nplwex + kchunk - 1) / kchunk;   // <= want: every partial fits
+  // Every partial W[z][n][m], m, n < nb, z < nsplit, is written by its CTA
+  // before k_gemm_reduce reads it, so nothing needs clearing between calls.
+  dim3 g(tiles_m, tiles_m);
+  qx::launch<double, true, false>(g, nb, nb, nplwex, 1.0, c, nplwex, hc, nplwex, 0.0, hsub, nb, 1, nullptr, nullptr,
+                                  nsplit, kchunk, W, (cudaStream_t)stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    qx::set_error("qx_hmatrix_static: launch: %s", cudaGetErrorString(e));
+    return QX_ERR_CUDA;
+  }
+  return QX_OK;
+}

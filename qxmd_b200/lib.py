@@ -27,7 +27,7 @@ EXPORTS = [
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
-    "qx_untryhc", "qx_eigen", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_rho_from_psi",
+    "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_rho_from_psi",
     "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
 ]
@@ -104,6 +104,7 @@ def lib(build_if_missing: bool = True):
         "qx_ekinetic": ([_ctx, _vp, _vp], C.c_int),
         "qx_enonloc": ([_ctx], C.c_int),
         "qx_hmatrix": ([_ctx, _vp], C.c_int),
+        "qx_hmatrix_static": ([_vp, _vp, C.c_int, C.c_int, _vp, _vp], C.c_int),
         "qx_gradres": ([_ctx, _vp, _vp, _vp], C.c_int),
         "qx_untryt": ([_ctx, _vp], C.c_int),
         "qx_untryhc": ([_ctx], C.c_int),
