@@ -48,13 +48,17 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
     if ptxas_v:
         flags += ["-Xptxas", "-v"]
+    procs = []
     for src in sources():
         obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + ".o")
         cmd = [nv] + flags + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.check_call(cmd)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    for cmd, pr in procs:
+        if pr.wait() != 0:
+            raise subprocess.CalledProcessError(pr.returncode, cmd)
     tmp = LIB + ".tmp"
     cmd = [nv] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static"]
     subprocess.check_call(cmd)

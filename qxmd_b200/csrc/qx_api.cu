@@ -67,7 +67,7 @@ struct qx_ctx {
   double *d_dk = nullptr, *d_occ = nullptr, *d_wocc = nullptr, *d_eig = nullptr, *d_ekib = nullptr, *d_w = nullptr;
   double *d_hsub = nullptr, *d_mat = nullptr, *d_V = nullptr;   // nb*nb, nb*nb, 2*nb*nb
   double *d_prod = nullptr;
-  double *d_eigws = nullptr;   // eigensolver work, 8*nb*nb + 16*nb
+  double *d_eigws = nullptr;   // eigensolver work, 8*nb*nb + 1024*nb
   int *d_info = nullptr;
   int *d_allpairs = nullptr;
   // state arrays in the context precision
@@ -333,7 +333,7 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   FAIL(dalloc(c, &c->d_hsub, sizeof(double) * nb * nb));
   FAIL(dalloc(c, &c->d_mat, sizeof(double) * nb * nb));
   FAIL(dalloc(c, &c->d_V, sizeof(double) * 2 * nb * nb));
-  FAIL(dalloc(c, &c->d_eigws, sizeof(double) * (8 * (size_t)nb * nb + 16 * nb)));
+  FAIL(dalloc(c, &c->d_eigws, sizeof(double) * (8 * (size_t)nb * nb + 1024 * (size_t)nb)));
   FAIL(dalloc(c, &c->d_info, sizeof(int) * 4));
   std::vector<int> pairs(2 * c->npair_all);
   for (int p = 0; p < c->npair_all; ++p) {
@@ -586,6 +586,8 @@ extern "C" int qx_sync(qx_ctx *c) {
   if (!c) return QX_ERR_ARG;
   CK(cudaStreamSynchronize(c->st));
   CKL();
+  const int te = tc_error_take();
+  if (te) { set_error("qx_sync: tensor-core GEMM wait timed out (code %d)", te); return QX_ERR_CUDA; }
   return QX_OK;
 }
 
@@ -631,6 +633,13 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
     Bufs<T> &b = pl.bufs<T>();
     T *proj = (T *)c->proj;
     const int np = pl.nproj;
+    // The tensor-core GEMMs take whole columns: with a band list they work on
+    // all ncol_max columns, which leaves the columns of bands not in the list
+    // holding unused values (the CG reads only active bands).
+    if (sizeof(T) == sizeof(float) && tc_enabled()) {
+      colmap = nullptr;
+      ncol_dev = nullptr;
+    }
     TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, colmap,
                 ncol_dev, c->st, c->gws, c->gws_bytes));
     scale_rows<T>(np, ncol_max, proj, np, b.vclalp, colmap, ncol_dev, c->st);
@@ -832,7 +841,7 @@ static int schmidt_impl(qx_ctx *c) {
   TRY(gemm<T>(true, false, nb, nb, ne, (T)1, (const T *)c->psi, ne, (const T *)c->psi, ne, (T)0, m, nb, 1, nullptr,
               nullptr, c->st, c->gws, c->gws_bytes));
   convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
-  TRY(cholinv(c->d_mat, nb, c->d_info, c->st));
+  TRY(cholinv(c->d_mat, nb, c->d_eigws, c->d_info, c->st));
   CKL();
   int info = 0;
   CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));

@@ -149,12 +149,36 @@ static void launch(dim3 g, int M, int N, int K, T alpha, const T *A, long lda, c
   note_launch();
 }
 
-// Split K when the output has too few tiles to fill the GPU and the caller
-// provides a workspace of at least nsplit*M*N elements.
+// Finish FP32 split-K partials W[z][n][m] (any producer with that layout).
+void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
+                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st) {
+  const long mn = (long)M * N;
+  const int g = (int)((mn + 255) / 256);
+  if (ta && tb) k_gemm_reduce<float, true, true><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else if (ta) k_gemm_reduce<float, true, false><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else if (tb) k_gemm_reduce<float, false, true><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else k_gemm_reduce<float, false, false><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  note_launch();
+}
+
+// FP32 without a column map goes to the tensor-core kernel (qx_tcgemm.cu)
+// when the operands meet its TMA rules; everything else, and all FP64 work,
+// runs on the CUDA-core kernel above.  Split K when the output has too few
+// tiles to fill the GPU and the caller provides a workspace of at least
+// nsplit*M*N elements.
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes) {
   if (M <= 0 || N <= 0) return 0;
+  if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0) {
+    const int r = tc_gemm(ta, tb, M, N, K, (float)alpha, (const float *)A, lda, (const float *)B, ldb, (float)beta,
+                          (float *)C, ldc, gamma, st, ws, ws_bytes);
+    if (r == 0) return 0;
+    if (r > 0) {
+      set_error("tensor-core GEMM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+      return 2;
+    }
+  }
   dim3 g((M + BM - 1) / BM, (N + BN - 1) / BN);
   const long tiles = (long)g.x * g.y;
   int nsplit = 1, kchunk = K;

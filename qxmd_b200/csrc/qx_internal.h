@@ -105,9 +105,22 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws = nullptr,
          size_t ws_bytes = 0);
 
+void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
+                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st);
+
+// qx_tcgemm.cu: tcgen05 3xTF32 GEMM with gemm<float>'s semantics (no column
+// map).  Returns 0 launched, -1 operands unsuitable (use the CUDA-core
+// kernel), > 0 launch error.
+int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
+            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes);
+bool tc_enabled();
+// Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
+int tc_error_take();
+
 // qx_dense.cu (FP64, nb x nb)
-int cholinv(double *S, int n, int *d_info, cudaStream_t st);
-// Symmetric eigen-decomposition; work >= 8*n*n + 16*n doubles.
+// work: >= 32*33 doubles, used when S does not fit shared memory.
+int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st);
+// Symmetric eigen-decomposition; work >= 8*n*n + 1024*n doubles.
 int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st);
 template <typename Tin, typename Tout>
 void convert(const Tin *in, Tout *out, long n, cudaStream_t st);

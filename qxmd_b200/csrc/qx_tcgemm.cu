@@ -1,0 +1,413 @@
+// Tensor-core GEMM for the FP32 band and projector contractions of the mixed
+// precision path: <beta|psi> and its back-application (hckbpp_ib_g,
+// nlkbpp.f90:1678-1713), S = C^T C (schmidt.f90:190-237), H_sub = C^T HC
+// (engrad.f90:869-895), subgs3 (engrad.f90:1122-1142), C*U
+// (eigen.f90:1482-1510) and C*L^-T (schmidt.f90:284-313).
+//
+// sm_100a only: operands staged by TMA (128-byte swizzle) into a 3-stage
+// shared-memory ring, products on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, 128 x 160 tile, accumulator in TMEM), read back
+// with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
+// is cut into x_hi = x with the low 13 mantissa bits cleared and
+// x_lo = x - x_hi (exact in FP32), and the tile product is
+// A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 (relative error about
+// 2^-21 per product).  The split is done in shared memory by the epilogue
+// warps between the TMA landing and the MMA issue, so HBM traffic is that of
+// a plain FP32 GEMM.
+//
+// Warp roles (192 threads): warp 0 issues TMA, warp 1 allocates TMEM and
+// issues the MMAs (one elected lane), warps 2-5 split the operands and run
+// the epilogue (TMEM lane quadrant = warp % 4).  Every mbarrier wait is
+// bounded by a 2 s clock; on timeout the kernel records an error code, stops
+// issuing, drains its own copies and MMAs and frees TMEM.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <mutex>
+
+#include "qx_internal.h"
+
+namespace qx {
+namespace tc {
+
+constexpr int BM = 128, BN = 160, BK = 32, STAGES = 3;
+constexpr int TMEM_COLS = 256;
+constexpr int A_BYTES = BM * BK * 4;                 // 16 KB
+constexpr int B_BYTES = BN * BK * 4;                 // 20 KB
+constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
+constexpr int STAGE_BYTES = 2 * (A_BYTES + B_BYTES); // 72 KB, a multiple of 1 KB
+constexpr int NTHREADS = 192;
+constexpr int BAR_BYTES = 128;
+constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + BAR_BYTES + 1024;   // + alignment slack
+constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+__device__ int g_tc_error = 0;
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of parity `parity` to complete, for at most WAIT_NS.
+__device__ __noinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int code) {
+  if (mbar_try(b, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  while (true) {
+    if (mbar_try(b, parity)) return true;
+    if (now_ns() - t0 > WAIT_NS) {
+      atomicCAS(&g_tc_error, 0, code);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          su32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(su32(bar))
+      : "memory");
+}
+
+// Shared-memory matrix descriptor, 128-byte swizzle (layout type 2), version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+               : "memory");
+}
+
+#define TMEM_LD32(taddr, r)                                                                                          \
+  asm volatile(                                                                                                      \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19," \
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                                     \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),   \
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),       \
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),      \
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                    \
+      : "r"(taddr))
+
+struct TcArgs {
+  int M, N, K;
+  int kb_per_split;      // k-blocks (of BK) per blockIdx.z
+  float alpha, beta;
+  const float *A;        // for the Gamma-metric epilogue
+  long lda;
+  const float *B;
+  long ldb;
+  float *C;
+  long ldc;
+  int gamma;             // 0 plain, 1 Gamma metric, 2 KB projection metric
+  float *W;              // split-K partials W[z][n][m], or null: write C
+};
+
+__device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int n16, int t) {
+  for (int i = t; i < n16; i += 128) {
+    const float4 x = hi[i];
+    float4 h, l;
+    h.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u); l.x = x.x - h.x;
+    h.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u); l.y = x.y - h.y;
+    h.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u); l.z = x.z - h.z;
+    h.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u); l.w = x.w - h.w;
+    hi[i] = h;
+    lo[i] = l;
+  }
+}
+
+// A_MN: A stored with M contiguous (A[k*lda + m]); else K contiguous
+// (A[m*lda + k]).  B_MN: B stored with N contiguous (B[k*ldb + n]); else K
+// contiguous (B[n*ldb + k]).
+template <bool A_MN, bool B_MN>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs p) {
+  extern __shared__ __align__(1024) uint8_t smraw[];
+  uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bars = (uint64_t *)(sm + (size_t)STAGES * STAGE_BYTES);
+  uint64_t *full = bars, *conv = bars + STAGES, *empty = bars + 2 * STAGES, *accb = bars + 3 * STAGES;
+  uint32_t *tmem_slot = (uint32_t *)(bars + 3 * STAGES + 1);
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kb0 = blockIdx.z * p.kb_per_split;
+  const int nkb_total = (p.K + BK - 1) / BK;
+  const int nkb = min(p.kb_per_split, nkb_total - kb0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&conv[s], 128);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accb, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int issued = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % STAGES;
+        if (!mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1, 1)) { abort_flag = 1; break; }
+        if (abort_flag) break;
+        uint8_t *st = sm + (size_t)s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], A_BYTES + B_BYTES);
+        const int k = (kb0 + kb) * BK;
+        if (A_MN) {
+          for (int c = 0; c < BM / 32; ++c) tma_load_2d(st + OFF_AH + c * 4096, &mapA, m0 + 32 * c, k, &full[s]);
+        } else {
+          tma_load_2d(st + OFF_AH, &mapA, k, m0, &full[s]);
+        }
+        if (B_MN) {
+          for (int c = 0; c < BN / 32; ++c) tma_load_2d(st + OFF_BH + c * 4096, &mapB, n0 + 32 * c, k, &full[s]);
+        } else {
+          tma_load_2d(st + OFF_BH, &mapB, k, n0, &full[s]);
+        }
+        ++issued;
+      }
+      // drain: every load this thread issued has landed before the CTA exits
+      for (int kb = max(0, issued - STAGES); kb < issued; ++kb) mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, 2);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      // kind::tf32, D F32, M = 128, N = 160
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((A_MN ? 1u : 0u) << 15) |
+                             ((B_MN ? 1u : 0u) << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % STAGES;
+        if (!mbar_wait(&conv[s], (kb / STAGES) & 1, 3)) { abort_flag = 1; break; }
+        if (abort_flag) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t st = su32(sm + (size_t)s * STAGE_BYTES);
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+          // K-major: 8 tf32 = 32 B further along the swizzled row; MN-major: 8 K rows = 1 KB
+          const uint32_t ao = A_MN ? kk * 1024 : kk * 32, bo = B_MN ? kk * 1024 : kk * 32;
+          const uint32_t alb = A_MN ? 4096 : 16, blb = B_MN ? 4096 : 16;
+          const uint64_t ah = sdesc(st + OFF_AH + ao, alb, 1024), al = sdesc(st + OFF_AL + ao, alb, 1024);
+          const uint64_t bh = sdesc(st + OFF_BH + bo, blb, 1024), bl = sdesc(st + OFF_BL + bo, blb, 1024);
+          const uint32_t first = (kb == 0 && kk == 0) ? 0u : 1u;
+          mma_tf32(tmem, ah, bh, idesc, first);
+          mma_tf32(tmem, ah, bl, idesc, 1u);
+          mma_tf32(tmem, al, bh, idesc, 1u);
+        }
+        mma_commit(&empty[s]);   // frees the stage when these MMAs are done
+      }
+      mma_commit(accb);          // all MMAs issued by this thread are complete
+    }
+  } else {
+    // ---------------- split (warps 2-5) ----------------
+    const int t = threadIdx.x - 64;   // 0..127
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
+      if (abort_flag) { mbar_arrive(&conv[s]); break; }
+      uint8_t *st = sm + (size_t)s * STAGE_BYTES;
+      split_tf32((float4 *)(st + OFF_AH), (float4 *)(st + OFF_AL), A_BYTES / 16, t);
+      split_tf32((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), B_BYTES / 16, t);
+      // generic-proxy writes -> visible to the tensor core (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&conv[s]);
+    }
+    // ---------------- epilogue ----------------
+    const bool ok = mbar_wait(accb, 0, 5) && !abort_flag;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const int quad = warp & 3;
+    const int gm = m0 + quad * 32 + lane;
+    float a0 = 0.f, a1 = 0.f;
+    if (ok && p.W == nullptr && p.gamma && gm < p.M) {
+      a0 = A_MN ? p.A[gm] : p.A[(long)gm * p.lda];
+      a1 = A_MN ? p.A[p.lda + gm] : p.A[(long)gm * p.lda + 1];
+    }
+#pragma unroll 1
+    for (int c = 0; c < BN / 32; ++c) {
+      uint32_t r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 32);
+      TMEM_LD32(taddr, r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!ok || gm >= p.M) continue;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int gn = n0 + c * 32 + j;
+        if (gn >= p.N) break;
+        float v = __uint_as_float(r[j]);
+        if (p.W) {
+          p.W[((long)blockIdx.z * p.N + gn) * p.M + gm] = v;
+          continue;
+        }
+        if (p.gamma) {
+          const float b0 = B_MN ? p.B[gn] : p.B[(long)gn * p.ldb];
+          v = 2.f * v - a0 * b0;
+          if (p.gamma == 2) {
+            const float b1 = B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1];
+            v -= 2.f * a1 * b1;
+          }
+        }
+        float *cp = p.C + (long)gn * p.ldc + gm;
+        *cp = (p.beta == 0.f) ? p.alpha * v : p.alpha * v + p.beta * *cp;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::once_flag g_once;
+static bool g_attr_done[4] = {false, false, false, false};
+
+static bool encode_ready() {
+  std::call_once(g_once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  });
+  return g_encode != nullptr;
+}
+
+// 2D FP32 tensor: inner extent `inner` (contiguous), `outer` rows `ld` floats
+// apart; box 32 x box_rows, 128-byte swizzle, out-of-range reads as zero.
+static bool make_map(CUtensorMap *m, const float *base, long inner, long outer, long ld, int box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+  cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1u, 1u};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+static bool enabled() {
+  static int en = -1;
+  if (en < 0) {
+    const char *e = getenv("QX_TC");
+    en = (e && e[0] == '0') ? 0 : 1;
+  }
+  return en == 1;
+}
+
+template <bool A_MN, bool B_MN>
+static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs &a, dim3 g, cudaStream_t st) {
+  const int idx = (A_MN ? 2 : 0) + (B_MN ? 1 : 0);
+  if (!g_attr_done[idx]) {
+    if (cudaFuncSetAttribute(k_tc_gemm<A_MN, B_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) !=
+        cudaSuccess)
+      return 1;
+    g_attr_done[idx] = true;
+  }
+  k_tc_gemm<A_MN, B_MN><<<g, NTHREADS, SMEM_BYTES, st>>>(ma, mb, a);
+  note_launch();
+  return 0;
+}
+
+}  // namespace tc
+
+bool tc_enabled() { return tc::enabled(); }
+
+// Tensor-core FP32 GEMM with the semantics of gemm<float> (no column map).
+// Returns 0 when launched, -1 when the operands do not meet the TMA rules
+// (the caller then uses the CUDA-core kernel), >0 on error.
+int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
+            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes) {
+  using tc::BM;
+  using tc::BN;
+  using tc::BK;
+  if (!tc::enabled() || M <= 0 || N <= 0 || K <= 0) return -1;
+  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (lda & 3) || (ldb & 3)) return -1;
+  if (!tc::encode_ready()) return -1;
+  // A: ta -> K contiguous (A[m*lda + k]); !ta -> M contiguous (A[k*lda + m])
+  const bool a_mn = !ta, b_mn = tb;
+  CUtensorMap ma, mb;
+  if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32) : tc::make_map(&ma, A, K, M, lda, BM))) return -1;
+  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32) : tc::make_map(&mb, B, K, N, ldb, BN))) return -1;
+  const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN, nkb = (K + BK - 1) / BK;
+  // split K until the grid covers the SMs about twice, at least 4 k-blocks a split
+  int nsplit = 1;
+  const long tiles = (long)tm * tn;
+  if (ws && tiles < 148) {
+    nsplit = (int)std::min<long>((2 * 148 + tiles - 1) / tiles, std::max(1, nkb / 4));
+    while (nsplit > 1 && (size_t)nsplit * M * N * sizeof(float) > ws_bytes) --nsplit;
+  }
+  const int kps = (nkb + nsplit - 1) / nsplit;
+  nsplit = (nkb + kps - 1) / kps;
+  tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr};
+  dim3 g(tm, tn, nsplit);
+  int rc;
+  if (a_mn && b_mn) rc = tc::launch_tc<true, true>(ma, mb, a, g, st);
+  else if (a_mn) rc = tc::launch_tc<true, false>(ma, mb, a, g, st);
+  else if (b_mn) rc = tc::launch_tc<false, true>(ma, mb, a, g, st);
+  else rc = tc::launch_tc<false, false>(ma, mb, a, g, st);
+  if (rc) return rc;
+  if (nsplit > 1)
+    gemm_reduce_f32(ta, tb, M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, (const float *)ws, st);
+  return 0;
+}
+
+// Error code recorded by a tensor-core GEMM whose wait timed out (0: none);
+// reading clears it.
+int tc_error_take() {
+  int h = 0, z = 0;
+  if (cudaMemcpyFromSymbol(&h, tc::g_tc_error, sizeof(int)) != cudaSuccess) return -1;
+  if (h) cudaMemcpyToSymbol(tc::g_tc_error, &z, sizeof(int));
+  return h;
+}
+
+}  // namespace qx

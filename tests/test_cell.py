@@ -70,6 +70,14 @@ def test_random_wavefunctions_lcg():
     assert np.all(np.abs(x) < 0.5)
 
 
+def test_lcg_minimal_standard_known_answer():
+    # rnd00 is the Park-Miller minimal standard generator (a = 16807,
+    # m = 2^31 - 1); its published check value: from seed 1 the 10000th
+    # state is 1043618065 (Park & Miller, CACM 31 (1988) 1192).
+    v = cell.random_wavefunctions(10000, 1, seed=1.0)[0, 9999]
+    assert round((v + 0.5) * 2147483647.0) == 1043618065
+
+
 def test_kb_tables_consistent_between_g_and_r(si8):
     # G-space table = Fourier transform of the real-space projector (same operator)
     s = si8

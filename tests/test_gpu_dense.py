@@ -1,0 +1,92 @@
+"""Band-space dense algebra at band counts that span several 32-wide blocks:
+Gram-Schmidt through the blocked FP64 Cholesky and triangular inverse
+(schmidt2 + rsdecmp/rsinvcd, schmidt.f90:117-544) and the subspace
+eigen-decomposition + rotation (untryt2/untryhc2, eigen.f90:1171-1451),
+against the oracle.  nb = 160 is the Si64 band count (matrix in shared
+memory); nb = 200 exceeds shared memory and runs from global memory.
+
+Tolerances: FP64 1e-10 (orthonormalised bands), eigenvalues 1e-10 relative;
+mixed precision (FP32 bands, 3xTF32 tensor-core contractions, FP64
+Cholesky/eigensolver) 1e-4.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from qxmd_b200 import cell
+from qxmd_b200.lib import QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context, QxError
+
+from gpu_util import need_gpu, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nb", [48, 160, 200])
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-10), (QX_PREC_MIXED, 1e-4)])
+def test_schmidt_many_blocks(si8, nb, prec, tol):
+    need_gpu()
+    c = cell.random_wavefunctions(si8.gs.nplwex, nb)
+    ref, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    ctx = Context(si8, prec, QX_NL_GSPACE, nband=nb)
+    try:
+        q = ctx.schmidt_host(c)
+    finally:
+        ctx.close()
+    assert relerr(q, ref) < tol
+    # orthonormal in the Gamma metric
+    s = 2.0 * q @ q.T - np.outer(q[:, 0], q[:, 0])
+    assert np.max(np.abs(s - np.eye(nb))) < (1e-10 if prec == QX_PREC_FP64 else 1e-4)
+
+
+def test_schmidt_reports_first_bad_pivot_in_later_block(si8):
+    need_gpu()
+    nb = 100
+    c = cell.random_wavefunctions(si8.gs.nplwex, nb)
+    c[70] = 0.0                      # the pivot of row 70 (third 32-wide block) is zero
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE, nband=nb)
+    try:
+        with pytest.raises(QxError) as e:
+            ctx.schmidt_host(c)
+        assert e.value.code == 3
+        assert "band 70" in str(e.value)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("nb", [48, 160, 200])
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_untryt_many_blocks(si8, nb, prec):
+    need_gpu()
+    c = cell.random_wavefunctions(si8.gs.nplwex, nb)
+    c, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    h = oracle.Ham(si8, 1)
+    hc = h.hpsi(c)
+    hm, _ = oracle.hmatrix(c, hc)
+    w_ref, u_ref, sweeps = oracle.jacobi(hm, maxsweep=80)
+    assert sweeps >= 0
+    ctx = Context(si8, prec, QX_NL_GSPACE, nband=nb)
+    try:
+        ctx.put_psi(c)
+        ctx.put_hpsi(hc)
+        ctx.hmatrix()
+        ev = ctx.untryt()
+        ctx.untryhc()
+        psi = ctx.get_psi()
+        hpsi = ctx.get_hpsi()
+    finally:
+        ctx.close()
+    etol = 1e-10 if prec == QX_PREC_FP64 else 1e-5
+    assert relerr(ev, w_ref) < etol
+    # the rotated bands diagonalise the subspace Hamiltonian
+    hm2 = 2.0 * psi @ hpsi.T - np.outer(psi[:, 0], hpsi[:, 0])
+    off = hm2 - np.diag(np.diag(hm2))
+    scale = np.max(np.abs(w_ref))
+    assert np.max(np.abs(off)) / scale < (1e-9 if prec == QX_PREC_FP64 else 1e-4)
+    assert relerr(np.diag(hm2), w_ref) < etol * 10
+    # and match the oracle's rotation where eigenvalues are separated
+    ref_psi = oracle.rotate(c, u_ref)
+    gaps = np.minimum(np.diff(w_ref, prepend=-np.inf), np.diff(w_ref, append=np.inf))
+    sep = gaps > 1e-6 * scale
+    assert relerr(psi[sep], ref_psi[sep]) < (1e-8 if prec == QX_PREC_FP64 else 1e-3)
