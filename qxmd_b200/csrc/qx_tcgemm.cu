@@ -4,7 +4,7 @@
 // (engrad.f90:869-895), subgs3 (engrad.f90:1122-1142), C*U
 // (eigen.f90:1482-1510) and C*L^-T (schmidt.f90:284-313).
 //
-// sm_100a only: operands staged by TMA (128-byte swizzle) into a 3-stage
+// sm_100a only: operands staged by TMA (128-byte swizzles) into a 3-stage
 // shared-memory ring, products on the 5th-generation tensor cores
 // (tcgen05.mma kind::tf32, 128 x 160 tile, accumulator in TMEM), read back
 // with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
@@ -93,13 +93,15 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// Shared-memory matrix descriptor, 128-byte swizzle (layout type 2), version 1.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+// Shared-memory matrix descriptor, version 1.  layout 2: 128-byte swizzle of
+// 16-byte chunks (K-major tiles); layout 1: 128-byte swizzle of 32-byte
+// chunks, the one MN-major layout the tensor cores accept for 32-bit operands.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
   uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
   d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
+  d |= (uint64_t)layout << 61;
   return d;
 }
 
@@ -230,11 +232,16 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         const uint32_t st = su32(sm + (size_t)s * STAGE_BYTES);
 #pragma unroll
         for (int kk = 0; kk < BK / 8; ++kk) {
-          // K-major: 8 tf32 = 32 B further along the swizzled row; MN-major: 8 K rows = 1 KB
+          // K-major (layout 2): rows of 128 B, 8-row groups 1 KB apart, the
+          // k-step is 8 tf32 = 32 B along the swizzled row.  MN-major (layout
+          // 1): 32-element MN chunks 4 KB apart (LBO), 4-row K groups 512 B
+          // apart (SBO), the k-step is 8 K rows = 1 KB.
           const uint32_t ao = A_MN ? kk * 1024 : kk * 32, bo = B_MN ? kk * 1024 : kk * 32;
           const uint32_t alb = A_MN ? 4096 : 16, blb = B_MN ? 4096 : 16;
-          const uint64_t ah = sdesc(st + OFF_AH + ao, alb, 1024), al = sdesc(st + OFF_AL + ao, alb, 1024);
-          const uint64_t bh = sdesc(st + OFF_BH + bo, blb, 1024), bl = sdesc(st + OFF_BL + bo, blb, 1024);
+          const uint32_t asb = A_MN ? 512 : 1024, bsb = B_MN ? 512 : 1024;
+          const uint32_t aly = A_MN ? 1 : 2, bly = B_MN ? 1 : 2;
+          const uint64_t ah = sdesc(st + OFF_AH + ao, alb, asb, aly), al = sdesc(st + OFF_AL + ao, alb, asb, aly);
+          const uint64_t bh = sdesc(st + OFF_BH + bo, blb, bsb, bly), bl = sdesc(st + OFF_BL + bo, blb, bsb, bly);
           const uint32_t first = (kb == 0 && kk == 0) ? 0u : 1u;
           mma_tf32(tmem, ah, bh, idesc, first);
           mma_tf32(tmem, ah, bl, idesc, 1u);
@@ -323,14 +330,18 @@ static bool encode_ready() {
 }
 
 // 2D FP32 tensor: inner extent `inner` (contiguous), `outer` rows `ld` floats
-// apart; box 32 x box_rows, 128-byte swizzle, out-of-range reads as zero.
-static bool make_map(CUtensorMap *m, const float *base, long inner, long outer, long ld, int box_rows) {
+// apart; box 32 x box_rows, out-of-range reads as zero.  K-major tiles use the
+// 128-byte swizzle of 16-byte chunks, MN-major tiles (mn) the 128-byte swizzle
+// of 32-byte chunks that matches descriptor layout 1.
+static bool make_map(CUtensorMap *m, const float *base, long inner, long outer, long ld, int box_rows, bool mn) {
   cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
   cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
   cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
   cuuint32_t es[2] = {1u, 1u};
   CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        mn ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
@@ -376,8 +387,8 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   // A: ta -> K contiguous (A[m*lda + k]); !ta -> M contiguous (A[k*lda + m])
   const bool a_mn = !ta, b_mn = tb;
   CUtensorMap ma, mb;
-  if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32) : tc::make_map(&ma, A, K, M, lda, BM))) return -1;
-  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32) : tc::make_map(&mb, B, K, N, ldb, BN))) return -1;
+  if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, true) : tc::make_map(&ma, A, K, M, lda, BM, false))) return -1;
+  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, true) : tc::make_map(&mb, B, K, N, ldb, BN, false))) return -1;
   const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN, nkb = (K + BK - 1) / BK;
   // split K until the grid covers the SMs about twice, at least 4 k-blocks a split
   int nsplit = 1;
