@@ -28,25 +28,70 @@ __device__ __forceinline__ double warp_sum(double v) {
 // diagonal S(i,i) - sum_k L(i,k)^2 that rsdecmp tests) is not > 1e-30
 // (schmidt.f90:256-267).
 constexpr int CB = 32;
-constexpr int CHT = 512;            // threads of k_cholinv (16 warps)
+constexpr int CHT = 256;            // threads of k_cholinv (8 warps)
 constexpr int DLD = CB + 1;         // leading dimension of the 32 x 32 temporary
 constexpr size_t CH_SMEM_MAX = 220 * 1024;
 
-// X = L^-1 of the lower-triangular bs x bs block at B (leading dimension ld),
-// in place, columns right to left (X(i,j) = -sum_{k=j+1..i} X(i,k) L(k,j) /
-// L(j,j)), lane = row.  Only the lower triangle is read or written.  Called
-// by one whole warp.
-__device__ __forceinline__ void warp_trinv(double *B, int ld, int bs, int lane) {
-  for (int j = bs - 1; j >= 0; --j) {
-    const double xjj = 1.0 / B[(long)j * ld + j];
-    double s = 0.0;
-    if (lane > j && lane < bs)
-      for (int k = j + 1; k <= lane; ++k) s += B[(long)k * ld + lane] * B[(long)j * ld + k];
-    __syncwarp();
-    if (lane == j) B[(long)j * ld + j] = xjj;
-    if (lane > j && lane < bs) B[(long)j * ld + lane] = -s * xjj;
-    __syncwarp();
+// Cholesky of the bs x bs diagonal block at B (leading dimension ld) in
+// registers: lane i holds row i, column k of L is broadcast by shuffles.
+// Writes L (lower triangle, diagonal included).  Returns the first row whose
+// pivot is not > 1e-30, or -1.  Called by one whole warp.
+__device__ __forceinline__ int warp_chol(double *B, int ld, int bs, int lane) {
+  double r[CB];
+#pragma unroll
+  for (int j = 0; j < CB; ++j) r[j] = (lane < bs && j < bs && j <= lane) ? B[(long)j * ld + lane] : 0.0;
+  int bad = -1;
+#pragma unroll
+  for (int k = 0; k < CB; ++k) {
+    if (k < bs) {
+      const double piv = __shfl_sync(0xffffffffu, r[k], k);
+      if (!(piv > 1.0e-30)) {   // uniform; also catches NaN
+        bad = k;
+        break;
+      }
+      const double sq = sqrt(piv), rs = 1.0 / sq;
+      const double lik = (lane == k) ? sq : r[k] * rs;   // l_ik for lanes i > k
+      r[k] = lik;
+#pragma unroll
+      for (int j = k + 1; j < CB; ++j) {
+        const double ljk = __shfl_sync(0xffffffffu, lik, j);
+        if (lane >= j) r[j] -= lik * ljk;
+      }
+    }
   }
+  if (bad < 0 && lane < bs) {
+#pragma unroll
+    for (int j = 0; j < CB; ++j)
+      if (j <= lane) B[(long)j * ld + lane] = r[j];
+  }
+  __syncwarp();
+  return bad;
+}
+
+// X = L^-1 of the lower-triangular bs x bs block at L (leading dimension ldl)
+// into X (leading dimension ldx; may equal L), lane j producing column j by
+// forward substitution with L's rows read as broadcasts.  Zeros above the
+// diagonal.  Called by one whole warp.
+__device__ __forceinline__ void warp_trinv(const double *L, int ldl, double *X, int ldx, int bs, int lane) {
+  double x[CB];
+#pragma unroll
+  for (int i = 0; i < CB; ++i) {
+    double s = (i == lane) ? 1.0 : 0.0;
+    if (i < bs) {
+#pragma unroll
+      for (int k = 0; k < i; ++k) s -= L[(long)k * ldl + i] * x[k];
+      x[i] = s / L[(long)i * ldl + i];
+    } else {
+      x[i] = 0.0;
+    }
+  }
+  __syncwarp();
+  if (lane < bs) {
+#pragma unroll
+    for (int i = 0; i < CB; ++i)
+      if (i < bs) X[(long)lane * ldx + i] = (i >= lane) ? x[i] : 0.0;
+  }
+  __syncwarp();
 }
 
 __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n, double *__restrict__ work,
@@ -70,40 +115,18 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   for (int J = 0; J < nblk; ++J) {
     const int j0 = J * CB, bs = min(CB, n - j0);
     if (warp == 0) {
-      // diagonal block, lane = row
-      for (int k = 0; k < bs; ++k) {
-        const double piv = A_(j0 + k, j0 + k);
-        if (!(piv > 1.0e-30)) {            // also catches NaN
-          if (lane == 0) bad = 1 + j0 + k;
-          break;
-        }
-        const double s = sqrt(piv), r = 1.0 / s;
-        __syncwarp();
-        if (lane > k && lane < bs) A_(j0 + lane, j0 + k) *= r;
-        if (lane == k) A_(j0 + k, j0 + k) = s;
-        __syncwarp();
-        if (lane > k && lane < bs) {
-          const double lik = A_(j0 + lane, j0 + k);
-          for (int j = k + 1; j <= lane; ++j) A_(j0 + lane, j0 + j) -= lik * A_(j0 + j, j0 + k);
-        }
-        __syncwarp();
+      const int b = warp_chol(&A_(j0, j0), ld, bs, lane);
+      if (b >= 0) {
+        if (lane == 0) bad = 1 + j0 + b;
+      } else if (j0 + bs < n) {
+        warp_trinv(&A_(j0, j0), ld, T, DLD, bs, lane);   // Linv_JJ for the panel
       }
     }
     __syncthreads();
     if (bad) break;
     const int r0 = j0 + bs, mr = n - r0;
     if (mr <= 0) break;
-    // panel: L(r, j0+c) = sum_{k <= c} A(r, j0+k) Linv_JJ(c, k), Linv_JJ
-    // formed in the temporary T
-    if (warp == 0) {
-      for (int q = lane; q < CB * CB; q += 32) {
-        const int jj = q >> 5, ii = q & 31;
-        T[jj * DLD + ii] = (ii >= jj && ii < bs && jj < bs) ? A_(j0 + ii, j0 + jj) : 0.0;
-      }
-      __syncwarp();
-      warp_trinv(T, DLD, bs, lane);
-    }
-    __syncthreads();
+    // panel: L(r, j0+c) = sum_{k <= c} A(r, j0+k) Linv_JJ(c, k)
     for (int r = r0 + warp; r < n; r += nw) {
       const double a = (lane < bs) ? A_(r, j0 + lane) : 0.0;
       double s = 0.0;
@@ -116,13 +139,12 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
     }
     __syncthreads();
     // trailing update of the lower triangle: A(r, c) -= sum_k L(r, j0+k) L(c, j0+k)
-    for (long q = tid; q < (long)mr * mr; q += CHT) {
-      const int c = (int)(q / mr), r = (int)(q - (long)c * mr);
-      if (r < c) continue;
-      double s = 0.0;
-      for (int k = 0; k < bs; ++k) s += A_(r0 + r, j0 + k) * A_(r0 + c, j0 + k);
-      A_(r0 + r, r0 + c) -= s;
-    }
+    for (int c = warp; c < mr; c += nw)
+      for (int r = c + lane; r < mr; r += 32) {
+        double s = 0.0;
+        for (int k = 0; k < bs; ++k) s += A_(r0 + r, j0 + k) * A_(r0 + c, j0 + k);
+        A_(r0 + r, r0 + c) -= s;
+      }
     __syncthreads();
   }
   if (bad) {
@@ -131,15 +153,13 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   }
   // ---- L^-1, blocked ----
   // zero the strict upper triangle (it still holds S)
-  for (long q = tid; q < (long)n * n; q += CHT) {
-    const int j = (int)(q / n), i = (int)(q - (long)j * n);
-    if (i < j) A_(i, j) = 0.0;
-  }
+  for (int j = warp; j < n; j += nw)
+    for (int i = lane; i < j; i += 32) A_(i, j) = 0.0;
   __syncthreads();
   // diagonal blocks in place, one warp each
   for (int J = warp; J < nblk; J += nw) {
     const int j0 = J * CB;
-    warp_trinv(&A_(j0, j0), ld, min(CB, n - j0), lane);
+    warp_trinv(&A_(j0, j0), ld, &A_(j0, j0), ld, min(CB, n - j0), lane);
   }
   __syncthreads();
   // row blocks top-down, column blocks left to right, in place:
@@ -148,16 +168,16 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
     const int i0 = I * CB, bi = min(CB, n - i0);
     for (int J = 0; J < I; ++J) {
       const int j0 = J * CB;
-      for (int q = tid; q < CB * CB; q += CHT) {
-        const int jj = q >> 5, ii = q & 31;
+      for (int jj = warp; jj < CB; jj += nw) {
+        const int ii = lane;
         double s = 0.0;
         if (ii < bi)
           for (int k = j0; k < i0; ++k) s += A_(i0 + ii, k) * A_(k, j0 + jj);
         T[jj * DLD + ii] = s;
       }
       __syncthreads();
-      for (int q = tid; q < CB * CB; q += CHT) {
-        const int jj = q >> 5, ii = q & 31;
+      for (int jj = warp; jj < CB; jj += nw) {
+        const int ii = lane;
         if (ii < bi) {
           double s = 0.0;
           for (int k = 0; k <= ii; ++k) s += A_(i0 + ii, i0 + k) * T[jj * DLD + k];
@@ -204,7 +224,7 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
 //      tridiagonal LU, one thread per cluster of close eigenvalues, members
 //      re-orthogonalised against each other; per-thread work arrays are
 //      interleaved across threads so every access is coalesced;
-//  (4) k_backtrans: V = Q Z, one warp per column.
+//  (4) k_backtrans: V = Q Z, one warp per column (in registers for n <= 256).
 // Eigenpairs are ascending; each eigenvector's largest-magnitude component is
 // made positive (first index on ties).  Every loop is bounded.
 
@@ -227,7 +247,17 @@ __device__ __forceinline__ void house(double x0, double sigma, double &tau, doub
   alpha = mu;
 }
 
-// gvec: 2n doubles of global memory for v and p when A is not in shared memory.
+// Per column k (m = n-k-1 trailing rows): warp 0 forms the reflector from
+// column k (which it updated itself in step k-1), then three barriers:
+// (1) reflector published; (2) matrix-vector product B v in 4 column groups
+// of 32-row strips, partial sums to `part`; (3) p = t * sum of the groups.
+// The rank-2 update B -= v w^T + w v^T (w = p - K v) is spread by columns
+// over the warps and needs no barrier of its own: v, and the scalars, are
+// double-buffered by column parity, so warp 0 can form the next reflector
+// while other warps finish this update, and the next matrix-vector product
+// starts only after barrier (1) of the next column.
+// gvec: 7n doubles of global memory for v (two buffers), p and part when A
+// is not in shared memory.
 __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n, double *__restrict__ d,
                                                  double *__restrict__ e, double *__restrict__ HV,
                                                  double *__restrict__ tau, int use_smem, double *__restrict__ gvec) {
@@ -235,9 +265,11 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
   __shared__ double sc[2];
   const int ld = use_smem ? (n | 1) : n;
   double *A = use_smem ? sm : Ag;
-  double *v = use_smem ? sm + (long)ld * n : gvec;
-  double *p = v + n;
+  double *vb = use_smem ? sm + (long)ld * n : gvec;   // 2 x n
+  double *p = vb + 2 * (long)n;                       // n
+  double *part = p + n;                               // 4 x n
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = TRD_T / 32, NG = 4;
 #define A_(i, j) A[(long)(j) * ld + (i)]
   if (use_smem)
     for (long q = tid; q < (long)n * n; q += TRD_T) {
@@ -247,6 +279,7 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
   __syncthreads();
   for (int k = 0; k + 2 < n; ++k) {
     const int m = n - k - 1;
+    double *v = vb + (k & 1) * (long)n;
     if (warp == 0) {
       double sg = 0.0;
       for (int i = 1 + lane; i < m; i += 32) { const double x = A_(k + 1 + i, k); sg += x * x; }
@@ -254,9 +287,9 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
       double t = 0.0, be = 1.0, al = 0.0;
       if (lane == 0) house(A_(k + 1, k), sg, t, be, al);
       t = __shfl_sync(0xffffffffu, t, 0);
-      be = __shfl_sync(0xffffffffu, be, 0);
+      const double rbe = 1.0 / __shfl_sync(0xffffffffu, be, 0);
       for (int i = lane; i < m; i += 32) {
-        const double vi = (i == 0) ? 1.0 : ((t != 0.0) ? A_(k + 1 + i, k) / be : 0.0);
+        const double vi = (i == 0) ? 1.0 : ((t != 0.0) ? A_(k + 1 + i, k) * rbe : 0.0);
         v[i] = vi;
         HV[(long)k * n + k + 1 + i] = vi;
       }
@@ -267,36 +300,35 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
         sc[k & 1] = t;
       }
     }
-    __syncthreads();
-    // uniform: written before the barrier; alternating slots keep a thread
-    // that reads late from seeing the next column's value
+    __syncthreads();                                   // (1)
     const double t = sc[k & 1];
-    if (t == 0.0) continue;
-    // p = t * B v, B = A(k+1:, k+1:); G lanes per row (G | 32)
-    int G = 1;
-    while (G < 32 && 2 * G * m <= TRD_T) G *= 2;
-    const int R = TRD_T / G, g = tid % G, r = tid / G;
-    for (int i0 = 0; i0 < m; i0 += R) {
-      const int i = i0 + r;
+    if (t == 0.0) continue;                            // uniform
+    const int nrb = (m + 31) >> 5;
+    for (int task = warp; task < nrb * NG; task += NW) {
+      const int rb = task / NG, g = task - rb * NG, i = rb * 32 + lane;
       double s = 0.0;
-      if (i < m)
-        for (int j = g; j < m; j += G) s += A_(k + 1 + i, k + 1 + j) * v[j];
-      for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (g == 0 && i < m) p[i] = t * s;
+      if (i < m) {
+        const double *col = &A_(k + 1 + i, k + 1);
+        for (int j = g; j < m; j += NG) s += col[(long)j * ld] * v[j];
+        part[g * n + i] = s;
+      }
     }
-    __syncthreads();
-    // K = t/2 v^T p (every warp computes it), w = p - K v, B -= v w^T + w v^T
+    __syncthreads();                                   // (2)
+    for (int i = tid; i < m; i += TRD_T) p[i] = t * (part[i] + part[n + i] + part[2 * n + i] + part[3 * n + i]);
+    __syncthreads();                                   // (3)
     double kk = 0.0;
     for (int i = lane; i < m; i += 32) kk += v[i] * p[i];
     const double K = 0.5 * t * warp_sum(kk);
-    for (long q = tid; q < (long)m * m; q += TRD_T) {
-      const int j = (int)(q / m), i = (int)(q - (long)j * m);
-      const double vi = v[i], vj = v[j];
-      const double wi = p[i] - K * vi, wj = p[j] - K * vj;
-      A_(k + 1 + i, k + 1 + j) -= vi * wj + wi * vj;
+    for (int j = warp; j < m; j += NW) {
+      const double vj = v[j], wj = p[j] - K * vj;
+      double *col = &A_(k + 1, k + 1 + j);
+      for (int i = lane; i < m; i += 32) {
+        const double vi = v[i], wi = p[i] - K * vi;
+        col[i] -= vi * wj + wi * vj;
+      }
     }
-    __syncthreads();
   }
+  __syncthreads();
   if (tid == 0) {
     if (n >= 2) {
       d[n - 2] = A_(n - 2, n - 2);
@@ -305,6 +337,15 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
     d[n - 1] = A_(n - 1, n - 1);
   }
 #undef A_
+}
+
+// 1/q: the hardware's approximate reciprocal refined by one Newton-Raphson
+// step r <- r (2 - q r), which squares the relative error (to about 1e-14);
+// only the signs of the Sturm pivots are used, so this accuracy is ample.
+__device__ __forceinline__ double recip_nr(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  return r * fma(-q, r, 2.0);
 }
 
 // Number of eigenvalues of T below x (Sturm count, pivots guarded by pmin).
@@ -316,7 +357,7 @@ __device__ __forceinline__ int sturm(const double *__restrict__ d, const double 
   if (q < 0.0) ++c;
   for (int i = 1; i < n; ++i) {
     const double ei = e[i - 1];
-    q = d[i] - x - ei * ei / q;
+    q = d[i] - x - ei * ei * recip_nr(q);
     if (fabs(q) < pmin) q = -pmin;
     if (q < 0.0) ++c;
   }
@@ -367,10 +408,17 @@ __global__ void k_bisect(const double *__restrict__ d, const double *__restrict_
 // earlier ones.  Thread t is active if eigenvalue t starts a cluster.
 // ws: 6 arrays of n x NT doubles, element (a, i) of thread t at
 // ws[(a*n + i)*NT + t] (coalesced across threads).  Z(:, t) = eigenvector t.
+// With use_smem the six arrays live in shared memory instead, interleaved
+// across the block's threads (6 * n * blockDim doubles).
 __global__ void k_invit(const double *__restrict__ d, const double *__restrict__ e, const double *__restrict__ w,
-                        int n, double *__restrict__ Z, double *__restrict__ ws, int NT, int *__restrict__ nclus) {
+                        int n, double *__restrict__ Z, double *__restrict__ wsg, int NTg, int *__restrict__ nclus,
+                        int use_smem) {
+  extern __shared__ double wss[];
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
+  double *ws = use_smem ? wss : wsg;
+  const int NT = use_smem ? (int)blockDim.x : NTg;
+  const int tt = use_smem ? (int)threadIdx.x : t;
   double tn = 0.0;
   for (int i = 0; i < n; ++i)
     tn = fmax(tn, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0));
@@ -380,7 +428,7 @@ __global__ void k_invit(const double *__restrict__ d, const double *__restrict__
   atomicAdd(nclus, 1);
   int tend = t + 1;
   while (tend < n && w[tend] - w[tend - 1] < gaptol) ++tend;
-#define WS(a, i) ws[((long)(a) * n + (i)) * NT + t]
+#define WS(a, i) ws[((long)(a) * n + (i)) * NT + tt]
   // 0: 1/U(i,i), 1: U(i,i+1), 2: U(i,i+2), 3: multiplier, 4: row swap flag, 5: z
   const double tiny = eps * tn + 1e-300;
   for (int c = t; c < tend; ++c) {
@@ -484,20 +532,88 @@ __global__ void __launch_bounds__(256) k_backtrans(const double *__restrict__ Z,
   for (int i = lane; i < n; i += 32) V[(long)c * n + i] = sg * z[i];
 }
 
+// The same for n <= 32*MC with the column and the next reflector held in
+// registers: the reflector k-1 is loaded while reflector k is applied, so
+// the L2 latency is off the chain.  Entries of HV above row k+1 are never
+// written and are excluded by selection, not by multiplication.
+template <int MC>
+__global__ void __launch_bounds__(256) k_backtrans_reg(const double *__restrict__ Z, const double *__restrict__ HV,
+                                                       const double *__restrict__ tau, int n,
+                                                       double *__restrict__ V) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (c >= n) return;   // whole warp
+  double z[MC], vn[MC];
+#pragma unroll
+  for (int q = 0; q < MC; ++q) {
+    const int i = lane + 32 * q;
+    z[q] = (i < n) ? Z[(long)c * n + i] : 0.0;
+    vn[q] = (n >= 3 && i < n) ? HV[(long)(n - 3) * n + i] : 0.0;
+  }
+  double tn = (n >= 3) ? tau[n - 3] : 0.0;
+  for (int k = n - 3; k >= 0; --k) {
+    double v[MC];
+    const double tk = tn;
+#pragma unroll
+    for (int q = 0; q < MC; ++q) v[q] = vn[q];
+    if (k > 0) {
+#pragma unroll
+      for (int q = 0; q < MC; ++q) {
+        const int i = lane + 32 * q;
+        vn[q] = (i < n) ? HV[(long)(k - 1) * n + i] : 0.0;
+      }
+      tn = tau[k - 1];
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < MC; ++q) {
+      const int i = lane + 32 * q;
+      s += (i > k && i < n) ? v[q] * z[q] : 0.0;
+    }
+    s = tk * warp_sum(s);
+#pragma unroll
+    for (int q = 0; q < MC; ++q) {
+      const int i = lane + 32 * q;
+      if (i > k && i < n) z[q] -= v[q] * s;
+    }
+  }
+  double mx = -1.0;
+  int km = 0;
+  double zk = 0.0;
+#pragma unroll
+  for (int q = 0; q < MC; ++q) {
+    const int i = lane + 32 * q;
+    if (i < n && fabs(z[q]) > mx) { mx = fabs(z[q]); km = i; zk = z[q]; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+    const int k2 = __shfl_xor_sync(0xffffffffu, km, o);
+    const double z2 = __shfl_xor_sync(0xffffffffu, zk, o);
+    if (m2 > mx || (m2 == mx && k2 < km)) { mx = m2; km = k2; zk = z2; }
+  }
+  const double sg = zk < 0.0 ? -1.0 : 1.0;
+#pragma unroll
+  for (int q = 0; q < MC; ++q) {
+    const int i = lane + 32 * q;
+    if (i < n) V[(long)c * n + i] = sg * z[q];
+  }
+}
+
 // A (n x n, destroyed), w (n) eigenvalues ascending, V (n x n) eigenvectors.
 // work: at least 8*n*n + 1024*n doubles.  info: number of eigenvalue clusters.
 int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st) {
   if (n < 1) { set_error("syev: n=%d", n); return 1; }
   const int NT = ((n + 127) / 128) * 128;
-  double *d = work, *e = d + n, *tau = e + n, *vp = tau + n, *HV = vp + 2 * (long)n, *Z = HV + (long)n * n,
-         *ws = Z + (long)n * n;   // 6 * n * NT <= 6n^2 + 762n: total <= 8n^2 + 767n
+  double *d = work, *e = d + n, *tau = e + n, *vp = tau + n, *HV = vp + 7 * (long)n, *Z = HV + (long)n * n,
+         *ws = Z + (long)n * n;   // 6 * n * NT <= 6n^2 + 762n: total <= 8n^2 + 772n
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM_MAX);
     cudaFuncSetAttribute(k_backtrans, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_invit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
-  const size_t smem = sizeof(double) * ((size_t)(n | 1) * n + 2 * (size_t)n);
+  const size_t smem = sizeof(double) * ((size_t)(n | 1) * n + 7 * (size_t)n);
   const int use = smem <= TRD_SMEM_MAX;
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
   k_sytrd<<<1, TRD_T, use ? smem : 0, st>>>(A, n, d, e, HV, tau, use, vp); note_launch();
@@ -507,11 +623,21 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     cudaMemcpyAsync(V, &one, sizeof(double), cudaMemcpyHostToDevice, st);
     return 0;
   }
-  k_bisect<<<(n * 32 + 255) / 256, 256, 0, st>>>(d, e, n, w); note_launch();
-  k_invit<<<NT / 128, 128, 0, st>>>(d, e, w, n, Z, ws, NT, d_info); note_launch();
-  const size_t bt = sizeof(double) * 8 * (size_t)n;
-  if (bt > 200 * 1024) { set_error("syev: n=%d too large for the back-transformation", n); return 1; }
-  k_backtrans<<<(n + 7) / 8, 256, bt, st>>>(Z, HV, tau, n, V); note_launch();
+  // one warp per eigenvalue, one warp per block: spread over the SMs
+  k_bisect<<<n, 32, 0, st>>>(d, e, n, w); note_launch();
+  const size_t wsm = sizeof(double) * 6 * (size_t)n * 16;
+  if (wsm <= 200 * 1024) {
+    k_invit<<<(n + 15) / 16, 16, wsm, st>>>(d, e, w, n, Z, ws, NT, d_info, 1); note_launch();
+  } else {
+    k_invit<<<NT / 128, 128, 0, st>>>(d, e, w, n, Z, ws, NT, d_info, 0); note_launch();
+  }
+  if (n <= 256) {
+    k_backtrans_reg<8><<<(n + 3) / 4, 128, 0, st>>>(Z, HV, tau, n, V); note_launch();
+  } else {
+    const size_t bt = sizeof(double) * 8 * (size_t)n;
+    if (bt > 200 * 1024) { set_error("syev: n=%d too large for the back-transformation", n); return 1; }
+    k_backtrans<<<(n + 7) / 8, 256, bt, st>>>(Z, HV, tau, n, V); note_launch();
+  }
   return 0;
 }
 

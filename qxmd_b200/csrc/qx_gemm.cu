@@ -112,8 +112,19 @@ __global__ void k_gemm_reduce(int M, int N, int nsplit, T alpha, const T *__rest
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (e >= (long)M * Nact) return;
   const int gn = (int)(e / M), gm = (int)(e - (long)gn * M);
+  // fixed summation order; loads issued eight at a time
+  const long zs = (long)N * M;
+  const T *w = W + (long)gn * M + gm;
   T v = 0;
-  for (int z = 0; z < nsplit; ++z) v += W[((long)z * N + gn) * M + gm];
+  int z = 0;
+  for (; z + 8 <= nsplit; z += 8) {
+    T t[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t[q] = w[(long)(z + q) * zs];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v += t[q];
+  }
+  for (; z < nsplit; ++z) v += w[(long)z * zs];
   const long cn = colmap ? colmap[gn] : gn;
   if (gamma) {
     const T a0 = TA ? A[(long)gm * lda] : A[gm];

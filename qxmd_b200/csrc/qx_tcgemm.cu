@@ -6,7 +6,7 @@
 //
 // sm_100a only: operands staged by TMA (128-byte swizzles) into a 3-stage
 // shared-memory ring, products on the 5th-generation tensor cores
-// (tcgen05.mma kind::tf32, 128 x 160 tile, accumulator in TMEM), read back
+// (tcgen05.mma kind::tf32, 128 x 160 or 128 x 80 tile, accumulator in TMEM), read back
 // with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
 // is cut into x_hi = x with the low 13 mantissa bits cleared and
 // x_lo = x - x_hi (exact in FP32), and the tile product is
@@ -33,16 +33,26 @@
 namespace qx {
 namespace tc {
 
-constexpr int BM = 128, BN = 160, BK = 32, STAGES = 3;
-constexpr int TMEM_COLS = 256;
+constexpr int BM = 128, BK = 32;
 constexpr int A_BYTES = BM * BK * 4;                 // 16 KB
-constexpr int B_BYTES = BN * BK * 4;                 // 20 KB
-constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
-constexpr int STAGE_BYTES = 2 * (A_BYTES + B_BYTES); // 72 KB, a multiple of 1 KB
 constexpr int NTHREADS = 192;
-constexpr int BAR_BYTES = 128;
-constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + BAR_BYTES + 1024;   // + alignment slack
+constexpr int BAR_BYTES = 256;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
+
+// Tile width BN (MMA N) and what follows from it.  BN = 160 covers a 160-band
+// block in one tile; BN = 80 doubles the tile count when M alone gives too
+// few tiles to fill the 148 SMs.
+template <int BN_> struct Cfg {
+  static constexpr int BN = BN_;
+  static constexpr int B_BYTES = BN * BK * 4;
+  static constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
+  static constexpr int STAGE_BYTES = 2 * (A_BYTES + B_BYTES);   // a multiple of 1 KB
+  static constexpr int STAGES = (4 * STAGE_BYTES <= 212 * 1024) ? 4 : 3;
+  static constexpr int TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + BAR_BYTES + 1024;   // + alignment slack
+  static_assert(BN % 16 == 0 && BN <= 256, "UMMA N for M = 128");
+  static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
+};
 
 __device__ int g_tc_error = 0;
 
@@ -116,14 +126,11 @@ __device__ __forceinline__ void mma_commit(uint64_t *bar) {
                : "memory");
 }
 
-#define TMEM_LD32(taddr, r)                                                                                          \
+#define TMEM_LD16(taddr, r)                                                                                          \
   asm volatile(                                                                                                      \
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19," \
-      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                                     \
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"      \
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),   \
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),       \
-        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),      \
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                    \
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])                     \
       : "r"(taddr))
 
 struct TcArgs {
@@ -156,15 +163,19 @@ __device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int n16, int 
 // A_MN: A stored with M contiguous (A[k*lda + m]); else K contiguous
 // (A[m*lda + k]).  B_MN: B stored with N contiguous (B[k*ldb + n]); else K
 // contiguous (B[n*ldb + k]).
-template <bool A_MN, bool B_MN>
+template <bool A_MN, bool B_MN, int BN_>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs p) {
+  typedef Cfg<BN_> G;
+  constexpr int BN = G::BN, STAGES = G::STAGES, STAGE_BYTES = G::STAGE_BYTES;
+  constexpr int B_BYTES = G::B_BYTES, OFF_AH = G::OFF_AH, OFF_AL = G::OFF_AL, OFF_BH = G::OFF_BH, OFF_BL = G::OFF_BL;
   extern __shared__ __align__(1024) uint8_t smraw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = (uint64_t *)(sm + (size_t)STAGES * STAGE_BYTES);
   uint64_t *full = bars, *conv = bars + STAGES, *empty = bars + 2 * STAGES, *accb = bars + 3 * STAGES;
   uint32_t *tmem_slot = (uint32_t *)(bars + 3 * STAGES + 1);
   __shared__ volatile int abort_flag;
+  __shared__ float sb0[BN], sb1[BN];   // B(0, n), B(1, n) of the tile (Gamma-metric epilogue)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -184,7 +195,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
-                 "r"(TMEM_COLS));
+                 "r"(G::TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -221,7 +232,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
-      // kind::tf32, D F32, M = 128, N = 160
+      // kind::tf32, D F32, M = 128, N = BN
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((A_MN ? 1u : 0u) << 15) |
                              ((B_MN ? 1u : 0u) << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
       for (int kb = 0; kb < nkb; ++kb) {
@@ -266,41 +277,56 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_arrive(&conv[s]);
     }
     // ---------------- epilogue ----------------
-    const bool ok = mbar_wait(accb, 0, 5) && !abort_flag;
-    asm volatile("tcgen05.fence::after_thread_sync;");
+    const bool direct = (p.W == nullptr);
+    if (direct && p.gamma) {
+      for (int j = t; j < BN; j += 128) {
+        const int gn = n0 + j;
+        sb0[j] = (gn < p.N) ? (B_MN ? p.B[gn] : p.B[(long)gn * p.ldb]) : 0.f;
+        sb1[j] = (gn < p.N) ? (B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1]) : 0.f;
+      }
+    }
+    asm volatile("bar.sync 1, 128;" ::: "memory");   // the four epilogue warps
     const int quad = warp & 3;
     const int gm = m0 + quad * 32 + lane;
     float a0 = 0.f, a1 = 0.f;
-    if (ok && p.W == nullptr && p.gamma && gm < p.M) {
+    if (direct && p.gamma && gm < p.M) {
       a0 = A_MN ? p.A[gm] : p.A[(long)gm * p.lda];
       a1 = A_MN ? p.A[p.lda + gm] : p.A[(long)gm * p.lda + 1];
     }
+    const bool ok = mbar_wait(accb, 0, 5) && !abort_flag;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const float alpha = p.alpha, beta = p.beta;
 #pragma unroll 1
-    for (int c = 0; c < BN / 32; ++c) {
-      uint32_t r[32];
-      const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 32);
-      TMEM_LD32(taddr, r);
+    for (int c = 0; c < BN / 16; ++c) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 16);
+      TMEM_LD16(taddr, r);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (!ok || gm >= p.M) continue;
+      const int nb = n0 + c * 16;
+      if (!direct) {
+        float *w = p.W + ((long)blockIdx.z * p.N + nb) * p.M + gm;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int gn = n0 + c * 32 + j;
-        if (gn >= p.N) break;
+        for (int j = 0; j < 16; ++j)
+          if (nb + j < p.N) w[(long)j * p.M] = __uint_as_float(r[j]);
+        continue;
+      }
+      float *cp = p.C + (long)nb * p.ldc + gm;
+      float old[16];
+      if (beta != 0.f) {
+        // issue every load of the chunk before the first store
+#pragma unroll
+        for (int j = 0; j < 16; ++j) old[j] = (nb + j < p.N) ? cp[(long)j * p.ldc] : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        if (nb + j >= p.N) break;
         float v = __uint_as_float(r[j]);
-        if (p.W) {
-          p.W[((long)blockIdx.z * p.N + gn) * p.M + gm] = v;
-          continue;
-        }
         if (p.gamma) {
-          const float b0 = B_MN ? p.B[gn] : p.B[(long)gn * p.ldb];
-          v = 2.f * v - a0 * b0;
-          if (p.gamma == 2) {
-            const float b1 = B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1];
-            v -= 2.f * a1 * b1;
-          }
+          v = 2.f * v - a0 * sb0[c * 16 + j];
+          if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
         }
-        float *cp = p.C + (long)gn * p.ldc + gm;
-        *cp = (p.beta == 0.f) ? p.alpha * v : p.alpha * v + p.beta * *cp;
+        cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
       }
     }
   }
@@ -308,7 +334,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::TMEM_COLS));
   }
 }
 
@@ -316,7 +342,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 // Host side.
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 static std::once_flag g_once;
-static bool g_attr_done[4] = {false, false, false, false};
 
 static bool encode_ready() {
   std::call_once(g_once, [] {
@@ -355,16 +380,16 @@ static bool enabled() {
   return en == 1;
 }
 
-template <bool A_MN, bool B_MN>
+template <bool A_MN, bool B_MN, int BN>
 static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs &a, dim3 g, cudaStream_t st) {
-  const int idx = (A_MN ? 2 : 0) + (B_MN ? 1 : 0);
-  if (!g_attr_done[idx]) {
-    if (cudaFuncSetAttribute(k_tc_gemm<A_MN, B_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES) !=
-        cudaSuccess)
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_tc_gemm<A_MN, B_MN, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Cfg<BN>::SMEM_BYTES) != cudaSuccess)
       return 1;
-    g_attr_done[idx] = true;
+    attr = true;
   }
-  k_tc_gemm<A_MN, B_MN><<<g, NTHREADS, SMEM_BYTES, st>>>(ma, mb, a);
+  k_tc_gemm<A_MN, B_MN, BN><<<g, NTHREADS, Cfg<BN>::SMEM_BYTES, st>>>(ma, mb, a);
   note_launch();
   return 0;
 }
@@ -379,22 +404,25 @@ bool tc_enabled() { return tc::enabled(); }
 int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
             float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes) {
   using tc::BM;
-  using tc::BN;
   using tc::BK;
   if (!tc::enabled() || M <= 0 || N <= 0 || K <= 0) return -1;
   if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (lda & 3) || (ldb & 3)) return -1;
   if (!tc::encode_ready()) return -1;
   // A: ta -> K contiguous (A[m*lda + k]); !ta -> M contiguous (A[k*lda + m])
   const bool a_mn = !ta, b_mn = tb;
+  const int tm = (M + BM - 1) / BM, nkb = (K + BK - 1) / BK;
+  // 80-wide tiles when 160-wide ones leave most SMs idle (MN-major B tiles
+  // come in 32-column chunks, so they keep 160)
+  const int bn = (!b_mn && (N <= 80 || (long)tm * ((N + 159) / 160) < 120)) ? 80 : 160;
+  const int tn = (N + bn - 1) / bn;
   CUtensorMap ma, mb;
   if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, true) : tc::make_map(&ma, A, K, M, lda, BM, false))) return -1;
-  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, true) : tc::make_map(&mb, B, K, N, ldb, BN, false))) return -1;
-  const int tm = (M + BM - 1) / BM, tn = (N + BN - 1) / BN, nkb = (K + BK - 1) / BK;
-  // split K until the grid covers the SMs about twice, at least 4 k-blocks a split
+  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, true) : tc::make_map(&mb, B, K, N, ldb, bn, false))) return -1;
+  // split K until the grid covers the SMs, at least 8 k-blocks a split
   int nsplit = 1;
   const long tiles = (long)tm * tn;
-  if (ws && tiles < 148) {
-    nsplit = (int)std::min<long>((2 * 148 + tiles - 1) / tiles, std::max(1, nkb / 4));
+  if (ws && tiles < 100) {
+    nsplit = (int)std::min<long>((148 + tiles - 1) / tiles, std::max(1, nkb / 8));
     while (nsplit > 1 && (size_t)nsplit * M * N * sizeof(float) > ws_bytes) --nsplit;
   }
   const int kps = (nkb + nsplit - 1) / nsplit;
@@ -402,10 +430,15 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr};
   dim3 g(tm, tn, nsplit);
   int rc;
-  if (a_mn && b_mn) rc = tc::launch_tc<true, true>(ma, mb, a, g, st);
-  else if (a_mn) rc = tc::launch_tc<true, false>(ma, mb, a, g, st);
-  else if (b_mn) rc = tc::launch_tc<false, true>(ma, mb, a, g, st);
-  else rc = tc::launch_tc<false, false>(ma, mb, a, g, st);
+  if (bn == 160) {
+    if (a_mn && b_mn) rc = tc::launch_tc<true, true, 160>(ma, mb, a, g, st);
+    else if (a_mn) rc = tc::launch_tc<true, false, 160>(ma, mb, a, g, st);
+    else if (b_mn) rc = tc::launch_tc<false, true, 160>(ma, mb, a, g, st);
+    else rc = tc::launch_tc<false, false, 160>(ma, mb, a, g, st);
+  } else {
+    if (a_mn) rc = tc::launch_tc<true, false, 80>(ma, mb, a, g, st);
+    else rc = tc::launch_tc<false, false, 80>(ma, mb, a, g, st);
+  }
   if (rc) return rc;
   if (nsplit > 1)
     gemm_reduce_f32(ta, tb, M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, (const float *)ws, st);
