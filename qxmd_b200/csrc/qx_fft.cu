@@ -19,6 +19,7 @@
 // and xrho.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "qx_internal.h"
 
@@ -703,6 +704,17 @@ static FftTabs<T> tabs(const Plan &pl, int d) {
   return t;
 }
 
+// The fused register-FFT plane pass is on unless QX_PLANE=0 (kept to compare
+// against the shared-memory passes).
+static bool plane_enabled() {
+  static int en = -1;
+  if (en < 0) {
+    const char *e = getenv("QX_PLANE");
+    en = (e && e[0] == '0') ? 0 : 1;
+  }
+  return en == 1;
+}
+
 template <typename T>
 int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
                       const double *dk, int accumulate, int nlmode, cudaStream_t st) {
@@ -715,6 +727,13 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
   dim3 gy(P.k3, npl);
   const size_t smy = fft_smem(P.L2, P.P1, cs);
+  if (sizeof(T) == sizeof(float) && nlmode != 2 && plane_enabled() &&
+      launch_plane_f32(P, npl, (float2 *)bf.bufA, (const float *)bf.vloc, st) == 0) {
+    dim3 gu((P.nplw + 1 + 127) / 128, npl);
+    k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
+    k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
+    return 0;
+  }
   k_ypass<T, +1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
   const int nlines = pl.xlines<T>();
   const int nch = (P.k2 + nlines - 1) / nlines;

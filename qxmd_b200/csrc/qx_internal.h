@@ -90,6 +90,9 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
 template <typename T> void set_fft_smem_limits(size_t bytes);
+// qx_fftplane.cu: fused y-x-y pass (FP32, k1 == k2 of a specialised length);
+// returns -1 when the grid is not covered.
+int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st);
 template <typename T> size_t fft_smem_need(const Plan &pl);
 int init_fft_roots();
 

@@ -8,12 +8,12 @@
 // shared-memory ring, products on the 5th-generation tensor cores
 // (tcgen05.mma kind::tf32, 128 x 160 or 128 x 80 tile, accumulator in TMEM), read back
 // with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
-// is cut into x_hi = x with the low 13 mantissa bits cleared and
-// x_lo = x - x_hi (exact in FP32), and the tile product is
+// is cut into x_hi = x rounded to the nearest TF32 value and x_lo = x - x_hi
+// rounded the same way, and the tile product is
 // A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 (relative error about
-// 2^-21 per product).  The split is done in shared memory by the epilogue
-// warps between the TMA landing and the MMA issue, so HBM traffic is that of
-// a plain FP32 GEMM.
+// 2^-22 per product, unbiased because both parts are rounded to nearest).
+// The split is done in shared memory by the epilogue warps between the TMA
+// landing and the MMA issue, so HBM traffic is that of a plain FP32 GEMM.
 //
 // Warp roles (192 threads): warp 0 issues TMA, warp 1 allocates TMEM and
 // issues the MMAs (one elected lane), warps 2-5 split the operands and run
@@ -147,14 +147,27 @@ struct TcArgs {
   float *W;              // split-K partials W[z][n][m], or null: write C
 };
 
+// Round to the nearest TF32 value (10 stored mantissa bits; ties away from
+// zero), by integer arithmetic on the bit pattern.  Values stored this way
+// pass through the tensor core's TF32 read unchanged.
+__device__ __forceinline__ float tf32_rn(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+// x = hi + lo with hi = tf32_rn(x) and lo = tf32_rn(x - hi): both exact TF32
+// values, |lo| <= 2^-11 |hi|, and the dropped part is below 2^-22 |x| with
+// either sign, so the three-product sum carries no truncation bias.
+__device__ __forceinline__ void split1(float x, float &h, float &l) {
+  h = tf32_rn(x);
+  l = tf32_rn(x - h);
+}
 __device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int n16, int t) {
   for (int i = t; i < n16; i += 128) {
     const float4 x = hi[i];
     float4 h, l;
-    h.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u); l.x = x.x - h.x;
-    h.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u); l.y = x.y - h.y;
-    h.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u); l.z = x.z - h.z;
-    h.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u); l.w = x.w - h.w;
+    split1(x.x, h.x, l.x);
+    split1(x.y, h.y, l.y);
+    split1(x.z, h.z, l.z);
+    split1(x.w, h.w, l.w);
     hi[i] = h;
     lo[i] = l;
   }
