@@ -10,6 +10,10 @@
 
 namespace qx {
 
+// One CTA per band; 1024 threads give each SM enough loads in flight for
+// these bandwidth-bound sweeps over a band.
+constexpr int CGT = 1024;
+
 template <typename T>
 __device__ __forceinline__ double ld(const T *p, long i) { return (double)p[i]; }
 
@@ -23,9 +27,9 @@ __device__ double bdot(const T *x, const T *y, int ne, double *red) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_cg_init(int ne, long ldx, const T *__restrict__ x,
+__global__ void __launch_bounds__(CGT) k_cg_init(int ne, long ldx, const T *__restrict__ x,
                                                          const T *__restrict__ hx, T *__restrict__ g, CgState s) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   const T *xb = x + b * ldx, *hb = hx + b * ldx;
   T *gb = g + b * ldx;
@@ -56,9 +60,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_cg_init(int ne, long ldx, const 
 
 // g <- prcd * g; zansap = <g|g>; h <- g + beta*h (h <- g on reset).
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_cg_prec(int ne, long ldx, T *__restrict__ g, T *__restrict__ h,
+__global__ void __launch_bounds__(CGT) k_cg_prec(int ne, long ldx, T *__restrict__ g, T *__restrict__ h,
                                                          const double *__restrict__ dk, CgState s) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   if (!s.active[b]) return;
   T *gb = g + b * ldx, *hb = h + b * ldx;
@@ -100,9 +104,9 @@ __global__ void k_cg_mask(int nb, T *__restrict__ Pm, CgState s) {
 
 // subgs4: h -= <x|h> x; cai = <h|hx>.
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_cg_orth(int ne, long ldx, const T *__restrict__ x,
+__global__ void __launch_bounds__(CGT) k_cg_orth(int ne, long ldx, const T *__restrict__ x,
                                                          const T *__restrict__ hx, T *__restrict__ h, CgState s) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   if (!s.active[b]) return;
   const T *xb = x + b * ldx, *hxb = hx + b * ldx;
@@ -118,16 +122,24 @@ __global__ void __launch_bounds__(QX_THREADS) k_cg_orth(int ne, long ldx, const 
   if (threadIdx.x == 0) s.cai[b] = 2.0 * c - ld(hb, 0) * ld(hxb, 0);
 }
 
-// Active-band list and the band pairs of the FFT pipeline.
+// Active-band list and the band pairs of the FFT pipeline: one warp compacts
+// 32 bands per round with a ballot and a population-count prefix.
 __global__ void k_cg_list(int nb, CgState s) {
-  if (threadIdx.x == 0) {
-    int n = 0;
-    for (int b = 0; b < nb; ++b)
-      if (s.active[b]) s.list[n++] = b;
-    for (int p = 0; p < (n + 1) / 2; ++p) {
-      s.pairs[2 * p] = s.list[2 * p];
-      s.pairs[2 * p + 1] = (2 * p + 1 < n) ? s.list[2 * p + 1] : -1;
-    }
+  const int lane = threadIdx.x & 31;
+  int n = 0;
+  for (int b0 = 0; b0 < nb; b0 += 32) {
+    const int b = b0 + lane;
+    const bool act = (b < nb) && s.active[b];
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    if (act) s.list[n + __popc(m & ((1u << lane) - 1u))] = b;
+    n += __popc(m);
+  }
+  __syncwarp();
+  for (int p = lane; p < (n + 1) / 2; p += 32) {
+    s.pairs[2 * p] = s.list[2 * p];
+    s.pairs[2 * p + 1] = (2 * p + 1 < n) ? s.list[2 * p + 1] : -1;
+  }
+  if (lane == 0) {
     *s.nact = n;
     *s.npair = (n + 1) / 2;
   }
@@ -136,10 +148,10 @@ __global__ void k_cg_list(int nb, CgState s) {
 // BKL 2x2 step (eigen.f90:593-622), line minimisation fallback (624-695),
 // x/hx update (698-709), residual and convergence test (731-764).
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
+__global__ void __launch_bounds__(CGT) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
                                                            T *__restrict__ g, const T *__restrict__ h,
                                                            const T *__restrict__ gh, CgState s, CgParm pm) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   if (!s.active[b]) return;
   T *xb = x + b * ldx, *hxb = hx + b * ldx, *gb = g + b * ldx;
@@ -224,9 +236,9 @@ __global__ void __launch_bounds__(QX_THREADS) k_cg_update(int ne, long ldx, T *_
 // ekinetic2 (engrad.f90:75-127): ekib(b) = 2*<c|T|c>, and sum occ*<c|T|c>
 // into *ekin (one CTA per band writes its term; summed by k_sum_occ).
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_ekin(int ne, long ldx, const T *__restrict__ x,
+__global__ void __launch_bounds__(CGT) k_ekin(int ne, long ldx, const T *__restrict__ x,
                                                       const double *__restrict__ dk, double *__restrict__ ekib) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   const T *xb = x + b * ldx;
   double s = 0.0;
@@ -237,10 +249,10 @@ __global__ void __launch_bounds__(QX_THREADS) k_ekin(int ne, long ldx, const T *
 
 // gradresnv (engrad.f90:1013-1067): per-band |eig*c - hc|^2 (Gamma metric).
 template <typename T>
-__global__ void __launch_bounds__(QX_THREADS) k_gradres(int ne, long ldx, const T *__restrict__ x,
+__global__ void __launch_bounds__(CGT) k_gradres(int ne, long ldx, const T *__restrict__ x,
                                                          const T *__restrict__ hx, const double *__restrict__ eig,
                                                          double *__restrict__ prod) {
-  __shared__ double red[QX_THREADS / 32];
+  __shared__ double red[CGT / 32];
   const int b = blockIdx.x;
   const T *xb = x + b * ldx, *hb = hx + b * ldx;
   const double e = eig[b];
@@ -269,29 +281,29 @@ __global__ void k_scale_rows(int nproj, int ncol, T *__restrict__ P, long ldp, c
 
 // ---- launchers -------------------------------------------------------------
 template <typename T> void cg_init(int nb, int ne, long ldx, const T *x, const T *hx, T *g, const CgState &s, cudaStream_t st) {
-  k_cg_init<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, s); note_launch();
+  k_cg_init<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, s); note_launch();
 }
 template <typename T> void cg_prec(int nb, int ne, long ldx, T *g, T *h, const double *dk, const CgState &s, cudaStream_t st) {
-  k_cg_prec<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, g, h, dk, s); note_launch();
+  k_cg_prec<T><<<nb, CGT, 0, st>>>(ne, ldx, g, h, dk, s); note_launch();
 }
 template <typename T> void cg_mask(int nb, T *Pm, const CgState &s, cudaStream_t st) {
   const long nn = (long)nb * nb;
   k_cg_mask<T><<<(int)((nn + 255) / 256), 256, 0, st>>>(nb, Pm, s); note_launch();
 }
 template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T *hx, T *h, const CgState &s, cudaStream_t st) {
-  k_cg_orth<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, h, s); note_launch();
+  k_cg_orth<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, h, s); note_launch();
 }
 void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); note_launch(); }
 template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
                                      const CgState &s, const CgParm &pm, cudaStream_t st) {
-  k_cg_update<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm); note_launch();
+  k_cg_update<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm); note_launch();
 }
 template <typename T> void ekin(int nb, int ne, long ldx, const T *x, const double *dk, double *ekib, cudaStream_t st) {
-  k_ekin<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, dk, ekib); note_launch();
+  k_ekin<T><<<nb, CGT, 0, st>>>(ne, ldx, x, dk, ekib); note_launch();
 }
 template <typename T> void gradres(int nb, int ne, long ldx, const T *x, const T *hx, const double *eig, double *prod,
                                    cudaStream_t st) {
-  k_gradres<T><<<nb, QX_THREADS, 0, st>>>(ne, ldx, x, hx, eig, prod); note_launch();
+  k_gradres<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, eig, prod); note_launch();
 }
 template <typename T> void scale_rows(int nproj, int ncol, T *P, long ldp, const T *v, const int *colmap,
                                       const int *ncol_dev, cudaStream_t st) {

@@ -32,31 +32,47 @@ constexpr int CHT = 256;            // threads of k_cholinv (8 warps)
 constexpr int DLD = CB + 1;         // leading dimension of the 32 x 32 temporary
 constexpr size_t CH_SMEM_MAX = 220 * 1024;
 
+// 1/sqrt(x): the hardware's approximate reciprocal square root refined by
+// two Newton-Raphson steps y <- y (3 - x y^2) / 2, each doubling the number
+// of correct bits, to full double precision.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = y * (1.5 - 0.5 * x * y * y);
+  y = y * (1.5 - 0.5 * x * y * y);
+  return y;
+}
+
 // Cholesky of the bs x bs diagonal block at B (leading dimension ld) in
-// registers: lane i holds row i, column k of L is broadcast by shuffles.
-// Writes L (lower triangle, diagonal included).  Returns the first row whose
-// pivot is not > 1e-30, or -1.  Called by one whole warp.
-__device__ __forceinline__ int warp_chol(double *B, int ld, int bs, int lane) {
+// registers: lane i holds row i; column k of L is broadcast through the
+// 32-double shared buffer cb (cheaper than 31 shuffles of doubles per step).
+// Writes L (lower triangle, diagonal included) and 1/L(k,k) to rd[k].
+// Returns the first row whose pivot is not > 1e-30, or -1.  One whole warp.
+__device__ __forceinline__ int warp_chol(double *B, int ld, int bs, int lane, double *rd, double *cb) {
   double r[CB];
 #pragma unroll
   for (int j = 0; j < CB; ++j) r[j] = (lane < bs && j < bs && j <= lane) ? B[(long)j * ld + lane] : 0.0;
+  // no early exit: a break would keep the loop from unrolling and r[] from
+  // staying in registers; after a failed pivot the remaining steps are skipped
   int bad = -1;
 #pragma unroll
   for (int k = 0; k < CB; ++k) {
-    if (k < bs) {
+    if (k < bs && bad < 0) {
       const double piv = __shfl_sync(0xffffffffu, r[k], k);
       if (!(piv > 1.0e-30)) {   // uniform; also catches NaN
         bad = k;
-        break;
+        continue;
       }
-      const double sq = sqrt(piv), rs = 1.0 / sq;
-      const double lik = (lane == k) ? sq : r[k] * rs;   // l_ik for lanes i > k
+      const double rs = rsqrt_nr(piv);
+      const double lik = (lane == k) ? piv * rs : r[k] * rs;   // L(k,k) on lane k, l_ik below
       r[k] = lik;
+      if (lane == k) rd[k] = rs;
+      cb[lane] = lik;
+      __syncwarp();
 #pragma unroll
-      for (int j = k + 1; j < CB; ++j) {
-        const double ljk = __shfl_sync(0xffffffffu, lik, j);
-        if (lane >= j) r[j] -= lik * ljk;
-      }
+      for (int j = k + 1; j < CB; ++j)
+        if (lane >= j) r[j] -= lik * cb[j];
+      __syncwarp();
     }
   }
   if (bad < 0 && lane < bs) {
@@ -70,9 +86,10 @@ __device__ __forceinline__ int warp_chol(double *B, int ld, int bs, int lane) {
 
 // X = L^-1 of the lower-triangular bs x bs block at L (leading dimension ldl)
 // into X (leading dimension ldx; may equal L), lane j producing column j by
-// forward substitution with L's rows read as broadcasts.  Zeros above the
-// diagonal.  Called by one whole warp.
-__device__ __forceinline__ void warp_trinv(const double *L, int ldl, double *X, int ldx, int bs, int lane) {
+// forward substitution with L's rows read as broadcasts and the diagonal
+// reciprocals rd[].  Zeros above the diagonal.  One whole warp.
+__device__ __forceinline__ void warp_trinv(const double *L, int ldl, const double *rd, double *X, int ldx, int bs,
+                                           int lane) {
   double x[CB];
 #pragma unroll
   for (int i = 0; i < CB; ++i) {
@@ -80,7 +97,7 @@ __device__ __forceinline__ void warp_trinv(const double *L, int ldl, double *X, 
     if (i < bs) {
 #pragma unroll
       for (int k = 0; k < i; ++k) s -= L[(long)k * ldl + i] * x[k];
-      x[i] = s / L[(long)i * ldl + i];
+      x[i] = s * rd[i];
     } else {
       x[i] = 0.0;
     }
@@ -101,13 +118,13 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   const int ld = use_smem ? (n | 1) : n;
   double *A = use_smem ? sm : Sg;
   double *T = use_smem ? sm + (long)ld * n : work;   // CB x DLD temporary
+  double *rd = T + CB * DLD;                         // n reciprocal pivots
+  __shared__ double cb[CB];                          // column broadcast of warp_chol
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = CHT / 32;
 #define A_(i, j) A[(long)(j) * ld + (i)]
   if (use_smem)
-    for (long q = tid; q < (long)n * n; q += CHT) {
-      const int j = (int)(q / n), i = (int)(q - (long)j * n);
-      A_(i, j) = Sg[q];
-    }
+    for (int j = warp; j < n; j += nw)
+      for (int i = lane; i < n; i += 32) A_(i, j) = Sg[(long)j * n + i];
   if (tid == 0) bad = 0;
   __syncthreads();
   const int nblk = (n + CB - 1) / CB;
@@ -115,36 +132,58 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   for (int J = 0; J < nblk; ++J) {
     const int j0 = J * CB, bs = min(CB, n - j0);
     if (warp == 0) {
-      const int b = warp_chol(&A_(j0, j0), ld, bs, lane);
+      const int b = warp_chol(&A_(j0, j0), ld, bs, lane, rd + j0, cb);
       if (b >= 0) {
         if (lane == 0) bad = 1 + j0 + b;
       } else if (j0 + bs < n) {
-        warp_trinv(&A_(j0, j0), ld, T, DLD, bs, lane);   // Linv_JJ for the panel
+        warp_trinv(&A_(j0, j0), ld, rd + j0, T, DLD, bs, lane);   // Linv_JJ for the panel
       }
     }
     __syncthreads();
     if (bad) break;
     const int r0 = j0 + bs, mr = n - r0;
     if (mr <= 0) break;
-    // panel: L(r, j0+c) = sum_{k <= c} A(r, j0+k) Linv_JJ(c, k)
-    for (int r = r0 + warp; r < n; r += nw) {
-      const double a = (lane < bs) ? A_(r, j0 + lane) : 0.0;
-      double s = 0.0;
-      for (int k = 0; k < bs; ++k) {
-        const double ak = __shfl_sync(0xffffffffu, a, k);
-        s += ak * ((k <= lane) ? T[k * DLD + lane] : 0.0);
+    // panel: L(r, j0+c) = sum_{k <= c} A(r, j0+k) Linv_JJ(c, k), lane = row
+    for (int rc = r0 + warp * 32; rc < n; rc += nw * 32) {
+      const int r = rc + lane;
+      if (r < n) {
+        double a[CB];
+#pragma unroll
+        for (int k = 0; k < CB; ++k) a[k] = (k < bs) ? A_(r, j0 + k) : 0.0;
+#pragma unroll
+        for (int c = 0; c < CB; ++c) {
+          if (c < bs) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k <= c; ++k) s += a[k] * T[k * DLD + c];
+            A_(r, j0 + c) = s;
+          }
+        }
       }
-      __syncwarp();
-      if (lane < bs) A_(r, j0 + lane) = s;
     }
     __syncthreads();
-    // trailing update of the lower triangle: A(r, c) -= sum_k L(r, j0+k) L(c, j0+k)
-    for (int c = warp; c < mr; c += nw)
-      for (int r = c + lane; r < mr; r += 32) {
-        double s = 0.0;
-        for (int k = 0; k < bs; ++k) s += A_(r0 + r, j0 + k) * A_(r0 + c, j0 + k);
-        A_(r0 + r, r0 + c) -= s;
+    // trailing update of the lower triangle, 32 x 32 tiles (row chunk qi,
+    // column chunk qj <= qi): A(r, c) -= sum_k L(r, j0+k) L(c, j0+k), lane = row
+    const int nq = (mr + 31) / 32;
+    for (int tile = warp; tile < nq * (nq + 1) / 2; tile += nw) {
+      int qi = 0;
+      while ((qi + 1) * (qi + 2) / 2 <= tile) ++qi;
+      const int qj = tile - qi * (qi + 1) / 2;
+      const int r = qi * 32 + lane;
+      double a[CB];
+#pragma unroll
+      for (int k = 0; k < CB; ++k) a[k] = (r < mr && k < bs) ? A_(r0 + r, j0 + k) : 0.0;
+      const int cend = min(qj * 32 + 32, mr);
+      for (int c = qj * 32; c < cend; ++c) {
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < CB; k += 2) {
+          s0 += a[k] * A_(r0 + c, j0 + k);
+          s1 += a[k + 1] * A_(r0 + c, j0 + k + 1);
+        }
+        if (r < mr && r >= c) A_(r0 + r, r0 + c) -= s0 + s1;
       }
+    }
     __syncthreads();
   }
   if (bad) {
@@ -159,48 +198,53 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   // diagonal blocks in place, one warp each
   for (int J = warp; J < nblk; J += nw) {
     const int j0 = J * CB;
-    warp_trinv(&A_(j0, j0), ld, &A_(j0, j0), ld, min(CB, n - j0), lane);
+    warp_trinv(&A_(j0, j0), ld, rd + j0, &A_(j0, j0), ld, min(CB, n - j0), lane);
   }
   __syncthreads();
   // row blocks top-down, column blocks left to right, in place:
   // X_IJ = -X_II * sum_{K=J}^{I-1} L_IK X_KJ  (L_IK, K >= J, not yet overwritten)
+  // lane = row ii, warp = columns jj = warp + 8 u (u < 4)
   for (int I = 1; I < nblk; ++I) {
     const int i0 = I * CB, bi = min(CB, n - i0);
     for (int J = 0; J < I; ++J) {
       const int j0 = J * CB;
-      for (int jj = warp; jj < CB; jj += nw) {
-        const int ii = lane;
-        double s = 0.0;
-        if (ii < bi)
-          for (int k = j0; k < i0; ++k) s += A_(i0 + ii, k) * A_(k, j0 + jj);
-        T[jj * DLD + ii] = s;
+      {
+        double acc[CB / (CHT / 32)] = {};
+        if (lane < bi)
+          for (int k = j0; k < i0; ++k) {
+            const double a = A_(i0 + lane, k);
+#pragma unroll
+            for (int u = 0; u < CB / (CHT / 32); ++u) acc[u] += a * A_(k, j0 + warp + u * nw);
+          }
+#pragma unroll
+        for (int u = 0; u < CB / (CHT / 32); ++u) T[(warp + u * nw) * DLD + lane] = acc[u];
       }
       __syncthreads();
-      for (int jj = warp; jj < CB; jj += nw) {
-        const int ii = lane;
-        if (ii < bi) {
-          double s = 0.0;
-          for (int k = 0; k <= ii; ++k) s += A_(i0 + ii, i0 + k) * T[jj * DLD + k];
-          A_(i0 + ii, j0 + jj) = -s;
+      if (lane < bi) {
+        double acc[CB / (CHT / 32)] = {};
+        for (int k = 0; k <= lane; ++k) {
+          const double a = A_(i0 + lane, i0 + k);
+#pragma unroll
+          for (int u = 0; u < CB / (CHT / 32); ++u) acc[u] += a * T[(warp + u * nw) * DLD + k];
         }
+#pragma unroll
+        for (int u = 0; u < CB / (CHT / 32); ++u) A_(i0 + lane, j0 + warp + u * nw) = -acc[u];
       }
       __syncthreads();
     }
   }
   if (use_smem)
-    for (long q = tid; q < (long)n * n; q += CHT) {
-      const int j = (int)(q / n), i = (int)(q - (long)j * n);
-      Sg[q] = A_(i, j);
-    }
+    for (int j = warp; j < n; j += nw)
+      for (int i = lane; i < n; i += 32) Sg[(long)j * n + i] = A_(i, j);
 #undef A_
   if (tid == 0) *info = 0;
 }
 
 // S: n x n column-major.  When S does not fit shared memory the kernel works
-// in S itself (L2-resident) and uses work (>= CB*DLD doubles) as temporary.
+// in S itself (L2-resident) and uses work (>= CB*DLD + n doubles) as temporary.
 int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
   if (n > 8192) { set_error("cholinv: n=%d too large", n); return 1; }
-  const size_t bytes = sizeof(double) * ((size_t)(n | 1) * n + CB * DLD);
+  const size_t bytes = sizeof(double) * ((size_t)(n | 1) * n + CB * DLD + n);
   const int use = bytes <= CH_SMEM_MAX;
   static bool attr = false;
   if (!attr) {
@@ -231,19 +275,32 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
 constexpr int TRD_T = 1024;
 constexpr size_t TRD_SMEM_MAX = 222 * 1024;
 
+// 1/x to full double precision: approximate reciprocal and two Newton-Raphson
+// steps r <- r (2 - x r).
+__device__ __forceinline__ double recip2_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  r = r * fma(-x, r, 2.0);
+  return r * fma(-x, r, 2.0);
+}
+
 // Householder reflector of x (GVL house): P = I - tau v v^T, v(0) = 1,
-// P x = |x| e1.  Returns tau, writes beta (v = x / beta for i >= 1) and |x|.
-__device__ __forceinline__ void house(double x0, double sigma, double &tau, double &beta, double &alpha) {
+// P x = |x| e1.  Returns tau, writes 1/beta (v = x / beta for i >= 1) and
+// |x|.  Square root and divisions by Newton-refined hardware approximations
+// (rsqrt_nr, recip2_nr): this is on the critical path of every column.
+__device__ __forceinline__ void house(double x0, double sigma, double &tau, double &rbeta, double &alpha) {
   if (sigma == 0.0) {
     tau = (x0 < 0.0) ? 2.0 : 0.0;
-    beta = 1.0;
+    rbeta = 1.0;
     alpha = fabs(x0);
     return;
   }
-  const double mu = sqrt(x0 * x0 + sigma);
-  const double v1 = (x0 <= 0.0) ? x0 - mu : -sigma / (x0 + mu);
-  tau = 2.0 * v1 * v1 / (sigma + v1 * v1);
-  beta = v1;
+  const double s2 = x0 * x0 + sigma;
+  const double mu = s2 * rsqrt_nr(s2);
+  const double v1 = (x0 <= 0.0) ? x0 - mu : -sigma * recip2_nr(x0 + mu);
+  const double v1s = v1 * v1;
+  tau = 2.0 * v1s * recip2_nr(sigma + v1s);
+  rbeta = recip2_nr(v1);
   alpha = mu;
 }
 
@@ -284,10 +341,10 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
       double sg = 0.0;
       for (int i = 1 + lane; i < m; i += 32) { const double x = A_(k + 1 + i, k); sg += x * x; }
       sg = warp_sum(sg);
-      double t = 0.0, be = 1.0, al = 0.0;
-      if (lane == 0) house(A_(k + 1, k), sg, t, be, al);
+      double t = 0.0, rb = 1.0, al = 0.0;
+      if (lane == 0) house(A_(k + 1, k), sg, t, rb, al);
       t = __shfl_sync(0xffffffffu, t, 0);
-      const double rbe = 1.0 / __shfl_sync(0xffffffffu, be, 0);
+      const double rbe = __shfl_sync(0xffffffffu, rb, 0);
       for (int i = lane; i < m; i += 32) {
         const double vi = (i == 0) ? 1.0 : ((t != 0.0) ? A_(k + 1 + i, k) * rbe : 0.0);
         v[i] = vi;
@@ -306,11 +363,17 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
     const int nrb = (m + 31) >> 5;
     for (int task = warp; task < nrb * NG; task += NW) {
       const int rb = task / NG, g = task - rb * NG, i = rb * 32 + lane;
-      double s = 0.0;
       if (i < m) {
-        const double *col = &A_(k + 1 + i, k + 1);
-        for (int j = g; j < m; j += NG) s += col[(long)j * ld] * v[j];
-        part[g * n + i] = s;
+        const double *__restrict__ col = &A_(k + 1 + i, k + 1);
+        const double *__restrict__ vv = v;
+        double s0 = 0.0, s1 = 0.0;
+        int j = g;
+        for (; j + NG < m; j += 2 * NG) {
+          s0 += col[(long)j * ld] * vv[j];
+          s1 += col[(long)(j + NG) * ld] * vv[j + NG];
+        }
+        if (j < m) s0 += col[(long)j * ld] * vv[j];
+        part[g * n + i] = s0 + s1;
       }
     }
     __syncthreads();                                   // (2)
@@ -319,12 +382,32 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
     double kk = 0.0;
     for (int i = lane; i < m; i += 32) kk += v[i] * p[i];
     const double K = 0.5 * t * warp_sum(kk);
-    for (int j = warp; j < m; j += NW) {
+    // rows of this lane: i = lane + 32 q; their v and w in registers when
+    // m <= 32 * RQ, otherwise reloaded per column
+    constexpr int RQ = 6;
+    double vi[RQ], wi[RQ];
+#pragma unroll
+    for (int q = 0; q < RQ; ++q) {
+      const int i = lane + 32 * q;
+      vi[q] = (i < m) ? v[i] : 0.0;
+      wi[q] = (i < m) ? p[i] - K * vi[q] : 0.0;
+    }
+    // warp 0 updates only column 0 of B (the next reflector's column) and then
+    // goes on to form the next reflector while warps 1..31 update the rest
+    for (int j = (warp == 0) ? 0 : warp; j < m; j += (warp == 0) ? m : NW - 1) {
       const double vj = v[j], wj = p[j] - K * vj;
-      double *col = &A_(k + 1, k + 1 + j);
-      for (int i = lane; i < m; i += 32) {
-        const double vi = v[i], wi = p[i] - K * vi;
-        col[i] -= vi * wj + wi * vj;
+      double *__restrict__ col = &A_(k + 1, k + 1 + j);
+      if (m <= 32 * RQ) {
+#pragma unroll
+        for (int q = 0; q < RQ; ++q) {
+          const int i = lane + 32 * q;
+          if (i < m) col[i] -= vi[q] * wj + wi[q] * vj;
+        }
+      } else {
+        for (int i = lane; i < m; i += 32) {
+          const double a = v[i], b = p[i] - K * a;
+          col[i] -= a * wj + b * vj;
+        }
       }
     }
   }

@@ -121,7 +121,7 @@ bool tc_enabled();
 int tc_error_take();
 
 // qx_dense.cu (FP64, nb x nb)
-// work: >= 32*33 doubles, used when S does not fit shared memory.
+// work: >= 32*33 + n doubles, used when S does not fit shared memory.
 int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st);
 // Symmetric eigen-decomposition; work >= 8*n*n + 1024*n doubles.
 int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st);

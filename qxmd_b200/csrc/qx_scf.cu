@@ -133,11 +133,15 @@ __global__ void __launch_bounds__(RB) k_mix(double *__restrict__ rho_in, const d
 }
 
 // out[k] = sum over nblk partial sums with stride `stride` and offset k.
+// One warp per output: lane-strided partial sums, then a shuffle tree (a fixed
+// order, so the result does not change from run to run).
 __global__ void k_reduce(const double *__restrict__ part, int nblk, int stride, int nk, double *__restrict__ out) {
-  for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int k = w; k < nk; k += blockDim.x >> 5) {
     double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(long)b * stride + k];
-    out[k] = s;
+    for (int b = lane; b < nblk; b += 32) s += part[(long)b * stride + k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[k] = s;
   }
 }
 
@@ -174,7 +178,7 @@ template <typename T>
 void xc_glocal(const double *rho, const double *vloc, const double2 *vh, long n, double rdelv, double *glocal,
                T *glocal_t, double *part, double *out2, cudaStream_t st) {
   k_xc_glocal<T><<<SCF_NBLK, RB, 0, st>>>(rho, vloc, vh, n, rdelv, glocal, glocal_t, part); note_launch();
-  k_reduce<<<1, 32, 0, st>>>(part, SCF_NBLK, 2, 2, out2); note_launch();
+  k_reduce<<<1, 64, 0, st>>>(part, SCF_NBLK, 2, 2, out2); note_launch();
 }
 template void xc_glocal<float>(const double *, const double *, const double2 *, long, double, double *, float *,
                                double *, double *, cudaStream_t);

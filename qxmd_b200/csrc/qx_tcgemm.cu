@@ -6,8 +6,8 @@
 //
 // sm_100a only: operands staged by TMA (128-byte swizzles) into a 3-stage
 // shared-memory ring, products on the 5th-generation tensor cores
-// (tcgen05.mma kind::tf32, 128 x 160 or 128 x 80 tile, accumulator in TMEM), read back
-// with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
+// (tcgen05.mma kind::tf32, 128 x 80 or 128 x 96 tiles, accumulators in TMEM),
+// read back with tcgen05.ld.  FP32 accuracy comes from the 3xTF32 split: each operand x
 // is cut into x_hi = x rounded to the nearest TF32 value and x_lo = x - x_hi
 // rounded the same way, and the tile product is
 // A_hi B_hi + A_hi B_lo + A_lo B_hi accumulated in FP32 (relative error about
@@ -39,18 +39,19 @@ constexpr int NTHREADS = 192;
 constexpr int BAR_BYTES = 256;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
-// Tile width BN (MMA N) and what follows from it.  BN = 160 covers a 160-band
-// block in one tile; BN = 80 doubles the tile count when M alone gives too
-// few tiles to fill the 148 SMs.
+// Tile width BN (MMA N) and what follows from it: 80 for K-major B, 96 (three
+// 32-column chunks) for MN-major B.  TMEM holds two BN-column accumulators
+// (at columns 0 and 128), used for alternate k-blocks.
 template <int BN_> struct Cfg {
   static constexpr int BN = BN_;
   static constexpr int B_BYTES = BN * BK * 4;
   static constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
   static constexpr int STAGE_BYTES = 2 * (A_BYTES + B_BYTES);   // a multiple of 1 KB
   static constexpr int STAGES = (4 * STAGE_BYTES <= 212 * 1024) ? 4 : 3;
-  static constexpr int TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  static constexpr int TMEM_COLS = 256;
+  static constexpr int ACC_STRIDE = 128;   // TMEM column offset of accumulator 1
   static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + BAR_BYTES + 1024;   // + alignment slack
-  static_assert(BN % 16 == 0 && BN <= 256, "UMMA N for M = 128");
+  static_assert(BN % 16 == 0 && BN <= ACC_STRIDE, "UMMA N for M = 128, two accumulators in TMEM");
   static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 };
 
@@ -185,8 +186,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   extern __shared__ __align__(1024) uint8_t smraw[];
   uint8_t *sm = (uint8_t *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   uint64_t *bars = (uint64_t *)(sm + (size_t)STAGES * STAGE_BYTES);
-  uint64_t *full = bars, *conv = bars + STAGES, *empty = bars + 2 * STAGES, *accb = bars + 3 * STAGES;
-  uint32_t *tmem_slot = (uint32_t *)(bars + 3 * STAGES + 1);
+  uint64_t *full = bars, *conv = bars + STAGES, *empty = bars + 2 * STAGES;
+  uint64_t *accf = bars + 3 * STAGES, *acce = accf + 2;   // accumulator full / drained
+  uint64_t *fin = acce + 2;                                // all MMAs of this CTA complete
+  uint32_t *tmem_slot = (uint32_t *)(fin + 1);
   __shared__ volatile int abort_flag;
   __shared__ float sb0[BN], sb1[BN];   // B(0, n), B(1, n) of the tile (Gamma-metric epilogue)
 
@@ -202,7 +205,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_init(&conv[s], 128);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accb, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 128);
+    }
+    mbar_init(fin, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -249,11 +256,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((A_MN ? 1u : 0u) << 15) |
                              ((B_MN ? 1u : 0u) << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
       for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % STAGES;
+        const int s = kb % STAGES, ab = kb & 1;
         if (!mbar_wait(&conv[s], (kb / STAGES) & 1, 3)) { abort_flag = 1; break; }
+        if (!mbar_wait(&acce[ab], ((kb >> 1) & 1) ^ 1, 6)) { abort_flag = 1; break; }
         if (abort_flag) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t st = su32(sm + (size_t)s * STAGE_BYTES);
+        const uint32_t dt = tmem + (uint32_t)(ab * G::ACC_STRIDE);
 #pragma unroll
         for (int kk = 0; kk < BK / 8; ++kk) {
           // K-major (layout 2): rows of 128 B, 8-row groups 1 KB apart, the
@@ -266,18 +275,46 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const uint32_t aly = A_MN ? 1 : 2, bly = B_MN ? 1 : 2;
           const uint64_t ah = sdesc(st + OFF_AH + ao, alb, asb, aly), al = sdesc(st + OFF_AL + ao, alb, asb, aly);
           const uint64_t bh = sdesc(st + OFF_BH + bo, blb, bsb, bly), bl = sdesc(st + OFF_BL + bo, blb, bsb, bly);
-          const uint32_t first = (kb == 0 && kk == 0) ? 0u : 1u;
-          mma_tf32(tmem, ah, bh, idesc, first);
-          mma_tf32(tmem, ah, bl, idesc, 1u);
-          mma_tf32(tmem, al, bh, idesc, 1u);
+          // each k-block starts its accumulator afresh: the tensor core's
+          // accumulation is kept to 12 products deep, the running sum is
+          // carried in FP32 registers by the draining warps
+          mma_tf32(dt, ah, bh, idesc, kk == 0 ? 0u : 1u);
+          mma_tf32(dt, ah, bl, idesc, 1u);
+          mma_tf32(dt, al, bh, idesc, 1u);
         }
         mma_commit(&empty[s]);   // frees the stage when these MMAs are done
+        mma_commit(&accf[ab]);   // accumulator ab holds this k-block
       }
-      mma_commit(accb);          // all MMAs issued by this thread are complete
+      // no MMA of this CTA may still run when TMEM is freed, on any path
+      mma_commit(fin);
+      mbar_wait(fin, 0, 7);
     }
   } else {
-    // ---------------- split (warps 2-5) ----------------
+    // ---------------- split and drain (warps 2-5) ----------------
     const int t = threadIdx.x - 64;   // 0..127
+    const int quad = warp & 3;
+    float acc[BN];
+#pragma unroll
+    for (int j = 0; j < BN; ++j) acc[j] = 0.f;
+    // add the k-block held in accumulator (j & 1) to acc and release it
+    auto drain = [&](int j) {
+      const int ab = j & 1;
+      const bool got = mbar_wait(&accf[ab], (j >> 1) & 1, 5);
+      if (!got) abort_flag = 1;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t base = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(ab * G::ACC_STRIDE);
+#pragma unroll
+      for (int c = 0; c < BN / 16; ++c) {
+        uint32_t r[16];
+        TMEM_LD16(base + (uint32_t)(c * 16), r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 16; ++q) acc[c * 16 + q] += __uint_as_float(r[q]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      mbar_arrive(&acce[ab]);
+    };
+    int converted = 0;
     for (int kb = 0; kb < nkb; ++kb) {
       const int s = kb % STAGES;
       if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
@@ -288,7 +325,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // generic-proxy writes -> visible to the tensor core (async proxy)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&conv[s]);
+      ++converted;
+      if (kb >= 1) drain(kb - 1);
     }
+    if (converted == nkb && nkb >= 1 && !abort_flag) drain(nkb - 1);
     // ---------------- epilogue ----------------
     const bool direct = (p.W == nullptr);
     if (direct && p.gamma) {
@@ -299,47 +339,43 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
     }
     asm volatile("bar.sync 1, 128;" ::: "memory");   // the four epilogue warps
-    const int quad = warp & 3;
     const int gm = m0 + quad * 32 + lane;
     float a0 = 0.f, a1 = 0.f;
     if (direct && p.gamma && gm < p.M) {
       a0 = A_MN ? p.A[gm] : p.A[(long)gm * p.lda];
       a1 = A_MN ? p.A[p.lda + gm] : p.A[(long)gm * p.lda + 1];
     }
-    const bool ok = mbar_wait(accb, 0, 5) && !abort_flag;
-    asm volatile("tcgen05.fence::after_thread_sync;");
+    const bool ok = !abort_flag;
     const float alpha = p.alpha, beta = p.beta;
-#pragma unroll 1
-    for (int c = 0; c < BN / 16; ++c) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(c * 16);
-      TMEM_LD16(taddr, r);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (!ok || gm >= p.M) continue;
-      const int nb = n0 + c * 16;
-      if (!direct) {
-        float *w = p.W + ((long)blockIdx.z * p.N + nb) * p.M + gm;
+    if (ok && gm < p.M) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (nb + j < p.N) w[(long)j * p.M] = __uint_as_float(r[j]);
-        continue;
-      }
-      float *cp = p.C + (long)nb * p.ldc + gm;
-      float old[16];
-      if (beta != 0.f) {
-        // issue every load of the chunk before the first store
+      for (int c = 0; c < BN / 16; ++c) {
+        const int nb = n0 + c * 16;
+        if (!direct) {
+          float *w = p.W + ((long)blockIdx.z * p.N + nb) * p.M + gm;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) old[j] = (nb + j < p.N) ? cp[(long)j * p.ldc] : 0.f;
-      }
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        if (nb + j >= p.N) break;
-        float v = __uint_as_float(r[j]);
-        if (p.gamma) {
-          v = 2.f * v - a0 * sb0[c * 16 + j];
-          if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < p.N) w[(long)j * p.M] = acc[c * 16 + j];
+          continue;
         }
-        cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
+        float *cp = p.C + (long)nb * p.ldc + gm;
+        float old[16];
+        if (beta != 0.f) {
+          // issue every load of the chunk before the first store
+#pragma unroll
+          for (int j = 0; j < 16; ++j) old[j] = (nb + j < p.N) ? cp[(long)j * p.ldc] : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          if (nb + j < p.N) {
+            float v = acc[c * 16 + j];
+            if (p.gamma) {
+              v = 2.f * v - a0 * sb0[c * 16 + j];
+              if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
+            }
+            cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
+          }
+        }
       }
     }
   }
@@ -424,9 +460,8 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   // A: ta -> K contiguous (A[m*lda + k]); !ta -> M contiguous (A[k*lda + m])
   const bool a_mn = !ta, b_mn = tb;
   const int tm = (M + BM - 1) / BM, nkb = (K + BK - 1) / BK;
-  // 80-wide tiles when 160-wide ones leave most SMs idle (MN-major B tiles
-  // come in 32-column chunks, so they keep 160)
-  const int bn = (!b_mn && (N <= 80 || (long)tm * ((N + 159) / 160) < 120)) ? 80 : 160;
+  // 80-wide tiles for K-major B, 96-wide (three 32-column chunks) for MN-major B
+  const int bn = b_mn ? 96 : 80;
   const int tn = (N + bn - 1) / bn;
   CUtensorMap ma, mb;
   if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, true) : tc::make_map(&ma, A, K, M, lda, BM, false))) return -1;
@@ -443,11 +478,9 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr};
   dim3 g(tm, tn, nsplit);
   int rc;
-  if (bn == 160) {
-    if (a_mn && b_mn) rc = tc::launch_tc<true, true, 160>(ma, mb, a, g, st);
-    else if (a_mn) rc = tc::launch_tc<true, false, 160>(ma, mb, a, g, st);
-    else if (b_mn) rc = tc::launch_tc<false, true, 160>(ma, mb, a, g, st);
-    else rc = tc::launch_tc<false, false, 160>(ma, mb, a, g, st);
+  if (bn == 96) {
+    if (a_mn) rc = tc::launch_tc<true, true, 96>(ma, mb, a, g, st);
+    else rc = tc::launch_tc<false, true, 96>(ma, mb, a, g, st);
   } else {
     if (a_mn) rc = tc::launch_tc<true, false, 80>(ma, mb, a, g, st);
     else rc = tc::launch_tc<false, false, 80>(ma, mb, a, g, st);
