@@ -202,6 +202,8 @@ static int alloc_pipe(qx_ctx *c) {
   TRY(dalloc(c, &b.zsph, sizeof(C) * ch * (pl.nplw + 1) * 2));
   TRY(dalloc(c, &b.vloc, sizeof(T) * pl.n));
   CK(cudaMemset(b.vloc, 0, sizeof(T) * pl.n));
+  if (sizeof(T) == sizeof(float) && plane_length_supported(pl.k1, pl.k2))
+    TRY(dalloc(c, &b.rho_part, sizeof(double) * RHO_GROUPS * pl.n));
   TRY(upload_tw<T>(c));
   // shared-memory opt-in for the largest launch of this plan
   const size_t need = fft_smem_need<T>(pl);

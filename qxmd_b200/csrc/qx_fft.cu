@@ -765,6 +765,9 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
   const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
   k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
+  if (sizeof(T) == sizeof(float) && plane_enabled() && bf.rho_part &&
+      launch_rho_plane_f32(P, npl, (const float2 *)bf.bufA, wocc, bf.rho_part, rho, accumulate, st) == 0)
+    return 0;
   dim3 gy(P.k3, npl);
   k_ypass<T, +1><<<gy, QX_THREADS, fft_smem(P.L2, P.P1, cs), st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
   const int nlines = pl.rholines;

@@ -85,6 +85,136 @@ __global__ void __launch_bounds__(64) k_plane(PipeParams P, float2 *__restrict__
   }
 }
 
+// Density for the same grids (softchg, chgdns.f90:388-454): per CTA one z
+// plane and one group of band pairs; for each pair the backward y- and
+// x-FFTs of the plane as above, then rho += occ_A/Omega psi_A(r)^2 +
+// occ_B/Omega psi_B(r)^2 accumulated in FP64 in shared memory (each thread
+// owns one grid row).  The group's partial plane goes to part[group]; a
+// second kernel sums the groups in a fixed order, so the result is the same
+// from run to run.
+template <int N>
+__global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__restrict__ bufA,
+                                                  const double *__restrict__ wocc, double *__restrict__ part,
+                                                  int npl, int per_group) {
+  using rf::out_pos;
+  const int i3 = blockIdx.x, grp = blockIdx.y;
+  const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
+  extern __shared__ double accs[];            // [N][N] FP64, then the [N][P1] complex tile
+  float2 *T = reinterpret_cast<float2 *>(accs + N * N);
+  const int t = threadIdx.x;
+  const float2 zero = make_float2(0.f, 0.f);
+  if (t < N)
+    for (int i1 = 0; i1 < N; ++i1) accs[t * N + i1] = 0.0;
+  const int np = min(npl, (P.npair_dev ? *P.npair_dev : P.npair) - P.pair0);
+  const int pl0 = grp * per_group, pl1 = min(np, pl0 + per_group);
+  for (int pl = pl0; pl < pl1; ++pl) {
+    const int p = P.pair0 + pl;
+    const float2 *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
+    if (t < P1) {
+      float2 x[N];
+#pragma unroll
+      for (int i2 = 0; i2 < N; ++i2) {
+        const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+        float2 v = zero;
+        if (j2 >= 0 && t >= P.row_lo[j2] && t <= P.row_hi[j2]) v = A[j2 * P1 + t];
+        x[i2] = v;
+      }
+      rf::fft<float, +1, N>(x);
+      rf::static_for<0, N>([&](auto ic) {
+        constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
+        T[i2 * P1 + t] = x[q];
+      });
+    }
+    __syncthreads();
+    if (t < N) {
+      float2 x[N];
+      const float2 *row = T + t * P1;
+#pragma unroll
+      for (int i1 = 0; i1 < N; ++i1) {
+        float2 v = zero;
+        if (i1 <= m1) v = row[i1 + m1];
+        else if (i1 >= N - m1) v = row[i1 - N + m1];
+        x[i1] = v;
+      }
+      rf::fft<float, +1, N>(x);
+      const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+      const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
+      double *a = accs + t * N;
+      rf::static_for<0, N>([&](auto ic) {
+        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+        const double re = x[q].x, im = x[q].y;
+        a[i1] += fa * re * re + fb * im * im;
+      });
+    }
+    __syncthreads();
+  }
+  if (t < N) {
+    double *dst = part + ((long)grp * P.k3 + i3) * N * N + (long)t * N;
+    for (int i1 = 0; i1 < N; ++i1) dst[i1] = accs[t * N + i1];
+  }
+}
+
+// rho = [rho +] sum over groups of part (fixed order).
+__global__ void k_rho_groups(const double *__restrict__ part, int ngrp, long n, double *__restrict__ rho,
+                             int accumulate) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double s = accumulate ? rho[i] : 0.0;
+    for (int g = 0; g < ngrp; ++g) s += part[(long)g * n + i];
+    rho[i] = s;
+  }
+}
+
+template <int N>
+static int rho_launch(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part, double *rho,
+                      int accumulate, cudaStream_t st) {
+  const size_t sm = sizeof(double) * (size_t)N * N + sizeof(float2) * (size_t)N * P.P1;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_rho_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    attr = true;
+  }
+  const int per_group = (npl + RHO_GROUPS - 1) / RHO_GROUPS;
+  dim3 g(P.k3, RHO_GROUPS);
+  k_rho_plane<N><<<g, 64, sm, st>>>(P, bufA, wocc, part, npl, per_group);
+  note_launch();
+  const long n = (long)P.k1 * P.k2 * P.k3;
+  k_rho_groups<<<148 * 4, 256, 0, st>>>(part, RHO_GROUPS, n, rho, accumulate);
+  note_launch();
+  return 0;
+}
+
+// Density of one chunk of pairs through the plane kernel; -1 if the grid has
+// no specialised length.  part: RHO_GROUPS * kfft0 doubles.
+int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part,
+                         double *rho, int accumulate, cudaStream_t st) {
+  if (P.k1 != P.k2 || P.P1 > P.k1 || P.P2 > P.k2 || !part) return -1;
+  switch (P.k1) {
+    case 20: return rho_launch<20>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 24: return rho_launch<24>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 27: return rho_launch<27>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 30: return rho_launch<30>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 32: return rho_launch<32>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 36: return rho_launch<36>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 40: return rho_launch<40>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 45: return rho_launch<45>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 48: return rho_launch<48>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 54: return rho_launch<54>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 60: return rho_launch<60>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 64: return rho_launch<64>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    default: return -1;
+  }
+}
+
+bool plane_length_supported(int k1, int k2) {
+  if (k1 != k2) return false;
+  switch (k1) {
+    case 20: case 24: case 27: case 30: case 32: case 36: case 40: case 45: case 48: case 54: case 60: case 64:
+      return true;
+    default:
+      return false;
+  }
+}
+
 template <int N>
 static int plane_launch(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st) {
   const size_t sm = sizeof(float2) * (size_t)N * P.P1;

@@ -44,6 +44,7 @@ struct Bufs {
   T *kb_vnl = nullptr;     // real-space projector values [npts][4]
   T *kbg = nullptr;        // G-space projectors [nproj][nplwex]
   T *vclalp = nullptr;     // [nproj]
+  double *rho_part = nullptr;   // RHO_GROUPS partial density planes (plane-kernel grids)
 };
 
 struct Plan {
@@ -93,6 +94,12 @@ template <typename T> void set_fft_smem_limits(size_t bytes);
 // qx_fftplane.cu: fused y-x-y pass (FP32, k1 == k2 of a specialised length);
 // returns -1 when the grid is not covered.
 int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st);
+// Density through the plane kernel: groups of pairs per z plane, partial
+// planes in part (RHO_GROUPS * kfft0 doubles) summed in a fixed order.
+constexpr int RHO_GROUPS = 8;
+int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part,
+                         double *rho, int accumulate, cudaStream_t st);
+bool plane_length_supported(int k1, int k2);
 template <typename T> size_t fft_smem_need(const Plan &pl);
 int init_fft_roots();
 

@@ -35,7 +35,7 @@ namespace tc {
 
 constexpr int BM = 128, BK = 32;
 constexpr int A_BYTES = BM * BK * 4;                 // 16 KB
-constexpr int NTHREADS = 192;
+constexpr int NTHREADS = 320;   // TMA, MMA, 8 split warps (4 of them drain)
 constexpr int BAR_BYTES = 256;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
@@ -154,15 +154,15 @@ struct TcArgs {
 __device__ __forceinline__ float tf32_rn(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
-// x = hi + lo with hi = tf32_rn(x) and lo = tf32_rn(x - hi): both exact TF32
-// values, |lo| <= 2^-11 |hi|, and the dropped part is below 2^-22 |x| with
-// either sign, so the three-product sum carries no truncation bias.
+// x = hi + lo with hi = tf32_rn(x) (exact TF32, |x - hi| <= 2^-12 |x| with
+// either sign) and lo = x - hi in FP32; the tensor core reads lo to TF32,
+// losing at most 2^-23 |x|, a bias far below the FP32 rounding of the sums.
 __device__ __forceinline__ void split1(float x, float &h, float &l) {
   h = tf32_rn(x);
-  l = tf32_rn(x - h);
+  l = x - h;
 }
 __device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int n16, int t) {
-  for (int i = t; i < n16; i += 128) {
+  for (int i = t; i < n16; i += 256) {
     const float4 x = hi[i];
     float4 h, l;
     split1(x.x, h.x, l.x);
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&conv[s], 128);
+      mbar_init(&conv[s], 256);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -290,8 +290,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_wait(fin, 0, 7);
     }
   } else {
-    // ---------------- split and drain (warps 2-5) ----------------
-    const int t = threadIdx.x - 64;   // 0..127
+    // ---------------- split (warps 2-9), drain and epilogue (warps 2-5) ----------------
+    const int t = threadIdx.x - 64;   // 0..255
+    const bool drains = warp < 6;
     const int quad = warp & 3;
     float acc[BN];
 #pragma unroll
@@ -326,54 +327,56 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&conv[s]);
       ++converted;
-      if (kb >= 1) drain(kb - 1);
+      if (drains && kb >= 1) drain(kb - 1);
     }
-    if (converted == nkb && nkb >= 1 && !abort_flag) drain(nkb - 1);
-    // ---------------- epilogue ----------------
-    const bool direct = (p.W == nullptr);
-    if (direct && p.gamma) {
-      for (int j = t; j < BN; j += 128) {
-        const int gn = n0 + j;
-        sb0[j] = (gn < p.N) ? (B_MN ? p.B[gn] : p.B[(long)gn * p.ldb]) : 0.f;
-        sb1[j] = (gn < p.N) ? (B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1]) : 0.f;
+    if (drains && converted == nkb && nkb >= 1 && !abort_flag) drain(nkb - 1);
+    if (drains) {   // warps 6-9 only split
+      // ---------------- epilogue ----------------
+      const bool direct = (p.W == nullptr);
+      if (direct && p.gamma) {
+        for (int j = t; j < BN; j += 128) {   // t < 128 here
+          const int gn = n0 + j;
+          sb0[j] = (gn < p.N) ? (B_MN ? p.B[gn] : p.B[(long)gn * p.ldb]) : 0.f;
+          sb1[j] = (gn < p.N) ? (B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1]) : 0.f;
+        }
       }
-    }
-    asm volatile("bar.sync 1, 128;" ::: "memory");   // the four epilogue warps
-    const int gm = m0 + quad * 32 + lane;
-    float a0 = 0.f, a1 = 0.f;
-    if (direct && p.gamma && gm < p.M) {
-      a0 = A_MN ? p.A[gm] : p.A[(long)gm * p.lda];
-      a1 = A_MN ? p.A[p.lda + gm] : p.A[(long)gm * p.lda + 1];
-    }
-    const bool ok = !abort_flag;
-    const float alpha = p.alpha, beta = p.beta;
-    if (ok && gm < p.M) {
-#pragma unroll
-      for (int c = 0; c < BN / 16; ++c) {
-        const int nb = n0 + c * 16;
-        if (!direct) {
-          float *w = p.W + ((long)blockIdx.z * p.N + nb) * p.M + gm;
-#pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (nb + j < p.N) w[(long)j * p.M] = acc[c * 16 + j];
-          continue;
-        }
-        float *cp = p.C + (long)nb * p.ldc + gm;
-        float old[16];
-        if (beta != 0.f) {
-          // issue every load of the chunk before the first store
-#pragma unroll
-          for (int j = 0; j < 16; ++j) old[j] = (nb + j < p.N) ? cp[(long)j * p.ldc] : 0.f;
-        }
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          if (nb + j < p.N) {
-            float v = acc[c * 16 + j];
-            if (p.gamma) {
-              v = 2.f * v - a0 * sb0[c * 16 + j];
-              if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
+      asm volatile("bar.sync 1, 128;" ::: "memory");   // the four epilogue warps
+      const int gm = m0 + quad * 32 + lane;
+      float a0 = 0.f, a1 = 0.f;
+      if (direct && p.gamma && gm < p.M) {
+        a0 = A_MN ? p.A[gm] : p.A[(long)gm * p.lda];
+        a1 = A_MN ? p.A[p.lda + gm] : p.A[(long)gm * p.lda + 1];
+      }
+      const bool ok = !abort_flag;
+      const float alpha = p.alpha, beta = p.beta;
+      if (ok && gm < p.M) {
+  #pragma unroll
+        for (int c = 0; c < BN / 16; ++c) {
+          const int nb = n0 + c * 16;
+          if (!direct) {
+            float *w = p.W + ((long)blockIdx.z * p.N + nb) * p.M + gm;
+  #pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (nb + j < p.N) w[(long)j * p.M] = acc[c * 16 + j];
+            continue;
+          }
+          float *cp = p.C + (long)nb * p.ldc + gm;
+          float old[16];
+          if (beta != 0.f) {
+            // issue every load of the chunk before the first store
+  #pragma unroll
+            for (int j = 0; j < 16; ++j) old[j] = (nb + j < p.N) ? cp[(long)j * p.ldc] : 0.f;
+          }
+  #pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            if (nb + j < p.N) {
+              float v = acc[c * 16 + j];
+              if (p.gamma) {
+                v = 2.f * v - a0 * sb0[c * 16 + j];
+                if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
+              }
+              cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
             }
-            cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
           }
         }
       }
