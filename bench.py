@@ -34,6 +34,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "SCF iter/s"
+# Pulay density mixing with the reference defaults (modules.f90:136-142:
+# imxchg 1, aslh 0.8, bslh 0.64 = 0.8^2, itratn 10, cmetric 20)
+PULAY_ASLH, PULAY_Q0, PULAY_ITRATN, PULAY_CMETRIC = 0.8, 0.8, 10, 20.0
 UNIT = "iter/s"
 WORKLOAD = "Si64 diamond 2x2x2, Gamma, Ecut 16 Ry / 64 Ry, 54^3 grid, 160 bands, G-space KB"
 # Average CG H|psi> band applications per SCF iteration of this workload after
@@ -54,6 +57,10 @@ def parse():
     ap.add_argument("--profile-step", action="store_true",
                     help="only the mixed-precision SCF iterations (warm-up, then --steps), no L2 flush, "
                          "no extra arms: the launch sequence profiled under ncu")
+    ap.add_argument("--sequential", action="store_true",
+                    help="with --profile-step: the plain FP64 path (one-rank band order) instead of mixed")
+    ap.add_argument("--accuracy-iters", type=int, default=40,
+                    help="SCF iterations (from the same start) after which the paths' energies are compared")
     return ap.parse_args()
 
 
@@ -164,15 +171,16 @@ def run_profile_step(args):
     import torch
 
     from qxmd_b200 import cell
-    from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_MIXED, launch_count
+    from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED, launch_count
     torch.cuda.set_device(0)
     sys_ = cell.si64()
-    ctx = Context(sys_, QX_PREC_MIXED, QX_NL_GSPACE)
+    ctx = Context(sys_, QX_PREC_FP64 if args.sequential else QX_PREC_MIXED, QX_NL_GSPACE)
     ctx.put_psi(cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband))
     ctx.schmidt()
-    ctx.scf_init()
+    ctx.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+    ctx.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
     ctx.scf_rho_from_psi()
-    parm = CgParm.defaults(int(sys_.cell.nel // 2))
+    parm = CgParm.defaults(int(sys_.cell.nel // 2), sequential=int(args.sequential))
     for _ in range(args.warmup):
         ctx.scf_iteration(parm)
     ctx.sync()
@@ -211,6 +219,22 @@ def run_profile_hpsi(args):
     ctx.close()
 
 
+def accuracy(acc, natom, iters):
+    """Total-energy and eigenvalue deviations of each path from the plain
+    FP64 path after the same number of SCF iterations from the same start."""
+    ref = acc["fp64"]
+    out = {"iterations": iters, "etot_fp64_ry": ref["etot"], "resid_fp64": ref["resid"],
+           "detot_last_fp64_ry": ref["detot_last"]}
+    for name in ("mixed", "fp64_batched"):
+        a = acc[name]
+        d = abs(a["etot"] - ref["etot"])
+        out[name] = {"etot_ry": a["etot"], "resid": a["resid"], "detot_last_ry": a["detot_last"],
+                     "err_ha_per_atom": 0.5 * d / natom,
+                     "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - ref["eig"])))}
+    out["err_ha_per_atom"] = out["mixed"]["err_ha_per_atom"]
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -221,21 +245,27 @@ def run_ours(args):
     sys_ = cell.si64()
     psi0 = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
     noband = int(sys_.cell.nel // 2)
-    parm = CgParm.defaults(noband)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
     K, W = args.steps, args.warmup
     res = {}
     clocks = Clocks(local)
-    for prec in (QX_PREC_MIXED, QX_PREC_FP64):
+    # mixed: FP32 FFT/H|psi> + 3xTF32 tensor-core contractions, CG over all
+    # bands at once; fp64: the plain drop-in (FP64, bands one after another as
+    # on one rank of the reference); fp64_batched: FP64 with the batched CG
+    variants = (("mixed", QX_PREC_MIXED, 0), ("fp64", QX_PREC_FP64, 1), ("fp64_batched", QX_PREC_FP64, 0))
+    ctxs = {}
+    for name, prec, seq in variants:
+        parm = CgParm.defaults(noband, sequential=seq)
         ctx = Context(sys_, prec, QX_NL_GSPACE)
         ctx.put_psi(psi0)
         ctx.schmidt()
-        ctx.scf_init()
+        ctx.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+        ctx.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
         ctx.scf_rho_from_psi()
         for _ in range(W):
             ctx.scf_iteration(parm)
         barrier(ws)
-        if prec == QX_PREC_MIXED:
+        if name == "mixed":
             clocks.start()
         n0 = launch_count()
         tot_ms, outs = 0.0, []
@@ -248,13 +278,18 @@ def run_ours(args):
             torch.cuda.synchronize()
             tot_ms += e0.elapsed_time(e1)
         launches = launch_count() - n0
-        if prec == QX_PREC_MIXED:
+        if name == "mixed":
             clk = clocks.stop()
         barrier(ws)
         tmax = max_over_ranks(tot_ms, ws)
         r = {"ms_per_step": tmax / K, "value": ws * K / (tmax / 1e3), "launches": launches,
              "etot_last": outs[-1]["etot"], "cg_bapps_per_iter": float(np.mean([o["ncg_hpsi"] for o in outs])),
              "eig_clusters": float(np.mean([o["eig_clusters"] for o in outs]))}
+        r["iters_done"] = W + K
+        res[name] = r
+        ctxs[name] = (ctx, parm)
+        if name == "fp64_batched":
+            continue
         # H|psi> band applications per second (enonloc: kinetic + local + KB, all bands)
         R = max(3, K)
         ctx.enonloc()
@@ -280,7 +315,7 @@ def run_ours(args):
             torch.cuda.synchronize()
             t += e0.elapsed_time(e1)
         r["fft_pipeline_ms"] = t / R
-        if prec == QX_PREC_MIXED:
+        if name == "mixed":
             # end to end through the host-array API: H2D psi (pinned), one
             # iteration, D2H psi, rho, eigenvalues
             hpsi = torch.empty((sys_.nband, sys_.gs.nplwex), dtype=torch.float64).pin_memory()
@@ -306,9 +341,22 @@ def run_ours(args):
                         "h2d_bytes_per_step": int(npsi.nbytes),
                         "d2h_bytes_per_step": int(npsi.nbytes + nrho.nbytes + neig.nbytes)}
             r["clocks"] = clk
-        res[prec] = r
+            r["iters_done"] += K
+    # accuracy: every variant continues from its timed iterations to the
+    # same total count, then the final total energies and eigenvalues are
+    # compared with the plain FP64 path's
+    acc = {}
+    for name, _, _ in variants:
+        ctx, parm = ctxs[name]
+        outs = [ctx.scf_iteration(parm) for _ in range(max(0, args.accuracy_iters - res[name]["iters_done"]))]
+        ctx.sync()
+        last = outs[-1] if outs else None
+        acc[name] = {"etot": last["etot"] if last else res[name]["etot_last"],
+                     "resid": last["resid"] if last else None,
+                     "detot_last": abs(outs[-1]["etot"] - outs[-2]["etot"]) if len(outs) > 1 else None,
+                     "eig": ctx.get_eig()}
         ctx.close()
-    mixed, fp64 = res[QX_PREC_MIXED], res[QX_PREC_FP64]
+    mixed, fp64, fp64b = res["mixed"], res["fp64"], res["fp64_batched"]
     hbm, peak_kind = peaks()
     N, ne = sys_.gs.kfft0, sys_.gs.nplwex
     bytes_per_bapp = 4 * N * 4 + 2 * ne * 4
@@ -321,13 +369,16 @@ def run_ours(args):
                    "precision": "mixed", "parallelism": "replicas" if ws > 1 else "single",
                    "l2": "256 MB buffer written between timed iterations"},
         "hpsi_band_apps_per_s": mixed["hpsi_band_apps_per_s"],
-        "fp64": {"value": fp64["value"], "ms_per_step": fp64["ms_per_step"],
-                 "hpsi_band_apps_per_s": fp64["hpsi_band_apps_per_s"]},
+        "fp64": {"path": "plain FP64 drop-in, one-rank band order (sequential CG, one graph launch per sweep)",
+                 "value": fp64["value"], "ms_per_step": fp64["ms_per_step"],
+                 "hpsi_band_apps_per_s": fp64["hpsi_band_apps_per_s"],
+                 "cg_bapps_per_iter": fp64["cg_bapps_per_iter"], "gpu_launches": fp64["launches"]},
+        "fp64_batched": {"path": "FP64, all bands at once (one band per rank order)",
+                         "value": fp64b["value"], "ms_per_step": fp64b["ms_per_step"],
+                         "cg_bapps_per_iter": fp64b["cg_bapps_per_iter"]},
         "mixed_over_fp64": mixed["value"] / fp64["value"],
-        # both paths run the same W + K SCF iterations from the same start
-        "accuracy": {"iterations": W + K, "etot_mixed_ry": mixed["etot_last"], "etot_fp64_ry": fp64["etot_last"],
-                     "err_ry_per_atom": abs(mixed["etot_last"] - fp64["etot_last"]) / sys_.cell.natom,
-                     "err_ha_per_atom": 0.5 * abs(mixed["etot_last"] - fp64["etot_last"]) / sys_.cell.natom},
+        "mixed_over_fp64_batched": mixed["value"] / fp64b["value"],
+        "accuracy": accuracy(acc, sys_.cell.natom, args.accuracy_iters),
         "cg_bapps_per_iter": mixed["cg_bapps_per_iter"],
         "eig_clusters": mixed["eig_clusters"],
         "e2e": mixed["e2e"],

@@ -50,6 +50,10 @@ typedef struct {
   int itermx, iteremx, noband;
   double tolera, roughfzan, roughfeig, threinn, wdinner;
   int ccreal4;   /* FP64 contexts: round the lower-band snapshot to real*4 */
+  int sequential; /* 0: all bands at once against the entry vectors (the
+                   * reference run with one band per rank); 1: bands one after
+                   * another, each against the final vectors of the bands below
+                   * (the reference run on one rank; one graph launch per call) */
 } qx_cgparm;
 
 /* Result of one SCF iteration (energies in Ry). */
@@ -164,7 +168,15 @@ int qx_softchg(qx_ctx *ctx);
  * vectors, column-major 3x3; eion: ion-ion energy added to etot. */
 int qx_scf_init(qx_ctx *ctx, const double *vloc, const double *cross, double ecutdens, double eion, double mixbeta,
                 double kerker_q0);
-/* rho_in <- rho_out of the current psi (start of an SCF run). */
+/* Density mixing after qx_scf_init.  itratn >= 2: Pulay mixing
+ * (mxchgg_pulay, chgdns.f90:954-1120; imxchg = 1) with itratn history entries
+ * (at most 16), residual metric (G^2 + q1)/G^2 from cmetric
+ * (chgdns.f90:661-668), Kerker factor mixbeta G^2/(G^2 + kerker_q0^2) (aslh,
+ * bslh of qx_scf_init); itratn 0 or 1: Kerker-filtered linear mixing (the
+ * default).  Reference defaults: itratn 10, cmetric 20, aslh 0.8, bslh 0.64. */
+int qx_scf_mixing(qx_ctx *ctx, int itratn, double cmetric);
+/* rho_in <- rho_out of the current psi (start of an SCF run; restarts the
+ * Pulay history). */
 int qx_scf_rho_from_psi(qx_ctx *ctx);
 int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
 

@@ -52,7 +52,7 @@ class _CGParm(C.Structure):
     _fields_ = [("itermx", C.c_int), ("iteremx", C.c_int), ("noband", C.c_int),
                 ("tolera", C.c_double), ("roughfzan", C.c_double),
                 ("roughfeig", C.c_double), ("threinn", C.c_double),
-                ("wdinner", C.c_double), ("ccreal4", C.c_int)]
+                ("wdinner", C.c_double), ("ccreal4", C.c_int), ("sequential", C.c_int)]
 
 
 _lib = None
@@ -170,12 +170,13 @@ class Ham:
         return e, ekib
 
     def eigen(self, gdcr, rhcr, ekib, noband, itermx=4, iteremx=4, tolera=1e-10,
-              roughfzan=0.3, roughfeig=0.3, threinn=0.0, wdinner=0.9, ccreal4=False):
+              roughfzan=0.3, roughfeig=0.3, threinn=0.0, wdinner=0.9, ccreal4=False,
+              sequential=False):
         x = _f64(gdcr).copy()
         hx = _f64(rhcr).copy()
         nb = x.shape[0]
         p = _CGParm(itermx, iteremx, noband, tolera, roughfzan, roughfeig, threinn, wdinner,
-                    int(ccreal4))
+                    int(ccreal4), int(sequential))
         eig = np.zeros(nb)
         bzan = np.zeros(nb)
         nri = np.zeros(nb, dtype=np.int32)

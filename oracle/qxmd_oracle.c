@@ -230,12 +230,17 @@ typedef struct {
   int itermx, iteremx, noband;
   double tolera, roughfzan, roughfeig, threinn, wdinner;
   int ccreal4;          /* 1: the lower-band snapshot cgjr is real*4 */
+  int sequential;       /* 1: one rank holds all bands (Gauss-Seidel order) */
 } orc_cgparm;
 
-/* eigen_BKL (eigen.f90:199-938) for all bands with the lower-band
- * snapshot semantics of one band per rank: band ib is projected against the
- * entry copy of bands 0..ib-1 (subgs3, engrad.f90:1072-1191), itself
- * (subgs4, engrad.f90:1196-1248), and updated by the BKL 2x2 step.
+/* eigen_BKL (eigen.f90:199-938) for all bands.  Band ib is projected
+ * against the snapshot cgjr of bands 0..ib-1 (subgs3, engrad.f90:1072-1191),
+ * itself (subgs4, engrad.f90:1196-1248), and updated by the BKL 2x2 step.
+ * pm->sequential = 0: the snapshot is the entry copy of every band, which is
+ * the reference run with one band per rank.  pm->sequential = 1: after band
+ * ib's last step its final vector replaces its snapshot column
+ * (cgjr(:,ib) = gdcr(:,ibb), eigen.f90:699), which is the reference run on
+ * one rank, where later bands see the updated lower bands.
  * lhcunt=.true., lortho=.false.: rhcr holds H*gdcr on entry.
  * Outputs eig, bzan (final residual) and nriter per band. */
 void orc_eigen_bkl(const orc_ham *h, const orc_cgparm *pm, int nb, double *gdcr,
@@ -323,6 +328,8 @@ void orc_eigen_bkl(const orc_ham *h, const orc_cgparm *pm, int nb, double *gdcr,
     eig[ib] = e;
     if (bzan) bzan[ib] = zansa;
     if (nriter) nriter[ib] = iter;
+    if (pm->sequential)
+      for (int i = 0; i < ne; ++i) snap[(long)ib * ne + i] = pm->ccreal4 ? (double)(float)x[i] : x[i];
   }
   free(snap); free(prcd); free(gnk); free(hnk); free(prod);
 }

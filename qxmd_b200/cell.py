@@ -266,19 +266,22 @@ def diamond_si(reps=(1, 1, 1), a: float = 10.26, seed: int = 1,
 
 @dataclasses.dataclass(frozen=True)
 class ModelPP:
-    """Appelbaum-Hamann-form local part and Gaussian s/p KB projectors.
+    """Appelbaum-Hamann-form local part and Gaussian s/p KB projectors, in Ry.
 
     v_loc(r) = -(2Z/r) erf(sqrt(alpha) r) + (v1 + v2 r^2) exp(-alpha r^2)
     beta_s(r) = A_s exp(-r^2/(2 sig^2)) Y_00,  beta_p(r) = A_p r exp(-r^2/(2 sig^2)) Y_1m
     normalised so that int beta_l(r)^2 r^2 dr = 1; KB energies e_s, e_p.
+    v1, v2 are Appelbaum and Hamann's Si values (3.042, -1.372 Hartree) in
+    Rydberg.  With these KB energies the Si cells keep a gap between the
+    occupied and the empty bands, so a fixed-occupation SCF converges.
     """
     zv: float = 4.0
     alpha: float = 0.6102
-    v1: float = 3.042
-    v2: float = -1.372
+    v1: float = 6.084
+    v2: float = -2.744
     sig: float = 0.8
-    e_s: float = 0.8
-    e_p: float = 0.4
+    e_s: float = 0.3
+    e_p: float = 0.15
     rcut: float = 4.0       # real-space projector sphere radius (bohr)
 
     @property

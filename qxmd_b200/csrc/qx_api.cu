@@ -82,7 +82,26 @@ struct qx_ctx {
   double2 *d_zg = nullptr;
   double *d_part = nullptr, *d_sc = nullptr;
   double eion = 0.0, mixbeta = 0.3, q02 = 1.0;
+  // Pulay mixing (itratn > 1) or Kerker-filtered linear mixing
+  int itratn = 0;
+  double cmetric = 20.0, g2min = 0.0, g2max = 0.0;
+  bool pulay_reset = true;
+  PulayDev *d_pulay = nullptr;
+  double2 *d_pu = nullptr, *d_pd = nullptr;
+  double *d_ppart = nullptr, *d_adot = nullptr;
   bool scf_ready = false;
+  // sequential CG: device band cursor, dot-product buffer and the captured
+  // while-loop graph (rebuilt when its buffers or parameters change)
+  int *d_seqi = nullptr;   // cur, pairs[2], list[1]
+  double *d_seqw = nullptr;
+  int seqw_len = 0;
+  cudaStream_t cap_st = nullptr;
+  cudaGraph_t seq_graph = nullptr;
+  cudaGraphExec_t seq_exec = nullptr;
+  std::vector<char> seq_key;
+  long seq_body_launches = 0;
+  double *d_stage = nullptr;   // host-transfer staging (mixed precision)
+  long stage_len = 0;
   std::vector<void *> allocs;
   size_t tsize() const { return prec == QX_PREC_FP64 ? sizeof(double) : sizeof(float); }
 };
@@ -385,12 +404,27 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
 extern "C" int qx_destroy(qx_ctx *c) {
   if (!c) return QX_OK;
   cudaStreamSynchronize(c->st);
+  if (c->seq_exec) cudaGraphExecDestroy(c->seq_exec);
+  if (c->seq_graph) cudaGraphDestroy(c->seq_graph);
+  if (c->cap_st) cudaStreamDestroy(c->cap_st);
   for (void *p : c->allocs) cudaFree(p);
   delete c;
   return QX_OK;
 }
 
 // ---------------------------------------------------------------------------
+// FP64 staging area of a mixed-precision context for host transfers; grown
+// on demand and kept, so repeated transfers allocate nothing.
+static int stage(qx_ctx *c, long n, double **out) {
+  if (c->stage_len < n) {
+    if (c->d_stage) CK(cudaStreamSynchronize(c->st));
+    TRY(dalloc(c, &c->d_stage, sizeof(double) * n));
+    c->stage_len = n;
+  }
+  *out = c->d_stage;
+  return 0;
+}
+
 template <typename T>
 static int upload_conv(qx_ctx *c, T *dst, const double *src, long n) {
   if (sizeof(T) == sizeof(double)) {
@@ -398,10 +432,9 @@ static int upload_conv(qx_ctx *c, T *dst, const double *src, long n) {
     return 0;
   }
   double *tmp = nullptr;
-  CK(cudaMallocAsync((void **)&tmp, sizeof(double) * n, c->st));
+  TRY(stage(c, n, &tmp));
   CK(cudaMemcpyAsync(tmp, src, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   convert<double, T>(tmp, dst, n, c->st);
-  CK(cudaFreeAsync(tmp, c->st));
   CKL();
   return 0;
 }
@@ -414,10 +447,9 @@ static int download_conv(qx_ctx *c, double *dst, const T *src, long n) {
     return 0;
   }
   double *tmp = nullptr;
-  CK(cudaMallocAsync((void **)&tmp, sizeof(double) * n, c->st));
+  TRY(stage(c, n, &tmp));
   convert<T, double>(src, tmp, n, c->st);
   CK(cudaMemcpyAsync(dst, tmp, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaFreeAsync(tmp, c->st));
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }
@@ -831,8 +863,123 @@ static int eigen_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out
   c->have_hsub = false;
   return 0;
 }
+// One CG step of band *cur (the body of the sequential loop): preconditioned
+// direction, subgs3 against the snapshot of the bands below (already final),
+// subgs4, H|h> of this one band, BKL update and, once the band stops, the
+// move to the next band.
+template <typename T>
+static int seq_body(qx_ctx *c, const CgParm &pm, const SeqArgs &q) {
+  const int nb = c->nb, ne = c->ne;
+  T *x = (T *)c->psi, *hx = (T *)c->hpsi, *g = (T *)c->g, *h = (T *)c->h, *gh = (T *)c->gh;
+  const T *snap = (const T *)c->snap;
+  const CgState &s = c->cg;
+  cg_prec<T>(nb, ne, ne, g, h, c->d_dk, s, c->st, q.cur);
+  seq_dots<T>(nb, q.cur, ne, snap, ne, h, ne, q.cur, 1, nullptr, c->d_seqw, c->st);
+  seq_axpy<T>(nb, q.cur, ne, snap, ne, c->d_seqw, -1.0, h, ne, q.cur, c->st);
+  cg_orth<T>(nb, ne, ne, x, hx, h, s, c->st, q.cur);
+  CKL();
+  const int fl = QX_HPSI_KINETIC | (c->nlmode == QX_NL_RSPACE ? QX_HPSI_NONLOCAL : 0);
+  TRY(hpsi_impl<T>(c, h, gh, q.pairs, nullptr, 1, nullptr, nullptr, 1, fl));
+  if (c->nlmode == QX_NL_GSPACE) {
+    const Bufs<T> &b = c->pl.bufs<T>();
+    const int np = c->pl.nproj;
+    seq_dots<T>(np, nullptr, ne, b.kbg, ne, h, ne, q.cur, 2, b.vclalp, c->d_seqw, c->st);
+    seq_axpy<T>(np, nullptr, ne, b.kbg, ne, c->d_seqw, 1.0, gh, ne, q.cur, c->st);
+  }
+  cg_update_seq<T>(ne, ne, x, hx, g, h, gh, s, pm, q, c->st);
+  CKL();
+  return 0;
+}
+
+// The sequential loop as one graph: a while node whose body is seq_body,
+// captured once per set of buffers and parameters.  The body's last kernel
+// clears the loop condition after the last band, so a whole CG sweep is one
+// graph launch with no host round trip per band or step.
+template <typename T>
+static int seq_graph(qx_ctx *c, const qx_cgparm *p, const CgParm &pm) {
+  const Bufs<T> &b = c->pl.bufs<T>();
+  const void *keyp[] = {c->psi, c->hpsi, c->snap, b.kbg, b.vclalp};
+  std::vector<char> key(sizeof(keyp) + sizeof(qx_cgparm) + 2 * sizeof(int));
+  memcpy(key.data(), keyp, sizeof(keyp));
+  memcpy(key.data() + sizeof(keyp), p, sizeof(qx_cgparm));
+  const int extra[2] = {c->nlmode, c->pl.nproj};
+  memcpy(key.data() + sizeof(keyp) + sizeof(qx_cgparm), extra, sizeof(extra));
+  if (c->seq_exec && key == c->seq_key) return 0;
+  if (c->seq_exec) { cudaGraphExecDestroy(c->seq_exec); c->seq_exec = nullptr; }
+  if (c->seq_graph) { cudaGraphDestroy(c->seq_graph); c->seq_graph = nullptr; }
+  if (!c->cap_st) CK(cudaStreamCreateWithFlags(&c->cap_st, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  c->seq_graph = g;
+  cudaGraphConditionalHandle hd;
+  CK(cudaGraphConditionalHandleCreate(&hd, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = hd;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  SeqArgs q{c->d_seqi, c->d_seqi + 1, c->d_seqi + 3, c->snap, c->nb,
+            (sizeof(T) == sizeof(double) && p->ccreal4) ? 1 : 0, hd};
+  CK(cudaStreamBeginCaptureToGraph(c->cap_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaStream_t user = c->st;
+  c->st = c->cap_st;
+  const long l0 = g_launches.load();
+  const int r = seq_body<T>(c, pm, q);
+  c->seq_body_launches = g_launches.load() - l0;
+  g_launches.fetch_sub(c->seq_body_launches);
+  c->st = user;
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(c->cap_st, &captured);
+  if (r) return r;
+  CK(ec);
+  CK(cudaGraphInstantiate(&c->seq_exec, g, 0));
+  c->seq_key = key;
+  return 0;
+}
+
+// eigen_BKL on one rank: bands one after another, band ib projected against
+// the final vectors of bands < ib (the reference's own order within a rank).
+template <typename T>
+static int eigen_seq_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out) {
+  const int nb = c->nb, ne = c->ne;
+  CgParm pm{p->itermx, p->iteremx, p->noband, p->tolera, p->roughfzan, p->roughfeig, p->threinn, p->wdinner};
+  T *x = (T *)c->psi, *hx = (T *)c->hpsi, *g = (T *)c->g;
+  const int need = std::max(nb, c->pl.nproj);
+  if (c->seqw_len < need) {
+    TRY(dalloc(c, &c->d_seqw, sizeof(double) * need));
+    c->seqw_len = need;
+  }
+  if (!c->d_seqi) TRY(dalloc(c, &c->d_seqi, sizeof(int) * 4));
+  // No entry snapshot: band ib reads the columns of bands < ib only, and each
+  // of those is written with its final vector before band ib starts.
+  cg_init<T>(nb, ne, ne, x, hx, g, c->cg, c->st);
+  CKL();
+  TRY(seq_graph<T>(c, p, pm));
+  SeqArgs q{c->d_seqi, c->d_seqi + 1, c->d_seqi + 3, c->snap, nb, 0, 0};
+  seq_reset(q, c->st);
+  CKL();
+  CK(cudaGraphLaunch(c->seq_exec, c->st));
+  CK(cudaMemcpyAsync(c->d_eig, c->cg.eig, sizeof(double) * nb, cudaMemcpyDeviceToDevice, c->st));
+  std::vector<int> iters(nb);
+  CK(cudaMemcpyAsync(iters.data(), c->cg.iter, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  int nh = 0;
+  for (int b = 0; b < nb; ++b) nh += iters[b];
+  g_launches.fetch_add(c->seq_body_launches * nh);
+  if (nriter) memcpy(nriter, iters.data(), sizeof(int) * nb);
+  if (nhpsi_out) *nhpsi_out = nh;
+  c->have_hsub = false;
+  return 0;
+}
+
 extern "C" int qx_eigen(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi) {
   if (!c || !p) return QX_ERR_ARG;
+  if (p->sequential)
+    return c->prec == QX_PREC_FP64 ? eigen_seq_impl<double>(c, p, nriter, nhpsi)
+                                   : eigen_seq_impl<float>(c, p, nriter, nhpsi);
   return c->prec == QX_PREC_FP64 ? eigen_impl<double>(c, p, nriter, nhpsi) : eigen_impl<float>(c, p, nriter, nhpsi);
 }
 
@@ -905,12 +1052,56 @@ extern "C" int qx_scf_init(qx_ctx *c, const double *vloc, const double *cross, d
   c->eion = eion;
   c->mixbeta = mixbeta;
   c->q02 = q0 * q0;
+  // smallest and largest nonzero |G|^2 of the density sphere (the metric of
+  // the Pulay residual, reclat.f90:205 and chgdns.f90:661-668)
+  {
+    const int k1 = c->pl.k1, k2 = c->pl.k2, k3 = c->pl.k3;
+    double mn = 0.0, mx = 0.0;
+    for (int i3 = 0; i3 < k3; ++i3)
+      for (int i2 = 0; i2 < k2; ++i2)
+        for (int i1 = 0; i1 < k1; ++i1) {
+          const double d1 = i1 <= k1 / 2 ? i1 : i1 - k1, d2 = i2 <= k2 / 2 ? i2 : i2 - k2,
+                       d3 = i3 <= k3 / 2 ? i3 : i3 - k3;
+          const double gx = cross[0] * d1 + cross[3] * d2 + cross[6] * d3;
+          const double gy = cross[1] * d1 + cross[4] * d2 + cross[7] * d3;
+          const double gz = cross[2] * d1 + cross[5] * d2 + cross[8] * d3;
+          const double q = gx * gx + gy * gy + gz * gz;
+          if (q > 0.0 && q <= ecutdens) {
+            if (mn == 0.0 || q < mn) mn = q;
+            if (q > mx) mx = q;
+          }
+        }
+    c->g2min = mn;
+    c->g2max = mx;
+  }
   c->scf_ready = true;
+  return QX_OK;
+}
+
+extern "C" int qx_scf_mixing(qx_ctx *c, int itratn, double cmetric) {
+  if (!c || itratn < 0 || itratn > PULAY_MAX) {
+    set_error("qx_scf_mixing: itratn must be in [0, %d]", PULAY_MAX);
+    return QX_ERR_ARG;
+  }
+  if (!c->scf_ready) { set_error("qx_scf_mixing: call qx_scf_init first"); return QX_ERR_STATE; }
+  const long n = c->pl.n;
+  if (itratn > 1 && !c->d_pulay) {
+    TRY(dalloc(c, &c->d_pulay, sizeof(PulayDev)));
+    TRY(dalloc(c, &c->d_pu, sizeof(double2) * n * PULAY_MAX));
+    TRY(dalloc(c, &c->d_pd, sizeof(double2) * n * PULAY_MAX));
+    TRY(dalloc(c, &c->d_ppart, sizeof(double) * SCF_NBLK * PULAY_MAX));
+    TRY(dalloc(c, &c->d_adot, sizeof(double) * PULAY_MAX));
+    CK(cudaMemsetAsync(c->d_pulay, 0, sizeof(PulayDev), c->st));
+  }
+  c->itratn = itratn;
+  c->cmetric = cmetric;
+  c->pulay_reset = true;
   return QX_OK;
 }
 
 extern "C" int qx_scf_rho_from_psi(qx_ctx *c) {
   if (!c) return QX_ERR_ARG;
+  c->pulay_reset = true;
   TRY(qx_softchg(c));
   CK(cudaMemcpyAsync(c->d_rho_in, c->d_rho_out, sizeof(double) * c->pl.n, cudaMemcpyDeviceToDevice, c->st));
   return QX_OK;
@@ -935,7 +1126,28 @@ static int scf_potential(qx_ctx *c) {
   return 0;
 }
 
+// mxchgg_pulay (chgdns.f90:954-1120): both densities through one complex
+// transform, history, coefficients and the new density on the device.
+static int scf_mix_pulay(qx_ctx *c) {
+  const long n = c->pl.n;
+  const double bbb = c->g2max - c->cmetric * c->g2min;
+  const double q1 = bbb > 1.0e-5 ? (c->cmetric - 1.0) * c->g2max * c->g2min / bbb : 0.0;
+  PulayState p{c->d_pulay, c->d_pu, c->d_pd, c->itratn, q1};
+  pulay_push(p, c->pulay_reset ? 1 : 0, c->st);
+  c->pulay_reset = false;
+  pack2(c->d_rho_in, c->d_rho_out, c->d_zg, n, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0 / (double)n, c->st));
+  pulay_store(c->d_zg, c->d_g2, c->pl.k1, c->pl.k2, c->pl.k3, p, c->st);
+  pulay_coef(c->d_g2, n, p, c->rvol, c->d_ppart, c->d_adot, c->st);
+  pulay_new(c->d_g2, n, p, c->mixbeta, c->q02, c->d_zg, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, +1, 1.0, c->st));
+  take_real(c->d_rho_in, c->d_rho_out, c->d_zg, n, c->rvol / (double)n, c->d_part, c->d_sc + 3, c->st);
+  CKL();
+  return 0;
+}
+
 static int scf_mix(qx_ctx *c) {
+  if (c->itratn > 1) return scf_mix_pulay(c);
   const long n = c->pl.n;
   real_to_cplx(c->d_rho_out, c->d_rho_in, c->d_zg, n, c->st);
   TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0 / (double)n, c->st));

@@ -61,10 +61,11 @@ __global__ void __launch_bounds__(CGT) k_cg_init(int ne, long ldx, const T *__re
 // g <- prcd * g; zansap = <g|g>; h <- g + beta*h (h <- g on reset).
 template <typename T>
 __global__ void __launch_bounds__(CGT) k_cg_prec(int ne, long ldx, T *__restrict__ g, T *__restrict__ h,
-                                                         const double *__restrict__ dk, CgState s) {
+                                                         const double *__restrict__ dk, CgState s,
+                                                         const int *__restrict__ cur, int nb) {
   __shared__ double red[CGT / 32];
-  const int b = blockIdx.x;
-  if (!s.active[b]) return;
+  const int b = cur ? *cur : blockIdx.x;
+  if (b >= nb || !s.active[b]) return;
   T *gb = g + b * ldx, *hb = h + b * ldx;
   const double e15 = 1.5 * s.ekib[b];
   double z = 0.0;
@@ -105,10 +106,11 @@ __global__ void k_cg_mask(int nb, T *__restrict__ Pm, CgState s) {
 // subgs4: h -= <x|h> x; cai = <h|hx>.
 template <typename T>
 __global__ void __launch_bounds__(CGT) k_cg_orth(int ne, long ldx, const T *__restrict__ x,
-                                                         const T *__restrict__ hx, T *__restrict__ h, CgState s) {
+                                                         const T *__restrict__ hx, T *__restrict__ h, CgState s,
+                                                         const int *__restrict__ cur, int nb) {
   __shared__ double red[CGT / 32];
-  const int b = blockIdx.x;
-  if (!s.active[b]) return;
+  const int b = cur ? *cur : blockIdx.x;
+  if (b >= nb || !s.active[b]) return;
   const T *xb = x + b * ldx, *hxb = hx + b * ldx;
   T *hb = h + b * ldx;
   const double hhx = bdot(xb, (const T *)hb, ne, red);
@@ -147,13 +149,22 @@ __global__ void k_cg_list(int nb, CgState s) {
 
 // BKL 2x2 step (eigen.f90:593-622), line minimisation fallback (624-695),
 // x/hx update (698-709), residual and convergence test (731-764).
-template <typename T>
+// SEQ: one CTA on band *q.cur; when the band stops, its final vector becomes
+// its snapshot column (cgjr(:,ib) = gdcr(:,ibb), eigen.f90:699, real*4 when
+// q.ccreal4) and the next band starts.
+template <typename T, bool SEQ>
 __global__ void __launch_bounds__(CGT) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
                                                            T *__restrict__ g, const T *__restrict__ h,
-                                                           const T *__restrict__ gh, CgState s, CgParm pm) {
+                                                           const T *__restrict__ gh, CgState s, CgParm pm,
+                                                           SeqArgs q) {
   __shared__ double red[CGT / 32];
-  const int b = blockIdx.x;
-  if (!s.active[b]) return;
+  __shared__ int stop_sh;
+  const int b = SEQ ? *q.cur : blockIdx.x;
+  if (SEQ && b >= q.nb) {
+    if (threadIdx.x == 0) cudaGraphSetConditional(q.handle, 0);
+    return;
+  }
+  if (!SEQ && !s.active[b]) return;
   T *xb = x + b * ldx, *hxb = hx + b * ldx, *gb = g + b * ldx;
   const T *hb = h + b * ldx, *ghb = gh + b * ldx;
   const double dinx = s.dinnerx[b];   // read before thread 0 may update it
@@ -230,6 +241,91 @@ __global__ void __launch_bounds__(CGT) k_cg_update(int ne, long ldx, T *__restri
       s.zansab[b] = zansa;
       s.eigb[b] = e;
     }
+    stop_sh = stop;
+  }
+  if constexpr (SEQ) {
+    __syncthreads();
+    if (stop_sh) {
+      // each thread reads back the elements of x it wrote above
+      T *sb = (T *)q.snap + b * ldx;
+      for (int i = threadIdx.x; i < ne; i += blockDim.x) {
+        const T v = xb[i];
+        sb[i] = q.ccreal4 ? (T)(float)v : v;
+      }
+      if (threadIdx.x == 0) {
+        const int nx = b + 1;
+        *q.cur = nx;
+        q.pairs[0] = nx;
+        q.pairs[1] = -1;
+        q.list[0] = nx;
+        if (nx >= q.nb) cudaGraphSetConditional(q.handle, 0);
+      }
+    }
+  }
+}
+
+__global__ void k_seq_reset(SeqArgs q) {
+  *q.cur = 0;
+  q.pairs[0] = 0;
+  q.pairs[1] = -1;
+  q.list[0] = 0;
+}
+
+// Band-space dot products against band *cur: one CTA per vector j.
+template <typename T>
+__global__ void __launch_bounds__(256) k_seq_dots(int nmax, const int *__restrict__ n_dev, int ne,
+                                                  const T *__restrict__ V, long ldv, const T *__restrict__ Y, long ldy,
+                                                  const int *__restrict__ cur, int gamma, const T *__restrict__ scale,
+                                                  double *__restrict__ out) {
+  __shared__ double red[8];
+  const int j = blockIdx.x;
+  const int n = n_dev ? min(nmax, *n_dev) : nmax;
+  if (j >= n) return;
+  const T *v = V + j * ldv, *y = Y + (long)*cur * ldy;
+  double sum = 0.0;
+  for (int i = threadIdx.x; i < ne; i += blockDim.x) sum += (double)v[i] * (double)y[i];
+  sum = block_sum(sum, red);
+  if (threadIdx.x == 0) {
+    double r = 2.0 * sum - (double)v[0] * (double)y[0];
+    if (gamma == 2) r -= 2.0 * (double)v[1] * (double)y[1];
+    if (scale) r *= (double)scale[j];
+    out[j] = r;
+  }
+}
+
+// Y_cur[i] += sign * sum_j coef[j] V_j[i]: a CTA owns 32 consecutive rows (one
+// per lane); warp w takes j = w, w+8, ..., and the eight partial sums are added
+// in a fixed order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_seq_axpy(int nmax, const int *__restrict__ n_dev, int ne,
+                                                  const T *__restrict__ V, long ldv, const double *__restrict__ coef,
+                                                  double sign, T *__restrict__ Y, long ldy,
+                                                  const int *__restrict__ cur) {
+  __shared__ double part[8][33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
+  const int n = n_dev ? min(nmax, *n_dev) : nmax;
+  double acc = 0.0;
+  if (i < ne) {
+    int j = w;
+    for (; j + 24 < n; j += 32) {
+      const T a0 = V[(long)j * ldv + i], a1 = V[(long)(j + 8) * ldv + i];
+      const T a2 = V[(long)(j + 16) * ldv + i], a3 = V[(long)(j + 24) * ldv + i];
+      acc += coef[j] * (double)a0;
+      acc += coef[j + 8] * (double)a1;
+      acc += coef[j + 16] * (double)a2;
+      acc += coef[j + 24] * (double)a3;
+    }
+    for (; j < n; j += 8) acc += coef[j] * (double)V[(long)j * ldv + i];
+  }
+  part[w][lane] = acc;
+  __syncthreads();
+  if (w == 0 && i < ne) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += part[q][lane];
+    T *y = Y + (long)*cur * ldy;
+    y[i] = (T)((double)y[i] + sign * t);
   }
 }
 
@@ -283,20 +379,36 @@ __global__ void k_scale_rows(int nproj, int ncol, T *__restrict__ P, long ldp, c
 template <typename T> void cg_init(int nb, int ne, long ldx, const T *x, const T *hx, T *g, const CgState &s, cudaStream_t st) {
   k_cg_init<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, s); note_launch();
 }
-template <typename T> void cg_prec(int nb, int ne, long ldx, T *g, T *h, const double *dk, const CgState &s, cudaStream_t st) {
-  k_cg_prec<T><<<nb, CGT, 0, st>>>(ne, ldx, g, h, dk, s); note_launch();
+template <typename T> void cg_prec(int nb, int ne, long ldx, T *g, T *h, const double *dk, const CgState &s, cudaStream_t st,
+                                   const int *cur) {
+  k_cg_prec<T><<<cur ? 1 : nb, CGT, 0, st>>>(ne, ldx, g, h, dk, s, cur, nb); note_launch();
 }
 template <typename T> void cg_mask(int nb, T *Pm, const CgState &s, cudaStream_t st) {
   const long nn = (long)nb * nb;
   k_cg_mask<T><<<(int)((nn + 255) / 256), 256, 0, st>>>(nb, Pm, s); note_launch();
 }
-template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T *hx, T *h, const CgState &s, cudaStream_t st) {
-  k_cg_orth<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, h, s); note_launch();
+template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T *hx, T *h, const CgState &s, cudaStream_t st,
+                                   const int *cur) {
+  k_cg_orth<T><<<cur ? 1 : nb, CGT, 0, st>>>(ne, ldx, x, hx, h, s, cur, nb); note_launch();
 }
 void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); note_launch(); }
 template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
                                      const CgState &s, const CgParm &pm, cudaStream_t st) {
-  k_cg_update<T><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm); note_launch();
+  k_cg_update<T, false><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm, SeqArgs{}); note_launch();
+}
+template <typename T> void cg_update_seq(int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh, const CgState &s,
+                                         const CgParm &pm, const SeqArgs &q, cudaStream_t st) {
+  k_cg_update<T, true><<<1, CGT, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm, q); note_launch();
+}
+void seq_reset(const SeqArgs &q, cudaStream_t st) { k_seq_reset<<<1, 1, 0, st>>>(q); note_launch(); }
+template <typename T> void seq_dots(int nmax, const int *n_dev, int ne, const T *V, long ldv, const T *Y, long ldy,
+                                    const int *cur, int gamma, const T *scale, double *out, cudaStream_t st) {
+  if (nmax <= 0) return;
+  k_seq_dots<T><<<nmax, 256, 0, st>>>(nmax, n_dev, ne, V, ldv, Y, ldy, cur, gamma, scale, out); note_launch();
+}
+template <typename T> void seq_axpy(int nmax, const int *n_dev, int ne, const T *V, long ldv, const double *coef,
+                                    double sign, T *Y, long ldy, const int *cur, cudaStream_t st) {
+  k_seq_axpy<T><<<(ne + 31) / 32, 256, 0, st>>>(nmax, n_dev, ne, V, ldv, coef, sign, Y, ldy, cur); note_launch();
 }
 template <typename T> void ekin(int nb, int ne, long ldx, const T *x, const double *dk, double *ekib, cudaStream_t st) {
   k_ekin<T><<<nb, CGT, 0, st>>>(ne, ldx, x, dk, ekib); note_launch();
@@ -313,9 +425,17 @@ template <typename T> void scale_rows(int nproj, int ncol, T *P, long ldp, const
 
 #define QX_INST(T)                                                                                          \
   template void cg_init<T>(int, int, long, const T *, const T *, T *, const CgState &, cudaStream_t);        \
-  template void cg_prec<T>(int, int, long, T *, T *, const double *, const CgState &, cudaStream_t);          \
+  template void cg_prec<T>(int, int, long, T *, T *, const double *, const CgState &, cudaStream_t,          \
+                           const int *);                                                                    \
   template void cg_mask<T>(int, T *, const CgState &, cudaStream_t);                                         \
-  template void cg_orth<T>(int, int, long, const T *, const T *, T *, const CgState &, cudaStream_t);        \
+  template void cg_orth<T>(int, int, long, const T *, const T *, T *, const CgState &, cudaStream_t,         \
+                           const int *);                                                                    \
+  template void cg_update_seq<T>(int, long, T *, T *, T *, const T *, const T *, const CgState &,            \
+                                 const CgParm &, const SeqArgs &, cudaStream_t);                            \
+  template void seq_dots<T>(int, const int *, int, const T *, long, const T *, long, const int *, int,      \
+                            const T *, double *, cudaStream_t);                                             \
+  template void seq_axpy<T>(int, const int *, int, const T *, long, const double *, double, T *, long,      \
+                            const int *, cudaStream_t);                                                     \
   template void cg_update<T>(int, int, long, T *, T *, T *, const T *, const T *, const CgState &,            \
                              const CgParm &, cudaStream_t);                                                  \
   template void ekin<T>(int, int, long, const T *, const double *, double *, cudaStream_t);                  \

@@ -27,8 +27,8 @@ EXPORTS = [
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
-    "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_rho_from_psi",
-    "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
+    "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing",
+    "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
 ]
 
@@ -42,13 +42,14 @@ class QxError(RuntimeError):
 class CgParm(C.Structure):
     _fields_ = [("itermx", C.c_int), ("iteremx", C.c_int), ("noband", C.c_int),
                 ("tolera", C.c_double), ("roughfzan", C.c_double), ("roughfeig", C.c_double),
-                ("threinn", C.c_double), ("wdinner", C.c_double), ("ccreal4", C.c_int)]
+                ("threinn", C.c_double), ("wdinner", C.c_double), ("ccreal4", C.c_int),
+                ("sequential", C.c_int)]
 
     @classmethod
     def defaults(cls, noband, **kw):
         """Defaults of modules.f90:171-182."""
         p = dict(itermx=4, iteremx=4, noband=noband, tolera=1e-10, roughfzan=0.3,
-                 roughfeig=0.3, threinn=0.0, wdinner=0.9, ccreal4=0)
+                 roughfeig=0.3, threinn=0.0, wdinner=0.9, ccreal4=0, sequential=0)
         p.update(kw)
         return cls(**p)
 
@@ -112,6 +113,7 @@ def lib(build_if_missing: bool = True):
         "qx_schmidt": ([_ctx], C.c_int),
         "qx_softchg": ([_ctx], C.c_int),
         "qx_scf_init": ([_ctx, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
+        "qx_scf_mixing": ([_ctx, C.c_int, C.c_double], C.c_int),
         "qx_scf_rho_from_psi": ([_ctx], C.c_int),
         "qx_scf_iteration": ([_ctx, C.POINTER(CgParm), C.POINTER(ScfOut)], C.c_int),
         "qxgpu_hcnonloc": ([_ctx, _dp, _dp, C.c_int], C.c_int),
@@ -296,6 +298,11 @@ class Context:
         s = self.sys
         _ck(self.L.qx_scf_init(self.h, _f64(s.vloc), _f64(s.gs.cross.ravel(order="F")),
                                s.gs.ecutdens, s.eewald, mixbeta, kerker_q0), "qx_scf_init")
+
+    def scf_mixing(self, itratn=10, cmetric=20.0):
+        """Pulay mixing with the reference defaults (itratn 10, cmetric 20);
+        itratn <= 1 returns to Kerker-filtered linear mixing."""
+        _ck(self.L.qx_scf_mixing(self.h, int(itratn), float(cmetric)), "qx_scf_mixing")
 
     def scf_rho_from_psi(self):
         _ck(self.L.qx_scf_rho_from_psi(self.h), "qx_scf_rho_from_psi")

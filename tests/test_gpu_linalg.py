@@ -99,6 +99,42 @@ def test_eigen_snapshot_semantics_real4(si8, si8_psi):
     assert relerr(x, ref[0]) < 1e-8
 
 
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+@pytest.mark.parametrize("nlmode", [QX_NL_GSPACE, QX_NL_RSPACE])
+def test_eigen_bkl_sequential(si8, si8_psi, prec, nlmode):
+    """One-rank order: bands one after another, each against the final
+    vectors of the bands below (one graph launch for the sweep)."""
+    need_gpu()
+    h = oracle.Ham(si8, nlmode)
+    hc = h.hpsi(si8_psi)
+    _, ekib = h.ekinetic(si8_psi)
+    x_ref, hx_ref, eig_ref, _, nri_ref = h.eigen(si8_psi, hc, ekib, noband=16, sequential=True)
+    ctx = Context(si8, prec, nlmode)
+    p = CgParm.defaults(16, sequential=1)
+    for _ in range(2):   # the second call replays the cached graph
+        x, hx, eig = ctx.eigen_host(si8_psi, hc, ekib, p)
+        if prec == QX_PREC_FP64:
+            assert relerr(eig, eig_ref) < 1e-10
+            assert relerr(x, x_ref) < 1e-8
+            assert relerr(hx, hx_ref) < 1e-8
+        else:
+            assert relerr(eig, eig_ref) < 1e-4
+            assert relerr(x, x_ref) < 1e-2
+
+
+def test_eigen_sequential_real4(si8, si8_psi):
+    """One-rank order with the real*4 snapshot of the CCREAL4 build."""
+    need_gpu()
+    h = oracle.Ham(si8, 1)
+    hc = h.hpsi(si8_psi)
+    _, ekib = h.ekinetic(si8_psi)
+    ref = h.eigen(si8_psi, hc, ekib, noband=16, ccreal4=True, sequential=True)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    x, hx, eig = ctx.eigen_host(si8_psi, hc, ekib, CgParm.defaults(16, ccreal4=1, sequential=1))
+    assert relerr(eig, ref[2]) < 1e-10
+    assert relerr(x, ref[0]) < 1e-8
+
+
 @pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-12), (QX_PREC_MIXED, 1e-5)])
 def test_softchg(si8, si8_psi, prec, tol):
     need_gpu()

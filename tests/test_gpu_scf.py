@@ -1,5 +1,6 @@
 """Whole SCF iterations (pwlda.f90:1628-3700 order) on the device against the
-oracle's iteration on the same inputs (Si8, G-space and real-space KB)."""
+oracle's iteration on the same inputs (Si8, G-space and real-space KB; linear
+Kerker and Pulay density mixing; batched and one-rank CG order)."""
 import numpy as np
 import pytest
 
@@ -43,3 +44,24 @@ def test_scf_mixed_tracks_fp64(si8, si8_psi):
     # same trajectory to FP32 accuracy over the first iterations
     assert abs(e[QX_PREC_MIXED][0] - e[QX_PREC_FP64][0]) < 1e-3
     assert abs(e[QX_PREC_MIXED][-1] - e[QX_PREC_FP64][-1]) < 5e-2
+
+
+@pytest.mark.parametrize("sequential", [0, 1])
+def test_scf_pulay_matches_oracle_fp64(si8, si8_psi, sequential):
+    """Pulay mixing (mxchgg_pulay, chgdns.f90:954-1120) with the reference
+    defaults aslh 0.8, bslh 0.64, cmetric 20, here with a 4-entry history so
+    that the restart after a full history is crossed too."""
+    need_gpu()
+    st = ScfState(si8, si8_psi, nlmode=QX_NL_GSPACE, mixbeta=0.8, kerker_q0=0.8, pulay=4)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    ctx.put_psi(si8_psi)
+    ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)
+    ctx.scf_mixing(4, 20.0)
+    ctx.scf_rho_from_psi()
+    p = CgParm.defaults(16, sequential=sequential)
+    for it in range(7):
+        g = ctx.scf_iteration(p)
+        r = st.iteration(noband=16, sequential=bool(sequential))
+        assert g["etot"] == pytest.approx(r["etot"], abs=1e-8 * max(1.0, abs(r["etot"])))
+        assert g["ncg_hpsi"] == r["ncg_hpsi"]
+        assert g["resid"] == pytest.approx(r["resid"], rel=1e-6)
