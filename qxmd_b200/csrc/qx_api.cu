@@ -102,6 +102,18 @@ struct qx_ctx {
   long seq_body_launches = 0;
   double *d_stage = nullptr;   // host-transfer staging (mixed precision)
   long stage_len = 0;
+  // SCF iteration without host round trips: results go to device slots
+  // (d_sc[5..6] gradres max/sum, d_info[0] eigen clusters, d_info[1] Cholesky
+  // status, d_info[2] CG band applications) read once at the end, and the
+  // whole iteration is captured as a graph per buffer arrangement
+  bool defer = false;
+  struct ScfGraph {
+    std::vector<char> key;
+    cudaGraphExec_t exec = nullptr;
+    void *psi = nullptr, *hpsi = nullptr, *tmp = nullptr;   // pointer arrangement after the iteration
+    long launches = 0;
+  };
+  std::vector<ScfGraph> scf_graphs;
   std::vector<void *> allocs;
   size_t tsize() const { return prec == QX_PREC_FP64 ? sizeof(double) : sizeof(float); }
 };
@@ -404,6 +416,7 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
 extern "C" int qx_destroy(qx_ctx *c) {
   if (!c) return QX_OK;
   cudaStreamSynchronize(c->st);
+  for (auto &g : c->scf_graphs) cudaGraphExecDestroy(g.exec);
   if (c->seq_exec) cudaGraphExecDestroy(c->seq_exec);
   if (c->seq_graph) cudaGraphDestroy(c->seq_graph);
   if (c->cap_st) cudaStreamDestroy(c->cap_st);
@@ -762,6 +775,11 @@ template <typename T>
 static int gradres_impl(qx_ctx *c, double *prod, double *zmax, double *zsum) {
   gradres<T>(c->nb, c->ne, c->ne, (const T *)c->psi, (const T *)c->hpsi, c->d_eig, c->d_prod, c->st);
   CKL();
+  if (c->defer) {
+    gradres_stats(c->d_prod, c->have_occ ? c->d_occ : nullptr, c->nb, c->d_sc + 5, c->st);
+    CKL();
+    return 0;
+  }
   std::vector<double> p(c->nb), o(c->nb, 0.0);
   CK(cudaMemcpyAsync(p.data(), c->d_prod, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
   if (c->have_occ) CK(cudaMemcpyAsync(o.data(), c->d_occ, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
@@ -796,17 +814,18 @@ static int untryt_impl(qx_ctx *c, double *ev, int *sweeps) {
   CK(cudaMemcpyAsync(c->d_mat, c->d_hsub, sizeof(double) * nb * nb, cudaMemcpyDeviceToDevice, c->st));
   TRY(syev(c->d_mat, nb, c->d_w, c->d_V, c->d_eigws, c->d_info, c->st));
   CKL();
-  int info = 0;
-  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   // U in the working precision for the GEMMs
   convert<double, T>(c->d_V, (T *)c->mat_t, (long)nb * nb, c->st);
   CKL();
   TRY(rotate<T>(c, c->psi));
+  c->have_u = true;
+  c->have_hsub = false;
+  if (c->defer) return 0;   // status read with the iteration's results
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (info <= 0) { set_error("untryt: eigen-decomposition produced no eigenvectors"); return QX_ERR_EIG; }
   if (sweeps) *sweeps = info;
-  c->have_u = true;
-  c->have_hsub = false;
   if (ev) CK(cudaMemcpy(ev, c->d_w, sizeof(double) * nb, cudaMemcpyDeviceToHost));
   return 0;
 }
@@ -854,6 +873,12 @@ static int eigen_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out
   }
   // eig and iteration counts
   CK(cudaMemcpyAsync(c->d_eig, s.eig, sizeof(double) * nb, cudaMemcpyDeviceToDevice, c->st));
+  c->have_hsub = false;
+  if (c->defer) {
+    iter_sum(s.iter, nb, c->d_info + 2, c->st);
+    CKL();
+    return 0;
+  }
   std::vector<int> iters(nb);
   CK(cudaMemcpyAsync(iters.data(), s.iter, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -963,6 +988,7 @@ static int eigen_seq_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi
   CKL();
   CK(cudaGraphLaunch(c->seq_exec, c->st));
   CK(cudaMemcpyAsync(c->d_eig, c->cg.eig, sizeof(double) * nb, cudaMemcpyDeviceToDevice, c->st));
+  if (c->defer) iter_sum(c->cg.iter, nb, c->d_info + 2, c->st);
   std::vector<int> iters(nb);
   CK(cudaMemcpyAsync(iters.data(), c->cg.iter, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -990,12 +1016,14 @@ static int schmidt_impl(qx_ctx *c) {
   TRY(gemm<T>(true, false, nb, nb, ne, (T)1, (const T *)c->psi, ne, (const T *)c->psi, ne, (T)0, m, nb, 1, nullptr,
               nullptr, c->st, c->gws, c->gws_bytes));
   convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
-  TRY(cholinv(c->d_mat, nb, c->d_eigws, c->d_info, c->st));
+  TRY(cholinv(c->d_mat, nb, c->d_eigws, c->d_info + 1, c->st));
   CKL();
-  int info = 0;
-  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  if (info) { set_error("schmidt: <psi|psi> not positive definite at band %d", info - 1); return QX_ERR_NOTPD; }
+  if (!c->defer) {   // deferred: the status is read with the iteration's results
+    int info = 0;
+    CK(cudaMemcpyAsync(&info, c->d_info + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (info) { set_error("schmidt: <psi|psi> not positive definite at band %d", info - 1); return QX_ERR_NOTPD; }
+  }
   convert<double, T>(c->d_mat, m, (long)nb * nb, c->st);
   // psi <- psi * Linv^T
   TRY(gemm<T>(false, true, ne, nb, nb, (T)1, (const T *)c->psi, ne, m, nb, (T)0, (T *)c->tmp, ne, 0, nullptr, nullptr,
@@ -1158,26 +1186,116 @@ static int scf_mix(qx_ctx *c) {
   return 0;
 }
 
-extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
-  if (!c || !p) return QX_ERR_ARG;
-  if (!c->scf_ready || !c->have_occ) { set_error("qx_scf_iteration: call qx_scf_init and qx_set_occ first"); return QX_ERR_STATE; }
+// One SCF iteration in pwlda_md order with every status and summary left on
+// the device (c->defer): no host round trip between the first kernel and the
+// final read.
+template <typename T>
+static int scf_body(qx_ctx *c, const qx_cgparm *p) {
   TRY(scf_potential(c));
   TRY(qx_enonloc(c));
   TRY(qx_hmatrix(c, nullptr));
-  double zmax = 0.0, zsum = 0.0;
-  if (out) TRY(qx_gradres(c, nullptr, &zmax, &zsum));
-  int sweeps = 0;
-  TRY(c->prec == QX_PREC_FP64 ? untryt_impl<double>(c, nullptr, &sweeps) : untryt_impl<float>(c, nullptr, &sweeps));
+  TRY(gradres_impl<T>(c, nullptr, nullptr, nullptr));
+  TRY(untryt_impl<T>(c, nullptr, nullptr));
   TRY(qx_untryhc(c));
   band_energy(c->d_w, c->d_occ, c->nb, c->d_sc + 4, c->st);
-  int nh = 0;
-  TRY(qx_eigen(c, p, nullptr, &nh));
+  CKL();
+  TRY(qx_eigen(c, p, nullptr, nullptr));
   TRY(qx_schmidt(c));
   TRY(qx_softchg(c));
   TRY(scf_mix(c));
-  double sc[5];
-  CK(cudaMemcpyAsync(sc, c->d_sc, sizeof(double) * 5, cudaMemcpyDeviceToHost, c->st));
+  return 0;
+}
+
+// QX_GRAPH=0 runs the same sync-free iteration as plain stream launches.
+static bool scf_graphs_enabled() {
+  const char *e = getenv("QX_GRAPH");
+  return !(e && e[0] == '0');
+}
+
+// The iteration as a CUDA graph: captured once per arrangement of the
+// rotating psi/hpsi/tmp buffers (two alternate), mixing restart flag and CG
+// parameters, then replayed.  The one-rank CG order launches its own graph
+// and runs outside this one.
+template <typename T>
+static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
+  const void *keyp[] = {c->psi, c->hpsi, c->tmp};
+  const int keyi[] = {c->pulay_reset ? 1 : 0, c->itratn, c->nlmode};
+  std::vector<char> key(sizeof(keyp) + sizeof(keyi) + sizeof(qx_cgparm));
+  memcpy(key.data(), keyp, sizeof(keyp));
+  memcpy(key.data() + sizeof(keyp), keyi, sizeof(keyi));
+  memcpy(key.data() + sizeof(keyp) + sizeof(keyi), p, sizeof(qx_cgparm));
+  qx_ctx::ScfGraph *g = nullptr;
+  for (auto &e : c->scf_graphs)
+    if (e.key == key) g = &e;
+  if (!g) {
+    if (c->scf_graphs.size() >= 4) {
+      for (auto &e : c->scf_graphs) cudaGraphExecDestroy(e.exec);
+      c->scf_graphs.clear();
+    }
+    if (!c->cap_st) CK(cudaStreamCreateWithFlags(&c->cap_st, cudaStreamNonBlocking));
+    // the capture runs the host side of the iteration (pointer rotation,
+    // flags) without executing anything; the graph then does the work
+    void *psi0 = c->psi, *hpsi0 = c->hpsi, *tmp0 = c->tmp;
+    const bool reset0 = c->pulay_reset;
+    CK(cudaStreamBeginCapture(c->cap_st, cudaStreamCaptureModeThreadLocal));
+    cudaStream_t user = c->st;
+    c->st = c->cap_st;
+    const long l0 = g_launches.load();
+    const int r = scf_body<T>(c, p);
+    const long nl = g_launches.load() - l0;
+    g_launches.fetch_sub(nl);
+    c->st = user;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->cap_st, &graph);
+    if (r || ec != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      c->psi = psi0; c->hpsi = hpsi0; c->tmp = tmp0; c->pulay_reset = reset0;
+      if (!r) set_error("qx_scf_iteration: graph capture failed: %s", cudaGetErrorString(ec));
+      return r ? r : QX_ERR_CUDA;
+    }
+    qx_ctx::ScfGraph e;
+    e.key = key;
+    e.psi = c->psi; e.hpsi = c->hpsi; e.tmp = c->tmp;
+    e.launches = nl;
+    const cudaError_t ei = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    c->psi = psi0; c->hpsi = hpsi0; c->tmp = tmp0;
+    if (ei != cudaSuccess) {
+      c->pulay_reset = reset0;
+      set_error("qx_scf_iteration: graph instantiation failed: %s", cudaGetErrorString(ei));
+      return QX_ERR_CUDA;
+    }
+    c->scf_graphs.push_back(e);
+    g = &c->scf_graphs.back();
+  }
+  CK(cudaGraphLaunch(g->exec, c->st));
+  g_launches.fetch_add(g->launches);
+  c->psi = g->psi; c->hpsi = g->hpsi; c->tmp = g->tmp;
+  c->pulay_reset = false;
+  c->have_glocal = true;
+  c->have_u = true;
+  c->have_hsub = false;
+  return 0;
+}
+
+extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
+  if (!c || !p) return QX_ERR_ARG;
+  if (!c->scf_ready || !c->have_occ) { set_error("qx_scf_iteration: call qx_scf_init and qx_set_occ first"); return QX_ERR_STATE; }
+  c->defer = true;
+  int r;
+  if (scf_graphs_enabled() && !p->sequential)
+    r = c->prec == QX_PREC_FP64 ? scf_graph_launch<double>(c, p) : scf_graph_launch<float>(c, p);
+  else
+    r = c->prec == QX_PREC_FP64 ? scf_body<double>(c, p) : scf_body<float>(c, p);
+  c->defer = false;
+  TRY(r);
+  double sc[7];
+  int info[3];
+  CK(cudaMemcpyAsync(sc, c->d_sc, sizeof(double) * 7, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(info, c->d_info, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (info[0] <= 0) { set_error("untryt: eigen-decomposition produced no eigenvectors"); return QX_ERR_EIG; }
+  if (info[1]) { set_error("schmidt: <psi|psi> not positive definite at band %d", info[1] - 1); return QX_ERR_NOTPD; }
   if (out) {
     out->ehartree = sc[0];
     out->exc = sc[1];
@@ -1185,9 +1303,9 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
     out->resid = sc[3];
     out->eband = sc[4];
     out->etot = sc[4] - sc[0] + sc[1] - sc[2] + c->eion;
-    out->zmax = zmax;
-    out->ncg_hpsi = nh;
-    out->eig_clusters = sweeps;
+    out->zmax = sc[5];
+    out->ncg_hpsi = info[2];
+    out->eig_clusters = info[0];
   }
   return QX_OK;
 }

@@ -362,6 +362,32 @@ __global__ void __launch_bounds__(CGT) k_gradres(int ne, long ldx, const T *__re
   if (threadIdx.x == 0) prod[b] = 2.0 * s - r0 * r0;
 }
 
+// Device-side summaries for a sync-free SCF iteration: out[0] = max_b prod,
+// out[1] = sum_b occ_b prod_b (gradresnv's zmax and occupation-weighted sum).
+__global__ void k_gradres_stats(const double *__restrict__ prod, const double *__restrict__ occ, int nb,
+                                double *__restrict__ out) {
+  const int lane = threadIdx.x;
+  double m = 0.0, s = 0.0;
+  for (int b = lane; b < nb; b += 32) {
+    m = fmax(m, prod[b]);
+    if (occ) s += occ[b] * prod[b];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  if (lane == 0) { out[0] = m; out[1] = s; }
+}
+
+// *out = sum of the per-band CG iteration counts (H|psi> band applications).
+__global__ void k_iter_sum(const int *__restrict__ iter, int nb, int *__restrict__ out) {
+  const int lane = threadIdx.x;
+  int s = 0;
+  for (int b = lane; b < nb; b += 32) s += iter[b];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) *out = s;
+}
+
 // Row scaling of the projection matrix P (nproj x ncol, column-major, columns
 // through colmap): P(j, n) *= v(j).
 template <typename T>
@@ -392,6 +418,10 @@ template <typename T> void cg_orth(int nb, int ne, long ldx, const T *x, const T
   k_cg_orth<T><<<cur ? 1 : nb, CGT, 0, st>>>(ne, ldx, x, hx, h, s, cur, nb); note_launch();
 }
 void cg_list(int nb, const CgState &s, cudaStream_t st) { k_cg_list<<<1, 32, 0, st>>>(nb, s); note_launch(); }
+void gradres_stats(const double *prod, const double *occ, int nb, double *out, cudaStream_t st) {
+  k_gradres_stats<<<1, 32, 0, st>>>(prod, occ, nb, out); note_launch();
+}
+void iter_sum(const int *iter, int nb, int *out, cudaStream_t st) { k_iter_sum<<<1, 32, 0, st>>>(iter, nb, out); note_launch(); }
 template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
                                      const CgState &s, const CgParm &pm, cudaStream_t st) {
   k_cg_update<T, false><<<nb, CGT, 0, st>>>(ne, ldx, x, hx, g, h, gh, s, pm, SeqArgs{}); note_launch();

@@ -52,6 +52,8 @@ template <typename T> void seq_dots(int nmax, const int *n_dev, int ne, const T 
 template <typename T> void seq_axpy(int nmax, const int *n_dev, int ne, const T *V, long ldv, const double *coef,
                                     double sign, T *Y, long ldy, const int *cur, cudaStream_t st);
 void cg_list(int nb, const CgState &s, cudaStream_t st);
+void gradres_stats(const double *prod, const double *occ, int nb, double *out, cudaStream_t st);
+void iter_sum(const int *iter, int nb, int *out, cudaStream_t st);
 template <typename T> void cg_update(int nb, int ne, long ldx, T *x, T *hx, T *g, const T *h, const T *gh,
                                      const CgState &s, const CgParm &pm, cudaStream_t st);
 template <typename T> void ekin(int nb, int ne, long ldx, const T *x, const double *dk, double *ekib, cudaStream_t st);

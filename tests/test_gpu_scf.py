@@ -65,3 +65,29 @@ def test_scf_pulay_matches_oracle_fp64(si8, si8_psi, sequential):
         assert g["etot"] == pytest.approx(r["etot"], abs=1e-8 * max(1.0, abs(r["etot"])))
         assert g["ncg_hpsi"] == r["ncg_hpsi"]
         assert g["resid"] == pytest.approx(r["resid"], rel=1e-6)
+
+
+def test_scf_graph_replay_matches_stream_launches(si8, si8_psi, monkeypatch):
+    """The iteration captured as a CUDA graph (and replayed for the alternating
+    buffer arrangements) gives the same numbers as the same launches issued
+    one by one."""
+    need_gpu()
+    p = CgParm.defaults(16)
+    res = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("QX_GRAPH", mode)
+        for prec in (QX_PREC_FP64, QX_PREC_MIXED):
+            ctx = Context(si8, prec, QX_NL_GSPACE)
+            ctx.put_psi(si8_psi)
+            ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)
+            ctx.scf_mixing(10, 20.0)
+            ctx.scf_rho_from_psi()
+            outs = [ctx.scf_iteration(p) for _ in range(6)]
+            res[mode, prec] = (outs, ctx.get_psi(), ctx.get_rho())
+    for prec in (QX_PREC_FP64, QX_PREC_MIXED):
+        (oa, pa, ra), (ob, pb, rb) = res["0", prec], res["1", prec]
+        for a, b in zip(oa, ob):
+            assert a["etot"] == b["etot"] and a["ncg_hpsi"] == b["ncg_hpsi"]
+            assert a["eig_clusters"] == b["eig_clusters"] and a["zmax"] == b["zmax"]
+        np.testing.assert_array_equal(pa, pb)
+        np.testing.assert_array_equal(ra, rb)
