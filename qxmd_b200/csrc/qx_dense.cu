@@ -111,8 +111,12 @@ __device__ __forceinline__ void warp_trinv(const double *L, int ldl, const doubl
   __syncwarp();
 }
 
+// USE_SMEM: the matrix lives in shared memory, and the compiler sees that
+// every access to it is a shared-memory access (no generic addressing).
+template <bool USE_SMEM>
 __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n, double *__restrict__ work,
-                                                  int *__restrict__ info, int use_smem) {
+                                                  int *__restrict__ info) {
+  constexpr bool use_smem = USE_SMEM;
   extern __shared__ double sm[];
   __shared__ int bad;
   const int ld = use_smem ? (n | 1) : n;
@@ -248,11 +252,13 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
   const int use = bytes <= CH_SMEM_MAX;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_cholinv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
+    cudaFuncSetAttribute(k_cholinv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
     attr = true;
   }
   if (!use && !work) { set_error("cholinv: n=%d needs a work buffer", n); return 1; }
-  k_cholinv<<<1, CHT, use ? bytes : 0, st>>>(S, n, work, d_info, use); note_launch();
+  if (use) k_cholinv<true><<<1, CHT, bytes, st>>>(S, n, work, d_info);
+  else k_cholinv<false><<<1, CHT, 0, st>>>(S, n, work, d_info);
+  note_launch();
   return 0;
 }
 
@@ -315,9 +321,11 @@ __device__ __forceinline__ void house(double x0, double sigma, double &tau, doub
 // starts only after barrier (1) of the next column.
 // gvec: 7n doubles of global memory for v (two buffers), p and part when A
 // is not in shared memory.
+template <bool USE_SMEM>
 __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n, double *__restrict__ d,
                                                  double *__restrict__ e, double *__restrict__ HV,
-                                                 double *__restrict__ tau, int use_smem, double *__restrict__ gvec) {
+                                                 double *__restrict__ tau, double *__restrict__ gvec) {
+  constexpr bool use_smem = USE_SMEM;
   extern __shared__ double sm[];
   __shared__ double sc[2];
   const int ld = use_smem ? (n | 1) : n;
@@ -691,7 +699,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
          *ws = Z + (long)n * n;   // 6 * n * NT <= 6n^2 + 762n: total <= 8n^2 + 772n
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_sytrd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM_MAX);
+    cudaFuncSetAttribute(k_sytrd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM_MAX);
     cudaFuncSetAttribute(k_backtrans, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_invit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
@@ -699,7 +707,9 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   const size_t smem = sizeof(double) * ((size_t)(n | 1) * n + 7 * (size_t)n);
   const int use = smem <= TRD_SMEM_MAX;
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
-  k_sytrd<<<1, TRD_T, use ? smem : 0, st>>>(A, n, d, e, HV, tau, use, vp); note_launch();
+  if (use) k_sytrd<true><<<1, TRD_T, smem, st>>>(A, n, d, e, HV, tau, vp);
+  else k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
+  note_launch();
   if (n == 1) {
     cudaMemcpyAsync(w, d, sizeof(double), cudaMemcpyDeviceToDevice, st);
     static const double one = 1.0;
