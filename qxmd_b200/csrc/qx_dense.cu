@@ -244,6 +244,242 @@ __global__ void __launch_bounds__(CHT) k_cholinv(double *__restrict__ Sg, int n,
   if (tid == 0) *info = 0;
 }
 
+// --------------------------------------------------------------------------
+// The same result for n <= CP_MAXN (and within shared memory), 12 warps, one
+// n x n shared-memory matrix (odd leading dimension) holding L in the lower
+// triangle and X^T = (L^-1)^T strictly above it (X's diagonal apart):
+//  * Cholesky right-looking in panels of PB = 8 columns: warp 0 factors the
+//    panel in registers (rows lane + 32 q, column values by shuffle, no CTA
+//    barrier inside the panel) and copies it row-major to Pr; all warps then
+//    apply the rank-8 update to the trailing lower triangle;
+//  * inverse in 32 x 32 blocks: the diagonal blocks inverted side by side
+//    (one warp each); M_IK = -X_II L_IK in place of L_IK (all blocks at
+//    once); X_IJ = sum_{K=J}^{I-1} M_IK X_KJ by block diagonals d = I - J
+//    (the blocks of one diagonal at once, two warps a block).  Every inner
+//    loop runs over compile-time indices into registers.
+constexpr int CPT = 384, CPW = CPT / 32, PB = 8, CP_MQ = 6;
+constexpr int CP_MAXN = 32 * CP_MQ;   // also bounded by shared memory
+
+__global__ void __launch_bounds__(CPT) k_cholinv_sm(double *__restrict__ Sg, int n, int *__restrict__ info) {
+  extern __shared__ double smf[];
+  __shared__ int bad;
+  const int ld = n | 1;
+  double *A = smf, *xd = A + (long)ld * n, *rd = xd + n, *Pr = rd + n;   // Pr: PB * n
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#define AA(i, j) A[(j) * ld + (i)]
+  if (tid == 0) bad = 0;
+  for (int j = warp; j < n; j += CPW)
+    for (int i = j + lane; i < n; i += 32) AA(i, j) = Sg[(long)j * n + i];
+  __syncthreads();
+  // ---------------- Cholesky ----------------
+  for (int j0 = 0; j0 < n; j0 += PB) {
+    const int pb = min(PB, n - j0);
+    if (warp == 0) {
+      double a[CP_MQ][PB];
+#pragma unroll
+      for (int q = 0; q < CP_MQ; ++q) {
+        const int r = j0 + lane + 32 * q, rr = min(r, n - 1);
+#pragma unroll
+        for (int c = 0; c < PB; ++c) {
+          const double v = AA(rr, min(j0 + c, n - 1));   // clamped address, then selection
+          a[q][c] = (c < pb && r < n && r >= j0 + c) ? v : 0.0;
+        }
+      }
+      int b = 0;
+#pragma unroll
+      for (int c = 0; c < PB; ++c) {
+        if (c < pb && b == 0) {   // uniform
+          const double piv = __shfl_sync(0xffffffffu, a[0][c], c);   // row j0 + c: lane c, q 0
+          if (!(piv > 1.0e-30)) {   // uniform; also catches NaN
+            b = 1 + j0 + c;
+          } else {
+            const double rs = rsqrt_nr(piv);
+#pragma unroll
+            for (int q = 0; q < CP_MQ; ++q) {
+              const int r = j0 + lane + 32 * q;
+              a[q][c] = (r == j0 + c) ? piv * rs : a[q][c] * rs;
+            }
+            if (lane == 0) rd[j0 + c] = rs;
+            // columns c2 > c; rows above row j0 + c2 pick up values that are
+            // never read (only rows >= j0 + c2 of column c2 are stored)
+#pragma unroll
+            for (int c2 = c + 1; c2 < PB; ++c2) {
+              const double l = __shfl_sync(0xffffffffu, a[0][c], c2);   // L(j0 + c2, j0 + c)
+#pragma unroll
+              for (int q = 0; q < CP_MQ; ++q) a[q][c2] -= a[q][c] * l;
+            }
+          }
+        }
+      }
+      if (b) {
+        if (lane == 0) bad = b;
+      } else {
+#pragma unroll
+        for (int q = 0; q < CP_MQ; ++q) {
+          const int r = j0 + lane + 32 * q;
+          if (r < n) {
+#pragma unroll
+            for (int c = 0; c < PB; ++c) {
+              if (c < pb && r >= j0 + c) AA(r, j0 + c) = a[q][c];
+              Pr[r * PB + c] = (c < pb) ? a[q][c] : 0.0;   // zero above the diagonal
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (bad) break;   // uniform
+    // trailing update: A(i, j) -= sum_c L(i, j0+c) L(j, j0+c), j0+pb <= j <= i;
+    // rows by lane in 32-row chunks, columns by warp, four columns at a time
+    const int t0 = j0 + pb;
+    if (t0 < n) {
+      const int nch = (n - t0 + 31) / 32;
+#pragma unroll 1
+      for (int ch = 0; ch < nch; ++ch) {
+        const int i = t0 + ch * 32 + lane;
+        const bool rowok = i < n;
+        double li[PB];
+#pragma unroll
+        for (int c = 0; c < PB; ++c) {
+          const double v = Pr[min(i, n - 1) * PB + c];
+          li[c] = rowok ? v : 0.0;
+        }
+        const int jend = min(n, t0 + ch * 32 + 32);   // columns up to this chunk's last row
+#pragma unroll 1
+        for (int jb = t0 + 4 * warp; jb < jend; jb += 4 * CPW) {
+          double acc[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int j = min(jb + u, n - 1);
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int c = 0; c < PB; c += 2) {
+              s0 += li[c] * Pr[j * PB + c];
+              s1 += li[c + 1] * Pr[j * PB + c + 1];
+            }
+            acc[u] = s0 + s1;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int j = jb + u;
+            if (rowok && j < jend && i >= j) AA(i, j) -= acc[u];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (bad) {
+    if (tid == 0) *info = bad;
+    return;
+  }
+  // ---------------- inverse ----------------
+  const int nblk = (n + 31) / 32;
+  // diagonal blocks: lane = column c of X_JJ, forward substitution down the
+  // rows; X(r, c), r > c, goes to A(c, r), the diagonal to xd
+  for (int J = warp; J < nblk; J += CPW) {
+    const int j0 = J * 32, bs = min(32, n - j0);
+    // rows past the matrix (last block) read row n - 1 and are zeroed
+    double x[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const int rr = min(j0 + r, n - 1);
+      double sum = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+      for (int k = 0; k < r; ++k) sum -= AA(rr, min(j0 + k, n - 1)) * x[k];
+      x[r] = (r < bs) ? sum * rd[rr] : 0.0;
+    }
+    if (lane < bs) {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        if (r < bs && r > lane) AA(j0 + lane, j0 + r) = x[r];
+        if (r == lane) xd[j0 + lane] = x[r];
+      }
+    }
+  }
+  __syncthreads();
+  // M_IK = -X_II L_IK in place of L_IK, one warp per block; lane = row i,
+  // which holds row i of X_II in registers
+  for (int pair = warp; pair < nblk * (nblk - 1) / 2; pair += CPW) {
+    int I = 1;
+    while (I * (I + 1) / 2 <= pair) ++I;
+    const int K = pair - I * (I - 1) / 2;
+    const int i0 = I * 32, k0 = K * 32, bi = min(32, n - i0);
+    const bool rowok = lane < bi;
+    // row i of X_II (zero past the diagonal and for rows past the matrix);
+    // loads from clamped addresses, selection after the load
+    const int ir = min(i0 + lane, n - 1);
+    double xr[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const int kr = min(i0 + k, n - 1);
+      const double v = AA(kr, ir), dv = xd[kr];
+      xr[k] = (!rowok || k > lane || k >= bi) ? 0.0 : (k == lane ? dv : v);
+    }
+#pragma unroll 1
+    for (int c = 0; c < 32; ++c) {   // the columns of block K are full (K < I)
+      const double *col = &AA(0, k0 + c);
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 32; k += 2) {
+        s0 += xr[k] * col[min(i0 + k, n - 1)];
+        s1 += xr[k + 1] * col[min(i0 + k + 1, n - 1)];
+      }
+      __syncwarp();
+      if (rowok) AA(i0 + lane, k0 + c) = -(s0 + s1);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // X_IJ = sum_{K=J}^{I-1} M_IK X_KJ by block diagonals; two warps a block
+  // (16 columns each), lane = row i; X(k, c) for k > c read from A(c, k)
+  for (int d = 1; d < nblk; ++d) {
+    const int nb_d = nblk - d;
+    for (int task = warp; task < nb_d * 2; task += CPW) {
+      const int J = task >> 1, half = task & 1, I = J + d;
+      const int i0 = I * 32, j0 = J * 32, bi = min(32, n - i0);
+      const int cb = j0 + 16 * half;
+      const int i = i0 + lane;
+      const bool rowok = lane < bi;
+      const int ir = min(i, n - 1);
+      double acc[16], xdv[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        acc[u] = 0.0;
+        xdv[u] = xd[cb + u];
+      }
+#pragma unroll 1
+      for (int K = J; K < I; ++K) {
+        const int k0 = K * 32;
+#pragma unroll 1
+        for (int kk = 0; kk < 32; ++kk) {
+          const int k = k0 + kk;
+          const double mv = AA(ir, k);
+          const double m = rowok ? mv : 0.0;
+          const double *xrow = &AA(cb, k);   // X(k, cb + u) = A(cb + u, k) for k > cb + u
+#pragma unroll
+          for (int u = 0; u < 16; ++u) {
+            const int c = cb + u;
+            const double xu = xrow[u];
+            const double xv = (k > c) ? xu : ((k == c) ? xdv[u] : 0.0);
+            acc[u] += m * xv;
+          }
+        }
+      }
+      if (rowok) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) AA(cb + u, i) = acc[u];   // X(i, c) to A(c, i)
+      }
+    }
+    __syncthreads();
+  }
+  // out: X in the lower triangle, zeros above
+  for (int j = warp; j < n; j += CPW)
+    for (int i = lane; i < n; i += 32) Sg[(long)j * n + i] = (i > j) ? AA(j, i) : ((i == j) ? xd[j] : 0.0);
+#undef AA
+  if (tid == 0) *info = 0;
+}
+
 // S: n x n column-major.  When S does not fit shared memory the kernel works
 // in S itself (L2-resident) and uses work (>= CB*DLD + n doubles) as temporary.
 int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
@@ -256,6 +492,17 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
     attr = true;
   }
   if (!use && !work) { set_error("cholinv: n=%d needs a work buffer", n); return 1; }
+  const size_t pbytes = sizeof(double) * ((size_t)(n | 1) * n + 2 * (size_t)n + (size_t)PB * n);
+  if (n <= CP_MAXN && pbytes <= CH_SMEM_MAX) {
+    static bool pattr = false;
+    if (!pattr) {
+      cudaFuncSetAttribute(k_cholinv_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
+      pattr = true;
+    }
+    k_cholinv_sm<<<1, CPT, pbytes, st>>>(S, n, d_info);
+    note_launch();
+    return 0;
+  }
   if (use) k_cholinv<true><<<1, CHT, bytes, st>>>(S, n, work, d_info);
   else k_cholinv<false><<<1, CHT, 0, st>>>(S, n, work, d_info);
   note_launch();
@@ -269,12 +516,14 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
 //  (1) k_sytrd: Householder tridiagonalisation T = Q^T A Q in one CTA, three
 //      barriers per column (reflector, matrix-vector product, rank-2 update);
 //  (2) k_bisect: eigenvalues of T by Sturm-count multisection, one warp per
-//      eigenvalue, 33 subintervals per round;
+//      eigenvalue, 33 subintervals per round, division-free counts;
 //  (3) k_invit: eigenvectors of T by inverse iteration with a pivoted
 //      tridiagonal LU, one thread per cluster of close eigenvalues, members
 //      re-orthogonalised against each other; per-thread work arrays are
 //      interleaved across threads so every access is coalesced;
-//  (4) k_backtrans: V = Q Z, one warp per column (in registers for n <= 256).
+//  (4) k_wy_t + k_backtrans_wy: V = Q Z, one warp per column, the reflectors
+//      in compact-WY blocks of 8 (k_backtrans, one reflector at a time, for
+//      n > 256).
 // Eigenpairs are ascending; each eigenvector's largest-magnitude component is
 // made positive (first index on ties).  Every loop is bounded.
 
@@ -430,28 +679,47 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
 #undef A_
 }
 
-// 1/q: the hardware's approximate reciprocal refined by one Newton-Raphson
-// step r <- r (2 - q r), which squares the relative error (to about 1e-14);
-// only the signs of the Sturm pivots are used, so this accuracy is ample.
-__device__ __forceinline__ double recip_nr(double q) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
-  return r * fma(-q, r, 2.0);
-}
-
-// Number of eigenvalues of T below x (Sturm count, pivots guarded by pmin).
-__device__ __forceinline__ int sturm(const double *__restrict__ d, const double *__restrict__ e, int n, double x,
-                                     double pmin) {
-  int c = 0;
-  double q = d[0] - x;
-  if (fabs(q) < pmin) q = -pmin;
-  if (q < 0.0) ++c;
-  for (int i = 1; i < n; ++i) {
-    const double ei = e[i - 1];
-    q = d[i] - x - ei * ei * recip_nr(q);
-    if (fabs(q) < pmin) q = -pmin;
-    if (q < 0.0) ++c;
+// Number of eigenvalues of T below x: sign changes of the Sturm sequence
+// p_0 = 1, p_1 = d_0 - x, p_i = (d_{i-1} - x) p_{i-1} - e_{i-2}^2 p_{i-2}
+// (zeros dropped).  No division on the dependent chain (one FMA a step; the
+// ratio form q_i = p_i / p_{i-1} needs a reciprocal a step); every 8 steps
+// both terms are rescaled by a power of two, which changes no sign.  d and
+// e2 = e^2 are read from shared memory (broadcasts), eight steps at a time.
+__device__ __forceinline__ void sturm_step(double di, double e2, double x, double &p1, double &p2, bool &neg,
+                                           int &c) {
+  const double p = fma(di - x, p1, -e2 * p2);
+  if (p != 0.0) {
+    const bool ng = p < 0.0;
+    c += (ng != neg) ? 1 : 0;
+    neg = ng;
   }
+  p2 = p1;
+  p1 = p;
+}
+__device__ __forceinline__ void sturm_rescale(double &p1, double &p2) {
+  const double m = fmax(fabs(p1), fabs(p2));
+  if (m > 0.0 && m < 1e300) {
+    const int ex = (int)((__double_as_longlong(m) >> 52) & 0x7ff);
+    const double sc = __longlong_as_double((long long)(2046 - ex) << 52);   // 2^(1023 - ex)
+    p1 *= sc;
+    p2 *= sc;
+  }
+}
+__device__ __forceinline__ int sturm_count(const double *__restrict__ d, const double *__restrict__ e2, int n,
+                                           double x) {
+  double p2 = 1.0, p1 = d[0] - x;
+  int c = p1 < 0.0 ? 1 : 0;
+  bool neg = p1 < 0.0;   // sign of the last nonzero term
+  int i = 1;
+  for (; i + 8 <= n; i += 8) {
+    double dd[8], ee[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) { dd[u] = d[i + u]; ee[u] = e2[i + u - 1]; }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) sturm_step(dd[u], ee[u], x, p1, p2, neg, c);
+    sturm_rescale(p1, p2);
+  }
+  for (; i < n; ++i) sturm_step(d[i], e2[i - 1], x, p1, p2, neg, c);
   return c;
 }
 
@@ -461,28 +729,32 @@ __device__ __forceinline__ int sturm(const double *__restrict__ d, const double 
 // is 2 eps |T| wide (at most 24 rounds).
 __global__ void k_bisect(const double *__restrict__ d, const double *__restrict__ e, int n, double *__restrict__ w) {
   const int t = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (t >= n) return;   // whole warp
+  extern __shared__ double bs_de[];   // d (n), then e^2 (n - 1)
+  if (t >= n) return;   // whole warp (one warp per block)
+  double *sd = bs_de, *se2 = bs_de + n;
   double lo = 1e300, hi = -1e300, tn = 0.0;
   for (int i = lane; i < n; i += 32) {
     const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
     lo = fmin(lo, d[i] - r);
     hi = fmax(hi, d[i] + r);
     tn = fmax(tn, fabs(d[i]) + r);
+    sd[i] = d[i];
+    if (i < n - 1) se2[i] = e[i] * e[i];
   }
+  __syncwarp();
   for (int o = 16; o > 0; o >>= 1) {
     lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
     hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     tn = fmax(tn, __shfl_xor_sync(0xffffffffu, tn, o));
   }
   const double eps = 2.220446049250313e-16;
-  const double pmin = 1e-300 + eps * eps * tn * tn * 1e-10;
   lo -= 2.0 * eps * tn + 1e-300;
   hi += 2.0 * eps * tn + 1e-300;
   for (int it = 0; it < 24; ++it) {
-    if (hi - lo <= 2.0 * eps * tn + 4.0 * pmin) break;
+    if (hi - lo <= 2.0 * eps * tn + 1e-290) break;
     const double h = (hi - lo) * (1.0 / 33.0);
     const double x = lo + (double)(lane + 1) * h;
-    const int c = sturm(d, e, n, x, pmin);
+    const int c = sturm_count(sd, se2, n, x);
     const unsigned bal = __ballot_sync(0xffffffffu, c > t);
     const int l = bal ? __ffs(bal) - 1 : 32;   // eigenvalue t lies in [x_{l-1}, x_l)
     const double nlo = (l == 0) ? lo : lo + (double)l * h;
@@ -530,20 +802,26 @@ __global__ void k_invit(const double *__restrict__ d, const double *__restrict__
       const double cdn = e[i];                 // subdiagonal below a
       const double dn = d[i + 1] - lam;        // next diagonal
       const double en = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+      // reciprocals by Newton-refined hardware approximations (recip2_nr,
+      // full double precision up to the last bit or two): inverse iteration
+      // needs an accurate factorisation of a nearby matrix, not correctly
+      // rounded quotients
       if (fabs(a) >= fabs(cdn)) {
         const double aa = (fabs(a) < tiny) ? tiny : a;
-        const double l = cdn / aa;
-        WS(0, i) = 1.0 / aa; WS(1, i) = b; WS(2, i) = 0.0; WS(3, i) = l; WS(4, i) = 0.0;
+        const double ra = recip2_nr(aa);
+        const double l = cdn * ra;
+        WS(0, i) = ra; WS(1, i) = b; WS(2, i) = 0.0; WS(3, i) = l; WS(4, i) = 0.0;
         a = dn - l * b;
         b = en;
       } else {
-        const double l = a / cdn;
-        WS(0, i) = 1.0 / cdn; WS(1, i) = dn; WS(2, i) = en; WS(3, i) = l; WS(4, i) = 1.0;
+        const double rc = recip2_nr(cdn);
+        const double l = a * rc;
+        WS(0, i) = rc; WS(1, i) = dn; WS(2, i) = en; WS(3, i) = l; WS(4, i) = 1.0;
         a = b - l * dn;
         b = -l * en;
       }
     }
-    WS(0, n - 1) = 1.0 / ((fabs(a) < tiny) ? tiny : a);
+    WS(0, n - 1) = recip2_nr((fabs(a) < tiny) ? tiny : a);
     // start vector: ones with a member-dependent pattern
     for (int i = 0; i < n; ++i) WS(5, i) = 1.0 + 0.01 * (double)((i * (c + 3)) % 7);
     for (int it = 0; it < 3; ++it) {
@@ -579,7 +857,7 @@ __global__ void k_invit(const double *__restrict__ d, const double *__restrict__
       }
       double nr = 0.0;
       for (int i = 0; i < n; ++i) { const double x = WS(5, i); nr += x * x; }
-      nr = 1.0 / sqrt(nr);
+      nr = rsqrt_nr(nr);
       for (int i = 0; i < n; ++i) WS(5, i) *= nr;
     }
     double *z = Z + (long)c * n;
@@ -623,49 +901,98 @@ __global__ void __launch_bounds__(256) k_backtrans(const double *__restrict__ Z,
   for (int i = lane; i < n; i += 32) V[(long)c * n + i] = sg * z[i];
 }
 
-// The same for n <= 32*MC with the column and the next reflector held in
-// registers: the reflector k-1 is loaded while reflector k is applied, so
-// the L2 latency is off the chain.  Entries of HV above row k+1 are never
-// written and are excluded by selection, not by multiplication.
+// --------------------------------------------------------------------------
+// Back-transformation with the reflectors in blocks of WYB (compact WY form,
+// as in LAPACK's dlarft/dlarfb): H_k0 H_k0+1 ... H_k0+b-1 = I - Y T Y^T, Y the
+// block's reflectors (v_k(k+1) = 1, zero above), T upper triangular.  A block
+// costs one batched warp reduction of WYB dot products instead of WYB
+// dependent ones.
+constexpr int WYB = 8;
+
+// T of every block, one warp per block: G = Y^T Y above the diagonal, then
+// T(i,j) = -tau_j sum_{l=i}^{j-1} T(i,l) G(l,j), T(j,j) = tau_j.
+__global__ void k_wy_t(const double *__restrict__ HV, const double *__restrict__ tau, int n, double *__restrict__ Tm) {
+  __shared__ double G[WYB][WYB];
+  const int blk = blockIdx.x, lane = threadIdx.x;
+  const int nref = n - 2, k0 = blk * WYB, b = min(WYB, nref - k0);
+  for (int p = 0; p < WYB * WYB; ++p) {
+    const int i = p / WYB, j = p - i * WYB;
+    if (i >= j || j >= b) continue;   // uniform
+    const double *vi = HV + (long)(k0 + i) * n, *vj = HV + (long)(k0 + j) * n;
+    double sum = 0.0;
+    for (int r = k0 + j + 1 + lane; r < n; r += 32) sum += vi[r] * vj[r];
+    sum = warp_sum(sum);
+    if (lane == 0) G[i][j] = sum;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    double T[WYB][WYB];
+    for (int i = 0; i < WYB; ++i)
+      for (int j = 0; j < WYB; ++j) T[i][j] = 0.0;
+    for (int j = 0; j < b; ++j) {
+      const double tj = tau[k0 + j];
+      T[j][j] = tj;
+      for (int i = 0; i < j; ++i) {
+        double acc = 0.0;
+        for (int l = i; l < j; ++l) acc += T[i][l] * G[l][j];
+        T[i][j] = -tj * acc;
+      }
+    }
+    for (int i = 0; i < WYB; ++i)
+      for (int j = 0; j < WYB; ++j) Tm[(long)blk * WYB * WYB + i * WYB + j] = T[i][j];
+  }
+}
+
+// V(:, c) = Q Z(:, c), one warp per column, blocks applied last to first; lane
+// holds rows lane + 32 q (q < MC).  Then the sign convention of k_backtrans.
 template <int MC>
-__global__ void __launch_bounds__(256) k_backtrans_reg(const double *__restrict__ Z, const double *__restrict__ HV,
-                                                       const double *__restrict__ tau, int n,
-                                                       double *__restrict__ V) {
+__global__ void __launch_bounds__(128) k_backtrans_wy(const double *__restrict__ Z, const double *__restrict__ HV,
+                                                      const double *__restrict__ Tm, int n, double *__restrict__ V) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x * (blockDim.x >> 5) + warp;
   if (c >= n) return;   // whole warp
-  double z[MC], vn[MC];
+  double z[MC];
 #pragma unroll
   for (int q = 0; q < MC; ++q) {
     const int i = lane + 32 * q;
     z[q] = (i < n) ? Z[(long)c * n + i] : 0.0;
-    vn[q] = (n >= 3 && i < n) ? HV[(long)(n - 3) * n + i] : 0.0;
   }
-  double tn = (n >= 3) ? tau[n - 3] : 0.0;
-  for (int k = n - 3; k >= 0; --k) {
-    double v[MC];
-    const double tk = tn;
+  const int nref = n - 2, nblk = (nref + WYB - 1) / WYB;
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int k0 = blk * WYB;
+    double y[WYB][MC];
+    double sv[WYB];
 #pragma unroll
-    for (int q = 0; q < MC; ++q) v[q] = vn[q];
-    if (k > 0) {
+    for (int j = 0; j < WYB; ++j) {
+      const int k = k0 + j;
+      sv[j] = 0.0;
 #pragma unroll
       for (int q = 0; q < MC; ++q) {
         const int i = lane + 32 * q;
-        vn[q] = (i < n) ? HV[(long)(k - 1) * n + i] : 0.0;
+        y[j][q] = (k < nref && i > k && i < n) ? HV[(long)k * n + i] : 0.0;
+        sv[j] += y[j][q] * z[q];
       }
-      tn = tau[k - 1];
     }
-    double s = 0.0;
+    // the WYB reductions side by side
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int j = 0; j < WYB; ++j) sv[j] += __shfl_xor_sync(0xffffffffu, sv[j], o);
+    const double *T = Tm + (long)blk * WYB * WYB;
+    double u[WYB];
+#pragma unroll
+    for (int i = 0; i < WYB; ++i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int j = i; j < WYB; ++j) acc += T[i * WYB + j] * sv[j];
+      u[i] = acc;
+    }
 #pragma unroll
     for (int q = 0; q < MC; ++q) {
-      const int i = lane + 32 * q;
-      s += (i > k && i < n) ? v[q] * z[q] : 0.0;
-    }
-    s = tk * warp_sum(s);
+      double acc = 0.0;
 #pragma unroll
-    for (int q = 0; q < MC; ++q) {
-      const int i = lane + 32 * q;
-      if (i > k && i < n) z[q] -= v[q] * s;
+      for (int j = 0; j < WYB; ++j) acc += y[j][q] * u[j];
+      z[q] -= acc;
     }
   }
   double mx = -1.0;
@@ -717,7 +1044,9 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     return 0;
   }
   // one warp per eigenvalue, one warp per block: spread over the SMs
-  k_bisect<<<n, 32, 0, st>>>(d, e, n, w); note_launch();
+  const size_t bsm = sizeof(double) * 2 * (size_t)n;
+  if (bsm > 48 * 1024) cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
+  k_bisect<<<n, 32, bsm, st>>>(d, e, n, w); note_launch();
   const size_t wsm = sizeof(double) * 6 * (size_t)n * 16;
   if (wsm <= 200 * 1024) {
     k_invit<<<(n + 15) / 16, 16, wsm, st>>>(d, e, w, n, Z, ws, NT, d_info, 1); note_launch();
@@ -725,7 +1054,10 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     k_invit<<<NT / 128, 128, 0, st>>>(d, e, w, n, Z, ws, NT, d_info, 0); note_launch();
   }
   if (n <= 256) {
-    k_backtrans_reg<8><<<(n + 3) / 4, 128, 0, st>>>(Z, HV, tau, n, V); note_launch();
+    double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
+    const int nblk = (n - 2 + WYB - 1) / WYB;
+    if (nblk > 0) { k_wy_t<<<nblk, 32, 0, st>>>(HV, tau, n, Tm); note_launch(); }
+    k_backtrans_wy<8><<<(n + 3) / 4, 128, 0, st>>>(Z, HV, Tm, n, V); note_launch();
   } else {
     const size_t bt = sizeof(double) * 8 * (size_t)n;
     if (bt > 200 * 1024) { set_error("syev: n=%d too large for the back-transformation", n); return 1; }
