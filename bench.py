@@ -230,8 +230,12 @@ def accuracy(acc, natom, iters):
         d = abs(a["etot"] - ref["etot"])
         out[name] = {"etot_ry": a["etot"], "resid": a["resid"], "detot_last_ry": a["detot_last"],
                      "err_ha_per_atom": 0.5 * d / natom,
-                     "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - ref["eig"])))}
+                     "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - ref["eig"]))),
+                     "force_max_abs_err_ha_per_bohr": 0.5 * float(np.max(np.abs(a["force"] - ref["force"])))}
     out["err_ha_per_atom"] = out["mixed"]["err_ha_per_atom"]
+    out["force_err_ha_per_bohr"] = out["mixed"]["force_max_abs_err_ha_per_bohr"]
+    out["force_max_abs_fp64_ha_per_bohr"] = 0.5 * float(np.max(np.abs(ref["force"])))
+    out["force_terms"] = "local pseudopotential (flocal_g) + G-space KB (kbnlpp_frc2); the ion-ion term is identical in all paths"
     return out
 
 
@@ -351,7 +355,10 @@ def run_ours(args):
         outs = [ctx.scf_iteration(parm) for _ in range(max(0, args.accuracy_iters - res[name]["iters_done"]))]
         ctx.sync()
         last = outs[-1] if outs else None
-        acc[name] = {"etot": last["etot"] if last else res[name]["etot_last"],
+        ctx.set_force_tables()
+        fl, fn = ctx.forces()
+        acc[name] = {"force": fl + fn,
+                     "etot": last["etot"] if last else res[name]["etot_last"],
                      "resid": last["resid"] if last else None,
                      "detot_last": abs(outs[-1]["etot"] - outs[-2]["etot"]) if len(outs) > 1 else None,
                      "eig": ctx.get_eig()}

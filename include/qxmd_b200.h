@@ -180,7 +180,34 @@ int qx_scf_mixing(qx_ctx *ctx, int itratn, double cmetric);
 int qx_scf_rho_from_psi(qx_ctx *ctx);
 int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
 
+/* ---- Hellmann-Feynman forces (force.f90:5-860 terms floc and fnlc) ------ */
+/* Geometry tables, set once per geometry after the KB tables (qx_set_kb_g)
+ * and qx_scf_init:
+ *   natom, ntype, ityp(natom): 0-based species of each atom;
+ *   satm(3, natom): fractional coordinates (the phases cos, sin of 2 pi k s
+ *     are built on the device by the recurrence of stscfn, bulk.f90:2086-2175);
+ *   n5: G vectors of the density half sphere, G = 0 first; ijk5(n5): 0-based
+ *     grid index of +G; ngabc(3, n5): integer coordinates (nga, ngb, ngc);
+ *   gvec5(3, n5): cartesian G (gx, gy, gz);
+ *   svco(n5, ntype): local form factor of each species (Ry; flocal_g);
+ *   gw(3, nplw + 1): cartesian G of the wavefunction half sphere.
+ * KB projector j of atom a is j = l + lmx * a with lmx = nproj / natom. */
+int qx_set_force_tables(qx_ctx *ctx, int natom, int ntype, const int *ityp, const double *satm, int n5,
+                        const int *ijk5, const int *ngabc, const double *gvec5, const double *svco,
+                        const double *gw);
+/* Forces (Ry/bohr, (3, natom) each) of the current psi and its density
+ * rho = sum occ/Omega |psi|^2:
+ *   floc: local pseudopotential in G space (flocal_g, nlkbpp.f90:1037-1120),
+ *     2 sum_{G != 0} G svco(G) (Re rho(G) sin G.R + Im rho(G) cos G.R);
+ *   fnl: G-space KB (kbnlpp_frc2, nlkbpp.f90:1878-2130),
+ *     4 sum_n occ_n sum_l vclalp_l <beta|psi_n> sum_{G != 0} G (beta_re psi_im - beta_im psi_re).
+ * The ion-ion (Ewald) term is geometry only and stays with the caller. */
+int qx_forces(qx_ctx *ctx, double *floc, double *fnl);
+
 /* ---- drop-in shims with the reference's host-array arguments ----------- */
+/* kbnlpp_frc2 (nlkbpp.f90:1878): fnlc(3, natom) += the G-space KB forces of
+ * cgjr(nplwex, nband) with the occupations of qx_set_occ. */
+int qxgpu_kbnlpp_frc2(qx_ctx *ctx, const double *cgjr, double *fnlc);
 /* hcnonloc: rhcr(nplwex, nb) += local (+ real-space KB) H products of cgjr. */
 int qxgpu_hcnonloc(qx_ctx *ctx, const double *cgjr, double *rhcr, int nb);
 /* hckbpp_g (nlkbpp.f90:1284-1393): rhcr += G-space KB products of cgjr. */

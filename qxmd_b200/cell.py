@@ -460,6 +460,62 @@ def ewald_energy(cell: Cell, gs: GSphere, eta: float | None = None) -> float:
     return 2.0 * (er + eg + eself + ebg)        # Hartree -> Rydberg
 
 
+def ewald_forces(cell: Cell, gs: GSphere, eta: float | None = None) -> np.ndarray:
+    """Ion-ion forces (Ry/bohr, (natom, 3)): minus the gradient of
+    ewald_energy with respect to each atom position, term by term (real-space
+    erfc sum and reciprocal sum over the density half sphere)."""
+    a = gs.rba
+    vol = gs.rvol
+    z = cell.zv
+    nat = cell.natom
+    if eta is None:
+        eta = (math.sqrt(math.pi) * nat ** (1 / 6) / vol ** (1 / 3)) ** 2
+    from math import erfc
+    se = math.sqrt(eta)
+    rc = 6.0 / se
+    nmax = [int(math.ceil(rc / np.linalg.norm(a[:, i]))) + 1 for i in range(3)]
+    shifts = []
+    for i in range(-nmax[0], nmax[0] + 1):
+        for j in range(-nmax[1], nmax[1] + 1):
+            for k in range(-nmax[2], nmax[2] + 1):
+                shifts.append(a @ np.array([i, j, k], dtype=np.float64))
+    shifts = np.array(shifts)
+    f = np.zeros((nat, 3))
+    for ia in range(nat):
+        d = cell.pos[ia] - cell.pos
+        for s in shifts:
+            v = d + s
+            rr = np.linalg.norm(v, axis=1)
+            m = (rr > 1e-10) & (rr < rc)
+            r = rr[m]
+            g = np.array([erfc(se * x) for x in r]) / r ** 2 + 2.0 * se / math.sqrt(math.pi) * np.exp(-eta * r * r) / r
+            f[ia] += z * z * np.sum((g / r)[:, None] * v[m], axis=0)
+    g2 = gs.recnrm[1:]
+    gv = gs.gvec[1:]
+    ph = gv @ cell.pos.T                                   # (ng, natom)
+    sf = np.exp(-1j * ph).sum(axis=1)                      # S(G)
+    w = 4.0 * math.pi / vol * np.exp(-g2 / (4 * eta)) / g2  # both +G and -G: x2 over the half sphere
+    for ia in range(nat):
+        im = np.imag(np.exp(-1j * ph[:, ia]) * np.conj(sf))
+        f[ia] += -2.0 * z * z * np.sum((w * im)[:, None] * gv, axis=0)
+    return 2.0 * f                                        # Hartree -> Rydberg
+
+
+def force_tables(s: "System") -> dict:
+    """Arguments of qx_set_force_tables for a system of one species: fractional
+    coordinates, the density half sphere (grid indices, integer and cartesian
+    G), the local form factor svco(G) = v_loc(|G|) (Ry, the per-atom
+    transform without 1/Omega) and the wavefunction half sphere's G."""
+    gs = s.gs
+    n5 = gs.nplw5 + 1
+    satm = np.linalg.solve(gs.rba, s.cell.pos.T).T
+    return dict(natom=s.cell.natom, ntype=1, ityp=np.zeros(s.cell.natom, dtype=np.int32),
+                satm=np.ascontiguousarray(satm), n5=n5, ijk5=gs.ijk_pos.astype(np.int32),
+                ngabc=np.ascontiguousarray(np.stack([gs.nga, gs.ngb, gs.ngc], axis=1).astype(np.int32)),
+                gvec5=np.ascontiguousarray(gs.gvec), svco=s.pp.vloc_g(gs.recnrm).astype(np.float64),
+                gw=np.ascontiguousarray(gs.gvec[: gs.nplw + 1]))
+
+
 def random_wavefunctions(nplwex: int, nband: int, seed: float = 25.0) -> np.ndarray:
     """Initial gdcr(nplwex, nband) from the Park-Miller generator rnd00
     (`funcs.f90:1673-1689`) with seed 25.0 (`savedd.f90:289, 911-918`):

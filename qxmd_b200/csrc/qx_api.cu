@@ -106,6 +106,14 @@ struct qx_ctx {
   // (d_sc[5..6] gradres max/sum, d_info[0] eigen clusters, d_info[1] Cholesky
   // status, d_info[2] CG band applications) read once at the end, and the
   // whole iteration is captured as a graph per buffer arrangement
+  // Hellmann-Feynman force tables (qx_set_force_tables)
+  int f_natom = 0, f_ntype = 0, f_n5 = 0, f_km[3] = {0, 0, 0}, f_ktot = 0;
+  int *d_ityp = nullptr, *d_ijk5 = nullptr, *d_ngabc = nullptr;
+  double *d_satm = nullptr, *d_gvec5 = nullptr, *d_svco = nullptr, *d_gw = nullptr, *d_dcq = nullptr,
+         *d_dsq = nullptr, *d_force = nullptr;
+  void *dtab = nullptr;    // 3 nproj x nplwex derivative tables (context precision)
+  void *dproj = nullptr;   // 3 nproj x nb
+  bool have_ftab = false;
   bool defer = false;
   struct ScfGraph {
     std::vector<char> key;
@@ -1307,6 +1315,112 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
     out->ncg_hpsi = info[2];
     out->eig_clusters = info[0];
   }
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Hellmann-Feynman forces
+extern "C" int qx_set_force_tables(qx_ctx *c, int natom, int ntype, const int *ityp, const double *satm, int n5,
+                                   const int *ijk5, const int *ngabc, const double *gvec5, const double *svco,
+                                   const double *gw) {
+  if (!c || natom <= 0 || ntype <= 0 || n5 <= 1 || !ityp || !satm || !ijk5 || !ngabc || !gvec5 || !svco || !gw) {
+    set_error("qx_set_force_tables: bad arguments");
+    return QX_ERR_ARG;
+  }
+  if (!c->have_kbg || c->pl.nproj % natom) {
+    set_error("qx_set_force_tables: G-space KB tables (qx_set_kb_g) with nproj a multiple of natom are needed");
+    return QX_ERR_STATE;
+  }
+  for (int a = 0; a < natom; ++a)
+    if (ityp[a] < 0 || ityp[a] >= ntype) { set_error("qx_set_force_tables: ityp out of range"); return QX_ERR_ARG; }
+  for (long i = 0; i < n5; ++i)
+    if (ijk5[i] < 0 || ijk5[i] >= c->pl.n) { set_error("qx_set_force_tables: ijk5 out of range"); return QX_ERR_ARG; }
+  int km[3] = {0, 0, 0};
+  for (long i = 0; i < 3L * n5; ++i) km[i % 3] = std::max(km[i % 3], std::abs(ngabc[i]));
+  const int ktot = 2 * (km[0] + km[1] + km[2]) + 3;
+  const int np = c->pl.nproj, ne = c->ne, nb = c->nb;
+  const size_t ts = c->tsize();
+  if (c->f_natom != natom || c->f_n5 != n5 || c->f_ntype != ntype || c->f_ktot != ktot || !c->d_force) {
+    TRY(dalloc(c, &c->d_ityp, sizeof(int) * natom));
+    TRY(dalloc(c, &c->d_satm, sizeof(double) * 3 * natom));
+    TRY(dalloc(c, &c->d_ijk5, sizeof(int) * n5));
+    TRY(dalloc(c, &c->d_ngabc, sizeof(int) * 3 * (size_t)n5));
+    TRY(dalloc(c, &c->d_gvec5, sizeof(double) * 3 * (size_t)n5));
+    TRY(dalloc(c, &c->d_svco, sizeof(double) * (size_t)n5 * ntype));
+    TRY(dalloc(c, &c->d_dcq, sizeof(double) * (size_t)natom * ktot));
+    TRY(dalloc(c, &c->d_dsq, sizeof(double) * (size_t)natom * ktot));
+    TRY(dalloc(c, &c->d_force, sizeof(double) * 6 * natom));
+  }
+  if (!c->d_gw) TRY(dalloc(c, &c->d_gw, sizeof(double) * 3 * (size_t)(ne / 2)));
+  if (!c->dtab) {
+    TRY(dalloc(c, &c->dtab, ts * 3 * (size_t)np * ne));
+    TRY(dalloc(c, &c->dproj, ts * 3 * (size_t)np * nb));
+  }
+  if (!c->d_zg) TRY(dalloc(c, &c->d_zg, sizeof(double2) * c->pl.n));
+  TRY(ensure_rho(c));
+  CK(cudaMemcpyAsync(c->d_ityp, ityp, sizeof(int) * natom, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_satm, satm, sizeof(double) * 3 * natom, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_ijk5, ijk5, sizeof(int) * n5, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_ngabc, ngabc, sizeof(int) * 3 * (size_t)n5, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_gvec5, gvec5, sizeof(double) * 3 * (size_t)n5, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_svco, svco, sizeof(double) * (size_t)n5 * ntype, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_gw, gw, sizeof(double) * 3 * (size_t)(ne / 2), cudaMemcpyHostToDevice, c->st));
+  // the host arrays may go away when this returns
+  CK(cudaStreamSynchronize(c->st));
+  c->f_natom = natom;
+  c->f_ntype = ntype;
+  c->f_n5 = n5;
+  c->f_ktot = ktot;
+  for (int d = 0; d < 3; ++d) c->f_km[d] = km[d];
+  phase_tables(natom, c->d_satm, km[0], km[1], km[2], ktot, c->d_dcq, c->d_dsq, c->st);
+  if (c->prec == QX_PREC_FP64)
+    dtab_build<double>(np, ne / 2 - 1, c->pl.b64.kbg, c->d_gw, (double *)c->dtab, c->st);
+  else
+    dtab_build<float>(np, ne / 2 - 1, c->pl.b32.kbg, c->d_gw, (float *)c->dtab, c->st);
+  CKL();
+  c->have_ftab = true;
+  return QX_OK;
+}
+
+template <typename T>
+static int forces_impl(qx_ctx *c, double *floc, double *fnl) {
+  const int natom = c->f_natom, np = c->pl.nproj, ne = c->ne, nb = c->nb;
+  const long n = c->pl.n;
+  TRY(qx_softchg(c));   // rho of the current psi
+  real_to_cplx(c->d_rho_out, nullptr, c->d_zg, n, c->st);
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0 / (double)n, c->st));
+  floc_g(natom, c->f_n5, c->d_ijk5, c->d_ngabc, c->d_gvec5, c->d_svco, c->d_ityp, c->d_zg, c->d_dcq, c->d_dsq,
+         c->f_km[0], c->f_km[1], c->f_km[2], c->f_ktot, c->d_force, c->st);
+  CKL();
+  const Bufs<T> &b = c->pl.bufs<T>();
+  T *P = (T *)c->proj, *D = (T *)c->dproj;
+  TRY(gemm<T>(true, false, np, nb, ne, (T)1, b.kbg, ne, (const T *)c->psi, ne, (T)0, P, np, 2, nullptr, nullptr,
+              c->st, c->gws, c->gws_bytes));
+  TRY(gemm<T>(true, false, 3 * np, nb, ne, (T)1, (const T *)c->dtab, ne, (const T *)c->psi, ne, (T)0, D, 3 * np, 0,
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+  fnl_reduce<T>(natom, np / natom, np, nb, P, D, b.vclalp, c->d_occ, c->d_force + 3 * natom, c->st);
+  CKL();
+  std::vector<double> f(6 * (size_t)natom);
+  CK(cudaMemcpyAsync(f.data(), c->d_force, sizeof(double) * 6 * natom, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (floc) memcpy(floc, f.data(), sizeof(double) * 3 * natom);
+  if (fnl) memcpy(fnl, f.data() + 3 * natom, sizeof(double) * 3 * natom);
+  return 0;
+}
+
+extern "C" int qx_forces(qx_ctx *c, double *floc, double *fnl) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_ftab || !c->have_occ) { set_error("qx_forces: call qx_set_force_tables and qx_set_occ first"); return QX_ERR_STATE; }
+  return c->prec == QX_PREC_FP64 ? forces_impl<double>(c, floc, fnl) : forces_impl<float>(c, floc, fnl);
+}
+
+extern "C" int qxgpu_kbnlpp_frc2(qx_ctx *c, const double *cgjr, double *fnlc) {
+  if (!c || !cgjr || !fnlc) return QX_ERR_ARG;
+  if (!c->have_ftab || !c->have_occ) { set_error("qxgpu_kbnlpp_frc2: call qx_set_force_tables and qx_set_occ first"); return QX_ERR_STATE; }
+  TRY(qx_put_psi(c, cgjr));
+  std::vector<double> fnl(3 * (size_t)c->f_natom);
+  TRY(c->prec == QX_PREC_FP64 ? forces_impl<double>(c, nullptr, fnl.data()) : forces_impl<float>(c, nullptr, fnl.data()));
+  for (size_t i = 0; i < fnl.size(); ++i) fnlc[i] += fnl[i];
   return QX_OK;
 }
 

@@ -137,4 +137,16 @@ void convert(const Tin *in, Tout *out, long n, cudaStream_t st);
 template <typename T>
 void symmetrize_lower(const T *in, double *out, double *diag, int n, cudaStream_t st);
 
+// qx_force.cu (Hellmann-Feynman forces)
+void phase_tables(int natom, const double *satm, int km1, int km2, int km3, int ktot, double *dcq, double *dsq,
+                  cudaStream_t st);
+void floc_g(int natom, int n5, const int *ijk5, const int *ngabc, const double *gvec5, const double *svco,
+            const int *ityp, const double2 *rhog, const double *dcq, const double *dsq, int km1, int km2, int km3,
+            int ktot, double *floc, cudaStream_t st);
+template <typename T>
+void dtab_build(int nproj, int nplw, const T *kbg, const double *gw, T *dtab, cudaStream_t st);
+template <typename T>
+void fnl_reduce(int natom, int lmx, int nproj, int nb, const T *P, const T *D, const T *vclalp, const double *occ,
+                double *fnl, cudaStream_t st);
+
 }  // namespace qx

@@ -12,6 +12,7 @@ import os
 import numpy as np
 
 from . import build as _build
+from . import cell
 
 _lib = None
 
@@ -27,7 +28,8 @@ EXPORTS = [
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
-    "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing",
+    "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing", "qx_set_force_tables", "qx_forces",
+    "qxgpu_kbnlpp_frc2",
     "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
 ]
@@ -114,6 +116,9 @@ def lib(build_if_missing: bool = True):
         "qx_softchg": ([_ctx], C.c_int),
         "qx_scf_init": ([_ctx, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
         "qx_scf_mixing": ([_ctx, C.c_int, C.c_double], C.c_int),
+        "qx_set_force_tables": ([_ctx, C.c_int, C.c_int, _ip, _dp, C.c_int, _ip, _ip, _dp, _dp, _dp], C.c_int),
+        "qx_forces": ([_ctx, _dp, _dp], C.c_int),
+        "qxgpu_kbnlpp_frc2": ([_ctx, _dp, _dp], C.c_int),
         "qx_scf_rho_from_psi": ([_ctx], C.c_int),
         "qx_scf_iteration": ([_ctx, C.POINTER(CgParm), C.POINTER(ScfOut)], C.c_int),
         "qxgpu_hcnonloc": ([_ctx, _dp, _dp, C.c_int], C.c_int),
@@ -298,6 +303,28 @@ class Context:
         s = self.sys
         _ck(self.L.qx_scf_init(self.h, _f64(s.vloc), _f64(s.gs.cross.ravel(order="F")),
                                s.gs.ecutdens, s.eewald, mixbeta, kerker_q0), "qx_scf_init")
+
+    def set_force_tables(self):
+        """qx_set_force_tables from the system's geometry (one species)."""
+        t = cell.force_tables(self.sys)
+        _ck(self.L.qx_set_force_tables(self.h, t["natom"], t["ntype"], np.ascontiguousarray(t["ityp"], dtype=np.int32),
+                                       _f64(t["satm"]), t["n5"], np.ascontiguousarray(t["ijk5"], dtype=np.int32),
+                                       np.ascontiguousarray(t["ngabc"], dtype=np.int32), _f64(t["gvec5"]),
+                                       _f64(t["svco"]), _f64(t["gw"])), "qx_set_force_tables")
+
+    def forces(self):
+        """(floc, fnl) of the current psi, each (natom, 3) Ry/bohr."""
+        nat = self.sys.cell.natom
+        fl = np.zeros((nat, 3))
+        fn = np.zeros((nat, 3))
+        _ck(self.L.qx_forces(self.h, fl, fn), "qx_forces")
+        return fl, fn
+
+    def kbnlpp_frc2_host(self, cgjr):
+        """qxgpu_kbnlpp_frc2: the G-space KB forces of host wavefunctions."""
+        out = np.zeros((self.sys.cell.natom, 3))
+        _ck(self.L.qxgpu_kbnlpp_frc2(self.h, _f64(cgjr), out), "qxgpu_kbnlpp_frc2")
+        return out
 
     def scf_mixing(self, itratn=10, cmetric=20.0):
         """Pulay mixing with the reference defaults (itratn 10, cmetric 20);
