@@ -231,8 +231,10 @@ static int alloc_pipe(qx_ctx *c) {
   Plan &pl = c->pl;
   Bufs<T> &b = pl.bufs<T>();
   const long per_pair = (long)pl.k3 * pl.P2 * pl.P1 + (long)pl.k3 * pl.k2 * pl.P1 + (long)(pl.nplw + 1) * 2;
+  // band pairs per pipeline launch: a chunk's z-transformed planes stay in
+  // L2 between the passes (Si64 FP32: 80 pairs, 25 MB of bufA, one chunk)
   const char *env = getenv("QX_CHUNK_MB");
-  const double mb = env ? atof(env) : 64.0;
+  const double mb = env ? atof(env) : 160.0;
   long ch = (long)(mb * 1048576.0 / (sizeof(C) * (double)per_pair));
   ch = std::max(1L, std::min(ch, (long)c->npair_all));
   pl.chunk = (int)ch;
