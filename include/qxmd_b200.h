@@ -179,6 +179,21 @@ int qx_scf_mixing(qx_ctx *ctx, int itratn, double cmetric);
  * Pulay history). */
 int qx_scf_rho_from_psi(qx_ctx *ctx);
 int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
+/* The same iteration in two halves, for many cells at once: qx_scf_launch
+ * enqueues it on the context's stream (graph replay, nothing waits);
+ * qx_scf_result waits for that stream and reads the results.  Launching every
+ * cell before reading any lets independent cells run concurrently. */
+int qx_scf_launch(qx_ctx *ctx, const qx_cgparm *p);
+int qx_scf_result(qx_ctx *ctx, qx_scf_out *out);
+
+/* ---- TDDFT-FSSH nonadiabatic overlaps --------------------------------- */
+/* Keep the current psi as the previous step's wavefunctions (gdcr_rec). */
+int qx_tddft_store(qx_ctx *ctx);
+/* tddft_fssh_cal_matrix (tddft_fssh.f90:1344-1414): aij(i, j) = <prev_i|psi_j>
+ * with the Gamma metric 2 sum - x(1) y(1), aij column-major nband x nband
+ * (element (i, j) at aij[i + j * nband]); tensor cores (3xTF32) in mixed
+ * contexts.  The FP64 amplitude propagation and hops stay with the caller. */
+int qx_tddft_overlap(qx_ctx *ctx, double *aij);
 
 /* ---- Hellmann-Feynman forces (force.f90:5-860 terms floc and fnlc) ------ */
 /* Geometry tables, set once per geometry after the KB tables (qx_set_kb_g)

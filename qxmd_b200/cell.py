@@ -583,5 +583,21 @@ def si64(ecutdens: float = 64.0, with_ewald=True) -> System:
     return build_system(diamond_si((2, 2, 2), seed=2), 16.0, ecutdens, 160, with_ewald=with_ewald)
 
 
+def batch_cell(i: int, with_ewald: bool = False) -> System:
+    """Cell i of the batch of independent cells: with default_rng(100 + i),
+    Si8, Si16 (2x1x1) or Si32 (2x2x1), a uniform +-3% strain per axis, Ecut
+    drawn from {10, 12, 14, 16} Ry (density cutoff 4 Ecut) and 0-16 empty
+    bands above the occupied ones (at most 80 bands); the displacements use
+    the same seed."""
+    rng = np.random.default_rng(100 + i)
+    reps = ((1, 1, 1), (2, 1, 1), (2, 2, 1))[int(rng.integers(3))]
+    strain = 1.0 + rng.uniform(-0.03, 0.03, 3)
+    ecut = float(rng.choice([10.0, 12.0, 14.0, 16.0]))
+    c = diamond_si(reps, seed=100 + i, strain=strain)
+    nocc = c.nel // 2
+    nband = min(80, nocc + int(rng.integers(0, 17)))
+    return build_system(c, ecut, 4.0 * ecut, nband, with_ewald=with_ewald)
+
+
 def si512(with_ewald=False) -> System:
     return build_system(diamond_si((4, 4, 4), seed=3), 12.0, 48.0, 1100, with_ewald=with_ewald)

@@ -111,6 +111,8 @@ struct qx_ctx {
   int *d_ityp = nullptr, *d_ijk5 = nullptr, *d_ngabc = nullptr;
   double *d_satm = nullptr, *d_gvec5 = nullptr, *d_svco = nullptr, *d_gw = nullptr, *d_dcq = nullptr,
          *d_dsq = nullptr, *d_force = nullptr;
+  void *prev = nullptr;    // wavefunctions of the previous MD step (gdcr_rec), context precision
+  bool have_prev = false;
   void *dtab = nullptr;    // 3 nproj x nplwex derivative tables (context precision)
   void *dproj = nullptr;   // 3 nproj x nb
   bool have_ftab = false;
@@ -1288,7 +1290,7 @@ static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
   return 0;
 }
 
-extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
+extern "C" int qx_scf_launch(qx_ctx *c, const qx_cgparm *p) {
   if (!c || !p) return QX_ERR_ARG;
   if (!c->scf_ready || !c->have_occ) { set_error("qx_scf_iteration: call qx_scf_init and qx_set_occ first"); return QX_ERR_STATE; }
   c->defer = true;
@@ -1298,7 +1300,11 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
   else
     r = c->prec == QX_PREC_FP64 ? scf_body<double>(c, p) : scf_body<float>(c, p);
   c->defer = false;
-  TRY(r);
+  return r;
+}
+
+extern "C" int qx_scf_result(qx_ctx *c, qx_scf_out *out) {
+  if (!c) return QX_ERR_ARG;
   double sc[7];
   int info[3];
   CK(cudaMemcpyAsync(sc, c->d_sc, sizeof(double) * 7, cudaMemcpyDeviceToHost, c->st));
@@ -1318,6 +1324,44 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
     out->eig_clusters = info[0];
   }
   return QX_OK;
+}
+
+extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
+  TRY(qx_scf_launch(c, p));
+  return qx_scf_result(c, out);
+}
+
+// ---------------------------------------------------------------------------
+// TDDFT-FSSH overlaps (tddft_fssh_cal_matrix, tddft_fssh.f90:1344-1414)
+extern "C" int qx_tddft_store(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  const size_t bytes = c->tsize() * (size_t)c->nb * c->ne;
+  if (!c->prev) TRY(dalloc(c, &c->prev, bytes));
+  CK(cudaMemcpyAsync(c->prev, c->psi, bytes, cudaMemcpyDeviceToDevice, c->st));
+  c->have_prev = true;
+  return QX_OK;
+}
+
+template <typename T>
+static int tddft_overlap_impl(qx_ctx *c, double *aij) {
+  const int nb = c->nb;
+  T *m = (T *)c->mat_t;
+  // m(i, j) = <prev_i | psi_j> (column-major), Gamma metric: aijr(i, j) of the reference
+  TRY(gemm<T>(true, false, nb, nb, c->ne, (T)1, (const T *)c->prev, c->ne, (const T *)c->psi, c->ne, (T)0, m, nb, 1,
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+  convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
+  CKL();
+  if (aij) {
+    CK(cudaMemcpyAsync(aij, c->d_mat, sizeof(double) * nb * nb, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return 0;
+}
+
+extern "C" int qx_tddft_overlap(qx_ctx *c, double *aij) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_prev) { set_error("qx_tddft_overlap: call qx_tddft_store at the previous step first"); return QX_ERR_STATE; }
+  return c->prec == QX_PREC_FP64 ? tddft_overlap_impl<double>(c, aij) : tddft_overlap_impl<float>(c, aij);
 }
 
 // ---------------------------------------------------------------------------

@@ -1045,7 +1045,11 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   }
   // one warp per eigenvalue, one warp per block: spread over the SMs
   const size_t bsm = sizeof(double) * 2 * (size_t)n;
-  if (bsm > 48 * 1024) cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
+  static size_t bsm_set = 48 * 1024;   // per process: only ever raised (contexts of several sizes coexist)
+  if (bsm > bsm_set) {
+    cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
+    bsm_set = bsm;
+  }
   k_bisect<<<n, 32, bsm, st>>>(d, e, n, w); note_launch();
   const size_t wsm = sizeof(double) * 6 * (size_t)n * 16;
   if (wsm <= 200 * 1024) {

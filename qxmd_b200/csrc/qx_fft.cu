@@ -21,6 +21,8 @@
 #include <cmath>
 #include <cstdlib>
 
+#include <mutex>
+
 #include "qx_internal.h"
 
 // --------------------------------------------------------------------------
@@ -833,8 +835,15 @@ template size_t fft_smem_need<float>(const Plan &);
 template size_t fft_smem_need<double>(const Plan &);
 
 // Opt every kernel above into the shared-memory size the largest plan needs.
+// The attribute is per process and contexts of different grids coexist, so
+// it only ever grows.
 template <typename T>
 void set_fft_smem_limits(size_t bytes) {
+  static std::mutex mu;
+  static size_t cur = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (bytes <= cur) return;
+  cur = bytes;
   cudaFuncSetAttribute(k_zinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_ypass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_ypass<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

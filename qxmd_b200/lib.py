@@ -29,6 +29,7 @@ EXPORTS = [
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
     "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing", "qx_set_force_tables", "qx_forces",
+    "qx_tddft_store", "qx_tddft_overlap", "qx_scf_launch", "qx_scf_result",
     "qxgpu_kbnlpp_frc2",
     "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
@@ -118,6 +119,10 @@ def lib(build_if_missing: bool = True):
         "qx_scf_mixing": ([_ctx, C.c_int, C.c_double], C.c_int),
         "qx_set_force_tables": ([_ctx, C.c_int, C.c_int, _ip, _dp, C.c_int, _ip, _ip, _dp, _dp, _dp], C.c_int),
         "qx_forces": ([_ctx, _dp, _dp], C.c_int),
+        "qx_tddft_store": ([_ctx], C.c_int),
+        "qx_scf_launch": ([_ctx, C.POINTER(CgParm)], C.c_int),
+        "qx_scf_result": ([_ctx, C.POINTER(ScfOut)], C.c_int),
+        "qx_tddft_overlap": ([_ctx, _dp], C.c_int),
         "qxgpu_kbnlpp_frc2": ([_ctx, _dp, _dp], C.c_int),
         "qx_scf_rho_from_psi": ([_ctx], C.c_int),
         "qx_scf_iteration": ([_ctx, C.POINTER(CgParm), C.POINTER(ScfOut)], C.c_int),
@@ -304,6 +309,16 @@ class Context:
         _ck(self.L.qx_scf_init(self.h, _f64(s.vloc), _f64(s.gs.cross.ravel(order="F")),
                                s.gs.ecutdens, s.eewald, mixbeta, kerker_q0), "qx_scf_init")
 
+    def tddft_store(self):
+        """Keep the current psi as the previous MD step's wavefunctions."""
+        _ck(self.L.qx_tddft_store(self.h), "qx_tddft_store")
+
+    def tddft_overlap(self):
+        """aij[i, j] = <prev_i|psi_j> (Gamma metric), (nband, nband)."""
+        out = np.zeros((self.nb, self.nb))
+        _ck(self.L.qx_tddft_overlap(self.h, out), "qx_tddft_overlap")
+        return out.T.copy()   # column-major (i + j nband) -> [i, j]
+
     def set_force_tables(self):
         """qx_set_force_tables from the system's geometry (one species)."""
         t = cell.force_tables(self.sys)
@@ -333,6 +348,15 @@ class Context:
 
     def scf_rho_from_psi(self):
         _ck(self.L.qx_scf_rho_from_psi(self.h), "qx_scf_rho_from_psi")
+
+    def scf_launch(self, parm: CgParm):
+        """Enqueue one SCF iteration on this context's stream."""
+        _ck(self.L.qx_scf_launch(self.h, C.byref(parm)), "qx_scf_launch")
+
+    def scf_result(self) -> dict:
+        out = ScfOut()
+        _ck(self.L.qx_scf_result(self.h, C.byref(out)), "qx_scf_result")
+        return out.asdict()
 
     def scf_iteration(self, parm: CgParm) -> dict:
         out = ScfOut()

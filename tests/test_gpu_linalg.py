@@ -173,3 +173,21 @@ def test_rfft3(si8):
     bx, by = ctx.rfft3_host(2, fx, fy)
     assert relerr(bx, x) < 1e-13
     assert np.all(by == 0.0)
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-12), (QX_PREC_MIXED, 1e-5)])
+def test_tddft_overlap(si8, si8_psi, prec, tol):
+    """tddft_fssh_cal_matrix (tddft_fssh.f90:1344-1414): aij = <psi_i(t)|psi_j(t+dt)>
+    with the Gamma metric, previous-step wavefunctions kept on the device."""
+    need_gpu()
+    rng = np.random.default_rng(7)
+    prev = si8_psi
+    cur = si8_psi + 1e-2 * rng.standard_normal(si8_psi.shape)
+    cur[:, 1] = 0.0
+    ctx = Context(si8, prec, QX_NL_GSPACE)
+    ctx.put_psi(prev)
+    ctx.tddft_store()
+    ctx.put_psi(cur)
+    a = ctx.tddft_overlap()
+    ref = np.array([[oracle.dot(prev[i], cur[j]) for j in range(16)] for i in range(16)])
+    assert relerr(a, ref) < tol
