@@ -37,6 +37,10 @@ METRIC = "SCF iter/s"
 # Pulay density mixing with the reference defaults (modules.f90:136-142:
 # imxchg 1, aslh 0.8, bslh 0.64 = 0.8^2, itratn 10, cmetric 20)
 PULAY_ASLH, PULAY_Q0, PULAY_ITRATN, PULAY_CMETRIC = 0.8, 0.8, 10, 20.0
+# dram__bytes_read.sum + dram__bytes_write.sum over the four launches of one
+# FP32 H|psi> pass of this workload (ncu, --profile-hpsi; the capture command
+# is listed with the figures in the profiles directory)
+HPSI_PASS_DRAM_BYTES = 69812480
 UNIT = "iter/s"
 WORKLOAD = "Si64 diamond 2x2x2, Gamma, Ecut 16 Ry / 64 Ry, 54^3 grid, 160 bands, G-space KB"
 # Average CG H|psi> band applications per SCF iteration of this workload after
@@ -451,7 +455,11 @@ def run_ours(args):
         "roofline": {"kernel": "H|psi> FFT pipeline (zinv, y, xvx, y, zfwd, unpack), FP32",
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_band_app": bytes_per_bapp, "traffic": None},
+                     "algorithmic_bytes_per_band_app": bytes_per_bapp,
+                     # DRAM read + write of one all-band pass (four launches),
+                     # from the ncu capture of this workload
+                     "traffic": HPSI_PASS_DRAM_BYTES, "traffic_unit": "bytes per 160-band pass",
+                     "algorithmic_bytes_per_pass": bytes_per_bapp * sys_.nband},
         "clocks": mixed["clocks"],
     }
     if ws == 1 and rank == 0:
