@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--profile-step", action="store_true",
                     help="only the mixed-precision SCF iterations (warm-up, then --steps), no L2 flush, "
                          "no extra arms: the launch sequence profiled under ncu")
+    ap.add_argument("--si512", action="store_true",
+                    help="only H|psi> band applications/s on the Si512 cell (1100 bands, 96^3 grid), mixed and FP64")
     ap.add_argument("--sequential", action="store_true",
                     help="with --profile-step: the plain FP64 path (one-rank band order) instead of mixed")
     ap.add_argument("--accuracy-iters", type=int, default=40,
@@ -241,6 +243,46 @@ def accuracy(acc, natom, iters):
     out["force_max_abs_fp64_ha_per_bohr"] = 0.5 * float(np.max(np.abs(ref["force"])))
     out["force_terms"] = "local pseudopotential (flocal_g) + G-space KB (kbnlpp_frc2); the ion-ion term is identical in all paths"
     return out
+
+
+def run_si512(args):
+    """H|psi> band applications per second (kinetic + local + G-space KB, all
+    1100 bands: qx_enonloc) on the Si512 cell, 96^3 grid, mixed and FP64.
+    The SCF iteration itself is not timed here: its one-CTA FP64 eigensolver
+    and Cholesky do not scale to 1100 bands."""
+    import torch
+
+    from qxmd_b200 import cell
+    from qxmd_b200.lib import Context, QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED
+    t0 = time.perf_counter()
+    sys_ = cell.si512()
+    setup_s = time.perf_counter() - t0
+    psi = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    out = {"metric": "H|psi> band-apps/s", "config": {"workload": "Si512 diamond 4x4x4, Gamma, Ecut 12 Ry / 48 Ry, "
+                                                                  "96^3 grid, 1100 bands, G-space KB",
+                                                      "nplwex": sys_.gs.nplwex, "nproj": int(sys_.kb_g.shape[1])},
+           "host_setup_s": setup_s}
+    for name, prec in (("mixed", QX_PREC_MIXED), ("fp64", QX_PREC_FP64)):
+        ctx = Context(sys_, prec, QX_NL_GSPACE)
+        ctx.put_psi(psi)
+        for _ in range(max(1, args.warmup)):
+            ctx.enonloc()
+        ctx.sync()
+        t = 0.0
+        R = max(2, args.steps)
+        for _ in range(R):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.enonloc()
+            e1.record()
+            torch.cuda.synchronize()
+            t += e0.elapsed_time(e1)
+        out[name] = {"value": sys_.nband * R / (t / 1e3), "ms_per_pass": t / R}
+        ctx.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    print(json.dumps(out), flush=True)
 
 
 def run_batch(K, W):
@@ -531,6 +573,8 @@ def main():
         run_profile_step(args)
     elif args.profile_hpsi:
         run_profile_hpsi(args)
+    elif args.si512:
+        run_si512(args)
     else:
         run_ours(args)
 

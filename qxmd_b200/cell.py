@@ -521,17 +521,29 @@ def random_wavefunctions(nplwex: int, nband: int, seed: float = 25.0) -> np.ndar
     (`funcs.f90:1673-1689`) with seed 25.0 (`savedd.f90:289, 911-918`):
     gdcr(i, n) = rn - 0.5 in band order, then gdcr(2, n) = 0.  Returned with
     shape (nband, nplwex) (row n = band n, the column-major Fortran layout)."""
-    a = 16807.0
-    m = 2147483647.0
-    x = float(seed)
+    a = 16807
+    m = 2147483647
     out = np.empty((nband, nplwex))
-    # The recurrence is exact in binary64 (products stay below 2^53), so a
-    # vectorised power-of-a jump would give identical values; the loop keeps
-    # the statement order of the reference.
     flat = out.reshape(-1)
-    for i in range(flat.size):
-        x = math.fmod(a * x, m)
-        flat[i] = x / m - 0.5
+    total = flat.size
+    # x_{k+1} = a x_k mod m is exact in binary64 (products below 2^53) and in
+    # int64, so the states are computed in blocks of B: x_{k+B} = (a^B mod m)
+    # x_k mod m (products below 2^62), giving the same values as the
+    # one-by-one recurrence of the reference.
+    B = min(total, 4096)
+    first = np.empty(B, dtype=np.int64)
+    x = int(seed)
+    for i in range(B):
+        x = (a * x) % m
+        first[i] = x
+    jump = pow(a, B, m)
+    states = np.empty(total, dtype=np.int64)
+    cur = first
+    for k0 in range(0, total, B):
+        n = min(B, total - k0)
+        states[k0:k0 + n] = cur[:n]
+        cur = (cur * jump) % m
+    flat[:] = states.astype(np.float64) / float(m) - 0.5
     out[:, 1] = 0.0
     return out
 
