@@ -186,6 +186,22 @@ int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
 int qx_scf_launch(qx_ctx *ctx, const qx_cgparm *p);
 int qx_scf_result(qx_ctx *ctx, qx_scf_out *out);
 
+/* ---- FP64 refinement sweep --------------------------------------------- */
+/* dst (an FP64 context of the same cell, after qx_scf_init) takes over src's
+ * state on the device: psi widened to FP64, src's rho_out as the next input
+ * density, the Pulay history restarted.  A few qx_scf_iteration calls on dst
+ * then refine a mixed-precision SCF solution to FP64. */
+int qx_refine_from(qx_ctx *dst, qx_ctx *src);
+
+/* ---- autotuner --------------------------------------------------------- */
+/* Times this context's launch choices on its own buffers and keeps the
+ * fastest: the K-split of each tensor-core contraction shape (shared by
+ * contexts of equal sizes) and, for FP32, the fused plane kernels against the
+ * generic y/x passes of the FFT pipeline.  Overwrites only scratch buffers;
+ * call after set-up and before the SCF iterations (captured iteration graphs
+ * are dropped).  report (nullable): a one-line summary. */
+int qx_autotune(qx_ctx *ctx, char *report, int report_len);
+
 /* ---- TDDFT-FSSH nonadiabatic overlaps --------------------------------- */
 /* Keep the current psi as the previous step's wavefunctions (gdcr_rec). */
 int qx_tddft_store(qx_ctx *ctx);

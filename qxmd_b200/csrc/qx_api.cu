@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
+#include <string>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -703,7 +705,7 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
                 ncol_dev, c->st, c->gws, c->gws_bytes));
     scale_rows<T>(np, ncol_max, proj, np, b.vclalp, colmap, ncol_dev, c->st);
     TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, colmap,
-                ncol_dev, c->st));
+                ncol_dev, c->st, c->gws, c->gws_bytes));
     CKL();
   }
   return 0;
@@ -813,7 +815,7 @@ static int rotate(qx_ctx *c, void *&arr) {
   const int nb = c->nb;
   const T *U = (const T *)c->mat_t;
   TRY(gemm<T>(false, false, c->ne, nb, nb, (T)1, (const T *)arr, c->ne, U, nb, (T)0, (T *)c->tmp, c->ne, 0, nullptr,
-              nullptr, c->st));
+              nullptr, c->st, c->gws, c->gws_bytes));
   CKL();
   std::swap(arr, c->tmp);
   return 0;
@@ -1329,6 +1331,117 @@ extern "C" int qx_scf_result(qx_ctx *c, qx_scf_out *out) {
 extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
   TRY(qx_scf_launch(c, p));
   return qx_scf_result(c, out);
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: times the candidates of this context's launch choices on its own
+// buffers (outputs into scratch) and keeps the fastest:
+//  * the K-split factor of each tensor-core contraction shape (process-wide);
+//  * the fused plane kernels against the generic y/x passes of the FP32 FFT
+//    pipeline (per context).
+// Reads psi/hpsi and overwrites only scratch (tmp, mat_t, proj); previously
+// captured SCF graphs are dropped so the next iteration is captured with the
+// new choices.
+static int time_ms(cudaStream_t st, const std::function<int()> &f, int reps, float *ms) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  TRY(f());   // warm-up
+  CK(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; ++r) TRY(f());
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  *ms /= reps;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return 0;
+}
+
+extern "C" int qx_autotune(qx_ctx *c, char *report, int report_len) {
+  if (!c) return QX_ERR_ARG;
+  std::string rep;
+  char buf[256];
+  const int nb = c->nb, ne = c->ne, np = c->pl.nproj;
+  if (c->prec == QX_PREC_MIXED && tc_enabled()) {
+    struct Shape { bool ta, tb; int M, N, K, gamma; const void *A; long lda; const void *B; long ldb; float beta; long ldc; const char *what; };
+    std::vector<Shape> shapes = {
+        {true, false, nb, nb, ne, 1, c->psi, ne, c->hpsi, ne, 0.f, nb, "C^T X"},
+        {false, false, ne, nb, nb, 0, c->psi, ne, c->mat_t, nb, 0.f, ne, "C U"},
+    };
+    if (c->have_kbg && np > 0) {
+      shapes.push_back({true, false, np, nb, ne, 2, c->pl.b32.kbg, ne, c->psi, ne, 0.f, np, "K^T C"});
+      shapes.push_back({false, false, ne, nb, np, 0, c->pl.b32.kbg, ne, c->proj, np, 1.f, ne, "K P"});
+    }
+    const int cand[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48};
+    for (const Shape &sh : shapes) {
+      const int nkb = (sh.K + 31) / 32;
+      float best = 1e30f;
+      int bests = 1;
+      for (int ns : cand) {
+        if (ns > nkb || (size_t)ns * sh.M * sh.N * sizeof(float) > c->gws_bytes) continue;
+        float ms = 0.f;
+        tc_split_force = ns;
+        const int r = time_ms(c->st, [&]() {
+          return gemm<float>(sh.ta, sh.tb, sh.M, sh.N, sh.K, 1.f, (const float *)sh.A, sh.lda, (const float *)sh.B,
+                             sh.ldb, sh.beta, (float *)c->tmp, sh.ldc, sh.gamma, nullptr, nullptr, c->st, c->gws,
+                             c->gws_bytes);
+        }, 3, &ms);
+        tc_split_force = 0;
+        TRY(r);
+        if (ms < best) { best = ms; bests = ns; }
+      }
+      tc_split_store(sh.ta, sh.tb, sh.M, sh.N, sh.K, sh.gamma, bests);
+      snprintf(buf, sizeof(buf), "%s %dx%dx%d: K split %d (%.1f us); ", sh.what, sh.M, sh.N, sh.K, bests, best * 1e3);
+      rep += buf;
+    }
+  }
+  if (c->prec == QX_PREC_MIXED && c->have_glocal && plane_length_supported(c->pl.k1, c->pl.k2)) {
+    float ms[2] = {0.f, 0.f};
+    for (int v = 0; v < 2; ++v) {
+      c->pl.use_plane = (v == 0);
+      TRY(time_ms(c->st, [&]() { return qx_hpsi(c, c->psi, c->tmp, nb, QX_HPSI_KINETIC); }, 3, &ms[v]));
+    }
+    c->pl.use_plane = ms[0] <= ms[1];
+    snprintf(buf, sizeof(buf), "H|psi> pass: fused planes %.1f us, y/x passes %.1f us -> %s", ms[0] * 1e3,
+             ms[1] * 1e3, c->pl.use_plane ? "fused planes" : "y/x passes");
+    rep += buf;
+  }
+  for (auto &g : c->scf_graphs) cudaGraphExecDestroy(g.exec);
+  c->scf_graphs.clear();
+  if (report && report_len > 0) {
+    strncpy(report, rep.c_str(), report_len - 1);
+    report[report_len - 1] = 0;
+  }
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 refinement sweep: an FP64 context of the same cell takes over the
+// converged state of a mixed-precision one on the device (psi widened to
+// FP64, rho_out as the next input density, the Pulay history restarted); the
+// caller then runs a few FP64 SCF iterations on it.
+extern "C" int qx_refine_from(qx_ctx *dst, qx_ctx *src) {
+  if (!dst || !src) return QX_ERR_ARG;
+  if (dst->prec != QX_PREC_FP64 || src->nb != dst->nb || src->ne != dst->ne || src->pl.n != dst->pl.n) {
+    set_error("qx_refine_from: needs an FP64 context of the same cell (bands, sphere, grid)");
+    return QX_ERR_ARG;
+  }
+  if (!dst->scf_ready || !src->d_rho_out) { set_error("qx_refine_from: call qx_scf_init on both contexts first"); return QX_ERR_STATE; }
+  TRY(ensure_rho(dst));
+  // src's work must be complete before dst's stream reads its buffers
+  CK(cudaStreamSynchronize(src->st));
+  const long n = (long)dst->nb * dst->ne;
+  if (src->prec == QX_PREC_FP64)
+    CK(cudaMemcpyAsync(dst->psi, src->psi, sizeof(double) * n, cudaMemcpyDeviceToDevice, dst->st));
+  else
+    convert<float, double>((const float *)src->psi, (double *)dst->psi, n, dst->st);
+  CK(cudaMemcpyAsync(dst->d_rho_in, src->d_rho_out, sizeof(double) * dst->pl.n, cudaMemcpyDeviceToDevice, dst->st));
+  CKL();
+  dst->pulay_reset = true;
+  dst->have_u = false;
+  dst->have_hsub = false;
+  return QX_OK;
 }
 
 // ---------------------------------------------------------------------------

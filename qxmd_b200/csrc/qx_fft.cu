@@ -729,7 +729,7 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
   dim3 gy(P.k3, npl);
   const size_t smy = fft_smem(P.L2, P.P1, cs);
-  if (sizeof(T) == sizeof(float) && nlmode != 2 && plane_enabled() &&
+  if (sizeof(T) == sizeof(float) && nlmode != 2 && pl.use_plane && plane_enabled() &&
       launch_plane_f32(P, npl, (float2 *)bf.bufA, (const float *)bf.vloc, st) == 0) {
     dim3 gu((P.nplw + 1 + 127) / 128, npl);
     k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
@@ -767,7 +767,7 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
   const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
   k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
-  if (sizeof(T) == sizeof(float) && plane_enabled() && bf.rho_part &&
+  if (sizeof(T) == sizeof(float) && pl.use_plane && plane_enabled() && bf.rho_part &&
       launch_rho_plane_f32(P, npl, (const float2 *)bf.bufA, wocc, bf.rho_part, rho, accumulate, st) == 0)
     return 0;
   dim3 gy(P.k3, npl);

@@ -70,6 +70,7 @@ struct Plan {
   int4 *d_line_ent = nullptr;
   // G-space KB
   int nproj = 0;
+  bool use_plane = true;   // FP32 fused plane kernels where supported (the autotuner may turn them off)
   mutable Bufs<float> b32;
   mutable Bufs<double> b64;
   template <typename T> Bufs<T> &bufs() const;
@@ -126,6 +127,11 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
 bool tc_enabled();
 // Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
 int tc_error_take();
+// autotuner hooks of the tensor-core GEMM: a per-shape K-split table and a
+// per-thread override used while timing candidates
+extern thread_local int tc_split_force;
+int tc_split_lookup(bool ta, bool tb, int M, int N, int K, int gamma);
+void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit);
 
 // qx_dense.cu (FP64, nb x nb)
 // work: >= 32*33 + n doubles, used when S does not fit shared memory.

@@ -26,6 +26,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <array>
+#include <map>
 #include <mutex>
 
 #include "qx_internal.h"
@@ -450,6 +452,21 @@ static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs 
 
 bool tc_enabled() { return tc::enabled(); }
 
+// K-split factors chosen by the autotuner, per shape (process-wide: contexts
+// of equal sizes share them), and the override the autotuner times with.
+static std::mutex g_split_mu;
+static std::map<std::array<long, 6>, int> g_split;
+thread_local int tc_split_force = 0;
+int tc_split_lookup(bool ta, bool tb, int M, int N, int K, int gamma) {
+  std::lock_guard<std::mutex> lk(g_split_mu);
+  auto it = g_split.find({(long)ta, (long)tb, M, N, K, gamma});
+  return it == g_split.end() ? 0 : it->second;
+}
+void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit) {
+  std::lock_guard<std::mutex> lk(g_split_mu);
+  g_split[{(long)ta, (long)tb, M, N, K, gamma}] = nsplit;
+}
+
 // Tensor-core FP32 GEMM with the semantics of gemm<float> (no column map).
 // Returns 0 when launched, -1 when the operands do not meet the TMA rules
 // (the caller then uses the CUDA-core kernel), >0 on error.
@@ -469,13 +486,19 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   CUtensorMap ma, mb;
   if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, true) : tc::make_map(&ma, A, K, M, lda, BM, false))) return -1;
   if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, true) : tc::make_map(&mb, B, K, N, ldb, bn, false))) return -1;
-  // split K until the grid covers the SMs, at least 8 k-blocks a split
+  // split K until the grid covers the SMs, at least 8 k-blocks a split, or
+  // as the autotuner measured for this shape
   int nsplit = 1;
   const long tiles = (long)tm * tn;
-  if (ws && tiles < 100) {
+  const int tuned = ws ? tc_split_lookup(ta, tb, M, N, K, gamma) : 0;
+  if (ws && tc_split_force > 0) {
+    nsplit = std::min(tc_split_force, nkb);
+  } else if (tuned > 0) {
+    nsplit = std::min(tuned, nkb);
+  } else if (ws && tiles < 100) {
     nsplit = (int)std::min<long>((148 + tiles - 1) / tiles, std::max(1, nkb / 8));
-    while (nsplit > 1 && (size_t)nsplit * M * N * sizeof(float) > ws_bytes) --nsplit;
   }
+  while (nsplit > 1 && (size_t)nsplit * M * N * sizeof(float) > ws_bytes) --nsplit;
   const int kps = (nkb + nsplit - 1) / nsplit;
   nsplit = (nkb + kps - 1) / kps;
   tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr};

@@ -29,7 +29,7 @@ EXPORTS = [
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
     "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing", "qx_set_force_tables", "qx_forces",
-    "qx_tddft_store", "qx_tddft_overlap", "qx_scf_launch", "qx_scf_result",
+    "qx_tddft_store", "qx_tddft_overlap", "qx_autotune", "qx_refine_from", "qx_scf_launch", "qx_scf_result",
     "qxgpu_kbnlpp_frc2",
     "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
@@ -120,6 +120,8 @@ def lib(build_if_missing: bool = True):
         "qx_set_force_tables": ([_ctx, C.c_int, C.c_int, _ip, _dp, C.c_int, _ip, _ip, _dp, _dp, _dp], C.c_int),
         "qx_forces": ([_ctx, _dp, _dp], C.c_int),
         "qx_tddft_store": ([_ctx], C.c_int),
+        "qx_autotune": ([_ctx, C.c_char_p, C.c_int], C.c_int),
+        "qx_refine_from": ([_ctx, _ctx], C.c_int),
         "qx_scf_launch": ([_ctx, C.POINTER(CgParm)], C.c_int),
         "qx_scf_result": ([_ctx, C.POINTER(ScfOut)], C.c_int),
         "qx_tddft_overlap": ([_ctx, _dp], C.c_int),
@@ -308,6 +310,16 @@ class Context:
         s = self.sys
         _ck(self.L.qx_scf_init(self.h, _f64(s.vloc), _f64(s.gs.cross.ravel(order="F")),
                                s.gs.ecutdens, s.eewald, mixbeta, kerker_q0), "qx_scf_init")
+
+    def refine_from(self, src: "Context"):
+        """qx_refine_from: take over src's converged state (this context FP64)."""
+        _ck(self.L.qx_refine_from(self.h, src.h), "qx_refine_from")
+
+    def autotune(self) -> str:
+        """qx_autotune; returns its one-line report."""
+        buf = C.create_string_buffer(2048)
+        _ck(self.L.qx_autotune(self.h, buf, 2048), "qx_autotune")
+        return buf.value.decode()
 
     def tddft_store(self):
         """Keep the current psi as the previous MD step's wavefunctions."""

@@ -91,3 +91,33 @@ def test_scf_graph_replay_matches_stream_launches(si8, si8_psi, monkeypatch):
             assert a["eig_clusters"] == b["eig_clusters"] and a["zmax"] == b["zmax"]
         np.testing.assert_array_equal(pa, pb)
         np.testing.assert_array_equal(ra, rb)
+
+
+def test_autotune_then_refine_to_fp64(si8, si8_psi):
+    """The autotuner's choices keep the mixed path's numbers, and the FP64
+    refinement sweep (qx_refine_from + 3 FP64 iterations) of a converged
+    mixed solution lands on the FP64 solution."""
+    need_gpu()
+    p = CgParm.defaults(16)
+
+    def setup(prec):
+        ctx = Context(si8, prec, QX_NL_GSPACE)
+        ctx.put_psi(si8_psi)
+        ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)
+        ctx.scf_mixing(10, 20.0)
+        return ctx
+
+    ref = setup(QX_PREC_FP64)
+    ref.scf_rho_from_psi()
+    e64 = [ref.scf_iteration(p)["etot"] for _ in range(30)][-1]
+    mixed = setup(QX_PREC_MIXED)
+    report = mixed.autotune()
+    assert "split" in report
+    mixed.put_psi(si8_psi)
+    mixed.scf_rho_from_psi()
+    emx = [mixed.scf_iteration(p)["etot"] for _ in range(30)][-1]
+    assert abs(emx - e64) / si8.cell.natom < 2e-6          # Ry/atom, FP32 level
+    fine = setup(QX_PREC_FP64)
+    fine.refine_from(mixed)
+    efine = [fine.scf_iteration(p)["etot"] for _ in range(3)][-1]
+    assert abs(efine - e64) / si8.cell.natom < 2e-9        # Ry/atom, FP64 level
