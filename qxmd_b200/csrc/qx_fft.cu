@@ -707,14 +707,10 @@ static FftTabs<T> tabs(const Plan &pl, int d) {
 }
 
 // The fused register-FFT plane pass is on unless QX_PLANE=0 (kept to compare
-// against the shared-memory passes).
+// against the shared-memory passes; read at every launch).
 static bool plane_enabled() {
-  static int en = -1;
-  if (en < 0) {
-    const char *e = getenv("QX_PLANE");
-    en = (e && e[0] == '0') ? 0 : 1;
-  }
-  return en == 1;
+  const char *e = getenv("QX_PLANE");
+  return !(e && e[0] == '0');
 }
 
 template <typename T>
