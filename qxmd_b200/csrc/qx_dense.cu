@@ -21,6 +21,16 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// f(DenseIC<I>{}) for I = B .. E-1: a compile-time index for register arrays,
+// used to branch on a uniform runtime slot instead of selecting over slots.
+template <int I> struct DenseIC { static constexpr int value = I; };
+template <int B, int E, typename F> __device__ __forceinline__ void dense_static_for(F &&f) {
+  if constexpr (B < E) {
+    f(DenseIC<B>{});
+    dense_static_for<B + 1, E>(f);
+  }
+}
+
 // --------------------------------------------------------------------------
 // Cholesky S = L L^T and L^-1, blocked by CB = 32.  Column-major n x n; on
 // return the lower triangle holds L^-1 and the upper triangle zeros.
@@ -480,6 +490,125 @@ __global__ void __launch_bounds__(CPT) k_cholinv_sm(double *__restrict__ Sg, int
   if (tid == 0) *info = 0;
 }
 
+// Cholesky and L^-1 together with the matrix in registers (n <= W NR and
+// n <= 32 NC; one CTA of W warps; thread (w, l) keeps rows NR w .. NR w + NR - 1
+// of the columns l + 32 c).  X = L^-1 is found by rows (X L = I top down)
+// with running right-hand sides R (R(i,:) = e_i at the start), stored where L
+// was consumed.  Step k: column k (the Schur complement) is published and
+// replaced by e_k, which starts R's column k; row k (R(k, 0..k)) is
+// published; one barrier; then with rs = 1 / L(k,k), m_i = S(i,k) rs (rows
+// i > k) and y = (R(k, 0..k) rs, m_(k+1..)), every row i > k takes one rank-1
+// update a(i,:) -= m_i y: the Cholesky update of the columns > k, the
+// forward-substitution update R(i,l) -= m_i X(k,l) of the columns <= k.  Row
+// k is final from then on; it is scaled by its rs when written out, which
+// gives X(k, 0..k).  The gathered column and row alternate by parity, so one
+// barrier a step suffices.  The matrix is staged through shared memory on
+// the way in (the lower triangle, as rsdecmp reads it) and out (coalesced
+// column-major stores).  info as k_cholinv_sm; S is left as it was on failure.
+template <int W, int NR, int NC>
+__global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ Sg, int n, int *__restrict__ info) {
+  constexpr int NROW = W * NR, NCOL = 32 * NC;
+  constexpr int NX = NROW > NCOL ? NROW : NCOL;
+  static_assert(NR <= 32, "lane r of a warp keeps m of the warp's row r");
+  extern __shared__ double stg[];   // n x (n | 1) staging
+  __shared__ double xcol[2][NX];
+  __shared__ double xrow[2][NCOL];
+  __shared__ double rsv[NX];
+  const int ld = n | 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = warp * NR;
+  for (long q = tid; q < (long)n * n; q += W * 32) {
+    const int j = (int)(q / n), i = (int)(q - (long)j * n);
+    stg[(long)j * ld + i] = Sg[q];
+  }
+  __syncthreads();
+  double a[NR][NC];
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const int row = r0 + r, col = lane + 32 * c;
+      const int hi = row > col ? row : col, lo = row > col ? col : row;
+      const double v = stg[(long)min(lo, n - 1) * ld + min(hi, n - 1)];   // S(hi, lo), clamped address
+      a[r][c] = (row < n && col < n) ? v : 0.0;
+    }
+  for (int k = 0; k < n; ++k) {
+    const int b = k & 1, kc = k >> 5;
+    if (lane == (k & 31))     // column k out, e_k in
+      dense_static_for<0, NC>([&](auto cc) {
+        constexpr int C = decltype(cc)::value;
+        if (C == kc) {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            xcol[b][r0 + r] = a[r][C];
+            a[r][C] = (r0 + r == k) ? 1.0 : 0.0;
+          }
+        }
+      });
+    if (warp == k / NR) {     // row k out
+      const int kr = k - r0;
+      dense_static_for<0, NR>([&](auto rr) {
+        constexpr int R = decltype(rr)::value;
+        if (R == kr) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) xrow[b][lane + 32 * c] = a[R][c];
+        }
+      });
+    }
+    __syncthreads();
+    const double piv = xcol[b][k];
+    if (!(piv > 1.0e-30)) {   // the same in every thread; also catches NaN
+      if (tid == 0) *info = 1 + k;
+      return;
+    }
+    const double rs = rsqrt_nr(piv);   // 1 / L(k,k)
+    if (tid == 0) rsv[k] = rs;
+    // lane r < NR: m of row r0 + r (0 for rows <= k, which the update then leaves as they are)
+    const int ri = min(r0 + lane, NX - 1);
+    const double mrow = (lane < NR && r0 + lane > k && r0 + lane < n) ? xcol[b][ri] * rs : 0.0;
+    if (r0 + NR > k + 1) {    // rows below k in this warp
+      double y[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int col = lane + 32 * c;
+        const double xr = xrow[b][col], xc = xcol[b][min(col, NX - 1)];
+        y[c] = ((col <= k) ? xr : ((col < n) ? xc : 0.0)) * rs;
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const double mi = __shfl_sync(0xffffffffu, mrow, r);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) a[r][c] = fma(-mi, y[c], a[r][c]);
+      }
+    }
+  }
+  __syncthreads();
+  // X to the staging area (lower triangle, zeros above), then out column-major
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    const int row = r0 + r;
+    const double sc = rsv[min(row, NX - 1)];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const int col = lane + 32 * c;
+      if (row < n && col < n) stg[(long)col * ld + row] = (row >= col) ? a[r][c] * sc : 0.0;
+    }
+  }
+  __syncthreads();
+  for (long q = tid; q < (long)n * n; q += W * 32) {
+    const int j = (int)(q / n), i = (int)(q - (long)j * n);
+    Sg[q] = stg[(long)j * ld + i];
+  }
+  if (tid == 0) *info = 0;
+}
+
+// QX_CHOLINV_REG=0 keeps the shared-memory kernels at every size (read at
+// every call).
+static bool cholinv_registers_enabled() {
+  const char *v = getenv("QX_CHOLINV_REG");
+  return !(v && v[0] == '0');
+}
+
 // S: n x n column-major.  When S does not fit shared memory the kernel works
 // in S itself (L2-resident) and uses work (>= CB*DLD + n doubles) as temporary.
 int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
@@ -493,6 +622,19 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
   }
   if (!use && !work) { set_error("cholinv: n=%d needs a work buffer", n); return 1; }
   const size_t pbytes = sizeof(double) * ((size_t)(n | 1) * n + 2 * (size_t)n + (size_t)PB * n);
+  const size_t rbytes = sizeof(double) * (size_t)(n | 1) * n;
+  if (n <= 160 && cholinv_registers_enabled()) {
+    static size_t rset = 48 * 1024;   // per process: only ever raised
+    if (rbytes > rset) {
+      cudaFuncSetAttribute(k_cholinv_rg<8, 10, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
+      cudaFuncSetAttribute(k_cholinv_rg<8, 20, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
+      rset = CH_SMEM_MAX;
+    }
+    if (n <= 80) k_cholinv_rg<8, 10, 3><<<1, 8 * 32, rbytes, st>>>(S, n, d_info);
+    else k_cholinv_rg<8, 20, 5><<<1, 8 * 32, rbytes, st>>>(S, n, d_info);
+    note_launch();
+    return 0;
+  }
   if (n <= CP_MAXN && pbytes <= CH_SMEM_MAX) {
     static bool pattr = false;
     if (!pattr) {
@@ -679,6 +821,154 @@ __global__ void __launch_bounds__(TRD_T) k_sytrd(double *__restrict__ Ag, int n,
 #undef A_
 }
 
+// The same tridiagonalisation with the whole matrix in registers (n <= W NR
+// and n <= 32 NC; one CTA of W warps): warp w holds rows NR w .. NR w + NR - 1,
+// lane l the columns l + 32 c, so thread (w, l) keeps an NR x NC block and no
+// element of A passes through shared memory after the load.  Per column k,
+// three barriers:
+//   (1) lane k mod 32 of every warp has put its piece of column k (and the
+//       partial sum of squares below the subdiagonal) in shared memory; every
+//       thread then forms the same reflector (house) and its own v entries;
+//   (2) column partial sums of A v over each warp's rows are in shared memory
+//       (A is symmetric, so (A v)_j is a column sum);
+//   (3) p = tau A v is summed, zero for rows <= k; every warp forms
+//       K = tau v^T p / 2, w = p - K v, and updates its block in registers:
+//       A_ij -= v_i w_j + w_i v_j (rows and columns <= k have v = w = 0).
+// The column buffer and the sums of squares alternate by column parity, so a
+// warp that gathers column k + 1 never overwrites what a slower warp still
+// reads for column k.  A must be symmetric; it is read by rows (coalesced).
+template <int TRR_W, int NR, int NC>
+__global__ void __launch_bounds__(TRR_W * 32, 1)
+    k_sytrd_rg(const double *__restrict__ Ag, int n, double *__restrict__ d, double *__restrict__ e,
+               double *__restrict__ HV, double *__restrict__ tau) {
+  constexpr int NROW = TRR_W * NR, NCOL = 32 * NC;
+  static_assert(NROW <= NCOL, "p is indexed by rows and by columns");
+  static_assert(NR <= 32, "lane r of a warp keeps v and w of the warp's row r");
+  __shared__ double xs[2][NROW];
+  __shared__ double sigp[2][TRR_W];
+  __shared__ double part[TRR_W][NCOL];
+  __shared__ double ps[NCOL];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int r0 = warp * NR;
+  double a[NR][NC];
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const int row = r0 + r, col = lane + 32 * c;
+      a[r][c] = (row < n && col < n) ? Ag[(long)row * n + col] : 0.0;
+    }
+  // column kk of A into xs[b] (all rows); sum of squares of rows > kk + 1 into sigp[b]
+  auto gather = [&](int kk, int b) {
+    if (lane == (kk & 31)) {
+      const int kc = kk >> 5;
+      dense_static_for<0, NC>([&](auto cc) {
+        constexpr int C = decltype(cc)::value;
+        if (C == kc) {
+          double sg[2] = {0.0, 0.0};
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            const double x = a[r][C];
+            xs[b][r0 + r] = x;
+            sg[r & 1] += (r0 + r > kk + 1) ? x * x : 0.0;
+          }
+          sigp[b][warp] = sg[0] + sg[1];
+        }
+      });
+    }
+  };
+  for (int k = 0; k + 2 < n; ++k) {
+    const int b = k & 1;
+    gather(k, b);
+    __syncthreads();                                                   // (1)
+    double sigma = 0.0;
+#pragma unroll
+    for (int w = 0; w < TRR_W; ++w) sigma += sigp[b][w];
+    double t = 0.0, rb = 1.0, al = 0.0;
+    house(xs[b][k + 1], sigma, t, rb, al);
+    const double *x = xs[b];
+    // v(i) = 1 at k + 1, x_i / beta below, 0 elsewhere (all of v is e1 when
+    // tau = 0); the load is unconditional (clamped index) and the selection
+    // follows, so unrolled uses do not serialise on it
+    auto vof = [&](int i) {
+      const double xv = x[min(i, NROW - 1)] * rb;
+      return (i == k + 1) ? 1.0 : ((i > k + 1 && i < n && t != 0.0) ? xv : 0.0);
+    };
+    if (tid == 0) {
+      tau[k] = t;
+      d[k] = x[k];
+      e[k] = al;
+    }
+    for (int i = k + 1 + tid; i < n; i += TRR_W * 32) HV[(long)k * n + i] = vof(i);
+    if (t == 0.0) continue;                                            // same in every thread
+    const bool rows_active = r0 + NR > k + 1;                          // uniform in the warp
+    // lane r < NR keeps v of row r0 + r; the warp reads it by shuffles
+    const double vrow = (lane < NR) ? vof(r0 + lane) : 0.0;
+    {
+      double sc[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) sc[c] = 0.0;
+      if (rows_active) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const double vr = __shfl_sync(0xffffffffu, vrow, r);
+#pragma unroll
+          for (int c = 0; c < NC; ++c) sc[c] = fma(a[r][c], vr, sc[c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) part[warp][lane + 32 * c] = sc[c];
+    }
+    __syncthreads();                                                   // (2)
+    for (int j = tid; j < NCOL; j += TRR_W * 32) {
+      double acc = 0.0;
+#pragma unroll
+      for (int w = 0; w < TRR_W; ++w) acc += part[w][j];
+      ps[j] = (j > k && j < n) ? t * acc : 0.0;
+    }
+    __syncthreads();                                                   // (3)
+    double kk = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) kk = fma(vof(lane + 32 * c), ps[lane + 32 * c], kk);
+    const double K = 0.5 * t * warp_sum(kk);
+    const double wrow = (lane < NR) ? fma(-K, vrow, ps[min(r0 + lane, NCOL - 1)]) : 0.0;
+    // A -= v w^T, then A -= w v^T: each pass keeps one vector of the lane's
+    // columns live beside the block
+    if (rows_active) {
+      double wc[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) wc[c] = fma(-K, vof(lane + 32 * c), ps[lane + 32 * c]);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const double vi = __shfl_sync(0xffffffffu, vrow, r);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) a[r][c] = fma(-vi, wc[c], a[r][c]);
+      }
+      double vc[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) vc[c] = vof(lane + 32 * c);
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const double wi = __shfl_sync(0xffffffffu, wrow, r);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) a[r][c] = fma(-wi, vc[c], a[r][c]);
+      }
+    }
+  }
+  // the last 2 x 2 block
+  if (n >= 2) {
+    gather(n - 2, 0);
+    __syncthreads();
+    if (tid == 0) {
+      d[n - 2] = xs[0][n - 2];
+      e[n - 2] = xs[0][n - 1];
+    }
+  }
+  gather(n - 1, 1);
+  __syncthreads();
+  if (tid == 0) d[n - 1] = xs[1][n - 1];
+}
+
 // Number of eigenvalues of T below x: sign changes of the Sturm sequence
 // p_0 = 1, p_1 = d_0 - x, p_i = (d_{i-1} - x) p_{i-1} - e_{i-2}^2 p_{i-2}
 // (zeros dropped).  No division on the dependent chain (one FMA a step; the
@@ -772,19 +1062,28 @@ __global__ void k_bisect(const double *__restrict__ d, const double *__restrict_
 // ws: 6 arrays of n x NT doubles, element (a, i) of thread t at
 // ws[(a*n + i)*NT + t] (coalesced across threads).  Z(:, t) = eigenvector t.
 // With use_smem the six arrays live in shared memory instead, interleaved
-// across the block's threads (6 * n * blockDim doubles).
-__global__ void k_invit(const double *__restrict__ d, const double *__restrict__ e, const double *__restrict__ w,
+// across the block's threads (6 * n * blockDim doubles).  d and e are staged
+// in shared memory behind them (2n doubles) so that no global load sits on
+// the dependent chains of the factorisation and the solves.
+__global__ void k_invit(const double *__restrict__ dg, const double *__restrict__ eg, const double *__restrict__ w,
                         int n, double *__restrict__ Z, double *__restrict__ wsg, int NTg, int *__restrict__ nclus,
                         int use_smem) {
   extern __shared__ double wss[];
+  double *d = wss + (use_smem ? 6L * n * blockDim.x : 0L), *e = d + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    e[i] = (i < n - 1) ? eg[i] : 0.0;
+  }
+  __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   double *ws = use_smem ? wss : wsg;
   const int NT = use_smem ? (int)blockDim.x : NTg;
   const int tt = use_smem ? (int)threadIdx.x : t;
   double tn = 0.0;
+#pragma unroll 4
   for (int i = 0; i < n; ++i)
-    tn = fmax(tn, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0));
+    tn = fmax(tn, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + fabs(e[i]));
   const double eps = 2.220446049250313e-16;
   const double gaptol = 1e-6 * tn;
   if (t > 0 && w[t] - w[t - 1] < gaptol) return;   // not a cluster head
@@ -827,6 +1126,7 @@ __global__ void k_invit(const double *__restrict__ d, const double *__restrict__
     for (int it = 0; it < 3; ++it) {
       // forward: row interchanges and multipliers
       double zi = WS(5, 0);
+#pragma unroll 4
       for (int i = 0; i < n - 1; ++i) {
         const double zn = WS(5, i + 1);
         if (WS(4, i) != 0.0) { WS(5, i) = zn; zi = zi - WS(3, i) * zn; }   // rows i, i+1 swapped
@@ -842,6 +1142,7 @@ __global__ void k_invit(const double *__restrict__ d, const double *__restrict__
         z2 = z1;
         z1 = z0;
       }
+#pragma unroll 4
       for (int i = n - 3; i >= 0; --i) {
         const double z0 = (WS(5, i) - WS(1, i) * z1 - WS(2, i) * z2) * WS(0, i);
         WS(5, i) = z0;
@@ -1017,6 +1318,13 @@ __global__ void __launch_bounds__(128) k_backtrans_wy(const double *__restrict__
   }
 }
 
+// QX_SYTRD_REG=0 keeps the shared-memory tridiagonalisation at every size
+// (read at every call).
+static bool sytrd_registers_enabled() {
+  const char *v = getenv("QX_SYTRD_REG");
+  return !(v && v[0] == '0');
+}
+
 // A (n x n, destroyed), w (n) eigenvalues ascending, V (n x n) eigenvectors.
 // work: at least 8*n*n + 1024*n doubles.  info: number of eigenvalue clusters.
 int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st) {
@@ -1034,8 +1342,16 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   const size_t smem = sizeof(double) * ((size_t)(n | 1) * n + 7 * (size_t)n);
   const int use = smem <= TRD_SMEM_MAX;
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
-  if (use) k_sytrd<true><<<1, TRD_T, smem, st>>>(A, n, d, e, HV, tau, vp);
-  else k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
+  const bool rg = sytrd_registers_enabled();
+  if (rg && n <= 80) {
+    k_sytrd_rg<8, 10, 3><<<1, 8 * 32, 0, st>>>(A, n, d, e, HV, tau);
+  } else if (rg && n <= 160) {
+    k_sytrd_rg<8, 20, 5><<<1, 8 * 32, 0, st>>>(A, n, d, e, HV, tau);
+  } else if (use) {
+    k_sytrd<true><<<1, TRD_T, smem, st>>>(A, n, d, e, HV, tau, vp);
+  } else {
+    k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
+  }
   note_launch();
   if (n == 1) {
     cudaMemcpyAsync(w, d, sizeof(double), cudaMemcpyDeviceToDevice, st);
@@ -1051,11 +1367,11 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     bsm_set = bsm;
   }
   k_bisect<<<n, 32, bsm, st>>>(d, e, n, w); note_launch();
-  const size_t wsm = sizeof(double) * 6 * (size_t)n * 16;
-  if (wsm <= 200 * 1024) {
-    k_invit<<<(n + 15) / 16, 16, wsm, st>>>(d, e, w, n, Z, ws, NT, d_info, 1); note_launch();
+  const size_t wsm = sizeof(double) * 6 * (size_t)n * 16, dem = sizeof(double) * 2 * (size_t)n;
+  if (wsm + dem <= 200 * 1024) {
+    k_invit<<<(n + 15) / 16, 16, wsm + dem, st>>>(d, e, w, n, Z, ws, NT, d_info, 1); note_launch();
   } else {
-    k_invit<<<NT / 128, 128, 0, st>>>(d, e, w, n, Z, ws, NT, d_info, 0); note_launch();
+    k_invit<<<NT / 128, 128, dem, st>>>(d, e, w, n, Z, ws, NT, d_info, 0); note_launch();
   }
   if (n <= 256) {
     double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
