@@ -98,6 +98,10 @@ struct qx_ctx {
   double *d_seqw = nullptr;
   int seqw_len = 0;
   cudaStream_t cap_st = nullptr;
+  // second stream of H|psi>: the G-space KB contractions run there beside the
+  // FFT pipeline (fork / join events; captured as parallel graph branches)
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraph_t seq_graph = nullptr;
   cudaGraphExec_t seq_exec = nullptr;
   std::vector<char> seq_key;
@@ -434,6 +438,10 @@ extern "C" int qx_destroy(qx_ctx *c) {
   if (c->seq_exec) cudaGraphExecDestroy(c->seq_exec);
   if (c->seq_graph) cudaGraphDestroy(c->seq_graph);
   if (c->cap_st) cudaStreamDestroy(c->cap_st);
+  if (c->st2) cudaStreamSynchronize(c->st2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st2) cudaStreamDestroy(c->st2);
   for (void *p : c->allocs) cudaFree(p);
   delete c;
   return QX_OK;
@@ -669,6 +677,13 @@ static PipeParams base_params(const qx_ctx *c) {
   return P;
 }
 
+// QX_KB_STREAM=0 keeps the G-space KB contractions behind the FFT pipeline
+// on one stream (read at every call).
+static bool kb_side_stream_enabled() {
+  const char *v = getenv("QX_KB_STREAM");
+  return !(v && v[0] == '0');
+}
+
 // H|c> for the bands listed in `pairs` (device, 2 per pair).  npair_dev
 // (device count) bounds the pairs; npair_max is the host bound.  colmap /
 // ncol_dev list the same bands for the G-space KB GEMMs.
@@ -683,31 +698,56 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
   const int nlm = (flags & QX_HPSI_NONLOCAL) ? c->nlmode : 0;
   const double *dk = (flags & QX_HPSI_KINETIC) ? c->d_dk : nullptr;
   const int acc = (flags & QX_HPSI_ACCUMULATE) ? 1 : 0;
-  for (int p0 = 0; p0 < npair_max; p0 += pl.chunk) {
-    P.pair0 = p0;
-    const int npl = std::min(pl.chunk, npair_max - p0);
-    P.npair = npair_max;
-    TRY(launch_hpsi_chunk<T>(pl, P, npl, cin, c->ne, out, c->ne, dk, acc, nlm == QX_NL_RSPACE ? 2 : 0, c->st));
-    CKL();
+  // G-space KB: out = [out +] beta D <beta|c> on the second stream while the
+  // FFT pipeline runs here; the pipeline's last kernel then adds the kinetic
+  // and local parts to it.  Otherwise the KB GEMMs follow the pipeline on
+  // this stream and add onto its result.
+  const bool kb = nlm == QX_NL_GSPACE;
+  const bool side = kb && kb_side_stream_enabled();
+  cudaStream_t kst = c->st;
+  if (side) {
+    if (!c->st2) {
+      CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(c->ev_fork, c->st));
+    CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+    kst = c->st2;
   }
-  if (nlm == QX_NL_GSPACE) {
+  auto kb_gemms = [&](T beta_out) -> int {
     Bufs<T> &b = pl.bufs<T>();
     T *proj = (T *)c->proj;
     const int np = pl.nproj;
     // The tensor-core GEMMs take whole columns: with a band list they work on
     // all ncol_max columns, which leaves the columns of bands not in the list
     // holding unused values (the CG reads only active bands).
+    const int *cm = colmap, *nd = ncol_dev;
     if (sizeof(T) == sizeof(float) && tc_enabled()) {
-      colmap = nullptr;
-      ncol_dev = nullptr;
+      cm = nullptr;
+      nd = nullptr;
     }
-    TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, colmap,
-                ncol_dev, c->st, c->gws, c->gws_bytes));
-    scale_rows<T>(np, ncol_max, proj, np, b.vclalp, colmap, ncol_dev, c->st);
-    TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, colmap,
-                ncol_dev, c->st, c->gws, c->gws_bytes));
+    TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, cm, nd, kst,
+                c->gws, c->gws_bytes));
+    scale_rows<T>(np, ncol_max, proj, np, b.vclalp, cm, nd, kst);
+    TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, beta_out, out, c->ne, 0, cm, nd,
+                kst, c->gws, c->gws_bytes));
+    CKL();
+    return 0;
+  };
+  if (side) {
+    TRY(kb_gemms(acc ? (T)1 : (T)0));
+    CK(cudaEventRecord(c->ev_join, c->st2));
+  }
+  for (int p0 = 0; p0 < npair_max; p0 += pl.chunk) {
+    P.pair0 = p0;
+    const int npl = std::min(pl.chunk, npair_max - p0);
+    P.npair = npair_max;
+    TRY(launch_hpsi_chunk<T>(pl, P, npl, cin, c->ne, out, c->ne, dk, side ? 1 : acc, nlm == QX_NL_RSPACE ? 2 : 0,
+                             c->st, (side && p0 == 0) ? c->ev_join : nullptr));
     CKL();
   }
+  if (kb && !side) TRY(kb_gemms((T)1));
   return 0;
 }
 

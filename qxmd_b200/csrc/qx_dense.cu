@@ -1097,28 +1097,29 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
     // perturb members apart so their LU factors differ
     const double lam = w[c] + (double)(c - t) * 4.0 * eps * tn;
     double a = d[0] - lam, b = (n > 1) ? e[0] : 0.0;
+    // branch-free: both pivot choices are formed and one is selected, so no
+    // load or store of a step waits on the comparison of the previous one
+#pragma unroll 2
     for (int i = 0; i < n - 1; ++i) {
       const double cdn = e[i];                 // subdiagonal below a
       const double dn = d[i + 1] - lam;        // next diagonal
-      const double en = (i + 1 < n - 1) ? e[i + 1] : 0.0;
+      const double en = e[i + 1];              // e[n - 1] is staged as 0
       // reciprocals by Newton-refined hardware approximations (recip2_nr,
       // full double precision up to the last bit or two): inverse iteration
       // needs an accurate factorisation of a nearby matrix, not correctly
       // rounded quotients
-      if (fabs(a) >= fabs(cdn)) {
-        const double aa = (fabs(a) < tiny) ? tiny : a;
-        const double ra = recip2_nr(aa);
-        const double l = cdn * ra;
-        WS(0, i) = ra; WS(1, i) = b; WS(2, i) = 0.0; WS(3, i) = l; WS(4, i) = 0.0;
-        a = dn - l * b;
-        b = en;
-      } else {
-        const double rc = recip2_nr(cdn);
-        const double l = a * rc;
-        WS(0, i) = rc; WS(1, i) = dn; WS(2, i) = en; WS(3, i) = l; WS(4, i) = 1.0;
-        a = b - l * dn;
-        b = -l * en;
-      }
+      const bool keep = fabs(a) >= fabs(cdn);  // no row interchange
+      const double aa = (fabs(a) < tiny) ? tiny : a;
+      const double r = recip2_nr(keep ? aa : cdn);
+      const double l = (keep ? cdn : a) * r;
+      WS(0, i) = r;
+      WS(1, i) = keep ? b : dn;
+      WS(2, i) = keep ? 0.0 : en;
+      WS(3, i) = l;
+      WS(4, i) = keep ? 0.0 : 1.0;
+      const double an = keep ? dn - l * b : b - l * dn;
+      b = keep ? en : -l * en;
+      a = an;
     }
     WS(0, n - 1) = recip2_nr((fabs(a) < tiny) ? tiny : a);
     // start vector: ones with a member-dependent pattern
@@ -1128,9 +1129,10 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
       double zi = WS(5, 0);
 #pragma unroll 4
       for (int i = 0; i < n - 1; ++i) {
-        const double zn = WS(5, i + 1);
-        if (WS(4, i) != 0.0) { WS(5, i) = zn; zi = zi - WS(3, i) * zn; }   // rows i, i+1 swapped
-        else { WS(5, i) = zi; zi = zn - WS(3, i) * zi; }
+        const double zn = WS(5, i + 1), l = WS(3, i);
+        const bool sw = WS(4, i) != 0.0;      // rows i, i+1 swapped
+        WS(5, i) = sw ? zn : zi;
+        zi = sw ? zi - l * zn : zn - l * zi;
       }
       WS(5, n - 1) = zi;
       // back substitution with U (two superdiagonals)
@@ -1156,9 +1158,13 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
         for (int i = 0; i < n; ++i) s += zq[i] * WS(5, i);
         for (int i = 0; i < n; ++i) WS(5, i) -= s * zq[i];
       }
-      double nr = 0.0;
-      for (int i = 0; i < n; ++i) { const double x = WS(5, i); nr += x * x; }
-      nr = rsqrt_nr(nr);
+      double nr4[4] = {0.0, 0.0, 0.0, 0.0};
+      int i4 = 0;
+      for (; i4 + 4 <= n; i4 += 4)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { const double x = WS(5, i4 + u); nr4[u] += x * x; }
+      for (; i4 < n; ++i4) { const double x = WS(5, i4); nr4[0] += x * x; }
+      const double nr = rsqrt_nr((nr4[0] + nr4[1]) + (nr4[2] + nr4[3]));
       for (int i = 0; i < n; ++i) WS(5, i) *= nr;
     }
     double *z = Z + (long)c * n;

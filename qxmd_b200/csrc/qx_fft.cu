@@ -715,7 +715,7 @@ static bool plane_enabled() {
 
 template <typename T>
 int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
-                      const double *dk, int accumulate, int nlmode, cudaStream_t st) {
+                      const double *dk, int accumulate, int nlmode, cudaStream_t st, cudaEvent_t before_unpack) {
   typedef typename c2t<T>::type C;
   const size_t cs = sizeof(C);
   Bufs<T> &bf = pl.bufs<T>();
@@ -729,6 +729,7 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
       launch_plane_f32(P, npl, (float2 *)bf.bufA, (const float *)bf.vloc, st) == 0) {
     dim3 gu((P.nplw + 1 + 127) / 128, npl);
     k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
+    if (before_unpack) cudaStreamWaitEvent(st, before_unpack, 0);
     k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
     return 0;
   }
@@ -750,6 +751,7 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   k_ypass<T, -1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
   k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
   dim3 gu((P.nplw + 1 + 127) / 128, npl);
+  if (before_unpack) cudaStreamWaitEvent(st, before_unpack, 0);
   k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
   return 0;
 }
@@ -857,9 +859,9 @@ void set_fft_smem_limits(size_t bytes) {
 }
 
 template int launch_hpsi_chunk<float>(const Plan &, const PipeParams &, int, const float *, long, float *, long,
-                                      const double *, int, int, cudaStream_t);
+                                      const double *, int, int, cudaStream_t, cudaEvent_t);
 template int launch_hpsi_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, double *, long,
-                                       const double *, int, int, cudaStream_t);
+                                       const double *, int, int, cudaStream_t, cudaEvent_t);
 template int launch_rho_chunk<float>(const Plan &, const PipeParams &, int, const float *, long, const double *,
                                      double *, int, cudaStream_t);
 template int launch_rho_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, const double *,

@@ -102,29 +102,44 @@ __global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, T alpha, cons
 }
 
 // Sum the split-K partials in a fixed order, apply the Gamma-metric
-// epilogue and alpha/beta, scatter through colmap.
+// epilogue and alpha/beta, scatter through colmap.  A block of RD_T threads
+// finishes 32 consecutive outputs: warp w sums the partials z = w, w + 8,
+// w + 16, ... (all loads of a lane independent, 128-byte rows across the
+// warp), then lane l of warp 0 adds the eight warp sums in order w = 0..7.
+constexpr int RD_T = 256;
 template <typename T, bool TA, bool TB>
-__global__ void k_gemm_reduce(int M, int N, int nsplit, T alpha, const T *__restrict__ A, long lda,
-                              const T *__restrict__ B, long ldb, T beta, T *__restrict__ Cm, long ldc, int gamma,
-                              const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
-                              const T *__restrict__ W) {
+__global__ void __launch_bounds__(RD_T) k_gemm_reduce(int M, int N, int nsplit, T alpha, const T *__restrict__ A,
+                                                      long lda, const T *__restrict__ B, long ldb, T beta,
+                                                      T *__restrict__ Cm, long ldc, int gamma,
+                                                      const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
+                                                      const T *__restrict__ W) {
+  __shared__ T ws[RD_T / 32][32];
   const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (e >= (long)M * Nact) return;
-  const int gn = (int)(e / M), gm = (int)(e - (long)gn * M);
-  // fixed summation order; loads issued eight at a time
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long e = blockIdx.x * 32L + lane;
+  const bool live = e < (long)M * Nact;
   const long zs = (long)N * M;
-  const T *w = W + (long)gn * M + gm;
   T v = 0;
-  int z = 0;
-  for (; z + 8 <= nsplit; z += 8) {
-    T t[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) t[q] = w[(long)(z + q) * zs];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v += t[q];
+  if (live) {
+    const T *w = W + e;   // element (n, m) of partial z at W[z][n][m], e = n * M + m
+    int z = warp;
+    for (; z + 3 * (RD_T / 32) < nsplit; z += 4 * (RD_T / 32)) {
+      const T t0 = w[(long)z * zs], t1 = w[(long)(z + 8) * zs], t2 = w[(long)(z + 16) * zs],
+              t3 = w[(long)(z + 24) * zs];
+      v += t0;
+      v += t1;
+      v += t2;
+      v += t3;
+    }
+    for (; z < nsplit; z += RD_T / 32) v += w[(long)z * zs];
   }
-  for (; z < nsplit; ++z) v += w[(long)z * zs];
+  ws[warp][lane] = v;
+  __syncthreads();
+  if (warp != 0 || !live) return;
+  v = ws[0][lane];
+#pragma unroll
+  for (int q = 1; q < RD_T / 32; ++q) v += ws[q][lane];
+  const int gn = (int)(e / M), gm = (int)(e - (long)gn * M);
   const long cn = colmap ? colmap[gn] : gn;
   if (gamma) {
     const T a0 = TA ? A[(long)gm * lda] : A[gm];
@@ -155,8 +170,8 @@ static void launch(dim3 g, int M, int N, int K, T alpha, const T *A, long lda, c
                                             kchunk, W);
   note_launch();
   const long mn = (long)M * N;
-  k_gemm_reduce<T, TA, TB><<<(int)((mn + 255) / 256), 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                     gamma, colmap, ncol_dev, W);
+  k_gemm_reduce<T, TA, TB><<<(int)((mn + 31) / 32), RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                    gamma, colmap, ncol_dev, W);
   note_launch();
 }
 
@@ -164,11 +179,11 @@ static void launch(dim3 g, int M, int N, int K, T alpha, const T *A, long lda, c
 void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
                      long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st) {
   const long mn = (long)M * N;
-  const int g = (int)((mn + 255) / 256);
-  if (ta && tb) k_gemm_reduce<float, true, true><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else if (ta) k_gemm_reduce<float, true, false><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else if (tb) k_gemm_reduce<float, false, true><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else k_gemm_reduce<float, false, false><<<g, 256, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  const int g = (int)((mn + 31) / 32);
+  if (ta && tb) k_gemm_reduce<float, true, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else if (ta) k_gemm_reduce<float, true, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else if (tb) k_gemm_reduce<float, false, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  else k_gemm_reduce<float, false, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
   note_launch();
 }
 

@@ -85,7 +85,8 @@ template <> inline int Plan::xlines<double>() const { return xl64; }
 // qx_fft.cu
 template <typename T>
 int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
-                      const double *dk, int accumulate, int nlmode, cudaStream_t st);
+                      const double *dk, int accumulate, int nlmode, cudaStream_t st,
+                      cudaEvent_t before_unpack = nullptr);
 template <typename T>
 int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const double *wocc,
                      double *rho, int accumulate, cudaStream_t st);
