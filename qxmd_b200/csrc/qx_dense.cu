@@ -494,25 +494,29 @@ __global__ void __launch_bounds__(CPT) k_cholinv_sm(double *__restrict__ Sg, int
 // n <= 32 NC; one CTA of W warps; thread (w, l) keeps rows NR w .. NR w + NR - 1
 // of the columns l + 32 c).  X = L^-1 is found by rows (X L = I top down)
 // with running right-hand sides R (R(i,:) = e_i at the start), stored where L
-// was consumed.  Step k: column k (the Schur complement) is published and
-// replaced by e_k, which starts R's column k; row k (R(k, 0..k)) is
-// published; one barrier; then with rs = 1 / L(k,k), m_i = S(i,k) rs (rows
-// i > k) and y = (R(k, 0..k) rs, m_(k+1..)), every row i > k takes one rank-1
-// update a(i,:) -= m_i y: the Cholesky update of the columns > k, the
-// forward-substitution update R(i,l) -= m_i X(k,l) of the columns <= k.  Row
-// k is final from then on; it is scaled by its rs when written out, which
-// gives X(k, 0..k).  The gathered column and row alternate by parity, so one
-// barrier a step suffices.  The matrix is staged through shared memory on
-// the way in (the lower triangle, as rsdecmp reads it) and out (coalesced
-// column-major stores).  info as k_cholinv_sm; S is left as it was on failure.
+// was consumed.  Columns go two at a time (k, k + 1; NR even, so rows k and
+// k + 1 sit in one warp): columns k and k + 1 (the Schur complement) are
+// published and replaced by e_k, e_(k+1), which start R's columns; rows k
+// and k + 1 (R(k, :), R(k+1, :)) are published; one barrier.  Then
+// L(k,k) = sqrt(piv0), l = L(k+1,k), L(k+1,k+1) = sqrt(piv1 - l^2),
+// m0_i = L(i,k), m1_i = L(i,k+1) and y0, y1 (the rows of X for the columns
+// <= k + 1, the L columns beyond) give every row below k one rank-2 update
+// a(i,:) -= m0_i y0 + m1_i y1: the Cholesky update of the columns > k + 1 and
+// the forward-substitution update of the columns <= k + 1 (y0 is 0 at k + 1:
+// that part of the Schur update is folded into piv1).  Rows k and k + 1 are
+// final from then on and are scaled by their 1 / L(i,i) when written out.
+// The gathered columns and rows alternate by parity, so one barrier a step
+// suffices.  The matrix is staged through shared memory on the way in (the
+// lower triangle, as rsdecmp reads it) and out (coalesced column-major
+// stores).  info as k_cholinv_sm; S is left as it was on failure.
 template <int W, int NR, int NC>
 __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ Sg, int n, int *__restrict__ info) {
   constexpr int NROW = W * NR, NCOL = 32 * NC;
   constexpr int NX = NROW > NCOL ? NROW : NCOL;
-  static_assert(NR <= 32, "lane r of a warp keeps m of the warp's row r");
+  static_assert(NR <= 32 && NR % 2 == 0, "lane r of a warp keeps m of row r; row pairs stay in one warp");
   extern __shared__ double stg[];   // n x (n | 1) staging
-  __shared__ double xcol[2][NX];
-  __shared__ double xrow[2][NCOL];
+  __shared__ double xcol[2][2][NX];
+  __shared__ double xrow[2][2][NX];
   __shared__ double rsv[NX];
   const int ld = n | 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -532,53 +536,76 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
       const double v = stg[(long)min(lo, n - 1) * ld + min(hi, n - 1)];   // S(hi, lo), clamped address
       a[r][c] = (row < n && col < n) ? v : 0.0;
     }
-  for (int k = 0; k < n; ++k) {
-    const int b = k & 1, kc = k >> 5;
-    if (lane == (k & 31))     // column k out, e_k in
+  for (int k = 0; k < n; k += 2) {
+    const int b = (k >> 1) & 1, kc = k >> 5, kl = k & 31;   // k even: k and k + 1 share slot kc
+    const bool two = k + 1 < n;
+    if (lane == kl || (two && lane == kl + 1)) {   // columns k, k + 1 out, e_k, e_(k+1) in
+      const int h = lane - kl, col = k + h;
       dense_static_for<0, NC>([&](auto cc) {
         constexpr int C = decltype(cc)::value;
         if (C == kc) {
 #pragma unroll
           for (int r = 0; r < NR; ++r) {
-            xcol[b][r0 + r] = a[r][C];
-            a[r][C] = (r0 + r == k) ? 1.0 : 0.0;
+            xcol[b][h][r0 + r] = a[r][C];
+            a[r][C] = (r0 + r == col) ? 1.0 : 0.0;
           }
         }
       });
-    if (warp == k / NR) {     // row k out
+    }
+    if (warp == k / NR) {     // rows k, k + 1 out
       const int kr = k - r0;
-      dense_static_for<0, NR>([&](auto rr) {
-        constexpr int R = decltype(rr)::value;
+      dense_static_for<0, NR / 2>([&](auto rr) {
+        constexpr int R = 2 * decltype(rr)::value;
         if (R == kr) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) xrow[b][lane + 32 * c] = a[R][c];
+          for (int c = 0; c < NC; ++c) {
+            xrow[b][0][lane + 32 * c] = a[R][c];
+            xrow[b][1][lane + 32 * c] = a[R + 1][c];
+          }
         }
       });
     }
     __syncthreads();
-    const double piv = xcol[b][k];
-    if (!(piv > 1.0e-30)) {   // the same in every thread; also catches NaN
+    const double *x0 = xcol[b][0], *x1 = xcol[b][1], *w0 = xrow[b][0], *w1 = xrow[b][1];
+    const double piv0 = x0[k];
+    if (!(piv0 > 1.0e-30)) {   // the same in every thread; also catches NaN
       if (tid == 0) *info = 1 + k;
       return;
     }
-    const double rs = rsqrt_nr(piv);   // 1 / L(k,k)
-    if (tid == 0) rsv[k] = rs;
-    // lane r < NR: m of row r0 + r (0 for rows <= k, which the update then leaves as they are)
-    const int ri = min(r0 + lane, NX - 1);
-    const double mrow = (lane < NR && r0 + lane > k && r0 + lane < n) ? xcol[b][ri] * rs : 0.0;
+    const double rs0 = rsqrt_nr(piv0);   // 1 / L(k,k)
+    const double l10 = two ? x0[k + 1] * rs0 : 0.0;
+    double rs1 = 0.0;
+    if (two) {
+      const double piv1 = x1[k + 1] - l10 * l10;
+      if (!(piv1 > 1.0e-30)) {
+        if (tid == 0) *info = 2 + k;
+        return;
+      }
+      rs1 = rsqrt_nr(piv1);
+    }
+    if (tid == 0) {
+      rsv[k] = rs0;
+      if (two) rsv[k + 1] = rs1;
+    }
+    // lane r < NR: m0, m1 of row r0 + r (0 where the row takes no update)
+    const int ri = r0 + lane, rc = min(ri, NX - 1);
+    const double m0row = (lane < NR && ri > k && ri < n) ? x0[rc] * rs0 : 0.0;
+    const double m1row = (two && lane < NR && ri > k + 1 && ri < n) ? (x1[rc] - m0row * l10) * rs1 : 0.0;
     if (r0 + NR > k + 1) {    // rows below k in this warp
-      double y[NC];
+      double y0[NC], y1[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const int col = lane + 32 * c;
-        const double xr = xrow[b][col], xc = xcol[b][min(col, NX - 1)];
-        y[c] = ((col <= k) ? xr : ((col < n) ? xc : 0.0)) * rs;
+        const int col = lane + 32 * c, cc = min(col, NX - 1);
+        const double s0 = (col <= k) ? w0[cc] : x0[cc];
+        const double s1 = (col <= k + 1) ? w1[cc] : x1[cc];
+        y0[c] = (col == k + 1 || col >= n) ? 0.0 : s0 * rs0;
+        y1[c] = (two && col < n) ? (s1 - l10 * y0[c]) * rs1 : 0.0;
       }
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double mi = __shfl_sync(0xffffffffu, mrow, r);
+        const double mi0 = __shfl_sync(0xffffffffu, m0row, r), mi1 = __shfl_sync(0xffffffffu, m1row, r);
 #pragma unroll
-        for (int c = 0; c < NC; ++c) a[r][c] = fma(-mi, y[c], a[r][c]);
+        for (int c = 0; c < NC; ++c) a[r][c] = fma(-mi1, y1[c], fma(-mi0, y0[c], a[r][c]));
       }
     }
   }
@@ -626,9 +653,17 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
   if (n <= 160 && cholinv_registers_enabled()) {
     static size_t rset = 48 * 1024;   // per process: only ever raised
     if (rbytes > rset) {
-      cudaFuncSetAttribute(k_cholinv_rg<8, 10, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
-      cudaFuncSetAttribute(k_cholinv_rg<8, 20, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CH_SMEM_MAX);
-      rset = CH_SMEM_MAX;
+      // exactly what this size needs: with the kernels' static buffers the
+      // opt-in ceiling is below the 227 KB of a CTA
+      const cudaError_t e1 = cudaFuncSetAttribute(k_cholinv_rg<8, 10, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)rbytes);
+      const cudaError_t e2 = cudaFuncSetAttribute(k_cholinv_rg<8, 20, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)rbytes);
+      if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        set_error("cholinv: n=%d: shared-memory opt-in failed: %s", n, cudaGetErrorString(e1 ? e1 : e2));
+        return 1;
+      }
+      rset = rbytes;
     }
     if (n <= 80) k_cholinv_rg<8, 10, 3><<<1, 8 * 32, rbytes, st>>>(S, n, d_info);
     else k_cholinv_rg<8, 20, 5><<<1, 8 * 32, rbytes, st>>>(S, n, d_info);
@@ -1061,15 +1096,17 @@ __global__ void k_bisect(const double *__restrict__ d, const double *__restrict_
 // earlier ones.  Thread t is active if eigenvalue t starts a cluster.
 // ws: 6 arrays of n x NT doubles, element (a, i) of thread t at
 // ws[(a*n + i)*NT + t] (coalesced across threads).  Z(:, t) = eigenvector t.
-// With use_smem the six arrays live in shared memory instead, interleaved
+// With SMT > 0 the six arrays live in shared memory instead, interleaved
 // across the block's threads (6 * n * blockDim doubles).  d and e are staged
 // in shared memory behind them (2n doubles) so that no global load sits on
 // the dependent chains of the factorisation and the solves.
+template <int SMT>
 __global__ void k_invit(const double *__restrict__ dg, const double *__restrict__ eg, const double *__restrict__ w,
-                        int n, double *__restrict__ Z, double *__restrict__ wsg, int NTg, int *__restrict__ nclus,
-                        int use_smem) {
+                        int n, double *__restrict__ Z, double *__restrict__ wsg, int NTg, int *__restrict__ nclus) {
+  // SMT > 0: the work arrays in shared memory for blocks of SMT threads
+  // (compile-time stride, shared-memory addressing); SMT == 0: global memory
   extern __shared__ double wss[];
-  double *d = wss + (use_smem ? 6L * n * blockDim.x : 0L), *e = d + n;
+  double *d = wss + (SMT ? 6 * n * SMT : 0), *e = d + n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e[i] = (i < n - 1) ? eg[i] : 0.0;
@@ -1077,9 +1114,9 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
   __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  double *ws = use_smem ? wss : wsg;
-  const int NT = use_smem ? (int)blockDim.x : NTg;
-  const int tt = use_smem ? (int)threadIdx.x : t;
+  double *ws = SMT ? wss : wsg;
+  const int NT = SMT ? SMT : NTg;
+  const int tt = SMT ? (int)threadIdx.x : t;
   double tn = 0.0;
 #pragma unroll 4
   for (int i = 0; i < n; ++i)
@@ -1090,7 +1127,7 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
   atomicAdd(nclus, 1);
   int tend = t + 1;
   while (tend < n && w[tend] - w[tend - 1] < gaptol) ++tend;
-#define WS(a, i) ws[((long)(a) * n + (i)) * NT + tt]
+#define WS(a, i) ws[((a) * n + (i)) * NT + tt]
   // 0: 1/U(i,i), 1: U(i,i+1), 2: U(i,i+2), 3: multiplier, 4: row swap flag, 5: z
   const double tiny = eps * tn + 1e-300;
   for (int c = t; c < tend; ++c) {
@@ -1342,7 +1379,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   if (!attr) {
     cudaFuncSetAttribute(k_sytrd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM_MAX);
     cudaFuncSetAttribute(k_backtrans, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_invit, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_invit<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
   const size_t smem = sizeof(double) * ((size_t)(n | 1) * n + 7 * (size_t)n);
@@ -1375,9 +1412,9 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   k_bisect<<<n, 32, bsm, st>>>(d, e, n, w); note_launch();
   const size_t wsm = sizeof(double) * 6 * (size_t)n * 16, dem = sizeof(double) * 2 * (size_t)n;
   if (wsm + dem <= 200 * 1024) {
-    k_invit<<<(n + 15) / 16, 16, wsm + dem, st>>>(d, e, w, n, Z, ws, NT, d_info, 1); note_launch();
+    k_invit<16><<<(n + 15) / 16, 16, wsm + dem, st>>>(d, e, w, n, Z, ws, NT, d_info); note_launch();
   } else {
-    k_invit<<<NT / 128, 128, dem, st>>>(d, e, w, n, Z, ws, NT, d_info, 0); note_launch();
+    k_invit<0><<<NT / 128, 128, dem, st>>>(d, e, w, n, Z, ws, NT, d_info); note_launch();
   }
   if (n <= 256) {
     double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
