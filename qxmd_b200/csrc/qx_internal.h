@@ -98,7 +98,7 @@ template <typename T> void set_fft_smem_limits(size_t bytes);
 int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st);
 // Density through the plane kernel: groups of pairs per z plane, partial
 // planes in part (RHO_GROUPS * kfft0 doubles) summed in a fixed order.
-constexpr int RHO_GROUPS = 8;
+constexpr int RHO_GROUPS = 16;
 int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part,
                          double *rho, int accumulate, cudaStream_t st);
 bool plane_length_supported(int k1, int k2);
