@@ -15,9 +15,10 @@
 // The split is done in shared memory by the epilogue warps between the TMA
 // landing and the MMA issue, so HBM traffic is that of a plain FP32 GEMM.
 //
-// Warp roles (192 threads): warp 0 issues TMA, warp 1 allocates TMEM and
-// issues the MMAs (one elected lane), warps 2-5 split the operands and run
-// the epilogue (TMEM lane quadrant = warp % 4).  Every mbarrier wait is
+// Warp roles (384 threads): warp 0 issues TMA, warp 1 allocates TMEM and
+// issues the MMAs (one elected lane), warps 6-11 split the operands, warps
+// 2-5 drain the accumulators and run the epilogue (TMEM lane quadrant =
+// warp % 4).  Every mbarrier wait is
 // bounded by a 2 s clock; on timeout the kernel records an error code, stops
 // issuing, drains its own copies and MMAs and frees TMEM.
 #include <cuda.h>
@@ -37,7 +38,8 @@ namespace tc {
 
 constexpr int BM = 128, BK = 32;
 constexpr int A_BYTES = BM * BK * 4;                 // 16 KB
-constexpr int NTHREADS = 320;   // TMA, MMA, 8 split warps (4 of them drain)
+constexpr int NTHREADS = 384;   // TMA, MMA, 4 drain/epilogue warps, 6 split warps
+constexpr int NSPLIT_T = NTHREADS - 192;
 constexpr int BAR_BYTES = 256;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
 
@@ -163,8 +165,10 @@ __device__ __forceinline__ void split1(float x, float &h, float &l) {
   h = tf32_rn(x);
   l = x - h;
 }
-__device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int n16, int t) {
-  for (int i = t; i < n16; i += 256) {
+template <int N16>
+__device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int t) {
+#pragma unroll
+  for (int i = t; i < N16; i += NSPLIT_T) {
     const float4 x = hi[i];
     float4 h, l;
     split1(x.x, h.x, l.x);
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&conv[s], 256);
+      mbar_init(&conv[s], NSPLIT_T);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -292,8 +296,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       mbar_wait(fin, 0, 7);
     }
   } else {
-    // ---------------- split (warps 2-9), drain and epilogue (warps 2-5) ----------------
-    const int t = threadIdx.x - 64;   // 0..255
+    // ---------------- split (warps 6-11); drain and epilogue (warps 2-5) ----------------
+    // The split of a stage runs ahead of the MMAs by up to STAGES k-blocks;
+    // the drain of accumulator j overlaps the MMAs of k-block j + 1.
     const bool drains = warp < 6;
     const int quad = warp & 3;
     float acc[BN];
@@ -317,26 +322,30 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       asm volatile("tcgen05.fence::before_thread_sync;");
       mbar_arrive(&acce[ab]);
     };
-    int converted = 0;
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % STAGES;
-      if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
-      if (abort_flag) { mbar_arrive(&conv[s]); break; }
-      uint8_t *st = sm + (size_t)s * STAGE_BYTES;
-      split_tf32((float4 *)(st + OFF_AH), (float4 *)(st + OFF_AL), A_BYTES / 16, t);
-      split_tf32((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), B_BYTES / 16, t);
-      // generic-proxy writes -> visible to the tensor core (async proxy)
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&conv[s]);
-      ++converted;
-      if (drains && kb >= 1) drain(kb - 1);
+    if (!drains) {
+      const int t = threadIdx.x - 192;   // 0 .. NSPLIT_T - 1 (warps 6-11)
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % STAGES;
+        if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
+        if (abort_flag) { mbar_arrive(&conv[s]); break; }
+        uint8_t *st = sm + (size_t)s * STAGE_BYTES;
+        split_tf32<A_BYTES / 16>((float4 *)(st + OFF_AH), (float4 *)(st + OFF_AL), t);
+        split_tf32<B_BYTES / 16>((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), t);
+        // generic-proxy writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&conv[s]);
+      }
+    } else {
+      for (int kb = 0; kb < nkb; ++kb) {
+        if (abort_flag) break;
+        drain(kb);
+      }
     }
-    if (drains && converted == nkb && nkb >= 1 && !abort_flag) drain(nkb - 1);
-    if (drains) {   // warps 6-9 only split
+    if (drains) {
       // ---------------- epilogue ----------------
       const bool direct = (p.W == nullptr);
       if (direct && p.gamma) {
-        for (int j = t; j < BN; j += 128) {   // t < 128 here
+        for (int j = threadIdx.x - 64; j < BN; j += 128) {   // the 128 threads of warps 2-5
           const int gn = n0 + j;
           sb0[j] = (gn < p.N) ? (B_MN ? p.B[gn] : p.B[(long)gn * p.ldb]) : 0.f;
           sb1[j] = (gn < p.N) ? (B_MN ? p.B[p.ldb + gn] : p.B[(long)gn * p.ldb + 1]) : 0.f;
