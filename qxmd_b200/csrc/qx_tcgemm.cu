@@ -52,10 +52,12 @@ template <int BN_> struct Cfg {
   static constexpr int OFF_AH = 0, OFF_AL = A_BYTES, OFF_BH = 2 * A_BYTES, OFF_BL = 2 * A_BYTES + B_BYTES;
   static constexpr int STAGE_BYTES = 2 * (A_BYTES + B_BYTES);   // a multiple of 1 KB
   static constexpr int STAGES = (4 * STAGE_BYTES <= 212 * 1024) ? 4 : 3;
-  static constexpr int TMEM_COLS = 256;
+  static constexpr int TMEM_COLS = 512;
   static constexpr int ACC_STRIDE = 128;   // TMEM column offset of accumulator 1
+  static constexpr int TA_BASE = 256;      // A hi/lo of stage s at TA_BASE + 64 s (+ 32 for lo)
   static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + BAR_BYTES + 1024;   // + alignment slack
   static_assert(BN % 16 == 0 && BN <= ACC_STRIDE, "UMMA N for M = 128, two accumulators in TMEM");
+  static_assert(TA_BASE + 64 * STAGES <= TMEM_COLS, "A stages in TMEM");
   static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 };
 
@@ -87,8 +89,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// Non-blocking probe of the phase (acquire semantics).
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Wait for the phase of parity `parity` to complete, for at most WAIT_NS.
-__device__ __noinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int code) {
+__device__ __noinline__ bool mbar_wait_slow(uint64_t *b, uint32_t parity, int code) {
   if (mbar_try(b, parity)) return true;
   const unsigned long long t0 = now_ns();
   while (true) {
@@ -98,6 +110,13 @@ __device__ __noinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int code) {
       return false;
     }
   }
+}
+// A completed phase is seen by the non-blocking probe at once; a blocking
+// try_wait costs a few hundred cycles even then, which on the MMA issuer's
+// path of every k-block adds up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, int code) {
+  if (mbar_test(b, parity)) return true;
+  return mbar_wait_slow(b, parity, code);
 }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
@@ -125,6 +144,26 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t ad, uint64_t 
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(
           tmem_d),
       "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+// A from tensor memory (M rows in lanes, 8 K columns of 32 bits), B from a
+// shared-memory descriptor.
+__device__ __forceinline__ void mma_tf32_at(uint32_t tmem_d, uint32_t tmem_a, uint64_t bd, uint32_t idesc,
+                                            uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}\n" ::"r"(
+          tmem_d),
+      "r"(tmem_a), "l"(bd), "r"(idesc), "r"(acc));
+}
+// 32 consecutive 32-bit columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
+      "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]),
+      "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]),
+      "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+      : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
@@ -165,10 +204,10 @@ __device__ __forceinline__ void split1(float x, float &h, float &l) {
   h = tf32_rn(x);
   l = x - h;
 }
-template <int N16>
+template <int N16, int STRIDE>
 __device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int t) {
 #pragma unroll
-  for (int i = t; i < N16; i += NSPLIT_T) {
+  for (int i = t; i < N16; i += STRIDE) {
     const float4 x = hi[i];
     float4 h, l;
     split1(x.x, h.x, l.x);
@@ -183,7 +222,11 @@ __device__ __forceinline__ void split_tf32(float4 *hi, float4 *lo, int t) {
 // A_MN: A stored with M contiguous (A[k*lda + m]); else K contiguous
 // (A[m*lda + k]).  B_MN: B stored with N contiguous (B[k*ldb + n]); else K
 // contiguous (B[n*ldb + k]).
-template <bool A_MN, bool B_MN, int BN_>
+// ATM: A's hi/lo parts go to tensor memory (warps 6-9, one TMEM lane
+// quadrant each) and the MMAs read A there; only B is split in shared memory
+// (warps 10-11).  The A tile is then read by the split warps alone: K-major A
+// keeps the 128-byte swizzle, MN-major A is loaded without swizzle.
+template <bool A_MN, bool B_MN, int BN_, bool ATM>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, TcArgs p) {
   typedef Cfg<BN_> G;
@@ -259,7 +302,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
       // kind::tf32, D F32, M = 128, N = BN
-      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((A_MN ? 1u : 0u) << 15) |
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((A_MN && !ATM ? 1u : 0u) << 15) |
                              ((B_MN ? 1u : 0u) << 16) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % STAGES, ab = kb & 1;
@@ -279,14 +322,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           const uint32_t alb = A_MN ? 4096 : 16, blb = B_MN ? 4096 : 16;
           const uint32_t asb = A_MN ? 512 : 1024, bsb = B_MN ? 512 : 1024;
           const uint32_t aly = A_MN ? 1 : 2, bly = B_MN ? 1 : 2;
-          const uint64_t ah = sdesc(st + OFF_AH + ao, alb, asb, aly), al = sdesc(st + OFF_AL + ao, alb, asb, aly);
           const uint64_t bh = sdesc(st + OFF_BH + bo, blb, bsb, bly), bl = sdesc(st + OFF_BL + bo, blb, bsb, bly);
           // each k-block starts its accumulator afresh: the tensor core's
           // accumulation is kept to 12 products deep, the running sum is
           // carried in FP32 registers by the draining warps
-          mma_tf32(dt, ah, bh, idesc, kk == 0 ? 0u : 1u);
-          mma_tf32(dt, ah, bl, idesc, 1u);
-          mma_tf32(dt, al, bh, idesc, 1u);
+          if (ATM) {
+            const uint32_t tah = tmem + (uint32_t)(G::TA_BASE + 64 * s + 8 * kk), tal = tah + 32;
+            mma_tf32_at(dt, tah, bh, idesc, kk == 0 ? 0u : 1u);
+            mma_tf32_at(dt, tah, bl, idesc, 1u);
+            mma_tf32_at(dt, tal, bh, idesc, 1u);
+          } else {
+            const uint64_t ah = sdesc(st + OFF_AH + ao, alb, asb, aly), al = sdesc(st + OFF_AL + ao, alb, asb, aly);
+            mma_tf32(dt, ah, bh, idesc, kk == 0 ? 0u : 1u);
+            mma_tf32(dt, ah, bl, idesc, 1u);
+            mma_tf32(dt, al, bh, idesc, 1u);
+          }
         }
         mma_commit(&empty[s]);   // frees the stage when these MMAs are done
         mma_commit(&accf[ab]);   // accumulator ab holds this k-block
@@ -322,22 +372,68 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       asm volatile("tcgen05.fence::before_thread_sync;");
       mbar_arrive(&acce[ab]);
     };
-    if (!drains) {
+    if (!drains && !ATM) {
       const int t = threadIdx.x - 192;   // 0 .. NSPLIT_T - 1 (warps 6-11)
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = kb % STAGES;
         if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
         if (abort_flag) { mbar_arrive(&conv[s]); break; }
         uint8_t *st = sm + (size_t)s * STAGE_BYTES;
-        split_tf32<A_BYTES / 16>((float4 *)(st + OFF_AH), (float4 *)(st + OFF_AL), t);
-        split_tf32<B_BYTES / 16>((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), t);
+        split_tf32<A_BYTES / 16, NSPLIT_T>((float4 *)(st + OFF_AH), (float4 *)(st + OFF_AL), t);
+        split_tf32<B_BYTES / 16, NSPLIT_T>((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), t);
         // generic-proxy writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&conv[s]);
+      }
+    } else if (!drains && warp < 10) {
+      // A: row q * 32 + lane of the tile (q = this warp's TMEM lane quadrant)
+      const int m = quad * 32 + lane;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % STAGES;
+        if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
+        // warp-uniform exit: the TMEM stores below are .sync.aligned
+        if (__any_sync(0xffffffffu, abort_flag != 0)) { mbar_arrive(&conv[s]); break; }
+        const float *sa = (const float *)(sm + (size_t)s * STAGE_BYTES + OFF_AH);
+        float x[32];
+        if (A_MN) {
+          // unswizzled 32 (m) x 32 (k) chunks, chunk q holds rows 32 q .. 32 q + 31
+#pragma unroll
+          for (int k = 0; k < 32; ++k) x[k] = sa[quad * 1024 + k * 32 + lane];
+        } else {
+          // 128-byte rows, 16-byte chunk j of row m at chunk position j ^ (m & 7)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float4 v = *(const float4 *)(sa + m * 32 + ((j ^ (m & 7)) << 2));
+            x[4 * j] = v.x;
+            x[4 * j + 1] = v.y;
+            x[4 * j + 2] = v.z;
+            x[4 * j + 3] = v.w;
+          }
+        }
+        float lo[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) split1(x[k], x[k], lo[k]);
+        const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(G::TA_BASE + 64 * s);
+        tmem_st32(ta, x);
+        tmem_st32(ta + 32, lo);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        mbar_arrive(&conv[s]);
+      }
+    } else if (!drains) {
+      const int t = threadIdx.x - 320;   // 0..63 (warps 10-11): B only
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % STAGES;
+        if (!mbar_wait(&full[s], (kb / STAGES) & 1, 4)) abort_flag = 1;
+        if (abort_flag) { mbar_arrive(&conv[s]); break; }
+        uint8_t *st = sm + (size_t)s * STAGE_BYTES;
+        split_tf32<B_BYTES / 16, 64>((float4 *)(st + OFF_BH), (float4 *)(st + OFF_BL), t);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive(&conv[s]);
       }
     } else {
       for (int kb = 0; kb < nkb; ++kb) {
-        if (abort_flag) break;
+        if (__any_sync(0xffffffffu, abort_flag != 0)) break;   // warp-uniform: TMEM loads are .sync.aligned
         drain(kb);
       }
     }
@@ -418,17 +514,19 @@ static bool encode_ready() {
 }
 
 // 2D FP32 tensor: inner extent `inner` (contiguous), `outer` rows `ld` floats
-// apart; box 32 x box_rows, out-of-range reads as zero.  K-major tiles use the
-// 128-byte swizzle of 16-byte chunks, MN-major tiles (mn) the 128-byte swizzle
-// of 32-byte chunks that matches descriptor layout 1.
-static bool make_map(CUtensorMap *m, const float *base, long inner, long outer, long ld, int box_rows, bool mn) {
+// apart; box 32 x box_rows, out-of-range reads as zero.  Tiles the tensor core
+// reads use the 128-byte swizzle of 16-byte chunks (K-major) or of 32-byte
+// chunks (MN-major, descriptor layout 1).
+// swz: 0 none, 1 the 128-byte swizzle of 16-byte chunks, 2 of 32-byte chunks.
+static bool make_map(CUtensorMap *m, const float *base, long inner, long outer, long ld, int box_rows, int swz) {
   cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
   cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
   cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
   cuuint32_t es[2] = {1u, 1u};
   CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void *)base, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        mn ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
+                        swz == 0 ? CU_TENSOR_MAP_SWIZZLE_NONE
+                                 : (swz == 2 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B),
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
@@ -443,18 +541,29 @@ static bool enabled() {
   return en == 1;
 }
 
-template <bool A_MN, bool B_MN, int BN>
+template <bool A_MN, bool B_MN, int BN, bool ATM>
 static int launch_tc(const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs &a, dim3 g, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_tc_gemm<A_MN, B_MN, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_tc_gemm<A_MN, B_MN, BN, ATM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Cfg<BN>::SMEM_BYTES) != cudaSuccess)
       return 1;
     attr = true;
   }
-  k_tc_gemm<A_MN, B_MN, BN><<<g, NTHREADS, Cfg<BN>::SMEM_BYTES, st>>>(ma, mb, a);
+  k_tc_gemm<A_MN, B_MN, BN, ATM><<<g, NTHREADS, Cfg<BN>::SMEM_BYTES, st>>>(ma, mb, a);
   note_launch();
   return 0;
+}
+template <bool A_MN, bool B_MN, int BN>
+static int launch_tc(bool atm, const CUtensorMap &ma, const CUtensorMap &mb, const TcArgs &a, dim3 g,
+                     cudaStream_t st) {
+  return atm ? launch_tc<A_MN, B_MN, BN, true>(ma, mb, a, g, st) : launch_tc<A_MN, B_MN, BN, false>(ma, mb, a, g, st);
+}
+
+// QX_TC_ATMEM=0 keeps A in shared memory for the tensor core (read per call).
+static bool atmem_enabled() {
+  const char *e = getenv("QX_TC_ATMEM");
+  return !(e && e[0] == '0');
 }
 
 }  // namespace tc
@@ -493,8 +602,9 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   const int bn = b_mn ? 96 : 80;
   const int tn = (N + bn - 1) / bn;
   CUtensorMap ma, mb;
-  if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, true) : tc::make_map(&ma, A, K, M, lda, BM, false))) return -1;
-  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, true) : tc::make_map(&mb, B, K, N, ldb, bn, false))) return -1;
+  const bool atm = tc::atmem_enabled();
+  if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, atm ? 0 : 2) : tc::make_map(&ma, A, K, M, lda, BM, 1))) return -1;
+  if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, 2) : tc::make_map(&mb, B, K, N, ldb, bn, 1))) return -1;
   // split K until the grid covers the SMs, at least 8 k-blocks a split, or
   // as the autotuner measured for this shape
   int nsplit = 1;
@@ -514,11 +624,11 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   dim3 g(tm, tn, nsplit);
   int rc;
   if (bn == 96) {
-    if (a_mn) rc = tc::launch_tc<true, true, 96>(ma, mb, a, g, st);
-    else rc = tc::launch_tc<false, true, 96>(ma, mb, a, g, st);
+    if (a_mn) rc = tc::launch_tc<true, true, 96>(atm, ma, mb, a, g, st);
+    else rc = tc::launch_tc<false, true, 96>(atm, ma, mb, a, g, st);
   } else {
-    if (a_mn) rc = tc::launch_tc<true, false, 80>(ma, mb, a, g, st);
-    else rc = tc::launch_tc<false, false, 80>(ma, mb, a, g, st);
+    if (a_mn) rc = tc::launch_tc<true, false, 80>(atm, ma, mb, a, g, st);
+    else rc = tc::launch_tc<false, false, 80>(atm, ma, mb, a, g, st);
   }
   if (rc) return rc;
   if (nsplit > 1)
