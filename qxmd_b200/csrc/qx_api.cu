@@ -677,6 +677,16 @@ static PipeParams base_params(const qx_ctx *c) {
   return P;
 }
 
+// The context's second stream and its fork/join events, made on first use.
+static int side_stream(qx_ctx *c) {
+  if (!c->st2) {
+    CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+  }
+  return 0;
+}
+
 // QX_KB_STREAM=0 keeps the G-space KB contractions behind the FFT pipeline
 // on one stream (read at every call).
 static bool kb_side_stream_enabled() {
@@ -706,11 +716,7 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
   const bool side = kb && kb_side_stream_enabled();
   cudaStream_t kst = c->st;
   if (side) {
-    if (!c->st2) {
-      CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
-      CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
-    }
+    TRY(side_stream(c));
     CK(cudaEventRecord(c->ev_fork, c->st));
     CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
     kst = c->st2;
@@ -866,7 +872,8 @@ static int untryt_impl(qx_ctx *c, double *ev, int *sweeps) {
   if (!c->have_hsub) { set_error("untryt: call hmatrix first"); return QX_ERR_STATE; }
   const int nb = c->nb;
   CK(cudaMemcpyAsync(c->d_mat, c->d_hsub, sizeof(double) * nb * nb, cudaMemcpyDeviceToDevice, c->st));
-  TRY(syev(c->d_mat, nb, c->d_w, c->d_V, c->d_eigws, c->d_info, c->st));
+  TRY(side_stream(c));
+  TRY(syev(c->d_mat, nb, c->d_w, c->d_V, c->d_eigws, c->d_info, c->st, c->st2, c->ev_fork, c->ev_join));
   CKL();
   // U in the working precision for the GEMMs
   convert<double, T>(c->d_V, (T *)c->mat_t, (long)nb * nb, c->st);

@@ -1370,7 +1370,11 @@ static bool sytrd_registers_enabled() {
 
 // A (n x n, destroyed), w (n) eigenvalues ascending, V (n x n) eigenvectors.
 // work: at least 8*n*n + 1024*n doubles.  info: number of eigenvalue clusters.
-int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st) {
+// side, evf, evj (optional): a second stream and two events; the T matrices
+// of the compact-WY blocks (which need only the reflectors) are then formed
+// there while the eigenvalues and the tridiagonal eigenvectors are found.
+int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st, cudaStream_t side,
+         cudaEvent_t evf, cudaEvent_t evj) {
   if (n < 1) { set_error("syev: n=%d", n); return 1; }
   const int NT = ((n + 127) / 128) * 128;
   double *d = work, *e = d + n, *tau = e + n, *vp = tau + n, *HV = vp + 7 * (long)n, *Z = HV + (long)n * n,
@@ -1396,6 +1400,20 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
   }
   note_launch();
+  // T of the WY blocks (n <= 256): on the side stream when one is given
+  double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
+  const bool fork = n <= 256 && n >= 2 && side && evf && evj;
+  if (n <= 256 && n >= 2) {
+    const int nblk = (n - 2 + WYB - 1) / WYB;
+    cudaStream_t ts = st;
+    if (fork) {
+      cudaEventRecord(evf, st);
+      cudaStreamWaitEvent(side, evf, 0);
+      ts = side;
+    }
+    if (nblk > 0) { k_wy_t<<<nblk, 32, 0, ts>>>(HV, tau, n, Tm); note_launch(); }
+    if (fork) cudaEventRecord(evj, side);
+  }
   if (n == 1) {
     cudaMemcpyAsync(w, d, sizeof(double), cudaMemcpyDeviceToDevice, st);
     static const double one = 1.0;
@@ -1417,9 +1435,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     k_invit<0><<<NT / 128, 128, dem, st>>>(d, e, w, n, Z, ws, NT, d_info); note_launch();
   }
   if (n <= 256) {
-    double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
-    const int nblk = (n - 2 + WYB - 1) / WYB;
-    if (nblk > 0) { k_wy_t<<<nblk, 32, 0, st>>>(HV, tau, n, Tm); note_launch(); }
+    if (fork) cudaStreamWaitEvent(st, evj, 0);
     k_backtrans_wy<8><<<(n + 3) / 4, 128, 0, st>>>(Z, HV, Tm, n, V); note_launch();
   } else {
     const size_t bt = sizeof(double) * 8 * (size_t)n;

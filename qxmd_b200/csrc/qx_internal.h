@@ -138,7 +138,8 @@ void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit
 // work: >= 32*33 + n doubles, used when S does not fit shared memory.
 int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st);
 // Symmetric eigen-decomposition; work >= 8*n*n + 1024*n doubles.
-int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st);
+int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cudaStream_t st,
+         cudaStream_t side = nullptr, cudaEvent_t evf = nullptr, cudaEvent_t evj = nullptr);
 template <typename Tin, typename Tout>
 void convert(const Tin *in, Tout *out, long n, cudaStream_t st);
 template <typename T>

@@ -135,24 +135,32 @@ __global__ void __launch_bounds__(RB) k_mix(double *__restrict__ rho_in, const d
 // out[k] = sum over nblk partial sums with stride `stride` and offset k.
 // One warp per output: lane-strided partial sums, then a shuffle tree (a fixed
 // order, so the result does not change from run to run).
+// Fixed-order sums of the partials: lane l of a warp adds blocks l, l + 32,
+// ... four at a time into four running sums (the loads of a round are
+// independent), then the lanes are combined by shuffles.
 __global__ void k_reduce(const double *__restrict__ part, int nblk, int stride, int nk, double *__restrict__ out) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int k = w; k < nk; k += blockDim.x >> 5) {
-    double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += part[(long)b * stride + k];
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+    int b = lane;
+    for (; b + 96 < nblk; b += 128)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) s4[u] += part[(long)(b + 32 * u) * stride + k];
+    for (; b < nblk; b += 32) s4[0] += part[(long)b * stride + k];
+    double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) out[k] = s;
   }
 }
 
-// sum_b occ_b * w_b
+// sum_b occ_b * w_b, one warp: lane l takes bands l, l + 32, ...
 __global__ void k_band_energy(const double *__restrict__ w, const double *__restrict__ occ, int nb,
                               double *__restrict__ out) {
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += occ[b] * w[b];
-    *out = s;
-  }
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += occ[b] * w[b];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // ---- Pulay mixing -------------------------------------------------------------
