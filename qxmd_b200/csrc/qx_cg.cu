@@ -152,8 +152,10 @@ __global__ void k_cg_list(int nb, CgState s) {
 // SEQ: one CTA on band *q.cur; when the band stops, its final vector becomes
 // its snapshot column (cgjr(:,ib) = gdcr(:,ibb), eigen.f90:699, real*4 when
 // q.ccreal4) and the next band starts.
+// All bands at once: two CTAs per SM (at most 32 registers), so that 160
+// bands fit one wave on 148 SMs.
 template <typename T, bool SEQ>
-__global__ void __launch_bounds__(CGT) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
+__global__ void __launch_bounds__(CGT, SEQ ? 1 : 2) k_cg_update(int ne, long ldx, T *__restrict__ x, T *__restrict__ hx,
                                                            T *__restrict__ g, const T *__restrict__ h,
                                                            const T *__restrict__ gh, CgState s, CgParm pm,
                                                            SeqArgs q) {
