@@ -348,16 +348,30 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   std::vector<int4> rent(ents.size());
   std::vector<int> fill(cnt.begin(), cnt.end() - 1);
   for (auto &e : ents) rent[fill[e.j2]++] = make_int4(e.a - lo[e.j2], e.i3, e.ig, e.sgn);
+  // z-columns: every (j2, a) with lo <= a <= hi, row by row
+  std::vector<int> col_ja, colq((size_t)pl.P2 * pl.P1, -1);
+  for (int j = 0; j < pl.P2; ++j)
+    for (int a = lo[j]; a <= hi[j]; ++a) {
+      colq[(size_t)j * pl.P1 + a] = (int)col_ja.size();
+      col_ja.push_back(j * pl.P1 + a);
+    }
+  pl.ncol = (int)col_ja.size();
+  std::vector<int> col_ig((size_t)k3 * std::max(1, pl.ncol), 0);
+  for (auto &e : ents) col_ig[(size_t)e.i3 * pl.ncol + colq[(size_t)e.j2 * pl.P1 + e.a]] = e.sgn > 0 ? e.ig + 1 : -(e.ig + 1);
   int rc = 0;
 #define FAIL(x) do { rc = (x); if (rc) { qx_destroy(c); return rc; } } while (0)
   FAIL(dalloc(c, &pl.d_row_lo, sizeof(int) * pl.P2));
   FAIL(dalloc(c, &pl.d_row_hi, sizeof(int) * pl.P2));
   FAIL(dalloc(c, &pl.d_row_off, sizeof(int) * (pl.P2 + 1)));
   FAIL(dalloc(c, &pl.d_row_ent, sizeof(int4) * rent.size()));
+  FAIL(dalloc(c, &pl.d_col_ja, sizeof(int) * std::max<size_t>(1, col_ja.size())));
+  FAIL(dalloc(c, &pl.d_col_ig, sizeof(int) * col_ig.size()));
   if (cudaMemcpy(pl.d_row_lo, lo.data(), sizeof(int) * pl.P2, cudaMemcpyHostToDevice) ||
       cudaMemcpy(pl.d_row_hi, hi.data(), sizeof(int) * pl.P2, cudaMemcpyHostToDevice) ||
       cudaMemcpy(pl.d_row_off, cnt.data(), sizeof(int) * (pl.P2 + 1), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(pl.d_row_ent, rent.data(), sizeof(int4) * rent.size(), cudaMemcpyHostToDevice)) {
+      cudaMemcpy(pl.d_row_ent, rent.data(), sizeof(int4) * rent.size(), cudaMemcpyHostToDevice) ||
+      (pl.ncol && cudaMemcpy(pl.d_col_ja, col_ja.data(), sizeof(int) * col_ja.size(), cudaMemcpyHostToDevice)) ||
+      cudaMemcpy(pl.d_col_ig, col_ig.data(), sizeof(int) * col_ig.size(), cudaMemcpyHostToDevice)) {
     set_error("qx_create: upload failed: %s", cudaGetErrorString(cudaGetLastError()));
     qx_destroy(c);
     return QX_ERR_CUDA;
@@ -669,6 +683,7 @@ static PipeParams base_params(const qx_ctx *c) {
   P.nplw = pl.nplw;
   P.L1 = pl.L[0]; P.L2 = pl.L[1]; P.L3 = pl.L[2];
   P.row_lo = pl.d_row_lo; P.row_hi = pl.d_row_hi; P.row_off = pl.d_row_off; P.row_ent = pl.d_row_ent;
+  P.col_ja = pl.d_col_ja; P.col_ig = pl.d_col_ig; P.ncol = pl.ncol;
   P.pairs = c->d_allpairs;
   P.npair_dev = nullptr;
   P.npair = c->npair_all;

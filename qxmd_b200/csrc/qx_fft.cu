@@ -722,13 +722,18 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
   const size_t smz = fft_smem(P.L3, P.P1 | 1, cs);
-  k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
+  const bool zc = sizeof(T) == sizeof(float) &&
+                  launch_zcols_inv_f32(P, npl, (const float *)cin, ldc, (float2 *)bf.bufA, st) == 0;
+  if (!zc) { k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch(); }
+  // the forward z pass stays on the shared-memory kernel: the column-wise
+  // one measured slower there (its scatter to the sphere is the cost)
+  auto zfwd = [&]() { k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch(); };
   dim3 gy(P.k3, npl);
   const size_t smy = fft_smem(P.L2, P.P1, cs);
   if (sizeof(T) == sizeof(float) && nlmode != 2 && pl.use_plane && plane_enabled() &&
       launch_plane_f32(P, npl, (float2 *)bf.bufA, (const float *)bf.vloc, st) == 0) {
     dim3 gu((P.nplw + 1 + 127) / 128, npl);
-    k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
+    zfwd();
     if (before_unpack) cudaStreamWaitEvent(st, before_unpack, 0);
     k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
     return 0;
@@ -749,7 +754,7 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
     k_xvx<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.vloc, nlines, nch, g1); note_launch();
   }
   k_ypass<T, -1><<<gy, QX_THREADS, smy, st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
-  k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
+  zfwd();
   dim3 gu((P.nplw + 1 + 127) / 128, npl);
   if (before_unpack) cudaStreamWaitEvent(st, before_unpack, 0);
   k_unpack<T><<<gu, 128, 0, st>>>(P, bf.zsph, cin, ldc, out, ldo, dk, accumulate); note_launch();
@@ -764,7 +769,10 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
   Bufs<T> &bf = pl.bufs<T>();
   const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
   dim3 gz(P.P2, npl);
-  k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
+  if (!(sizeof(T) == sizeof(float) &&
+        launch_zcols_inv_f32(P, npl, (const float *)cin, ldc, (float2 *)bf.bufA, st) == 0)) {
+    k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
+  }
   if (sizeof(T) == sizeof(float) && pl.use_plane && plane_enabled() && bf.rho_part &&
       launch_rho_plane_f32(P, npl, (const float2 *)bf.bufA, wocc, bf.rho_part, rho, accumulate, st) == 0)
     return 0;

@@ -85,6 +85,125 @@ __global__ void __launch_bounds__(64) k_plane(PipeParams P, float2 *__restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// The z transforms of the FP32 pipeline, one sphere z-column (j2, a) of one
+// band pair per thread with the whole line in registers (replacing the
+// shared-memory k_zinv / k_zfwd for the specialised lengths).  The column's
+// coefficients come from the z-column table (col_ig, i3-major, so a warp's
+// lookups are one row); positions without a sphere entry are zero.
+//   inverse: two real bands packed as c_A + i c_B (their +G and -G halves),
+//            backward z-FFT, written to bufA[pair][i3][j2][a];
+//   forward: read the column from bufA, forward z-FFT, scale by 1/N and
+//            scatter to zsph as k_zfwd does.
+constexpr int ZC_T = 64;
+
+template <int N>
+__global__ void __launch_bounds__(ZC_T) k_zcols_inv(PipeParams P, const float *__restrict__ cin, long ldc,
+                                                     float2 *__restrict__ bufA) {
+  using rf::out_pos;
+  const int q = blockIdx.x * ZC_T + threadIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= (P.npair_dev ? *P.npair_dev : P.npair) || q >= P.ncol) return;
+  const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+  const float *cA = cin + (long)bA * ldc;
+  const float *cB = bB >= 0 ? cin + (long)bB * ldc : nullptr;
+  float2 x[N];
+#pragma unroll
+  for (int i3 = 0; i3 < N; ++i3) {
+    const int code = P.col_ig[i3 * P.ncol + q];
+    float2 z = make_float2(0.f, 0.f);
+    if (code != 0) {
+      const int ig = (code > 0 ? code : -code) - 1;
+      const float ra = cA[2 * ig], ia = ig ? cA[2 * ig + 1] : 0.f;
+      const float rb = cB ? cB[2 * ig] : 0.f, ib = (cB && ig) ? cB[2 * ig + 1] : 0.f;
+      if (code > 0) { z.x = ra - ib; z.y = ia + rb; }
+      else          { z.x = ra + ib; z.y = rb - ia; }
+    }
+    x[i3] = z;
+  }
+  rf::fft<float, +1, N>(x);
+  float2 *dst = bufA + (long)pl * N * P.P2 * P.P1 + P.col_ja[q];
+  rf::static_for<0, N>([&](auto ic) {
+    constexpr int i3 = decltype(ic)::value;
+    dst[(long)i3 * P.P2 * P.P1] = x[out_pos(N, i3)];
+  });
+}
+
+template <int N>
+__global__ void __launch_bounds__(ZC_T) k_zcols_fwd(PipeParams P, const float2 *__restrict__ bufA,
+                                                     float2 *__restrict__ zsph) {
+  using rf::out_pos;
+  const int q = blockIdx.x * ZC_T + threadIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= (P.npair_dev ? *P.npair_dev : P.npair) || q >= P.ncol) return;
+  const float2 *src = bufA + (long)pl * N * P.P2 * P.P1 + P.col_ja[q];
+  float2 x[N];
+#pragma unroll
+  for (int i3 = 0; i3 < N; ++i3) x[i3] = src[(long)i3 * P.P2 * P.P1];
+  rf::fft<float, -1, N>(x);
+  const float s = (float)P.inv_n;
+  float2 *Z = zsph + (long)pl * (P.nplw + 1) * 2;
+  rf::static_for<0, N>([&](auto ic) {
+    constexpr int i3 = decltype(ic)::value;
+    const int code = P.col_ig[i3 * P.ncol + q];
+    if (code != 0) {
+      float2 z = x[out_pos(N, i3)];
+      z.x *= s;
+      z.y *= s;
+      if (code > 0) {
+        const int ig = code - 1;
+        Z[2 * ig] = z;
+        if (ig == 0) Z[1] = z;
+      } else {
+        Z[2 * (-code - 1) + 1] = z;
+      }
+    }
+  });
+}
+
+template <int N>
+static int zcols_launch(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, const float2 *src,
+                        float2 *zsph, bool inv, cudaStream_t st) {
+  dim3 g((P.ncol + ZC_T - 1) / ZC_T, npl);
+  if (inv) k_zcols_inv<N><<<g, ZC_T, 0, st>>>(P, cin, ldc, bufA);
+  else k_zcols_fwd<N><<<g, ZC_T, 0, st>>>(P, src, zsph);
+  note_launch();
+  return 0;
+}
+
+// QX_ZCOLS=0 keeps the shared-memory z passes (read at every call).
+static bool zcols_enabled() {
+  const char *e = getenv("QX_ZCOLS");
+  return !(e && e[0] == '0');
+}
+
+static int zcols_dispatch(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, const float2 *src,
+                          float2 *zsph, bool inv, cudaStream_t st) {
+  if (!zcols_enabled() || P.ncol <= 0) return -1;
+  switch (P.k3) {
+    case 20: return zcols_launch<20>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 24: return zcols_launch<24>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 27: return zcols_launch<27>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 30: return zcols_launch<30>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 32: return zcols_launch<32>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 36: return zcols_launch<36>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 40: return zcols_launch<40>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 45: return zcols_launch<45>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 48: return zcols_launch<48>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 54: return zcols_launch<54>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 60: return zcols_launch<60>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 64: return zcols_launch<64>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    default: return -1;
+  }
+}
+
+int launch_zcols_inv_f32(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, cudaStream_t st) {
+  return zcols_dispatch(P, npl, cin, ldc, bufA, nullptr, nullptr, true, st);
+}
+int launch_zcols_fwd_f32(const PipeParams &P, int npl, const float2 *bufA, float2 *zsph, cudaStream_t st) {
+  return zcols_dispatch(P, npl, nullptr, 0, nullptr, bufA, zsph, false, st);
+}
+
 // Density for the same grids (softchg, chgdns.f90:388-454): per CTA one z
 // plane and one group of band pairs; for each pair the backward y- and
 // x-FFTs of the plane as above, then rho += occ_A/Omega psi_A(r)^2 +

@@ -16,6 +16,11 @@ struct PipeParams {
   FftLen L1, L2, L3;
   const int *row_lo, *row_hi, *row_off;
   const int4 *row_ent;      // {line = a - lo, i3, ig, sign(+1 : +G, -1 : -G)}
+  // sphere z-columns (j2, a): col_ja[q] = j2 * P1 + a; col_ig[i3 * ncol + q] =
+  // ig + 1 for the +G entry at (a, j2, i3), -(ig + 1) for the -G entry, 0 none
+  const int *col_ja;
+  const int *col_ig;
+  int ncol;
   const int *pairs;         // band indices, 2 per pair, -1 = empty slot
   const int *npair_dev;     // number of valid pairs (device), or null
   int npair;                // pair bound when npair_dev is null
@@ -61,6 +66,9 @@ struct Plan {
   // sphere rows
   int *d_row_lo = nullptr, *d_row_hi = nullptr, *d_row_off = nullptr;
   int4 *d_row_ent = nullptr;
+  // sphere z-columns (see PipeParams)
+  int *d_col_ja = nullptr, *d_col_ig = nullptr;
+  int ncol = 0;
   // real-space KB
   int natom = 0, npts = 0;
   int *d_kb_off = nullptr, *d_kb_mesh = nullptr;
@@ -102,6 +110,10 @@ constexpr int RHO_GROUPS = 16;
 int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part,
                          double *rho, int accumulate, cudaStream_t st);
 bool plane_length_supported(int k1, int k2);
+// Column-wise z transforms (one sphere z-column per thread, FP32, register
+// FFTs of length k3); -1 when k3 has no specialised length.
+int launch_zcols_inv_f32(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, cudaStream_t st);
+int launch_zcols_fwd_f32(const PipeParams &P, int npl, const float2 *bufA, float2 *zsph, cudaStream_t st);
 template <typename T> size_t fft_smem_need(const Plan &pl);
 int init_fft_roots();
 
