@@ -515,9 +515,10 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
   constexpr int NX = NROW > NCOL ? NROW : NCOL;
   static_assert(NR <= 32 && NR % 2 == 0, "lane r of a warp keeps m of row r; row pairs stay in one warp");
   extern __shared__ double stg[];   // n x (n | 1) staging
-  __shared__ double xcol[2][2][NX];
-  __shared__ double xrow[2][2][NX];
+  __shared__ __align__(16) double xcol[2][2][NX];
+  __shared__ __align__(16) double xrow[2][2][NX];
   __shared__ double rsv[NX];
+  __shared__ double2 mw[W][NR];     // m0, m1 of each warp's rows (read back as broadcasts)
   const int ld = n | 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * NR;
@@ -545,9 +546,10 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
         constexpr int C = decltype(cc)::value;
         if (C == kc) {
 #pragma unroll
-          for (int r = 0; r < NR; ++r) {
-            xcol[b][h][r0 + r] = a[r][C];
+          for (int r = 0; r < NR; r += 2) {
+            *reinterpret_cast<double2 *>(&xcol[b][h][r0 + r]) = make_double2(a[r][C], a[r + 1][C]);
             a[r][C] = (r0 + r == col) ? 1.0 : 0.0;
+            a[r + 1][C] = (r0 + r + 1 == col) ? 1.0 : 0.0;
           }
         }
       });
@@ -591,6 +593,8 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
     const int ri = r0 + lane, rc = min(ri, NX - 1);
     const double m0row = (lane < NR && ri > k && ri < n) ? x0[rc] * rs0 : 0.0;
     const double m1row = (two && lane < NR && ri > k + 1 && ri < n) ? (x1[rc] - m0row * l10) * rs1 : 0.0;
+    if (lane < NR) mw[warp][lane] = make_double2(m0row, m1row);
+    __syncwarp();
     if (r0 + NR > k + 1) {    // rows below k in this warp
       double y0[NC], y1[NC];
 #pragma unroll
@@ -603,11 +607,12 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
       }
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double mi0 = __shfl_sync(0xffffffffu, m0row, r), mi1 = __shfl_sync(0xffffffffu, m1row, r);
+        const double2 mi = mw[warp][r];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) a[r][c] = fma(-mi1, y1[c], fma(-mi0, y0[c], a[r][c]));
+        for (int c = 0; c < NC; ++c) a[r][c] = fma(-mi.y, y1[c], fma(-mi.x, y0[c], a[r][c]));
       }
     }
+    __syncwarp();   // mw is rewritten in the next step
   }
   __syncthreads();
   // X to the staging area (lower triangle, zeros above), then out column-major
@@ -879,10 +884,11 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
   constexpr int NROW = TRR_W * NR, NCOL = 32 * NC;
   static_assert(NROW <= NCOL, "p is indexed by rows and by columns");
   static_assert(NR <= 32, "lane r of a warp keeps v and w of the warp's row r");
-  __shared__ double xs[2][NROW];
+  __shared__ __align__(16) double xs[2][NROW];
   __shared__ double sigp[2][TRR_W];
   __shared__ double part[TRR_W][NCOL];
   __shared__ double ps[NCOL];
+  __shared__ double vsm[TRR_W][NR], wsm[TRR_W][NR];   // v, w of each warp's rows (read back as broadcasts)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * NR;
   double a[NR][NC];
@@ -902,10 +908,11 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
         if (C == kc) {
           double sg[2] = {0.0, 0.0};
 #pragma unroll
-          for (int r = 0; r < NR; ++r) {
-            const double x = a[r][C];
-            xs[b][r0 + r] = x;
-            sg[r & 1] += (r0 + r > kk + 1) ? x * x : 0.0;
+          for (int r = 0; r < NR; r += 2) {
+            const double x0 = a[r][C], x1 = a[r + 1][C];
+            *reinterpret_cast<double2 *>(&xs[b][r0 + r]) = make_double2(x0, x1);
+            sg[0] += (r0 + r > kk + 1) ? x0 * x0 : 0.0;
+            sg[1] += (r0 + r + 1 > kk + 1) ? x1 * x1 : 0.0;
           }
           sigp[b][warp] = sg[0] + sg[1];
         }
@@ -939,6 +946,8 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
     const bool rows_active = r0 + NR > k + 1;                          // uniform in the warp
     // lane r < NR keeps v of row r0 + r; the warp reads it by shuffles
     const double vrow = (lane < NR) ? vof(r0 + lane) : 0.0;
+    if (lane < NR) vsm[warp][lane] = vrow;
+    __syncwarp();
     {
       double sc[NC];
 #pragma unroll
@@ -946,7 +955,7 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
       if (rows_active) {
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          const double vr = __shfl_sync(0xffffffffu, vrow, r);
+          const double vr = vsm[warp][r];
 #pragma unroll
           for (int c = 0; c < NC; ++c) sc[c] = fma(a[r][c], vr, sc[c]);
         }
@@ -967,6 +976,8 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
     for (int c = 0; c < NC; ++c) kk = fma(vof(lane + 32 * c), ps[lane + 32 * c], kk);
     const double K = 0.5 * t * warp_sum(kk);
     const double wrow = (lane < NR) ? fma(-K, vrow, ps[min(r0 + lane, NCOL - 1)]) : 0.0;
+    if (lane < NR) wsm[warp][lane] = wrow;
+    __syncwarp();
     // A -= v w^T, then A -= w v^T: each pass keeps one vector of the lane's
     // columns live beside the block
     if (rows_active) {
@@ -975,7 +986,7 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
       for (int c = 0; c < NC; ++c) wc[c] = fma(-K, vof(lane + 32 * c), ps[lane + 32 * c]);
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double vi = __shfl_sync(0xffffffffu, vrow, r);
+        const double vi = vsm[warp][r];
 #pragma unroll
         for (int c = 0; c < NC; ++c) a[r][c] = fma(-vi, wc[c], a[r][c]);
       }
@@ -984,11 +995,12 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
       for (int c = 0; c < NC; ++c) vc[c] = vof(lane + 32 * c);
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
-        const double wi = __shfl_sync(0xffffffffu, wrow, r);
+        const double wi = wsm[warp][r];
 #pragma unroll
         for (int c = 0; c < NC; ++c) a[r][c] = fma(-wi, vc[c], a[r][c]);
       }
     }
+    __syncwarp();   // vsm, wsm are rewritten in the next step
   }
   // the last 2 x 2 block
   if (n >= 2) {
