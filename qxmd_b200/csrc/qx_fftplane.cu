@@ -274,11 +274,16 @@ __global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__
 }
 
 // rho = [rho +] sum over groups of part (fixed order).
-__global__ void k_rho_groups(const double *__restrict__ part, int ngrp, long n, double *__restrict__ rho,
-                             int accumulate) {
+// Sum of the RHO_GROUPS partial planes in group order (all loads of an
+// element issued together).
+__global__ void k_rho_groups(const double *__restrict__ part, long n, double *__restrict__ rho, int accumulate) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double v[RHO_GROUPS];
+#pragma unroll
+    for (int g = 0; g < RHO_GROUPS; ++g) v[g] = part[(long)g * n + i];
     double s = accumulate ? rho[i] : 0.0;
-    for (int g = 0; g < ngrp; ++g) s += part[(long)g * n + i];
+#pragma unroll
+    for (int g = 0; g < RHO_GROUPS; ++g) s += v[g];
     rho[i] = s;
   }
 }
@@ -297,7 +302,7 @@ static int rho_launch(const PipeParams &P, int npl, const float2 *bufA, const do
   k_rho_plane<N><<<g, 64, sm, st>>>(P, bufA, wocc, part, npl, per_group);
   note_launch();
   const long n = (long)P.k1 * P.k2 * P.k3;
-  k_rho_groups<<<148 * 4, 256, 0, st>>>(part, RHO_GROUPS, n, rho, accumulate);
+  k_rho_groups<<<148 * 4, 256, 0, st>>>(part, n, rho, accumulate);
   note_launch();
   return 0;
 }
