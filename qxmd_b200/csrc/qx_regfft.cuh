@@ -90,6 +90,14 @@ template <> struct C2<double> { typedef double2 t; };
 
 template <typename C> QX_HD C add(C a, C b) { a.x += b.x; a.y += b.y; return a; }
 template <typename C> QX_HD C sub(C a, C b) { a.x -= b.x; a.y -= b.y; return a; }
+#if defined(__CUDA_ARCH__)
+// FP32 pairs on the packed two-wide FP32 unit of sm_100: one instruction for
+// both components (a - b as a + (-1) b, exact like the subtraction).
+template <> __device__ __forceinline__ float2 add<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 sub<float2>(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+#endif
 
 // x * exp(SIGN * 2 pi i p / q) with a compile-time root.
 template <typename T, int SIGN, long P, long Q>
