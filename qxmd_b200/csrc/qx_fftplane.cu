@@ -15,8 +15,12 @@
 
 namespace qx {
 
+// Resident CTAs per SM asked of the register allocator: 8 (128 registers)
+// where that needs no spills.
+constexpr int plane_minb(int n) { return n <= 54 ? 8 : 1; }
+
 template <int N>
-__global__ void __launch_bounds__(64) k_plane(PipeParams P, float2 *__restrict__ bufA, const float *__restrict__ vloc) {
+__global__ void __launch_bounds__(64, plane_minb(N)) k_plane(PipeParams P, float2 *__restrict__ bufA, const float *__restrict__ vloc) {
   using rf::out_pos;
   const int i3 = blockIdx.x;
   const int pl = blockIdx.y, p = P.pair0 + pl;
