@@ -1016,6 +1016,181 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
   if (tid == 0) d[n - 1] = xs[1][n - 1];
 }
 
+// ---------------------------------------------------------------------------
+// Grid barrier for the cooperative kernels below (all CTAs co-resident by the
+// cooperative launch).  bar[0]: arrival count, bar[1]: generation, both zero
+// before the launch.  The last CTA to arrive resets the count and advances
+// the generation; the others poll the generation (L2 loads) for at most
+// GB_WAIT_NS, after which the barrier reports failure (every later barrier of
+// that CTA fails as well, so all CTAs leave their loops).  Writes before the
+// barrier are published by the block barrier plus thread 0's fence; reads of
+// data written by other CTAs use __ldcg (L2), never a possibly stale L1 line.
+constexpr unsigned long long GB_WAIT_NS = 2000000000ull;
+__device__ __forceinline__ unsigned long long gb_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblk, int *okflag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (*okflag) {
+      const unsigned g0 = __ldcg(bar + 1);
+      __threadfence();
+      if (atomicAdd(bar, 1u) == nblk - 1) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        const unsigned long long t0 = gb_now();
+        while (__ldcg(bar + 1) == g0) {
+          if (gb_now() - t0 > GB_WAIT_NS) {
+            *okflag = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return *okflag != 0;
+}
+
+// Householder tridiagonalisation over the whole GPU for large n (one
+// cooperative launch of G CTAs, the role of k_sytrd when the matrix does not
+// fit one SM): CTA c keeps the columns j = c + G q of A in shared memory.
+// Per column k (m = n - k - 1 trailing rows), two grid barriers:
+//   (1) the owner of column k has formed the reflector (house) and written v
+//       (and tau) to global memory;
+//   (2) every CTA has written p_j = tau (A v)_j for its columns (column dot
+//       products: A is symmetric) and its part of v^T p;
+// then every CTA forms K = tau v^T p / 2 (the G parts in a fixed order),
+// w = p - K v, and updates its own columns, A_ij -= v_i w_j + w_i v_j.  v
+// alternates between two buffers by column parity; p and the parts are
+// rewritten only after the next barrier (1), which every CTA reaches after
+// its reads.  gs: 3n + G + 2 doubles of global scratch; bar: two zeroed
+// unsigned ints.  On a barrier time-out *info is made negative.
+constexpr int TRG_T = 256;
+
+__global__ void __launch_bounds__(TRG_T) k_sytrd_grid(const double *__restrict__ Ag, int n, double *__restrict__ d,
+                                                      double *__restrict__ e, double *__restrict__ HV,
+                                                      double *__restrict__ tau, double *gs, unsigned *bar,
+                                                      int *info) {
+  const int G = gridDim.x, c = blockIdx.x;
+  const int nq = (n + G - 1) / G;
+  extern __shared__ double sm[];
+  double *A = sm;                     // [nq][n]: column j = c + G q at A + q n
+  double *vs = A + (long)nq * n;      // v by row
+  double *pw = vs + n;                // p by row
+  double *vbuf = gs, *pbuf = gs + 2 * (long)n, *kpart = gs + 3 * (long)n, *tbuf = kpart + G;
+  __shared__ double red[TRG_T / 32];
+  __shared__ double tK[2];
+  __shared__ int ok;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = TRG_T / 32;
+  if (tid == 0) ok = 1;
+  for (long q = tid; q < (long)nq * n; q += TRG_T) {
+    const int qq = (int)(q / n), i = (int)(q - (long)qq * n), j = c + G * qq;
+    A[q] = (j < n) ? Ag[(long)j * n + i] : 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k + 2 < n; ++k) {
+    const int own = k % G, par = k & 1;
+    double *vb = vbuf + (long)par * n;
+    if (c == own && warp == 0) {
+      const double *col = A + (long)(k / G) * n;
+      double sg = 0.0;
+      for (int i = k + 2 + lane; i < n; i += 32) {
+        const double x = col[i];
+        sg += x * x;
+      }
+      sg = warp_sum(sg);
+      double t = 0.0, rb = 1.0, al = 0.0;
+      if (lane == 0) house(col[k + 1], sg, t, rb, al);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      const double rbe = __shfl_sync(0xffffffffu, rb, 0);
+      for (int i = k + 1 + lane; i < n; i += 32) {
+        const double vi = (i == k + 1) ? 1.0 : ((t != 0.0) ? col[i] * rbe : 0.0);
+        vb[i] = vi;
+        HV[(long)k * n + i] = vi;
+      }
+      if (lane == 0) {
+        tau[k] = t;
+        d[k] = col[k];
+        e[k] = al;
+        tbuf[par] = t;
+      }
+    }
+    if (!grid_barrier(bar, G, &ok)) break;                        // (1)
+    const double t = __ldcg(tbuf + par);
+    if (t == 0.0) continue;                                        // the same in every CTA
+    for (int i = k + 1 + tid; i < n; i += TRG_T) vs[i] = __ldcg(vb + i);
+    __syncthreads();
+    const int q_lo = (k + 1 > c) ? (k + 1 - c + G - 1) / G : 0;
+    double kk = 0.0;
+    for (int q = q_lo + warp; q < nq; q += NW) {
+      const int j = c + G * q;
+      if (j >= n) break;                                           // uniform in the warp
+      const double *col = A + (long)q * n;
+      double s0 = 0.0, s1 = 0.0;
+      int i = k + 1 + lane;
+      for (; i + 32 < n; i += 64) {
+        s0 += col[i] * vs[i];
+        s1 += col[i + 32] * vs[i + 32];
+      }
+      if (i < n) s0 += col[i] * vs[i];
+      const double pj = t * warp_sum(s0 + s1);
+      if (lane == 0) {
+        pbuf[j] = pj;
+        kk += vs[j] * pj;
+      }
+    }
+    if (lane == 0) red[warp] = kk;
+    __syncthreads();
+    if (tid == 0) {
+      double x = 0.0;
+      for (int w = 0; w < NW; ++w) x += red[w];
+      kpart[c] = x;
+    }
+    if (!grid_barrier(bar, G, &ok)) break;                        // (2)
+    if (warp == 0) {
+      double x = 0.0;
+      for (int r = lane; r < G; r += 32) x += __ldcg(kpart + r);
+      x = warp_sum(x);
+      if (lane == 0) tK[1] = 0.5 * t * x;
+    }
+    for (int i = k + 1 + tid; i < n; i += TRG_T) pw[i] = __ldcg(pbuf + i);
+    __syncthreads();
+    const double K = tK[1];
+    for (int q = q_lo + warp; q < nq; q += NW) {
+      const int j = c + G * q;
+      if (j >= n) break;
+      const double vj = vs[j], wj = pw[j] - K * vj;
+      double *col = A + (long)q * n;
+      for (int i = k + 1 + lane; i < n; i += 32) {
+        const double vi = vs[i], wi = pw[i] - K * vi;
+        col[i] -= vi * wj + wi * vj;
+      }
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (!ok) {
+    if (tid == 0) atomicExch(info, -(1 << 30));
+    return;
+  }
+  if (tid == 0) {
+    if (n >= 2 && c == (n - 2) % G) {
+      const double *col = A + (long)((n - 2) / G) * n;
+      d[n - 2] = col[n - 2];
+      e[n - 2] = col[n - 1];
+    }
+    if (c == (n - 1) % G) d[n - 1] = A[(long)((n - 1) / G) * n + n - 1];
+  }
+}
+
 // Number of eigenvalues of T below x: sign changes of the Sturm sequence
 // p_0 = 1, p_1 = d_0 - x, p_i = (d_{i-1} - x) p_{i-1} - e_{i-2}^2 p_{i-2}
 // (zeros dropped).  No division on the dependent chain (one FMA a step; the
@@ -1373,6 +1548,48 @@ __global__ void __launch_bounds__(128) k_backtrans_wy(const double *__restrict__
   }
 }
 
+// The cooperative tridiagonalisation when the matrix fits the shared memory
+// of the GPU's CTAs (one per SM) and cooperative launch is available; false
+// if it was not launched.  Scratch in vp (7n doubles): v (2n), p (n), the
+// per-CTA parts (G), tau (2), then the barrier words.  QX_SYTRD_GRID=0
+// turns it off (read at every call).
+static bool sytrd_grid(double *A, int n, double *d, double *e, double *HV, double *tau, double *vp, int *d_info,
+                       cudaStream_t st) {
+  const char *env = getenv("QX_SYTRD_GRID");
+  if (env && env[0] == '0') return false;
+  int dev = 0, nsm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) return false;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+  const int G = std::min(nsm, n);
+  const int nq = (n + G - 1) / G;
+  const size_t sm = sizeof(double) * ((size_t)nq * n + 2 * (size_t)n);
+  if (sm > 200 * 1024 || 3L * n + G + 2 + 1 > 7L * n) return false;
+  static size_t sm_set = 48 * 1024;   // per process: only ever raised
+  if (sm > sm_set) {
+    if (cudaFuncSetAttribute(k_sytrd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+      return false;
+    sm_set = 200 * 1024;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sytrd_grid, TRG_T, sm) != cudaSuccess || per_sm < 1)
+    return false;
+  double *gs = vp;
+  unsigned *bar = reinterpret_cast<unsigned *>(vp + 3L * n + G + 2);
+  if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const double *Ac = A;
+  void *args[] = {(void *)&Ac, (void *)&n, (void *)&d, (void *)&e, (void *)&HV, (void *)&tau, (void *)&gs,
+                  (void *)&bar, (void *)&d_info};
+  if (cudaLaunchCooperativeKernel((const void *)k_sytrd_grid, dim3(G), dim3(TRG_T), args, sm, st) != cudaSuccess) {
+    cudaGetLastError();   // not launched: the one-CTA kernel runs instead
+    return false;
+  }
+  return true;
+}
+
 // QX_SYTRD_REG=0 keeps the shared-memory tridiagonalisation at every size
 // (read at every call).
 static bool sytrd_registers_enabled() {
@@ -1408,7 +1625,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     k_sytrd_rg<8, 20, 5><<<1, 8 * 32, 0, st>>>(A, n, d, e, HV, tau);
   } else if (use) {
     k_sytrd<true><<<1, TRD_T, smem, st>>>(A, n, d, e, HV, tau, vp);
-  } else {
+  } else if (!sytrd_grid(A, n, d, e, HV, tau, vp, d_info, st)) {
     k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
   }
   note_launch();
