@@ -1098,6 +1098,7 @@ static int schmidt_impl(qx_ctx *c) {
     int info = 0;
     CK(cudaMemcpyAsync(&info, c->d_info + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    if (info < 0) { set_error("schmidt: a grid barrier of the Cholesky kernel timed out"); return QX_ERR_CUDA; }
     if (info) { set_error("schmidt: <psi|psi> not positive definite at band %d", info - 1); return QX_ERR_NOTPD; }
   }
   convert<double, T>(c->d_mat, m, (long)nb * nb, c->st);
@@ -1375,6 +1376,7 @@ extern "C" int qx_scf_result(qx_ctx *c, qx_scf_out *out) {
   CK(cudaMemcpyAsync(info, c->d_info, sizeof(int) * 3, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (info[0] <= 0) { set_error("untryt: eigen-decomposition produced no eigenvectors"); return QX_ERR_EIG; }
+  if (info[1] < 0) { set_error("schmidt: a grid barrier of the Cholesky kernel timed out"); return QX_ERR_CUDA; }
   if (info[1]) { set_error("schmidt: <psi|psi> not positive definite at band %d", info[1] - 1); return QX_ERR_NOTPD; }
   if (out) {
     out->ehartree = sc[0];

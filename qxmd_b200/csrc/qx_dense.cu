@@ -31,6 +31,48 @@ template <int B, int E, typename F> __device__ __forceinline__ void dense_static
   }
 }
 
+// ---------------------------------------------------------------------------
+// Grid barrier for the cooperative kernels of this file (all CTAs co-resident by the
+// cooperative launch).  bar[0]: arrival count, bar[1]: generation, both zero
+// before the launch.  The last CTA to arrive resets the count and advances
+// the generation; the others poll the generation (L2 loads) for at most
+// GB_WAIT_NS, after which the barrier reports failure (every later barrier of
+// that CTA fails as well, so all CTAs leave their loops).  Writes before the
+// barrier are published by the block barrier plus thread 0's fence; reads of
+// data written by other CTAs use __ldcg (L2), never a possibly stale L1 line.
+constexpr unsigned long long GB_WAIT_NS = 2000000000ull;
+__device__ __forceinline__ unsigned long long gb_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblk, int *okflag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (*okflag) {
+      const unsigned g0 = __ldcg(bar + 1);
+      __threadfence();
+      if (atomicAdd(bar, 1u) == nblk - 1) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicAdd(bar + 1, 1u);
+      } else {
+        const unsigned long long t0 = gb_now();
+        while (__ldcg(bar + 1) == g0) {
+          if (gb_now() - t0 > GB_WAIT_NS) {
+            *okflag = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return *okflag != 0;
+}
+
 // --------------------------------------------------------------------------
 // Cholesky S = L L^T and L^-1, blocked by CB = 32.  Column-major n x n; on
 // return the lower triangle holds L^-1 and the upper triangle zeros.
@@ -634,6 +676,131 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
   if (tid == 0) *info = 0;
 }
 
+// Cholesky and L^-1 over the whole GPU for large n (one cooperative launch of
+// G CTAs; the algorithm of k_cholinv_rg, one rank-1 update a column): CTA c
+// keeps the columns j = c + G q in shared memory.  Step k: the owner of column
+// k publishes it (the Schur complement) and replaces it by e_k; every CTA
+// publishes its entries of row k (R(k, .) left of k); one grid barrier; then
+// with rs = 1 / L(k,k), m_i = S(i,k) rs and y_j = R(k,j) rs (j <= k) or m_j
+// (j > k), every CTA applies a(i,j) -= m_i y_j to the rows i > k of its
+// columns.  Row k is final from then on and is scaled by rs when written out.
+// The published column and row alternate by parity.  gs: 5n doubles of
+// global scratch (column, row, 1/L(k,k)); bar: two zeroed unsigned ints.
+// info as k_cholinv_sm (S left as it was on a bad pivot); -1 on a barrier
+// time-out.
+constexpr int CHG_T = 256;
+
+__global__ void __launch_bounds__(CHG_T) k_cholinv_grid(double *__restrict__ Sg, int n, double *gs, unsigned *bar,
+                                                        int *__restrict__ info) {
+  const int G = gridDim.x, c = blockIdx.x;
+  const int nq = (n + G - 1) / G;
+  extern __shared__ double sm[];
+  double *A = sm;                     // [nq][n]: column j = c + G q at A + q n
+  double *mc = A + (long)nq * n;      // the published column of this step
+  double *xcol = gs, *xrow = gs + 2 * (long)n, *rsv = gs + 4 * (long)n;
+  __shared__ int ok;
+  const int tid = threadIdx.x;
+  if (tid == 0) ok = 1;
+  // the lower triangle, as rsdecmp reads it
+  for (long q = tid; q < (long)nq * n; q += CHG_T) {
+    const int qq = (int)(q / n), i = (int)(q - (long)qq * n), j = c + G * qq;
+    double v = 0.0;
+    if (j < n) v = (i >= j) ? Sg[(long)j * n + i] : Sg[(long)i * n + j];
+    A[q] = v;
+  }
+  __syncthreads();
+  bool bad = false;
+  for (int k = 0; k < n; ++k) {
+    const int par = k & 1;
+    double *xc = xcol + (long)par * n, *xr = xrow + (long)par * n;
+    if (c == k % G) {
+      double *col = A + (long)(k / G) * n;
+      for (int i = tid; i < n; i += CHG_T) {
+        xc[i] = col[i];
+        col[i] = (i == k) ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    for (int q = tid; q < nq; q += CHG_T) {
+      const int j = c + G * q;
+      if (j < n) xr[j] = A[(long)q * n + k];
+    }
+    if (!grid_barrier(bar, G, &ok)) break;
+    const double piv = __ldcg(xc + k);
+    if (!(piv > 1.0e-30)) {   // the same in every CTA; also catches NaN
+      if (c == 0 && tid == 0) *info = 1 + k;
+      bad = true;
+      break;
+    }
+    const double rs = rsqrt_nr(piv);
+    if (c == 0 && tid == 0) rsv[k] = rs;
+    for (int i = k + 1 + tid; i < n; i += CHG_T) mc[i] = __ldcg(xc + i) * rs;
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int q = warp; q < nq; q += CHG_T / 32) {
+      const int j = c + G * q;
+      if (j >= n) break;   // uniform in the warp
+      const double y = ((j <= k) ? __ldcg(xr + j) : __ldcg(xc + j)) * rs;
+      double *col = A + (long)q * n;
+      for (int i = k + 1 + lane; i < n; i += 32) col[i] = fma(-mc[i], y, col[i]);
+    }
+    __syncthreads();
+  }
+  if (bad) return;
+  if (!grid_barrier(bar, G, &ok) || !ok) {
+    if (tid == 0) atomicExch(info, -1);
+    return;
+  }
+  // X: row i scaled by 1 / L(i,i), zeros above the diagonal
+  for (long q = tid; q < (long)nq * n; q += CHG_T) {
+    const int qq = (int)(q / n), i = (int)(q - (long)qq * n), j = c + G * qq;
+    if (j < n) Sg[(long)j * n + i] = (i >= j) ? A[q] * __ldcg(rsv + i) : 0.0;
+  }
+  if (c == 0 && tid == 0 && *info >= 0) *info = 0;
+}
+
+// The cooperative Cholesky + inverse when the columns fit one CTA per SM and
+// cooperative launch is available; false if it was not launched.  work:
+// at least 5n doubles + 2 unsigned ints.  QX_CHOLINV_GRID=0 turns it off
+// (read at every call).
+static bool cholinv_grid(double *S, int n, double *work, int *d_info, cudaStream_t st) {
+  const char *env = getenv("QX_CHOLINV_GRID");
+  if ((env && env[0] == '0') || !work) return false;
+  int dev = 0, nsm = 0, coop = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) return false;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop) return false;
+  const int G = std::min(nsm, n);
+  const int nq = (n + G - 1) / G;
+  const size_t sm = sizeof(double) * ((size_t)nq * n + (size_t)n);
+  if (sm > 200 * 1024) return false;
+  static size_t sm_set = 48 * 1024;   // per process: only ever raised
+  if (sm > sm_set) {
+    if (cudaFuncSetAttribute(k_cholinv_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+      return false;
+    sm_set = 200 * 1024;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cholinv_grid, CHG_T, sm) != cudaSuccess ||
+      per_sm < 1)
+    return false;
+  double *gs = work;
+  unsigned *bar = reinterpret_cast<unsigned *>(work + 5L * n);
+  if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess ||
+      cudaMemsetAsync(d_info, 0, sizeof(int), st) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  void *args[] = {(void *)&S, (void *)&n, (void *)&gs, (void *)&bar, (void *)&d_info};
+  if (cudaLaunchCooperativeKernel((const void *)k_cholinv_grid, dim3(G), dim3(CHG_T), args, sm, st) !=
+      cudaSuccess) {
+    cudaGetLastError();   // not launched: the one-CTA kernels run instead
+    return false;
+  }
+  note_launch();
+  return true;
+}
+
 // QX_CHOLINV_REG=0 keeps the shared-memory kernels at every size (read at
 // every call).
 static bool cholinv_registers_enabled() {
@@ -675,6 +842,7 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
     note_launch();
     return 0;
   }
+  if (n > 192 && cholinv_grid(S, n, work, d_info, st)) return 0;
   if (n <= CP_MAXN && pbytes <= CH_SMEM_MAX) {
     static bool pattr = false;
     if (!pattr) {
@@ -1014,48 +1182,6 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
   gather(n - 1, 1);
   __syncthreads();
   if (tid == 0) d[n - 1] = xs[1][n - 1];
-}
-
-// ---------------------------------------------------------------------------
-// Grid barrier for the cooperative kernels below (all CTAs co-resident by the
-// cooperative launch).  bar[0]: arrival count, bar[1]: generation, both zero
-// before the launch.  The last CTA to arrive resets the count and advances
-// the generation; the others poll the generation (L2 loads) for at most
-// GB_WAIT_NS, after which the barrier reports failure (every later barrier of
-// that CTA fails as well, so all CTAs leave their loops).  Writes before the
-// barrier are published by the block barrier plus thread 0's fence; reads of
-// data written by other CTAs use __ldcg (L2), never a possibly stale L1 line.
-constexpr unsigned long long GB_WAIT_NS = 2000000000ull;
-__device__ __forceinline__ unsigned long long gb_now() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblk, int *okflag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (*okflag) {
-      const unsigned g0 = __ldcg(bar + 1);
-      __threadfence();
-      if (atomicAdd(bar, 1u) == nblk - 1) {
-        atomicExch(bar, 0u);
-        __threadfence();
-        atomicAdd(bar + 1, 1u);
-      } else {
-        const unsigned long long t0 = gb_now();
-        while (__ldcg(bar + 1) == g0) {
-          if (gb_now() - t0 > GB_WAIT_NS) {
-            *okflag = 0;
-            break;
-          }
-          __nanosleep(64);
-        }
-      }
-      __threadfence();
-    }
-  }
-  __syncthreads();
-  return *okflag != 0;
 }
 
 // Householder tridiagonalisation over the whole GPU for large n (one

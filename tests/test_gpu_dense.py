@@ -2,8 +2,9 @@
 Gram-Schmidt through the blocked FP64 Cholesky and triangular inverse
 (schmidt2 + rsdecmp/rsinvcd, schmidt.f90:117-544) and the subspace
 eigen-decomposition + rotation (untryt2/untryhc2, eigen.f90:1171-1451),
-against the oracle.  nb = 160 is the Si64 band count (matrix in shared
-memory); nb = 200 exceeds shared memory and runs from global memory.
+against the oracle.  nb = 160 is the Si64 band count (matrix in one CTA's
+registers); nb = 200 exceeds one SM and runs on the cooperative kernels that
+spread the columns over one CTA per SM.
 
 Tolerances: FP64 1e-10 (orthonormalised bands), eigenvalues 1e-10 relative;
 mixed precision (FP32 bands, 3xTF32 tensor-core contractions, FP64
@@ -39,17 +40,20 @@ def test_schmidt_many_blocks(si8, nb, prec, tol):
     assert np.max(np.abs(s - np.eye(nb))) < (1e-10 if prec == QX_PREC_FP64 else 1e-4)
 
 
-def test_schmidt_reports_first_bad_pivot_in_later_block(si8):
+@pytest.mark.parametrize("nb,bad", [(100, 70), (200, 170)])
+def test_schmidt_reports_first_bad_pivot_in_later_block(si8, nb, bad):
+    """A zero band gives a zero Cholesky pivot at its row and the error names
+    it.  nb = 100 runs the one-CTA register kernel, nb = 200 the cooperative
+    whole-GPU kernel."""
     need_gpu()
-    nb = 100
     c = cell.random_wavefunctions(si8.gs.nplwex, nb)
-    c[70] = 0.0                      # the pivot of row 70 (third 32-wide block) is zero
+    c[bad] = 0.0
     ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE, nband=nb)
     try:
         with pytest.raises(QxError) as e:
             ctx.schmidt_host(c)
         assert e.value.code == 3
-        assert "band 70" in str(e.value)
+        assert "band %d" % bad in str(e.value)
     finally:
         ctx.close()
 
