@@ -8,8 +8,10 @@
 // blocks factored inside one warp, panel and trailing updates spread over
 // the CTA, one warp per eigenvalue for multisection, one warp per column for
 // the back-transformation.  Matrices live in shared memory (odd leading
-// dimension) when they fit and in global memory (L2) otherwise.  No wait in
-// these kernels depends on another block.
+// dimension) when they fit and in global memory (L2) otherwise.  For large
+// n the Cholesky and the tridiagonalisation spread the columns over one CTA
+// per SM in a cooperative launch, with bounded grid barriers; no other wait
+// in these kernels depends on another block.
 #include <algorithm>
 
 #include "qx_internal.h"
