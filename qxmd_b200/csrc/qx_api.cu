@@ -748,9 +748,10 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
       cm = nullptr;
       nd = nullptr;
     }
+    // proj = D <beta|c>: the KB energies D (vclalp) scale the rows in the
+    // contraction's epilogue
     TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, cm, nd, kst,
-                c->gws, c->gws_bytes));
-    scale_rows<T>(np, ncol_max, proj, np, b.vclalp, cm, nd, kst);
+                c->gws, c->gws_bytes, (const T *)b.vclalp));
     TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, beta_out, out, c->ne, 0, cm, nd,
                 kst, c->gws, c->gws_bytes));
     CKL();

@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "qx_internal.h"
+#include "qx_cg.h"
 
 namespace qx {
 
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(RD_T) k_gemm_reduce(int M, int N, int nsplit, 
                                                       long lda, const T *__restrict__ B, long ldb, T beta,
                                                       T *__restrict__ Cm, long ldc, int gamma,
                                                       const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
-                                                      const T *__restrict__ W) {
+                                                      const T *__restrict__ W, const T *__restrict__ rowscale) {
   __shared__ T ws[RD_T / 32][32];
   const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -151,6 +152,7 @@ __global__ void __launch_bounds__(RD_T) k_gemm_reduce(int M, int N, int nsplit, 
       v -= (T)2 * a1 * b1;
     }
   }
+  if (rowscale) v *= rowscale[gm];
   T *c = Cm + cn * ldc + gm;
   *c = (beta == (T)0) ? alpha * v : alpha * v + beta * *c;
 }
@@ -171,19 +173,20 @@ static void launch(dim3 g, int M, int N, int K, T alpha, const T *A, long lda, c
   note_launch();
   const long mn = (long)M * N;
   k_gemm_reduce<T, TA, TB><<<(int)((mn + 31) / 32), RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc,
-                                                                    gamma, colmap, ncol_dev, W);
+                                                                    gamma, colmap, ncol_dev, W, nullptr);
   note_launch();
 }
 
 // Finish FP32 split-K partials W[z][n][m] (any producer with that layout).
 void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
-                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st) {
+                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st,
+                     const float *rowscale) {
   const long mn = (long)M * N;
   const int g = (int)((mn + 31) / 32);
-  if (ta && tb) k_gemm_reduce<float, true, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else if (ta) k_gemm_reduce<float, true, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else if (tb) k_gemm_reduce<float, false, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
-  else k_gemm_reduce<float, false, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W);
+  if (ta && tb) k_gemm_reduce<float, true, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W, rowscale);
+  else if (ta) k_gemm_reduce<float, true, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W, rowscale);
+  else if (tb) k_gemm_reduce<float, false, true><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W, rowscale);
+  else k_gemm_reduce<float, false, false><<<g, RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, nullptr, nullptr, W, rowscale);
   note_launch();
 }
 
@@ -194,11 +197,13 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
 // nsplit*M*N elements.
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
-         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes) {
+         long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes,
+         const T *rowscale) {
   if (M <= 0 || N <= 0) return 0;
+  if (rowscale && beta != (T)0) { set_error("gemm: a row scale needs beta = 0"); return 1; }
   if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0) {
     const int r = tc_gemm(ta, tb, M, N, K, (float)alpha, (const float *)A, lda, (const float *)B, ldb, (float)beta,
-                          (float *)C, ldc, gamma, st, ws, ws_bytes);
+                          (float *)C, ldc, gamma, st, ws, ws_bytes, (const float *)rowscale);
     if (r == 0) return 0;
     if (r > 0) {
       set_error("tensor-core GEMM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -226,13 +231,14 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
   else if (ta) launch<T, true, false>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
   else if (tb) launch<T, false, true>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
   else launch<T, false, false>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, nsplit, kchunk, W, st);
+  if (rowscale) scale_rows<T>(M, N, C, ldc, rowscale, colmap, ncol_dev, st);
   return 0;
 }
 
 template int gemm<float>(bool, bool, int, int, int, float, const float *, long, const float *, long, float, float *,
-                         long, int, const int *, const int *, cudaStream_t, void *, size_t);
+                         long, int, const int *, const int *, cudaStream_t, void *, size_t, const float *);
 template int gemm<double>(bool, bool, int, int, int, double, const double *, long, const double *, long, double,
-                          double *, long, int, const int *, const int *, cudaStream_t, void *, size_t);
+                          double *, long, int, const int *, const int *, cudaStream_t, void *, size_t, const double *);
 
 }  // namespace qx
 

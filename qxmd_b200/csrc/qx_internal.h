@@ -127,16 +127,17 @@ int init_fft_roots();
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws = nullptr,
-         size_t ws_bytes = 0);
+         size_t ws_bytes = 0, const T *rowscale = nullptr);
 
 void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
-                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st);
+                     long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st,
+                     const float *rowscale = nullptr);
 
 // qx_tcgemm.cu: tcgen05 3xTF32 GEMM with gemm<float>'s semantics (no column
 // map).  Returns 0 launched, -1 operands unsuitable (use the CUDA-core
 // kernel), > 0 launch error.
 int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
-            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes);
+            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes, const float *rowscale = nullptr);
 bool tc_enabled();
 // Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
 int tc_error_take();

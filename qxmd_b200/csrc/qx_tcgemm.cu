@@ -189,6 +189,7 @@ struct TcArgs {
   long ldc;
   int gamma;             // 0 plain, 1 Gamma metric, 2 KB projection metric
   float *W;              // split-K partials W[z][n][m], or null: write C
+  const float *rowscale; // C(m, :) scaled by rowscale[m] (beta = 0), or null
 };
 
 // Round to the nearest TF32 value (10 stored mantissa bits; ties away from
@@ -456,6 +457,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       const bool ok = !abort_flag;
       const float alpha = p.alpha, beta = p.beta;
+      const float rs = (direct && p.rowscale && gm < p.M) ? p.rowscale[gm] : 1.f;
       if (ok && gm < p.M) {
   #pragma unroll
         for (int c = 0; c < BN / 16; ++c) {
@@ -482,6 +484,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 v = 2.f * v - a0 * sb0[c * 16 + j];
                 if (p.gamma == 2) v -= 2.f * a1 * sb1[c * 16 + j];
               }
+              if (p.rowscale) v *= rs;
               cp[(long)j * p.ldc] = (beta == 0.f) ? alpha * v : alpha * v + beta * old[j];
             }
           }
@@ -589,7 +592,8 @@ void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit
 // Returns 0 when launched, -1 when the operands do not meet the TMA rules
 // (the caller then uses the CUDA-core kernel), >0 on error.
 int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
-            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes) {
+            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes,
+            const float *rowscale) {
   using tc::BM;
   using tc::BK;
   if (!tc::enabled() || M <= 0 || N <= 0 || K <= 0) return -1;
@@ -620,7 +624,8 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   while (nsplit > 1 && (size_t)nsplit * M * N * sizeof(float) > ws_bytes) --nsplit;
   const int kps = (nkb + nsplit - 1) / nsplit;
   nsplit = (nkb + kps - 1) / kps;
-  tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr};
+  tc::TcArgs a{M, N, K, kps, alpha, beta, A, lda, B, ldb, C, ldc, gamma, nsplit > 1 ? (float *)ws : nullptr,
+               rowscale};
   dim3 g(tm, tn, nsplit);
   int rc;
   if (bn == 96) {
@@ -632,7 +637,8 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   }
   if (rc) return rc;
   if (nsplit > 1)
-    gemm_reduce_f32(ta, tb, M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, (const float *)ws, st);
+    gemm_reduce_f32(ta, tb, M, N, nsplit, alpha, A, lda, B, ldb, beta, C, ldc, gamma, (const float *)ws, st,
+                    rowscale);
   return 0;
 }
 
