@@ -1476,7 +1476,10 @@ __global__ void k_invit(const double *__restrict__ dg, const double *__restrict_
     WS(0, n - 1) = recip2_nr((fabs(a) < tiny) ? tiny : a);
     // start vector: ones with a member-dependent pattern
     for (int i = 0; i < n; ++i) WS(5, i) = 1.0 + 0.01 * (double)((i * (c + 3)) % 7);
-    for (int it = 0; it < 3; ++it) {
+    // an isolated eigenvalue (bisected to 2 eps |T|) needs two solves; the
+    // members of a cluster, re-orthogonalised each round, get three
+    const int nit = (tend - t == 1) ? 2 : 3;
+    for (int it = 0; it < nit; ++it) {
       // forward: row interchanges and multipliers
       double zi = WS(5, 0);
 #pragma unroll 4
