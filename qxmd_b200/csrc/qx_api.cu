@@ -78,6 +78,10 @@ struct qx_ctx {
   void *proj = nullptr;    // nproj*nb in T
   void *gws = nullptr;     // split-K GEMM workspace
   size_t gws_bytes = 0;
+  // FP32 contractions whose band arrays have a row stride (nplwex) that is not
+  // a multiple of four floats: room to restage operands for the tensor maps
+  void *tcpad = nullptr;
+  size_t tcpad_bytes = 0;
   CgState cg;
   // density side
   double *d_rho_in = nullptr, *d_rho_out = nullptr, *d_vloc = nullptr, *d_glocal = nullptr, *d_g2 = nullptr;
@@ -265,6 +269,20 @@ static int alloc_pipe(qx_ctx *c) {
   return 0;
 }
 
+// Restaging room for the tensor-core contractions when nplwex is not a
+// multiple of four (rows of band arrays then break the 16-byte stride rule
+// of the tensor maps): `rows` rows of nplwex rounded up to four floats.
+static int tcpad_reserve(qx_ctx *c, long rows) {
+  if (c->prec != QX_PREC_MIXED || (c->ne & 3) == 0) return 0;
+  const size_t need = sizeof(float) * (size_t)rows * (size_t)((c->ne + 3) & ~3L);
+  if (need <= c->tcpad_bytes) return 0;
+  void *p = nullptr;
+  TRY(dalloc(c, &p, need));
+  c->tcpad = p;
+  c->tcpad_bytes = need;
+  return 0;
+}
+
 extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, int nplw, const int *ijkgd,
                          const double *dkgnrm, int nband, void *stream) {
   if (!out || !ijkgd || !dkgnrm || k1 <= 0 || k2 <= 0 || k3 <= 0 || nplw < 0 || nband <= 0 ||
@@ -419,6 +437,7 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   FAIL(dalloc(c, &c->mat_t, ts * nb * nb));
   c->gws_bytes = sizeof(double) * (size_t)64 * 1024 * 1024 / 8;   // 64 MB
   FAIL(dalloc(c, &c->gws, c->gws_bytes));
+  FAIL(tcpad_reserve(c, 2L * nb));
   cudaMemset(c->psi, 0, blk);
   cudaMemset(c->hpsi, 0, blk);
   // CG state
@@ -535,6 +554,7 @@ extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const doub
   TRY(up(c, kbg, eqlmr, (long)nproj * c->ne));
   TRY(up(c, vcl, vclalp, nproj));
   c->pl.nproj = nproj;
+  TRY(tcpad_reserve(c, (long)nproj + c->nb));
   if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
   else { c->pl.b32.kbg = (float *)kbg; c->pl.b32.vclalp = (float *)vcl; }
   c->proj = proj;
@@ -751,9 +771,9 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
     // proj = D <beta|c>: the KB energies D (vclalp) scale the rows in the
     // contraction's epilogue
     TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, cm, nd, kst,
-                c->gws, c->gws_bytes, (const T *)b.vclalp));
+                c->gws, c->gws_bytes, (const T *)b.vclalp, c->tcpad, c->tcpad_bytes));
     TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, beta_out, out, c->ne, 0, cm, nd,
-                kst, c->gws, c->gws_bytes));
+                kst, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
     CKL();
     return 0;
   };
@@ -832,7 +852,7 @@ static int hmatrix_impl(qx_ctx *c, double *hsub) {
   T *m = (T *)c->mat_t;
   // m(j, i) = <psi_j | hpsi_i>
   TRY(gemm<T>(true, false, nb, nb, c->ne, (T)1, (const T *)c->psi, c->ne, (const T *)c->hpsi, c->ne, (T)0, m, nb, 1,
-              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   symmetrize_lower<T>(m, c->d_hsub, c->d_eig, nb, c->st);
   CKL();
   c->have_hsub = true;
@@ -877,7 +897,7 @@ static int rotate(qx_ctx *c, void *&arr) {
   const int nb = c->nb;
   const T *U = (const T *)c->mat_t;
   TRY(gemm<T>(false, false, c->ne, nb, nb, (T)1, (const T *)arr, c->ne, U, nb, (T)0, (T *)c->tmp, c->ne, 0, nullptr,
-              nullptr, c->st, c->gws, c->gws_bytes));
+              nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   CKL();
   std::swap(arr, c->tmp);
   return 0;
@@ -937,9 +957,9 @@ static int eigen_impl(qx_ctx *c, const qx_cgparm *p, int *nriter, int *nhpsi_out
   for (int it = 0; it < maxit; ++it) {
     cg_prec<T>(nb, ne, ne, g, h, c->d_dk, s, c->st);
     // subgs3: Pm = snap^T h ; Pm masked to j < i, active i ; h -= snap * Pm
-    TRY(gemm<T>(true, false, nb, nb, ne, (T)1, snap, ne, h, ne, (T)0, pm_t, nb, 1, nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+    TRY(gemm<T>(true, false, nb, nb, ne, (T)1, snap, ne, h, ne, (T)0, pm_t, nb, 1, nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
     cg_mask<T>(nb, pm_t, s, c->st);
-    TRY(gemm<T>(false, false, ne, nb, nb, (T)-1, snap, ne, pm_t, nb, (T)1, h, ne, 0, nullptr, nullptr, c->st));
+    TRY(gemm<T>(false, false, ne, nb, nb, (T)-1, snap, ne, pm_t, nb, (T)1, h, ne, 0, nullptr, nullptr, c->st, nullptr, 0, nullptr, c->tcpad, c->tcpad_bytes));
     cg_orth<T>(nb, ne, ne, x, hx, h, s, c->st);
     cg_list(nb, s, c->st);
     CKL();
@@ -1091,7 +1111,7 @@ static int schmidt_impl(qx_ctx *c) {
   const int nb = c->nb, ne = c->ne;
   T *m = (T *)c->mat_t;
   TRY(gemm<T>(true, false, nb, nb, ne, (T)1, (const T *)c->psi, ne, (const T *)c->psi, ne, (T)0, m, nb, 1, nullptr,
-              nullptr, c->st, c->gws, c->gws_bytes));
+              nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
   TRY(cholinv(c->d_mat, nb, c->d_eigws, c->d_info + 1, c->st));
   CKL();
@@ -1105,7 +1125,7 @@ static int schmidt_impl(qx_ctx *c) {
   convert<double, T>(c->d_mat, m, (long)nb * nb, c->st);
   // psi <- psi * Linv^T
   TRY(gemm<T>(false, true, ne, nb, nb, (T)1, (const T *)c->psi, ne, m, nb, (T)0, (T *)c->tmp, ne, 0, nullptr, nullptr,
-              c->st));
+              c->st, nullptr, 0, nullptr, c->tcpad, c->tcpad_bytes));
   CKL();
   std::swap(c->psi, c->tmp);
   return 0;
@@ -1450,7 +1470,7 @@ extern "C" int qx_autotune(qx_ctx *c, char *report, int report_len) {
         const int r = time_ms(c->st, [&]() {
           return gemm<float>(sh.ta, sh.tb, sh.M, sh.N, sh.K, 1.f, (const float *)sh.A, sh.lda, (const float *)sh.B,
                              sh.ldb, sh.beta, (float *)c->tmp, sh.ldc, sh.gamma, nullptr, nullptr, c->st, c->gws,
-                             c->gws_bytes);
+                             c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes);
         }, 3, &ms);
         tc_split_force = 0;
         TRY(r);
@@ -1526,7 +1546,7 @@ static int tddft_overlap_impl(qx_ctx *c, double *aij) {
   T *m = (T *)c->mat_t;
   // m(i, j) = <prev_i | psi_j> (column-major), Gamma metric: aijr(i, j) of the reference
   TRY(gemm<T>(true, false, nb, nb, c->ne, (T)1, (const T *)c->prev, c->ne, (const T *)c->psi, c->ne, (T)0, m, nb, 1,
-              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   convert<T, double>(m, c->d_mat, (long)nb * nb, c->st);
   CKL();
   if (aij) {
@@ -1619,9 +1639,9 @@ static int forces_impl(qx_ctx *c, double *floc, double *fnl) {
   const Bufs<T> &b = c->pl.bufs<T>();
   T *P = (T *)c->proj, *D = (T *)c->dproj;
   TRY(gemm<T>(true, false, np, nb, ne, (T)1, b.kbg, ne, (const T *)c->psi, ne, (T)0, P, np, 2, nullptr, nullptr,
-              c->st, c->gws, c->gws_bytes));
+              c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   TRY(gemm<T>(true, false, 3 * np, nb, ne, (T)1, (const T *)c->dtab, ne, (const T *)c->psi, ne, (T)0, D, 3 * np, 0,
-              nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+              nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   fnl_reduce<T>(natom, np / natom, np, nb, P, D, b.vclalp, c->d_occ, c->d_force + 3 * natom, c->st);
   CKL();
   std::vector<double> f(6 * (size_t)natom);
@@ -1668,9 +1688,9 @@ static int kbg_only(qx_ctx *c, const T *cin, T *out, int nb) {
   Bufs<T> &b = pl.bufs<T>();
   const int np = pl.nproj;
   T *proj = (T *)c->proj;
-  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st, c->gws, c->gws_bytes));
+  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   scale_rows<T>(np, nb, proj, np, b.vclalp, nullptr, nullptr, c->st);
-  TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st));
+  TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st, nullptr, 0, nullptr, c->tcpad, c->tcpad_bytes));
   CKL();
   return 0;
 }

@@ -198,12 +198,12 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes,
-         const T *rowscale) {
+         const T *rowscale, void *pad, size_t pad_bytes) {
   if (M <= 0 || N <= 0) return 0;
   if (rowscale && beta != (T)0) { set_error("gemm: a row scale needs beta = 0"); return 1; }
   if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0) {
     const int r = tc_gemm(ta, tb, M, N, K, (float)alpha, (const float *)A, lda, (const float *)B, ldb, (float)beta,
-                          (float *)C, ldc, gamma, st, ws, ws_bytes, (const float *)rowscale);
+                          (float *)C, ldc, gamma, st, ws, ws_bytes, (const float *)rowscale, pad, pad_bytes);
     if (r == 0) return 0;
     if (r > 0) {
       set_error("tensor-core GEMM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -236,9 +236,11 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
 }
 
 template int gemm<float>(bool, bool, int, int, int, float, const float *, long, const float *, long, float, float *,
-                         long, int, const int *, const int *, cudaStream_t, void *, size_t, const float *);
+                         long, int, const int *, const int *, cudaStream_t, void *, size_t, const float *, void *,
+                         size_t);
 template int gemm<double>(bool, bool, int, int, int, double, const double *, long, const double *, long, double,
-                          double *, long, int, const int *, const int *, cudaStream_t, void *, size_t, const double *);
+                          double *, long, int, const int *, const int *, cudaStream_t, void *, size_t, const double *,
+                          void *, size_t);
 
 }  // namespace qx
 

@@ -127,7 +127,7 @@ int init_fft_roots();
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws = nullptr,
-         size_t ws_bytes = 0, const T *rowscale = nullptr);
+         size_t ws_bytes = 0, const T *rowscale = nullptr, void *pad = nullptr, size_t pad_bytes = 0);
 
 void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, const float *A, long lda, const float *B,
                      long ldb, float beta, float *C, long ldc, int gamma, const float *W, cudaStream_t st,
@@ -137,7 +137,8 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
 // map).  Returns 0 launched, -1 operands unsuitable (use the CUDA-core
 // kernel), > 0 launch error.
 int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
-            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes, const float *rowscale = nullptr);
+            float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes, const float *rowscale = nullptr, void *pad = nullptr,
+            size_t pad_bytes = 0);
 bool tc_enabled();
 // Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
 int tc_error_take();

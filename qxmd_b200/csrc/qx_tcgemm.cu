@@ -588,18 +588,57 @@ void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit
   g_split[{(long)ta, (long)tb, M, N, K, gamma}] = nsplit;
 }
 
+namespace tc {
+// Rows of `inner` floats, `ld` apart, copied to rows `ldp` apart (ldp a
+// multiple of 4): an operand whose row stride breaks the 16-byte rule of the
+// tensor maps, restaged for the TMA.
+__global__ void k_pad_rows(const float *__restrict__ src, long ld, long inner, long rows, float *__restrict__ dst,
+                           long ldp) {
+  const long tot = rows * inner;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
+    const long r = q / inner, i = q - r * inner;
+    dst[r * ldp + i] = src[r * ld + i];
+  }
+}
+}  // namespace tc
+
 // Tensor-core FP32 GEMM with the semantics of gemm<float> (no column map).
 // Returns 0 when launched, -1 when the operands do not meet the TMA rules
-// (the caller then uses the CUDA-core kernel), >0 on error.
+// (the caller then uses the CUDA-core kernel), >0 on error.  pad (optional,
+// pad_bytes): room to restage an operand whose row stride is not a multiple
+// of four floats (or whose base is not 16-byte aligned) before the launch.
 int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
             float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes,
-            const float *rowscale) {
+            const float *rowscale, void *pad, size_t pad_bytes) {
   using tc::BM;
   using tc::BK;
   if (!tc::enabled() || M <= 0 || N <= 0 || K <= 0) return -1;
-  if (((uintptr_t)A & 15) || ((uintptr_t)B & 15) || (lda & 3) || (ldb & 3)) return -1;
   if (!tc::encode_ready()) return -1;
   // A: ta -> K contiguous (A[m*lda + k]); !ta -> M contiguous (A[k*lda + m])
+  {
+    const bool bad_a = ((uintptr_t)A & 15) || (lda & 3), bad_b = ((uintptr_t)B & 15) || (ldb & 3);
+    if (bad_a || bad_b) {
+      // restage into pad: rows of the contiguous extent, stride rounded up to 4
+      const long a_in = ta ? K : M, a_rows = ta ? M : K, b_in = tb ? N : K, b_rows = tb ? K : N;
+      const long a_ld = (a_in + 3) & ~3L, b_ld = (b_in + 3) & ~3L;
+      const size_t need = sizeof(float) * ((bad_a ? a_ld * a_rows : 0) + (bad_b ? b_ld * b_rows : 0));
+      if (!pad || ((uintptr_t)pad & 15) || need > pad_bytes) return -1;
+      float *dst = (float *)pad;
+      if (bad_a) {
+        tc::k_pad_rows<<<148 * 8, 256, 0, st>>>(A, lda, a_in, a_rows, dst, a_ld);
+        note_launch();
+        A = dst;
+        lda = a_ld;
+        dst += a_ld * a_rows;
+      }
+      if (bad_b) {
+        tc::k_pad_rows<<<148 * 8, 256, 0, st>>>(B, ldb, b_in, b_rows, dst, b_ld);
+        note_launch();
+        B = dst;
+        ldb = b_ld;
+      }
+    }
+  }
   const bool a_mn = !ta, b_mn = tb;
   const int tm = (M + BM - 1) / BM, nkb = (K + BK - 1) / BK;
   // 80-wide tiles for K-major B, 96-wide (three 32-column chunks) for MN-major B

@@ -94,3 +94,23 @@ def test_untryt_many_blocks(si8, nb, prec):
     gaps = np.minimum(np.diff(w_ref, prepend=-np.inf), np.diff(w_ref, append=np.inf))
     sep = gaps > 1e-6 * scale
     assert relerr(psi[sep], ref_psi[sep]) < (1e-8 if prec == QX_PREC_FP64 else 1e-3)
+
+
+def test_mixed_contractions_with_unaligned_band_stride():
+    """nplwex = 5042 is not a multiple of four floats, so the band arrays'
+    rows break the 16-byte stride rule of the tensor maps: the tensor-core
+    contractions restage their operands (Gram-Schmidt here: S = C^T C and
+    C L^-T), with the FP32 tolerance of the mixed path against the oracle."""
+    need_gpu()
+    s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), 170.0 / 4.0, 170.0, 48, with_ewald=False)
+    assert s.gs.nplwex % 4 == 2
+    c = cell.random_wavefunctions(s.gs.nplwex, 48)
+    ref, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    for _ in range(2):
+        ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, nband=48)
+        try:
+            q = ctx.schmidt_host(c)
+        finally:
+            ctx.close()
+        assert relerr(q, ref) < 1e-4
