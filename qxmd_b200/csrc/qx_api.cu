@@ -82,6 +82,11 @@ struct qx_ctx {
   // a multiple of four floats: room to restage operands for the tensor maps
   void *tcpad = nullptr;
   size_t tcpad_bytes = 0;
+  // FP32 KB projector table rows at stride nplwex rounded up to four floats
+  // (made once in qx_set_kb_g when nplwex % 4 != 0, so that the <beta|psi>
+  // contractions restage only the band operand)
+  float *kbgp = nullptr;
+  long kbgp_ld = 0;
   CgState cg;
   // density side
   double *d_rho_in = nullptr, *d_rho_out = nullptr, *d_vloc = nullptr, *d_glocal = nullptr, *d_g2 = nullptr;
@@ -544,6 +549,18 @@ extern "C" int qx_set_glocal(qx_ctx *c, const double *glocal) {
   return QX_OK;
 }
 
+// The KB projector table as a contraction operand: the padded FP32 copy
+// where there is one, else the table itself at stride nplwex.
+template <typename T>
+static const T *kbg_operand(const qx_ctx *c, long *ld) {
+  if (sizeof(T) == sizeof(float) && c->kbgp) {
+    *ld = c->kbgp_ld;
+    return (const T *)c->kbgp;
+  }
+  *ld = c->ne;
+  return c->pl.bufs<T>().kbg;
+}
+
 extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const double *vclalp) {
   if (!c || nproj <= 0 || !eqlmr || !vclalp) { set_error("qx_set_kb_g: bad arguments"); return QX_ERR_ARG; }
   const size_t ts = c->tsize();
@@ -555,8 +572,20 @@ extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const doub
   TRY(up(c, vcl, vclalp, nproj));
   c->pl.nproj = nproj;
   TRY(tcpad_reserve(c, (long)nproj + c->nb));
+  c->kbgp = nullptr;
+  c->kbgp_ld = 0;
   if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
-  else { c->pl.b32.kbg = (float *)kbg; c->pl.b32.vclalp = (float *)vcl; }
+  else {
+    c->pl.b32.kbg = (float *)kbg;
+    c->pl.b32.vclalp = (float *)vcl;
+    if (c->ne & 3) {
+      const long ldp = (c->ne + 3) & ~3L;
+      TRY(dalloc(c, &c->kbgp, sizeof(float) * (size_t)nproj * ldp));
+      pad_rows_f32((const float *)kbg, c->ne, c->ne, nproj, c->kbgp, ldp, c->st);
+      CKL();
+      c->kbgp_ld = ldp;
+    }
+  }
   c->proj = proj;
   c->have_kbg = true;
   return QX_OK;
@@ -770,9 +799,11 @@ static int hpsi_impl(qx_ctx *c, const T *cin, T *out, const int *pairs, const in
     }
     // proj = D <beta|c>: the KB energies D (vclalp) scale the rows in the
     // contraction's epilogue
-    TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, cm, nd, kst,
+    long kld = 0;
+    const T *kb = kbg_operand<T>(c, &kld);
+    TRY(gemm<T>(true, false, np, ncol_max, c->ne, (T)1, kb, kld, cin, c->ne, (T)0, proj, np, 2, cm, nd, kst,
                 c->gws, c->gws_bytes, (const T *)b.vclalp, c->tcpad, c->tcpad_bytes));
-    TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, b.kbg, c->ne, proj, np, beta_out, out, c->ne, 0, cm, nd,
+    TRY(gemm<T>(false, false, c->ne, ncol_max, np, (T)1, kb, kld, proj, np, beta_out, out, c->ne, 0, cm, nd,
                 kst, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
     CKL();
     return 0;
@@ -1638,7 +1669,9 @@ static int forces_impl(qx_ctx *c, double *floc, double *fnl) {
   CKL();
   const Bufs<T> &b = c->pl.bufs<T>();
   T *P = (T *)c->proj, *D = (T *)c->dproj;
-  TRY(gemm<T>(true, false, np, nb, ne, (T)1, b.kbg, ne, (const T *)c->psi, ne, (T)0, P, np, 2, nullptr, nullptr,
+  long kld = 0;
+  const T *kb = kbg_operand<T>(c, &kld);
+  TRY(gemm<T>(true, false, np, nb, ne, (T)1, kb, kld, (const T *)c->psi, ne, (T)0, P, np, 2, nullptr, nullptr,
               c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   TRY(gemm<T>(true, false, 3 * np, nb, ne, (T)1, (const T *)c->dtab, ne, (const T *)c->psi, ne, (T)0, D, 3 * np, 0,
               nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
@@ -1688,9 +1721,11 @@ static int kbg_only(qx_ctx *c, const T *cin, T *out, int nb) {
   Bufs<T> &b = pl.bufs<T>();
   const int np = pl.nproj;
   T *proj = (T *)c->proj;
-  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, b.kbg, c->ne, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
+  long kld = 0;
+  const T *kb = kbg_operand<T>(c, &kld);
+  TRY(gemm<T>(true, false, np, nb, c->ne, (T)1, kb, kld, cin, c->ne, (T)0, proj, np, 2, nullptr, nullptr, c->st, c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
   scale_rows<T>(np, nb, proj, np, b.vclalp, nullptr, nullptr, c->st);
-  TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, b.kbg, c->ne, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st, nullptr, 0, nullptr, c->tcpad, c->tcpad_bytes));
+  TRY(gemm<T>(false, false, c->ne, nb, np, (T)1, kb, kld, proj, np, (T)1, out, c->ne, 0, nullptr, nullptr, c->st, nullptr, 0, nullptr, c->tcpad, c->tcpad_bytes));
   CKL();
   return 0;
 }

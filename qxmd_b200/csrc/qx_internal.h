@@ -140,6 +140,9 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
             float beta, float *C, long ldc, int gamma, cudaStream_t st, void *ws, size_t ws_bytes, const float *rowscale = nullptr, void *pad = nullptr,
             size_t pad_bytes = 0);
 bool tc_enabled();
+// Copies `rows` rows of `inner` floats from stride ld to stride ldp (the
+// tensor maps' 16-byte row-stride rule wants ldp a multiple of four).
+void pad_rows_f32(const float *src, long ld, long inner, long rows, float *dst, long ldp, cudaStream_t st);
 // Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
 int tc_error_take();
 // autotuner hooks of the tensor-core GEMM: a per-shape K-split table and a

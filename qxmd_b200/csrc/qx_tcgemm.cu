@@ -592,15 +592,33 @@ namespace tc {
 // Rows of `inner` floats, `ld` apart, copied to rows `ldp` apart (ldp a
 // multiple of 4): an operand whose row stride breaks the 16-byte rule of the
 // tensor maps, restaged for the TMA.
+// One row per blockIdx.y (rows beyond gridDim.y in steps of it), pairs of
+// floats when both strides and both bases allow 8-byte accesses.
 __global__ void k_pad_rows(const float *__restrict__ src, long ld, long inner, long rows, float *__restrict__ dst,
                            long ldp) {
-  const long tot = rows * inner;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
-    const long r = q / inner, i = q - r * inner;
-    dst[r * ldp + i] = src[r * ld + i];
+  const bool pairs = ((ld | ldp) & 1) == 0 && (((uintptr_t)src | (uintptr_t)dst) & 7) == 0;
+  for (long r = blockIdx.y; r < rows; r += gridDim.y) {
+    const float *s = src + r * ld;
+    float *d = dst + r * ldp;
+    if (pairs) {
+      const long h = inner >> 1;
+      for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < h; i += (long)gridDim.x * blockDim.x)
+        reinterpret_cast<float2 *>(d)[i] = reinterpret_cast<const float2 *>(s)[i];
+      if ((inner & 1) && blockIdx.x == 0 && threadIdx.x == 0) d[inner - 1] = s[inner - 1];
+    } else {
+      for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < inner; i += (long)gridDim.x * blockDim.x)
+        d[i] = s[i];
+    }
   }
 }
 }  // namespace tc
+
+void pad_rows_f32(const float *src, long ld, long inner, long rows, float *dst, long ldp, cudaStream_t st) {
+  if (rows <= 0 || inner <= 0) return;
+  tc::k_pad_rows<<<dim3((unsigned)std::min<long>(32, (inner / 2 + 255) / 256 + 1), (unsigned)std::min<long>(rows, 65535)),
+                   256, 0, st>>>(src, ld, inner, rows, dst, ldp);
+  note_launch();
+}
 
 // Tensor-core FP32 GEMM with the semantics of gemm<float> (no column map).
 // Returns 0 when launched, -1 when the operands do not meet the TMA rules
@@ -625,15 +643,13 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
       if (!pad || ((uintptr_t)pad & 15) || need > pad_bytes) return -1;
       float *dst = (float *)pad;
       if (bad_a) {
-        tc::k_pad_rows<<<148 * 8, 256, 0, st>>>(A, lda, a_in, a_rows, dst, a_ld);
-        note_launch();
+        pad_rows_f32(A, lda, a_in, a_rows, dst, a_ld, st);
         A = dst;
         lda = a_ld;
         dst += a_ld * a_rows;
       }
       if (bad_b) {
-        tc::k_pad_rows<<<148 * 8, 256, 0, st>>>(B, ldb, b_in, b_rows, dst, b_ld);
-        note_launch();
+        pad_rows_f32(B, ldb, b_in, b_rows, dst, b_ld, st);
         B = dst;
         ldb = b_ld;
       }

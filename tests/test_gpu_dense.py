@@ -99,8 +99,10 @@ def test_untryt_many_blocks(si8, nb, prec):
 def test_mixed_contractions_with_unaligned_band_stride():
     """nplwex = 5042 is not a multiple of four floats, so the band arrays'
     rows break the 16-byte stride rule of the tensor maps: the tensor-core
-    contractions restage their operands (Gram-Schmidt here: S = C^T C and
-    C L^-T), with the FP32 tolerance of the mixed path against the oracle."""
+    contractions restage their operands (Gram-Schmidt: S = C^T C and C L^-T;
+    the KB contractions <beta|psi> and K P read a padded copy of the projector
+    table made once), with the FP32 tolerances of the mixed path against the
+    oracle."""
     need_gpu()
     s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), 170.0 / 4.0, 170.0, 48, with_ewald=False)
     assert s.gs.nplwex % 4 == 2
@@ -111,6 +113,14 @@ def test_mixed_contractions_with_unaligned_band_stride():
         ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, nband=48)
         try:
             q = ctx.schmidt_host(c)
+            ctx.put_psi(q)
+            ctx.enonloc()
+            hq = ctx.get_hpsi()
+            kb = ctx.hckbpp_g_host(q, np.zeros_like(q))
         finally:
             ctx.close()
         assert relerr(q, ref) < 1e-4
+        h = oracle.Ham(s, QX_NL_GSPACE)
+        assert relerr(hq, h.hpsi(q)) < 2e-5
+        kref = np.array([h.hckbpp(q[b], np.zeros_like(q[b]))[0] for b in range(q.shape[0])])
+        assert relerr(kb, kref) < 2e-4
