@@ -249,6 +249,38 @@ def accuracy(acc, natom, iters):
     return out
 
 
+def kb_build_timing(sys_, ctx, R, W, flush):
+    """Per-geometry rebuild of the G-space KB projector tables on the device
+    (qx_build_kb_g: phases, setbgq into the context's table, as an MD step
+    needs), the atoms moved a little every call; CUDA-event time per build
+    and the table bytes written (FP32 table, plus its padded copy when
+    nplwex % 4 != 0)."""
+    import torch
+
+    from qxmd_b200 import cell
+    b = cell.kb_builder_tables(sys_.gs, sys_.cell, sys_.pp)
+    ctx.set_kb_builder(b)
+    rng = np.random.default_rng(11)
+    geoms = [b["satm"] + rng.uniform(-0.005, 0.005, b["satm"].shape) for _ in range(R + W)]
+    for g in geoms[:W]:
+        ctx.build_kb_g(b["ityp"], g)
+    ctx.sync()
+    t = 0.0
+    for g in geoms[W:]:
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.build_kb_g(b["ityp"], g)
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1)
+    nproj, ne = b["lmx"] * sys_.cell.natom, sys_.gs.nplwex
+    nbytes = 4 * nproj * ne * (2 if ne % 4 else 1)
+    ms = t / R
+    return {"ms_per_geometry": ms, "table_bytes_written": nbytes, "gb_per_s": nbytes / (ms * 1e-3) / 1e9,
+            "builds_timed": R}
+
+
 def run_si512(args):
     """H|psi> band applications per second (kinetic + local + G-space KB, all
     1100 bands: qx_enonloc) on the Si512 cell, 96^3 grid, mixed and FP64;
@@ -312,6 +344,7 @@ def run_si512(args):
     out["scf_mixed"] = {"value": R / (t / 1e3), "unit": "iter/s", "ms_per_iter": t / R,
                         "cg_bapps_per_iter": nh / R, "etot_last_ry": r["etot"],
                         "iterations_before": max(1, args.warmup)}
+    out["kb_tables"] = kb_build_timing(sys_, ctx, max(3, args.steps), max(3, args.warmup), flush)
     ctx.close()
     print(json.dumps(out), flush=True)
 
@@ -515,6 +548,9 @@ def run_ours(args):
                                     "eig": ref_ctx.get_eig(), "ms": e0.elapsed_time(e1)}
             ref_ctx.close()
         ctx.close()
+    kb_ctx = Context(sys_, QX_PREC_MIXED, QX_NL_GSPACE)
+    kb_tables = kb_build_timing(sys_, kb_ctx, max(3, K), max(3, W), flush)
+    kb_ctx.close()
     mixed, fp64, fp64b = res["mixed"], res["fp64"], res["fp64_batched"]
     batch = run_batch(K, W) if ws == 1 else None
     hbm, peak_kind = peaks()
@@ -537,6 +573,7 @@ def run_ours(args):
                          "value": fp64b["value"], "ms_per_step": fp64b["ms_per_step"],
                          "cg_bapps_per_iter": fp64b["cg_bapps_per_iter"]},
         "batch48": batch,
+        "kb_tables": kb_tables,
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "mixed_over_fp64_batched": mixed["value"] / fp64b["value"],
         "accuracy": accuracy(acc, sys_.cell.natom, args.accuracy_iters),

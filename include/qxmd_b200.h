@@ -89,6 +89,26 @@ int qx_set_glocal(qx_ctx *ctx, const double *glocal);
 /* G-space KB tables, eqlmr_(nplwex, nproj) and vclalp(nproj)
  * (setbgq nlkbpp.f90:2135-2187, setnlc_g nlkbpp.f90:1236-1279). */
 int qx_set_kb_g(qx_ctx *ctx, int nproj, const double *eqlmr, const double *vclalp);
+/* The same tables built on the device, for MD steps.  Once per cell
+ * (setqlm nlkbpp.f90:2196-2247 with tbqlma of ppkb.f90:3228-3236):
+ *   ntype species of lmx projector channels each, channel ch = l + lmx * it;
+ *   tbqlm((mxqlm + 1), lmx * ntype): radial tables at |G| = k * dlqlm(it);
+ *   qlm((nplw + 1), nlm): angular factors; channel ch uses column lmidx[ch];
+ *   even[ch]: 1 for even l (litoll: cos/-sin), 0 for odd l (-sin/-cos);
+ *   vclalp(lmx * ntype): KB energy of each channel;
+ *   ngabc(3, nplw + 1): integer coordinates of the half-sphere G vectors.
+ * The radial table must reach the largest |G| (2 int(|G|/(2 dl)) + 2 <= mxqlm). */
+int qx_set_kb_builder(qx_ctx *ctx, int ntype, int lmx, int mxqlm, const double *dlqlm, const double *tbqlm, int nlm,
+                      const double *qlm, const int *lmidx, const int *even, const double *vclalp, const int *ngabc);
+/* Once per geometry (setbgq nlkbpp.f90:2135-2187 with the phases of
+ * stscfn_pw pwlda.f90:5711-5850): eqlmr_ and vclalp of natom atoms of
+ * species ityp(natom) (0-based) at fractional coordinates satm(3, natom),
+ * projector j = l + lmx * a.  Reuses the table buffers when the projector
+ * count is unchanged, so captured SCF-iteration graphs stay valid. */
+int qx_build_kb_g(qx_ctx *ctx, int natom, const int *ityp, const double *satm);
+/* Reads back the G-space KB tables in use (eqlmr_(nplwex, nproj), vclalp(nproj);
+ * either pointer may be null), converted to double. */
+int qx_get_kb_g(qx_ctx *ctx, double *eqlmr, double *vclalp);
 /* Real-space KB tables (setnlc nlkbppr.f90:1010-1768, used by calnlc
  * nlkbppr.f90:1773-1900): atom a owns points off[a]..off[a+1]-1 with
  * zero-based grid index mesh[] and projector values vnl[point*lmx + l];

@@ -1,0 +1,74 @@
+"""ORACLE -- test infrastructure only.  The G-space KB projector table
+eqlmr_ restated in numpy (FP64) from the reference's table builders:
+
+* setqlm (nlkbpp.f90:2196-2247): radial table tbqlm at |G| by the
+  three-point forward-difference interpolation, m = 2 int(|G|/(2 dl)),
+  d = (|G|/dl - m)/2, f = d((d-1) a_m + t_{m+2} - t_m) + t_m, with
+  a_m = tbqlma = 2(t_m + t_{m+2} - 2 t_{m+1}) (ppkb.f90:3228-3236), times the
+  channel's angular factor;
+* stscfn_pw (pwlda.f90:5711-5850): cos/sin(G.R_a) composed from the
+  per-dimension angle-addition tables (phase_tables of oracle.forces);
+* setbgq (nlkbpp.f90:2135-2187): even l -> (cos f, -sin f), odd l ->
+  (-sin f, -cos f) per half-sphere G, projector j = l + lmx * a.
+
+PARITY UNPINNED as the rest of the oracle; the tests tie this builder to the
+analytic model tables that the H|psi> parity tests use.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .forces import phase_tables
+
+
+def setqlm(ag: np.ndarray, dl: float, tb: np.ndarray, ang: np.ndarray) -> np.ndarray:
+    """Interpolated radial table times the angular factor at |G| = ag."""
+    m = 2 * (ag / (2.0 * dl)).astype(np.int64)
+    d = 0.5 * (ag / dl - m)
+    t0, t1, t2 = tb[m], tb[m + 1], tb[m + 2]
+    a = 2.0 * (t0 + t2 - 2.0 * t1)
+    return (d * ((d - 1.0) * a + t2 - t0) + t0) * ang
+
+
+def structure_phases(satm: np.ndarray, ngabc: np.ndarray):
+    """ycos, ysin (natom, nG) of stscfn_pw for integer G coordinates ngabc (nG, 3)."""
+    kmax = int(np.abs(ngabc).max())
+    dcq, dsq = phase_tables(satm, kmax)
+    k = ngabc + kmax
+    nat = satm.shape[0]
+    yc = np.empty((nat, ngabc.shape[0]))
+    ys = np.empty_like(yc)
+    for a in range(nat):
+        c1, c2, c3 = dcq[a, 0, k[:, 0]], dcq[a, 1, k[:, 1]], dcq[a, 2, k[:, 2]]
+        s1, s2, s3 = dsq[a, 0, k[:, 0]], dsq[a, 1, k[:, 1]], dsq[a, 2, k[:, 2]]
+        cc12 = c1 * c2 - s1 * s2
+        sc12 = s1 * c2 + c1 * s2
+        yc[a] = cc12 * c3 - sc12 * s3
+        ys[a] = sc12 * c3 + cc12 * s3
+    return yc, ys
+
+
+def setbgq(b: dict, ityp: np.ndarray, satm: np.ndarray):
+    """eqlmr_ (nplwex, nproj) and vclalp (nproj) from the builder arguments
+    b (the dict of qxmd_b200.cell.kb_builder_tables) and a geometry."""
+    ag = np.sqrt(b["g2"])
+    lmx, ntype = b["lmx"], b["ntype"]
+    zzz = np.empty((ntype * lmx, ag.size))
+    for ch in range(ntype * lmx):
+        zzz[ch] = setqlm(ag, b["dlqlm"][ch // lmx], b["tbqlm"][ch], b["qlm"][b["lmidx"][ch]])
+    yc, ys = structure_phases(satm, b["ngabc"])
+    nat = satm.shape[0]
+    tab = np.zeros((2 * ag.size, lmx * nat))
+    vcl = np.zeros(lmx * nat)
+    for a in range(nat):
+        it = int(ityp[a])
+        for l in range(lmx):
+            ch = l + lmx * it
+            f = zzz[ch]
+            j = l + lmx * a
+            if b["even"][ch]:
+                tab[0::2, j], tab[1::2, j] = yc[a] * f, -ys[a] * f
+            else:
+                tab[0::2, j], tab[1::2, j] = -ys[a] * f, -yc[a] * f
+            vcl[j] = b["vclalp"][ch]
+    return tab, vcl

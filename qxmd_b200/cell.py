@@ -360,6 +360,31 @@ def kb_tables_g(gs: GSphere, cell: Cell, pp: ModelPP):
     return tab, vclalp
 
 
+def kb_builder_tables(gs: GSphere, cell: Cell, pp: ModelPP, dl: float = 0.005) -> dict:
+    """Arguments of qx_set_kb_builder / qx_build_kb_g for the model
+    pseudopotential (one species): radial tables tbqlm on |G| = k dl (s:
+    F_0 Y_00; p: F_1/|G| Y_1, so that the angular factor of p_m is G_m), the
+    angular factors qlm (1, gx, gy, gz) per half-sphere G, the parities of
+    setbgq and the KB energies; plus the geometry (fractional coordinates)
+    and |G|^2 for the oracle.  Arrays are in numpy row-major order of the
+    C interface's column-major arguments."""
+    n = gs.nplw
+    g2 = np.ascontiguousarray(gs.recnrm[: n + 1])
+    mxqlm = 2 * int(math.sqrt(float(g2.max())) / (2.0 * dl)) + 6
+    k = np.arange(mxqlm + 1) * dl
+    f0, f1g = pp.radial_g(k)
+    tbqlm = np.ascontiguousarray(np.stack([f0 * Y00, f1g * Y1, f1g * Y1, f1g * Y1]))
+    g = gs.gvec[: n + 1]
+    qlm = np.ascontiguousarray(np.stack([np.ones(n + 1), g[:, 0], g[:, 1], g[:, 2]]))
+    satm = np.ascontiguousarray(np.linalg.solve(gs.rba, cell.pos.T).T)
+    return dict(ntype=1, lmx=4, mxqlm=mxqlm, dlqlm=np.array([dl]), tbqlm=tbqlm, nlm=4, qlm=qlm,
+                lmidx=np.arange(4, dtype=np.int32), even=np.array([1, 0, 0, 0], dtype=np.int32),
+                vclalp=np.array([pp.e_s, pp.e_p, pp.e_p, pp.e_p]) / gs.rvol,
+                ngabc=np.ascontiguousarray(np.stack([gs.nga[: n + 1], gs.ngb[: n + 1], gs.ngc[: n + 1]],
+                                                    axis=1).astype(np.int32)),
+                ityp=np.zeros(cell.natom, dtype=np.int32), satm=satm, g2=g2)
+
+
 @dataclasses.dataclass
 class KBReal:
     """Real-space KB tables (the meaning of meshnl/npmsnl/numsnl/vnlcr in

@@ -131,6 +131,11 @@ struct qx_ctx {
   void *dtab = nullptr;    // 3 nproj x nplwex derivative tables (context precision)
   void *dproj = nullptr;   // 3 nproj x nb
   bool have_ftab = false;
+  // G-space KB table builder (qx_set_kb_builder, qx_build_kb_g)
+  int kb_ntype = 0, kb_lmx = 0, kb_km[3] = {0, 0, 0}, kb_ktot = 0, kb_natom_cap = 0;
+  double *d_kb_zzz = nullptr, *d_kb_vclt = nullptr, *d_kb_dcq = nullptr, *d_kb_dsq = nullptr, *d_kb_satm = nullptr;
+  int *d_kb_even = nullptr, *d_kb_ngabc = nullptr, *d_kb_ityp = nullptr;
+  bool have_kb_builder = false;
   bool defer = false;
   struct ScfGraph {
     std::vector<char> key;
@@ -589,6 +594,142 @@ extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const doub
   c->proj = proj;
   c->have_kbg = true;
   return QX_OK;
+}
+
+extern "C" int qx_set_kb_builder(qx_ctx *c, int ntype, int lmx, int mxqlm, const double *dlqlm, const double *tbqlm,
+                                 int nlm, const double *qlm, const int *lmidx, const int *even, const double *vclalp,
+                                 const int *ngabc) {
+  if (!c || ntype <= 0 || lmx <= 0 || mxqlm < 2 || nlm <= 0 || !dlqlm || !tbqlm || !qlm || !lmidx || !even ||
+      !vclalp || !ngabc) {
+    set_error("qx_set_kb_builder: bad arguments");
+    return QX_ERR_ARG;
+  }
+  if (lmx > 256) { set_error("qx_set_kb_builder: at most 256 projectors per atom"); return QX_ERR_ARG; }
+  const int nplw1 = c->ne / 2, nchan = lmx * ntype;
+  for (int i = 0; i < nchan; ++i)
+    if (lmidx[i] < 0 || lmidx[i] >= nlm) { set_error("qx_set_kb_builder: lmidx out of range"); return QX_ERR_ARG; }
+  // the interpolation reads t_{m+2}: the table must reach the largest |G|
+  std::vector<double> dk(c->ne);
+  CK(cudaMemcpy(dk.data(), c->d_dk, sizeof(double) * c->ne, cudaMemcpyDeviceToHost));
+  double g2max = 0.0;
+  for (int g = 0; g < nplw1; ++g) g2max = std::max(g2max, dk[2 * g]);
+  for (int it = 0; it < ntype; ++it) {
+    if (!(dlqlm[it] > 0.0)) { set_error("qx_set_kb_builder: dlqlm must be positive"); return QX_ERR_ARG; }
+    const double ag = std::sqrt(g2max);
+    const long m = 2 * (long)(ag / (2.0 * dlqlm[it]));
+    if (m + 2 > mxqlm) { set_error("qx_set_kb_builder: radial table too short for the largest |G|"); return QX_ERR_ARG; }
+  }
+  int km[3] = {0, 0, 0};
+  for (long i = 0; i < 3L * nplw1; ++i) km[i % 3] = std::max(km[i % 3], std::abs(ngabc[i]));
+  double *d_dl = nullptr, *d_tb = nullptr, *d_qlm = nullptr;
+  int *d_lmidx = nullptr;
+  TRY(dalloc(c, &d_dl, sizeof(double) * ntype));
+  TRY(dalloc(c, &d_tb, sizeof(double) * (size_t)(mxqlm + 1) * nchan));
+  TRY(dalloc(c, &d_qlm, sizeof(double) * (size_t)nplw1 * nlm));
+  TRY(dalloc(c, &d_lmidx, sizeof(int) * nchan));
+  TRY(dalloc(c, &c->d_kb_zzz, sizeof(double) * (size_t)nplw1 * nchan));
+  TRY(dalloc(c, &c->d_kb_even, sizeof(int) * nchan));
+  TRY(dalloc(c, &c->d_kb_vclt, sizeof(double) * nchan));
+  TRY(dalloc(c, &c->d_kb_ngabc, sizeof(int) * 3 * (size_t)nplw1));
+  CK(cudaMemcpyAsync(d_dl, dlqlm, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(d_tb, tbqlm, sizeof(double) * (size_t)(mxqlm + 1) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(d_qlm, qlm, sizeof(double) * (size_t)nplw1 * nlm, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(d_lmidx, lmidx, sizeof(int) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kb_even, even, sizeof(int) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kb_vclt, vclalp, sizeof(double) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kb_ngabc, ngabc, sizeof(int) * 3 * (size_t)nplw1, cudaMemcpyHostToDevice, c->st));
+  setqlm(nplw1, nchan, lmx, mxqlm, d_dl, d_tb, d_qlm, d_lmidx, c->d_dk, c->d_kb_zzz, c->st);
+  CKL();
+  c->kb_ntype = ntype;
+  c->kb_lmx = lmx;
+  for (int d = 0; d < 3; ++d) c->kb_km[d] = km[d];
+  c->kb_ktot = 2 * (km[0] + km[1] + km[2]) + 3;
+  c->kb_natom_cap = 0;
+  c->have_kb_builder = true;
+  return QX_OK;
+}
+
+extern "C" int qx_build_kb_g(qx_ctx *c, int natom, const int *ityp, const double *satm) {
+  if (!c || natom <= 0 || natom > 65535 || !ityp || !satm) { set_error("qx_build_kb_g: bad arguments"); return QX_ERR_ARG; }
+  if (!c->have_kb_builder) { set_error("qx_build_kb_g: qx_set_kb_builder first"); return QX_ERR_STATE; }
+  for (int a = 0; a < natom; ++a)
+    if (ityp[a] < 0 || ityp[a] >= c->kb_ntype) { set_error("qx_build_kb_g: ityp out of range"); return QX_ERR_ARG; }
+  const int lmx = c->kb_lmx, nproj = lmx * natom, ne = c->ne;
+  const size_t ts = c->tsize();
+  if (!c->have_kbg || c->pl.nproj != nproj) {
+    // first build (or a new projector count): the tables of qx_set_kb_g
+    void *kbg = nullptr, *vcl = nullptr, *proj = nullptr;
+    TRY(dalloc(c, &kbg, ts * (size_t)nproj * ne));
+    TRY(dalloc(c, &vcl, ts * nproj));
+    TRY(dalloc(c, &proj, ts * (size_t)nproj * c->nb));
+    c->pl.nproj = nproj;
+    TRY(tcpad_reserve(c, (long)nproj + c->nb));
+    c->kbgp = nullptr;
+    c->kbgp_ld = 0;
+    if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
+    else {
+      c->pl.b32.kbg = (float *)kbg;
+      c->pl.b32.vclalp = (float *)vcl;
+      if (ne & 3) {
+        c->kbgp_ld = (ne + 3) & ~3L;
+        TRY(dalloc(c, &c->kbgp, sizeof(float) * (size_t)nproj * c->kbgp_ld));
+      }
+    }
+    c->proj = proj;
+  }
+  if (natom > c->kb_natom_cap) {
+    TRY(dalloc(c, &c->d_kb_ityp, sizeof(int) * natom));
+    TRY(dalloc(c, &c->d_kb_satm, sizeof(double) * 3 * natom));
+    TRY(dalloc(c, &c->d_kb_dcq, sizeof(double) * (size_t)natom * c->kb_ktot));
+    TRY(dalloc(c, &c->d_kb_dsq, sizeof(double) * (size_t)natom * c->kb_ktot));
+    c->kb_natom_cap = natom;
+  }
+  CK(cudaMemcpyAsync(c->d_kb_ityp, ityp, sizeof(int) * natom, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kb_satm, satm, sizeof(double) * 3 * natom, cudaMemcpyHostToDevice, c->st));
+  const int *km = c->kb_km;
+  phase_tables(natom, c->d_kb_satm, km[0], km[1], km[2], c->kb_ktot, c->d_kb_dcq, c->d_kb_dsq, c->st);
+  if (c->prec == QX_PREC_FP64)
+    setbgq<double>(natom, ne / 2, ne, lmx, c->d_kb_ityp, c->d_kb_ngabc, c->d_kb_dcq, c->d_kb_dsq, km[0], km[1], km[2],
+                   c->kb_ktot, c->d_kb_zzz, c->d_kb_even, c->d_kb_vclt, c->pl.b64.kbg, nullptr, 0,
+                   c->pl.b64.vclalp, c->st);
+  else
+    setbgq<float>(natom, ne / 2, ne, lmx, c->d_kb_ityp, c->d_kb_ngabc, c->d_kb_dcq, c->d_kb_dsq, km[0], km[1], km[2],
+                  c->kb_ktot, c->d_kb_zzz, c->d_kb_even, c->d_kb_vclt, c->pl.b32.kbg, c->kbgp, c->kbgp_ld,
+                  c->pl.b32.vclalp, c->st);
+  CKL();
+  c->have_kbg = true;
+  return QX_OK;
+}
+
+template <typename T>
+static int get_kb_g(qx_ctx *c, double *eqlmr, double *vclalp) {
+  const Bufs<T> &b = c->pl.bufs<T>();
+  const long np = c->pl.nproj, ne = c->ne;
+  std::vector<T> h((size_t)np * ne), v((size_t)np);
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaMemcpy(h.data(), b.kbg, sizeof(T) * h.size(), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(v.data(), b.vclalp, sizeof(T) * v.size(), cudaMemcpyDeviceToHost));
+  if (eqlmr)
+    for (size_t i = 0; i < h.size(); ++i) eqlmr[i] = (double)h[i];
+  if (vclalp)
+    for (size_t i = 0; i < v.size(); ++i) vclalp[i] = (double)v[i];
+  if (sizeof(T) == sizeof(float) && c->kbgp && eqlmr) {
+    // the padded copy must hold the same rows
+    std::vector<float> p((size_t)np * c->kbgp_ld);
+    CK(cudaMemcpy(p.data(), c->kbgp, sizeof(float) * p.size(), cudaMemcpyDeviceToHost));
+    for (long j = 0; j < np; ++j)
+      if (std::memcmp(p.data() + j * c->kbgp_ld, (const float *)(const void *)h.data() + j * ne, sizeof(float) * ne)) {
+        set_error("qx_get_kb_g: padded copy of projector %ld differs", j);
+        return QX_ERR_STATE;
+      }
+  }
+  return QX_OK;
+}
+
+extern "C" int qx_get_kb_g(qx_ctx *c, double *eqlmr, double *vclalp) {
+  if (!c) { set_error("qx_get_kb_g: null"); return QX_ERR_ARG; }
+  if (!c->have_kbg) { set_error("qx_get_kb_g: G-space tables not set"); return QX_ERR_STATE; }
+  return c->prec == QX_PREC_FP64 ? get_kb_g<double>(c, eqlmr, vclalp) : get_kb_g<float>(c, eqlmr, vclalp);
 }
 
 extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const int *mesh, const double *vnl,

@@ -174,4 +174,12 @@ template <typename T>
 void fnl_reduce(int natom, int lmx, int nproj, int nb, const T *P, const T *D, const T *vclalp, const double *occ,
                 double *fnl, cudaStream_t st);
 
+// qx_tables.cu (G-space KB projector tables: setqlm once per cell, setbgq once per geometry)
+void setqlm(int nplw1, int nchan, int lmx, int mxqlm, const double *dlqlm, const double *tbqlm, const double *qlm,
+            const int *lmidx, const double *dk, double *zzz, cudaStream_t st);
+template <typename T>
+void setbgq(int natom, int nplw1, int ne, int lmx, const int *ityp, const int *ngabc, const double *dcq,
+            const double *dsq, int km1, int km2, int km3, int ktot, const double *zzz, const int *even,
+            const double *vcl_type, T *kbg, float *kbgp, long ldp, T *vcl, cudaStream_t st);
+
 }  // namespace qx

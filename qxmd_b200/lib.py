@@ -25,6 +25,7 @@ QX_ERR = {1: "ARG", 2: "CUDA", 3: "NOTPD", 4: "EIG", 5: "STATE"}
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [
     "qx_last_error", "qx_version", "qx_launch_count", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
+    "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g",
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
@@ -91,6 +92,9 @@ def lib(build_if_missing: bool = True):
         "qx_destroy": ([_ctx], C.c_int),
         "qx_set_glocal": ([_ctx, _dp], C.c_int),
         "qx_set_kb_g": ([_ctx, C.c_int, _dp, _dp], C.c_int),
+        "qx_set_kb_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _ip, _ip, _dp, _ip], C.c_int),
+        "qx_build_kb_g": ([_ctx, C.c_int, _ip, _dp], C.c_int),
+        "qx_get_kb_g": ([_ctx, _dp, _dp], C.c_int),
         "qx_set_kb_r": ([_ctx, C.c_int, C.c_int, _ip, _ip, _dp, _dp, C.c_double], C.c_int),
         "qx_set_nlmode": ([_ctx, C.c_int], C.c_int),
         "qx_set_occ": ([_ctx, _dp, C.c_double], C.c_int),
@@ -330,6 +334,26 @@ class Context:
         out = np.zeros((self.nb, self.nb))
         _ck(self.L.qx_tddft_overlap(self.h, out), "qx_tddft_overlap")
         return out.T.copy()   # column-major (i + j nband) -> [i, j]
+
+    def set_kb_builder(self, b: dict):
+        """qx_set_kb_builder from the dict of cell.kb_builder_tables."""
+        _ck(self.L.qx_set_kb_builder(self.h, b["ntype"], b["lmx"], b["mxqlm"], _f64(b["dlqlm"]), _f64(b["tbqlm"]),
+                                     b["nlm"], _f64(b["qlm"]), np.ascontiguousarray(b["lmidx"], dtype=np.int32),
+                                     np.ascontiguousarray(b["even"], dtype=np.int32), _f64(b["vclalp"]),
+                                     np.ascontiguousarray(b["ngabc"], dtype=np.int32)), "qx_set_kb_builder")
+
+    def build_kb_g(self, ityp, satm):
+        """qx_build_kb_g: the G-space KB tables of the geometry satm (natom, 3) fractional."""
+        satm = _f64(satm)
+        _ck(self.L.qx_build_kb_g(self.h, satm.shape[0], np.ascontiguousarray(ityp, dtype=np.int32), satm),
+            "qx_build_kb_g")
+
+    def get_kb_g(self, nproj):
+        """(eqlmr_ (nplwex, nproj), vclalp (nproj)) read back from the device."""
+        tab = np.zeros((nproj, self.ne))
+        vcl = np.zeros(nproj)
+        _ck(self.L.qx_get_kb_g(self.h, tab, vcl), "qx_get_kb_g")
+        return tab.T.copy(), vcl
 
     def set_force_tables(self):
         """qx_set_force_tables from the system's geometry (one species)."""

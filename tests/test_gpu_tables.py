@@ -1,0 +1,95 @@
+"""G-space KB tables built on the device (qx_set_kb_builder once per cell,
+qx_build_kb_g once per geometry: setqlm nlkbpp.f90:2196-2247, setbgq
+nlkbpp.f90:2135-2187, phases of stscfn_pw pwlda.f90:5711-5850) against the
+oracle's restatement, and H|psi> after an MD-like move of the atoms that
+rebuilds the tables in place.
+
+Tolerances: the FP64 table 1e-13 of its largest entry (the device cos/sin
+and fused multiply-adds against numpy); the FP32 table 2e-7 (one rounding);
+H|psi> as in the H|psi> parity tests (FP64 1e-11, mixed 2e-5)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle
+from oracle import tables
+from qxmd_b200 import cell
+from qxmd_b200.lib import QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context
+
+from gpu_util import need_gpu, relerr
+
+pytestmark = pytest.mark.gpu
+TAB_TOL = {QX_PREC_FP64: 1e-13, QX_PREC_MIXED: 2e-7}
+H_TOL = {QX_PREC_FP64: 1e-11, QX_PREC_MIXED: 2e-5}
+
+
+def _moved(satm, step):
+    rng = np.random.default_rng(40 + step)
+    return satm + rng.uniform(-0.01, 0.01, satm.shape)
+
+
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_build_kb_g_matches_oracle_and_rebuilds_in_place(si8, si8_psi, prec):
+    need_gpu()
+    b = cell.kb_builder_tables(si8.gs, si8.cell, si8.pp)
+    ctx = Context(si8, prec, QX_NL_GSPACE)
+    try:
+        ctx.set_kb_builder(b)
+        satm = b["satm"]
+        for step in range(3):
+            ctx.build_kb_g(b["ityp"], satm)
+            ref, vref = tables.setbgq(b, b["ityp"], satm)
+            tab, vcl = ctx.get_kb_g(ref.shape[1])
+            assert np.max(np.abs(tab - ref)) / np.max(np.abs(ref)) < TAB_TOL[prec]
+            assert relerr(vcl, vref) < TAB_TOL[prec]
+            ctx.put_psi(si8_psi)
+            ctx.enonloc()
+            hc = ctx.get_hpsi()
+            h = oracle.Ham(dataclasses.replace(si8, kb_g=ref, vclalp=vref), QX_NL_GSPACE)
+            assert relerr(hc, h.hpsi(si8_psi)) < H_TOL[prec]
+            satm = _moved(satm, step)
+    finally:
+        ctx.close()
+
+
+def test_build_kb_g_unaligned_band_stride():
+    """nplwex % 4 = 2 (Si8 at 170 Ry): the builder also fills the padded FP32
+    copy the tensor-core contractions read (qx_get_kb_g fails if a row of
+    that copy differs), and H|psi> matches the oracle."""
+    need_gpu()
+    s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), 170.0 / 4.0, 170.0, 48, with_ewald=False)
+    assert s.gs.nplwex % 4 == 2
+    b = cell.kb_builder_tables(s.gs, s.cell, s.pp)
+    c = cell.random_wavefunctions(s.gs.nplwex, 48)
+    c, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, nband=48)
+    try:
+        ctx.set_kb_builder(b)
+        satm = _moved(b["satm"], 7)
+        ctx.build_kb_g(b["ityp"], satm)
+        ref, vref = tables.setbgq(b, b["ityp"], satm)
+        tab, _ = ctx.get_kb_g(ref.shape[1])
+        assert np.max(np.abs(tab - ref)) / np.max(np.abs(ref)) < TAB_TOL[QX_PREC_MIXED]
+        ctx.put_psi(c)
+        ctx.enonloc()
+        hc = ctx.get_hpsi()
+    finally:
+        ctx.close()
+    h = oracle.Ham(dataclasses.replace(s, kb_g=ref, vclalp=vref), QX_NL_GSPACE)
+    assert relerr(hc, h.hpsi(c)) < H_TOL[QX_PREC_MIXED]
+
+
+def test_build_kb_g_rejects_short_radial_table(si8):
+    need_gpu()
+    b = dict(cell.kb_builder_tables(si8.gs, si8.cell, si8.pp))
+    b["mxqlm"] = 8
+    b["tbqlm"] = np.ascontiguousarray(b["tbqlm"][:, :9])
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    try:
+        with pytest.raises(Exception) as e:
+            ctx.set_kb_builder(b)
+        assert "radial table too short" in str(e.value)
+    finally:
+        ctx.close()
