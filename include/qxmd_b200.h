@@ -115,6 +115,26 @@ int qx_get_kb_g(qx_ctx *ctx, double *eqlmr, double *vclalp);
  * clalp(lmx) = clalp_ncr; rdelv = volume per grid point.  lmx must be 4. */
 int qx_set_kb_r(qx_ctx *ctx, int natom, int lmx, const int *off, const int *mesh, const double *vnl,
                 const double *clalp, double rdelv);
+/* The real-space tables built on the device, for MD steps (setnlc
+ * nlkbppr.f90:1010-1560).  Once per cell: ntype species of lmx = 4 channels,
+ * radial tables tabnl((mxnl + 1), 4 * ntype) at r = k * dltnl(it), projector
+ * radius rcut(ntype), poly(4 * ntype): the real solid-harmonic polynomial
+ * that multiplies each channel's radial value (0: 1; 1-3: x, y, z; 4-8: xy,
+ * yz, zx, x^2 - y^2, 3z^2 - r^2 of the displacement from the atom), clalp(4)
+ * KB energies, rdelv the volume per grid point, rba(3, 3) the lattice
+ * vectors as columns (row-major here: rba[3 * x + j] = component x of
+ * vector j).  The sphere must fit in half the cell along every axis. */
+int qx_set_kb_r_builder(qx_ctx *ctx, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
+                        const double *tabnl, const int *poly, const double *clalp, double rdelv, const double *rba);
+/* Once per geometry: the points of every atom (species ityp(natom), 0-based,
+ * fractional coordinates satm(3, natom)) within its projector radius, their
+ * projector values, and the x-line index of the real-space KB kernels.  The
+ * buffers grow by 25 % when the point count outgrows them (captured graphs
+ * are then dropped); otherwise they are reused in place. */
+int qx_build_kb_r(qx_ctx *ctx, int natom, const int *ityp, const double *satm);
+/* Reads back the real-space tables in use: *npts, and when not null
+ * off(natom + 1), mesh(npts), vnl(4 * npts) (double). */
+int qx_get_kb_r(qx_ctx *ctx, int *npts, int *off, int *mesh, double *vnl);
 int qx_set_nlmode(qx_ctx *ctx, int mode);
 /* occ(nband) and the cell volume (softchg weights occ/rvol, chgdns.f90:421). */
 int qx_set_occ(qx_ctx *ctx, const double *occ, double rvol);

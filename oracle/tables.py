@@ -11,7 +11,14 @@ eqlmr_ restated in numpy (FP64) from the reference's table builders:
 * setbgq (nlkbpp.f90:2135-2187): even l -> (cos f, -sin f), odd l ->
   (-sin f, -cos f) per half-sphere G, projector j = l + lmx * a.
 
-PARITY UNPINNED as the rest of the oracle; the tests tie this builder to the
+* setnlc (nlkbppr.f90:1010-1560): for each atom the grid points of the box
+  around its nearest grid point (x fastest, periodic wrap in place of the
+  reference's image atoms) within the projector radius, the radial table
+  interpolated at r by the same three-point formula (tabnl/tabnla) times the
+  channel's real solid-harmonic polynomial of the displacement; and the
+  x-line index of those points ordered by point.
+
+PARITY UNPINNED as the rest of the oracle; the tests tie these builders to the
 analytic model tables that the H|psi> parity tests use.
 """
 from __future__ import annotations
@@ -72,3 +79,42 @@ def setbgq(b: dict, ityp: np.ndarray, satm: np.ndarray):
                 tab[0::2, j], tab[1::2, j] = -ys[a] * f, -yc[a] * f
             vcl[j] = b["vclalp"][ch]
     return tab, vcl
+
+
+def _poly(c: int, x, y, z):
+    return [np.ones_like(x), x, y, z, x * y, y * z, z * x, x * x - y * y, 3 * z * z - (x * x + y * y + z * z)][c]
+
+
+def box_halfwidths(rba: np.ndarray, grid, rmax: float):
+    binv = np.linalg.inv(rba)
+    return [int(rmax * np.linalg.norm(binv[i]) * grid[i] + 0.5) + 1 for i in range(3)]
+
+
+def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray):
+    """(off (natom+1), mesh (npts), vnl (npts, 4)) in box order; b is the dict
+    of qxmd_b200.cell.kbr_builder_tables."""
+    k = np.array(b["grid"])
+    nd = box_halfwidths(b["rba"], b["grid"], float(np.max(b["rcut"])))
+    o3, o2, o1 = np.meshgrid(np.arange(-nd[2], nd[2] + 1), np.arange(-nd[1], nd[1] + 1),
+                             np.arange(-nd[0], nd[0] + 1), indexing="ij")
+    o = np.stack([o1.ravel(), o2.ravel(), o3.ravel()], axis=1)
+    offs, meshes, vals = [0], [], []
+    for a in range(satm.shape[0]):
+        it = int(ityp[a])
+        s = satm[a]
+        n = np.floor(s * k + 0.5).astype(np.int64) + o
+        f = n / k - s
+        d = f @ b["rba"].T
+        r2 = np.einsum("ij,ij->i", d, d)
+        sel = r2 <= b["rcut"][it] ** 2
+        n, d = n[sel], d[sel]
+        w = n % k
+        meshes.append((w[:, 0] + k[0] * (w[:, 1] + k[1] * w[:, 2])).astype(np.int32))
+        r = np.sqrt(r2[sel])
+        v = np.empty((r.size, 4))
+        for l in range(4):
+            ch = l + 4 * it
+            v[:, l] = setqlm(r, b["dltnl"][it], b["tabnl"][ch], _poly(int(b["poly"][ch]), d[:, 0], d[:, 1], d[:, 2]))
+        vals.append(v)
+        offs.append(offs[-1] + r.size)
+    return np.asarray(offs, dtype=np.int32), np.concatenate(meshes), np.concatenate(vals, axis=0)

@@ -136,6 +136,17 @@ struct qx_ctx {
   double *d_kb_zzz = nullptr, *d_kb_vclt = nullptr, *d_kb_dcq = nullptr, *d_kb_dsq = nullptr, *d_kb_satm = nullptr;
   int *d_kb_even = nullptr, *d_kb_ngabc = nullptr, *d_kb_ityp = nullptr;
   bool have_kb_builder = false;
+  // real-space table builder (qx_set_kb_r_builder, qx_build_kb_r)
+  KbrGeom kbr_geom = {};
+  int kbr_ntype = 0, kbr_mxnl = 0, kbr_natom = 0;
+  long kbr_cap = 0;
+  double *d_kbr_dl = nullptr, *d_kbr_rcut = nullptr, *d_kbr_tab = nullptr, *d_kbr_satm = nullptr;
+  int *d_kbr_poly = nullptr, *d_kbr_ityp = nullptr, *d_kbr_cnt = nullptr, *d_kbr_off = nullptr,
+      *d_kbr_mesh = nullptr, *d_kbr_ptatom = nullptr, *d_kbr_lcnt = nullptr, *d_kbr_loff = nullptr,
+      *d_kbr_cursor = nullptr;
+  int4 *d_kbr_lent = nullptr;
+  void *d_kbr_vnl = nullptr, *d_kbr_sumr = nullptr, *d_kbr_bufR = nullptr;
+  bool have_kbr_builder = false;
   bool defer = false;
   struct ScfGraph {
     std::vector<char> key;
@@ -160,6 +171,14 @@ static int dalloc(qx_ctx *c, P **p, size_t bytes) {
   TRY(dalloc(c, &v, bytes));
   *p = (P *)v;
   return 0;
+}
+
+// Captured SCF-iteration graphs hold the table pointers of their capture:
+// every call that replaces a table buffer drops them (the next iteration
+// captures again).
+static void drop_scf_graphs(qx_ctx *c) {
+  for (auto &g : c->scf_graphs) cudaGraphExecDestroy(g.exec);
+  c->scf_graphs.clear();
 }
 
 extern "C" const char *qx_last_error(void) { return g_err; }
@@ -576,6 +595,7 @@ extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const doub
   TRY(up(c, kbg, eqlmr, (long)nproj * c->ne));
   TRY(up(c, vcl, vclalp, nproj));
   c->pl.nproj = nproj;
+  drop_scf_graphs(c);
   TRY(tcpad_reserve(c, (long)nproj + c->nb));
   c->kbgp = nullptr;
   c->kbgp_ld = 0;
@@ -663,6 +683,7 @@ extern "C" int qx_build_kb_g(qx_ctx *c, int natom, const int *ityp, const double
     TRY(dalloc(c, &vcl, ts * nproj));
     TRY(dalloc(c, &proj, ts * (size_t)nproj * c->nb));
     c->pl.nproj = nproj;
+    drop_scf_graphs(c);
     TRY(tcpad_reserve(c, (long)nproj + c->nb));
     c->kbgp = nullptr;
     c->kbgp_ld = 0;
@@ -769,6 +790,7 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
   pl.natom = natom;
   pl.npts = npts;
   pl.rdelv = rdelv;
+  drop_scf_graphs(c);
   // real-space line buffer and projection sums, per chunk
   const long ch = pl.chunk;
   if (c->prec == QX_PREC_FP64) {
@@ -781,6 +803,167 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
     TRY(dalloc(c, &pl.b32.sumr, sizeof(float2) * ch * natom * 4));
   }
   c->have_kbr = true;
+  return QX_OK;
+}
+
+extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
+                                   const double *tabnl, const int *poly, const double *clalp, double rdelv,
+                                   const double *rba) {
+  if (!c || ntype <= 0 || lmx != 4 || mxnl < 2 || !dltnl || !rcut || !tabnl || !poly || !clalp || !rba ||
+      !(rdelv > 0.0)) {
+    set_error("qx_set_kb_r_builder: bad arguments (lmx must be 4)");
+    return QX_ERR_ARG;
+  }
+  Plan &pl = c->pl;
+  double rmax = 0.0;
+  for (int it = 0; it < ntype; ++it) {
+    if (!(dltnl[it] > 0.0) || !(rcut[it] > 0.0)) { set_error("qx_set_kb_r_builder: dltnl, rcut must be positive"); return QX_ERR_ARG; }
+    if (2 * (long)(rcut[it] / (2.0 * dltnl[it])) + 2 > mxnl) {
+      set_error("qx_set_kb_r_builder: radial table too short for the projector radius");
+      return QX_ERR_ARG;
+    }
+    rmax = std::max(rmax, rcut[it]);
+  }
+  for (int i = 0; i < lmx * ntype; ++i)
+    if (poly[i] < 0 || poly[i] > 8) { set_error("qx_set_kb_r_builder: poly out of range"); return QX_ERR_ARG; }
+  // inverse lattice (rows b_i: s_i = b_i . r); the sphere must fit in one cell
+  const double *a = rba;
+  const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                     a[2] * (a[3] * a[7] - a[4] * a[6]);
+  if (!(std::fabs(det) > 0.0)) { set_error("qx_set_kb_r_builder: singular lattice"); return QX_ERR_ARG; }
+  double b[9];
+  b[0] = (a[4] * a[8] - a[5] * a[7]) / det; b[1] = (a[2] * a[7] - a[1] * a[8]) / det; b[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+  b[3] = (a[5] * a[6] - a[3] * a[8]) / det; b[4] = (a[0] * a[8] - a[2] * a[6]) / det; b[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+  b[6] = (a[3] * a[7] - a[4] * a[6]) / det; b[7] = (a[1] * a[6] - a[0] * a[7]) / det; b[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+  KbrGeom G = {};
+  const int kk[3] = {pl.k1, pl.k2, pl.k3};
+  for (int i = 0; i < 9; ++i) G.rba[i] = a[i];
+  for (int i = 0; i < 3; ++i) {
+    const double bn = std::sqrt(b[3 * i] * b[3 * i] + b[3 * i + 1] * b[3 * i + 1] + b[3 * i + 2] * b[3 * i + 2]);
+    G.k[i] = kk[i];
+    G.nd[i] = (int)(rmax * bn * kk[i] + 0.5) + 1;
+    if (2.0 * rmax * bn >= 1.0 || 2 * G.nd[i] + 1 > kk[i]) {
+      set_error("qx_set_kb_r_builder: projector sphere wider than half the cell");
+      return QX_ERR_ARG;
+    }
+  }
+  const int nchan = lmx * ntype;
+  TRY(dalloc(c, &c->d_kbr_dl, sizeof(double) * ntype));
+  TRY(dalloc(c, &c->d_kbr_rcut, sizeof(double) * ntype));
+  TRY(dalloc(c, &c->d_kbr_tab, sizeof(double) * (size_t)(mxnl + 1) * nchan));
+  TRY(dalloc(c, &c->d_kbr_poly, sizeof(int) * nchan));
+  TRY(dalloc(c, &pl.d_kb_clalp, sizeof(double) * lmx));
+  CK(cudaMemcpyAsync(c->d_kbr_dl, dltnl, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kbr_rcut, rcut, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kbr_tab, tabnl, sizeof(double) * (size_t)(mxnl + 1) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kbr_poly, poly, sizeof(int) * nchan, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(pl.d_kb_clalp, clalp, sizeof(double) * lmx, cudaMemcpyHostToDevice, c->st));
+  drop_scf_graphs(c);
+  c->kbr_geom = G;
+  c->kbr_ntype = ntype;
+  c->kbr_mxnl = mxnl;
+  pl.rdelv = rdelv;
+  c->have_kbr_builder = true;
+  return QX_OK;
+}
+
+extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double *satm) {
+  if (!c || natom <= 0 || natom > 65535 || !ityp || !satm) { set_error("qx_build_kb_r: bad arguments"); return QX_ERR_ARG; }
+  if (!c->have_kbr_builder) { set_error("qx_build_kb_r: qx_set_kb_r_builder first"); return QX_ERR_STATE; }
+  for (int a = 0; a < natom; ++a)
+    if (ityp[a] < 0 || ityp[a] >= c->kbr_ntype) { set_error("qx_build_kb_r: ityp out of range"); return QX_ERR_ARG; }
+  Plan &pl = c->pl;
+  const size_t ts = c->tsize();
+  const long nlines = (long)pl.k2 * pl.k3;
+  bool moved = false;   // a table buffer was (re)allocated: captured graphs hold stale pointers
+  if (natom != c->kbr_natom) {
+    TRY(dalloc(c, &c->d_kbr_ityp, sizeof(int) * natom));
+    TRY(dalloc(c, &c->d_kbr_satm, sizeof(double) * 3 * natom));
+    TRY(dalloc(c, &c->d_kbr_cnt, sizeof(int) * natom));
+    TRY(dalloc(c, &c->d_kbr_off, sizeof(int) * (natom + 1)));
+    TRY(dalloc(c, &c->d_kbr_sumr, 2 * ts * (size_t)pl.chunk * natom * 4));
+    c->kbr_natom = natom;
+    moved = true;
+  }
+  if (!c->d_kbr_loff) {
+    TRY(dalloc(c, &c->d_kbr_lcnt, sizeof(int) * nlines));
+    TRY(dalloc(c, &c->d_kbr_loff, sizeof(int) * (nlines + 1)));
+    TRY(dalloc(c, &c->d_kbr_cursor, sizeof(int) * nlines));
+    TRY(dalloc(c, &c->d_kbr_bufR, 2 * ts * (size_t)pl.chunk * pl.n));
+    moved = true;
+  }
+  CK(cudaMemcpyAsync(c->d_kbr_ityp, ityp, sizeof(int) * natom, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_kbr_satm, satm, sizeof(double) * 3 * natom, cudaMemcpyHostToDevice, c->st));
+  const KbrGeom &G = c->kbr_geom;
+  kbr_count(G, natom, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_cnt, c->d_kbr_off, c->st);
+  int total = 0;
+  CK(cudaMemcpyAsync(&total, c->d_kbr_off + natom, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (total > c->kbr_cap) {
+    const long cap = (long)(total * 1.25) + 64;
+    TRY(dalloc(c, &c->d_kbr_mesh, sizeof(int) * cap));
+    TRY(dalloc(c, &c->d_kbr_ptatom, sizeof(int) * cap));
+    TRY(dalloc(c, &c->d_kbr_lent, sizeof(int4) * cap));
+    TRY(dalloc(c, &c->d_kbr_vnl, ts * 4 * (size_t)cap));
+    c->kbr_cap = cap;
+    moved = true;
+  }
+  if (c->prec == QX_PREC_FP64)
+    kbr_fill<double>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
+                     c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh, c->d_kbr_ptatom,
+                     (double *)c->d_kbr_vnl, c->st);
+  else
+    kbr_fill<float>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
+                    c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh, c->d_kbr_ptatom,
+                    (float *)c->d_kbr_vnl, c->st);
+  if (kbr_lines(c->d_kbr_off, natom, c->d_kbr_mesh, c->d_kbr_ptatom, pl.k1, nlines, c->d_kbr_lcnt, c->d_kbr_loff,
+                c->d_kbr_cursor, c->d_kbr_lent, c->st)) {
+    set_error("qx_build_kb_r: memset failed");
+    return QX_ERR_CUDA;
+  }
+  CKL();
+  if (pl.d_kb_off != c->d_kbr_off || pl.d_kb_mesh != c->d_kbr_mesh || pl.d_line_off != c->d_kbr_loff ||
+      pl.d_line_ent != c->d_kbr_lent)
+    moved = true;
+  pl.d_kb_off = c->d_kbr_off;
+  pl.d_kb_mesh = c->d_kbr_mesh;
+  pl.d_line_off = c->d_kbr_loff;
+  pl.d_line_ent = c->d_kbr_lent;
+  if (c->prec == QX_PREC_FP64) {
+    moved |= pl.b64.kb_vnl != (double *)c->d_kbr_vnl || pl.b64.sumr != (double2 *)c->d_kbr_sumr;
+    pl.b64.kb_vnl = (double *)c->d_kbr_vnl;
+    pl.b64.bufR = (double2 *)c->d_kbr_bufR;
+    pl.b64.sumr = (double2 *)c->d_kbr_sumr;
+  } else {
+    moved |= pl.b32.kb_vnl != (float *)c->d_kbr_vnl || pl.b32.sumr != (float2 *)c->d_kbr_sumr;
+    pl.b32.kb_vnl = (float *)c->d_kbr_vnl;
+    pl.b32.bufR = (float2 *)c->d_kbr_bufR;
+    pl.b32.sumr = (float2 *)c->d_kbr_sumr;
+  }
+  pl.natom = natom;
+  pl.npts = total;
+  if (moved) drop_scf_graphs(c);
+  c->have_kbr = true;
+  return QX_OK;
+}
+
+extern "C" int qx_get_kb_r(qx_ctx *c, int *npts, int *off, int *mesh, double *vnl) {
+  if (!c || !npts) { set_error("qx_get_kb_r: null"); return QX_ERR_ARG; }
+  if (!c->have_kbr) { set_error("qx_get_kb_r: real-space tables not set"); return QX_ERR_STATE; }
+  const Plan &pl = c->pl;
+  CK(cudaStreamSynchronize(c->st));
+  *npts = pl.npts;
+  if (off) CK(cudaMemcpy(off, pl.d_kb_off, sizeof(int) * (pl.natom + 1), cudaMemcpyDeviceToHost));
+  if (mesh) CK(cudaMemcpy(mesh, pl.d_kb_mesh, sizeof(int) * pl.npts, cudaMemcpyDeviceToHost));
+  if (vnl) {
+    if (c->prec == QX_PREC_FP64) {
+      CK(cudaMemcpy(vnl, pl.b64.kb_vnl, sizeof(double) * 4 * pl.npts, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> h((size_t)4 * pl.npts);
+      CK(cudaMemcpy(h.data(), pl.b32.kb_vnl, sizeof(float) * h.size(), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < h.size(); ++i) vnl[i] = h[i];
+    }
+  }
   return QX_OK;
 }
 

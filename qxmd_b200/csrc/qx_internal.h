@@ -181,5 +181,19 @@ template <typename T>
 void setbgq(int natom, int nplw1, int ne, int lmx, const int *ityp, const int *ngabc, const double *dcq,
             const double *dsq, int km1, int km2, int km3, int ktot, const double *zzz, const int *even,
             const double *vcl_type, T *kbg, float *kbgp, long ldp, T *vcl, cudaStream_t st);
+// real-space tables (setnlc): geometry of the point search
+struct KbrGeom {
+  double rba[9];   // lattice vectors as columns, row-major (x row, y row, z row)
+  int k[3];        // FFT grid
+  int nd[3];       // box half-widths in grid points
+};
+void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm, const double *rcut, int *cnt,
+               int *off, cudaStream_t st);
+template <typename T>
+void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
+              const double *dltnl, const double *tabnl, int mxnl, const int *poly, const int *off, long cap,
+              int *mesh, int *ptatom, T *vnl, cudaStream_t st);
+int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int k1, long nlines, int *lcnt,
+              int *loff, int *cursor, int4 *lent, cudaStream_t st);
 
 }  // namespace qx

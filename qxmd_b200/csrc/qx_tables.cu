@@ -13,7 +13,15 @@
 //      even l: eqlmr_(2g+1) =  cos f,  eqlmr_(2g+2) = -sin f
 //      odd l:  eqlmr_(2g+1) = -sin f,  eqlmr_(2g+2) = -cos f
 //    written straight into the context's projector table (and its padded
-//    FP32 copy) together with the per-projector KB energies.
+//    FP32 copy) together with the per-projector KB energies;
+//  * real-space tables, once per geometry (setnlc, nlkbppr.f90:1010-1560):
+//    the grid points within the projector radius of each atom (the box of
+//    grid points around the atom's nearest grid point, periodic wrap), in
+//    box order (x fastest), with the projector values interpolated from the
+//    radial table by the same three-point formula times a real solid
+//    harmonic polynomial of the displacement, then the x-line index (points
+//    of each grid line, ordered by point) that the real-space KB kernels of
+//    the FFT pipeline read.
 #include "qx_internal.h"
 
 namespace qx {
@@ -27,7 +35,7 @@ __global__ void k_setqlm(int nplw1, int nchan, int lmx, int mxqlm, const double 
     const int it = ch / lmx;
     const double dl = dlqlm[it];
     const double ag = sqrt(dk[2 * g]);
-    const int m = 2 * (int)(ag / (2.0 * dl));
+    const int m = min(2 * (int)(ag / (2.0 * dl)), mxqlm - 2);
     const double d = 0.5 * (ag / dl - (double)m);
     const double *t = tbqlm + (long)ch * (mxqlm + 1);
     const double t0 = t[m], t1 = t[m + 1], t2 = t[m + 2];
@@ -96,5 +104,218 @@ template void setbgq<float>(int, int, int, int, const int *, const int *, const 
 template void setbgq<double>(int, int, int, int, const int *, const int *, const double *, const double *, int, int,
                              int, int, const double *, const int *, const double *, double *, float *, long,
                              double *, cudaStream_t);
+
+// ---- real-space tables ---------------------------------------------------
+__device__ __forceinline__ int kbr_wrap(int n, int k) {
+  n %= k;
+  return n < 0 ? n + k : n;
+}
+
+// Box point q of atom a: wrapped grid index and displacement r - R_a (bohr).
+__device__ __forceinline__ void kbr_point(const KbrGeom &G, const double *s, long q, int &mesh, double &dx,
+                                          double &dy, double &dz) {
+  const int w1 = 2 * G.nd[0] + 1, w2 = 2 * G.nd[1] + 1;
+  const int o1 = (int)(q % w1) - G.nd[0];
+  const int o2 = (int)((q / w1) % w2) - G.nd[1];
+  const int o3 = (int)(q / ((long)w1 * w2)) - G.nd[2];
+  const int n1 = (int)floor(s[0] * G.k[0] + 0.5) + o1, n2 = (int)floor(s[1] * G.k[1] + 0.5) + o2,
+            n3 = (int)floor(s[2] * G.k[2] + 0.5) + o3;
+  const double f1 = (double)n1 / G.k[0] - s[0], f2 = (double)n2 / G.k[1] - s[1], f3 = (double)n3 / G.k[2] - s[2];
+  dx = G.rba[0] * f1 + G.rba[1] * f2 + G.rba[2] * f3;
+  dy = G.rba[3] * f1 + G.rba[4] * f2 + G.rba[5] * f3;
+  dz = G.rba[6] * f1 + G.rba[7] * f2 + G.rba[8] * f3;
+  mesh = kbr_wrap(n1, G.k[0]) + G.k[0] * (kbr_wrap(n2, G.k[1]) + G.k[1] * kbr_wrap(n3, G.k[2]));
+}
+
+// real solid-harmonic polynomials of degree <= 2 (normalisation in the table)
+__device__ __forceinline__ double kbr_poly(int c, double x, double y, double z) {
+  switch (c) {
+    case 0: return 1.0;
+    case 1: return x;
+    case 2: return y;
+    case 3: return z;
+    case 4: return x * y;
+    case 5: return y * z;
+    case 6: return z * x;
+    case 7: return x * x - y * y;
+    default: return 3.0 * z * z - (x * x + y * y + z * z);
+  }
+}
+
+__global__ void k_kbr_count(KbrGeom G, const int *__restrict__ ityp, const double *__restrict__ satm,
+                            const double *__restrict__ rcut, int *__restrict__ cnt) {
+  const int a = blockIdx.x;
+  const double *s = satm + 3 * a;
+  const double rc2 = rcut[ityp[a]] * rcut[ityp[a]];
+  const long nbox = (long)(2 * G.nd[0] + 1) * (2 * G.nd[1] + 1) * (2 * G.nd[2] + 1);
+  int c = 0;
+  for (long q = threadIdx.x; q < nbox; q += blockDim.x) {
+    int m;
+    double dx, dy, dz;
+    kbr_point(G, s, q, m, dx, dy, dz);
+    c += (dx * dx + dy * dy + dz * dz <= rc2) ? 1 : 0;
+  }
+  __shared__ int red[32];
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    cnt[a] = t;
+  }
+}
+
+// Exclusive scan of n counts by one block of 1024 threads: out[0..n],
+// out[n] = total.  If cursor is given, it receives out[0..n-1] too.
+__global__ void __launch_bounds__(1024) k_scan1(const int *__restrict__ in, long n, int *__restrict__ out,
+                                                int *__restrict__ cursor) {
+  __shared__ int part[1024];
+  const int t = threadIdx.x;
+  const long per = (n + 1023) / 1024, lo = std::min<long>(n, t * per), hi = std::min<long>(n, lo + per);
+  int sum = 0;
+  for (long i = lo; i < hi; ++i) sum += in[i];
+  part[t] = sum;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = part[t] - sum;
+  for (long i = lo; i < hi; ++i) {
+    out[i] = run;
+    if (cursor) cursor[i] = run;
+    run += in[i];
+  }
+  if (t == 1023) out[n] = part[1023];
+}
+
+template <typename T>
+__global__ void k_kbr_fill(KbrGeom G, int lmx, const int *__restrict__ ityp, const double *__restrict__ satm,
+                           const double *__restrict__ rcut, const double *__restrict__ dltnl,
+                           const double *__restrict__ tabnl, int mxnl, const int *__restrict__ poly,
+                           const int *__restrict__ off, int natom, long cap, int *__restrict__ mesh,
+                           int *__restrict__ ptatom, T *__restrict__ vnl) {
+  if (off[natom] > cap) return;   // the host grows the buffers and launches again
+  const int a = blockIdx.x, it = ityp[a];
+  const double *s = satm + 3 * a;
+  const double rc2 = rcut[it] * rcut[it], dl = dltnl[it];
+  const long nbox = (long)(2 * G.nd[0] + 1) * (2 * G.nd[1] + 1) * (2 * G.nd[2] + 1);
+  __shared__ int wsum[32];
+  __shared__ int base;
+  if (threadIdx.x == 0) base = off[a];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (long q0 = 0; q0 < nbox; q0 += blockDim.x) {
+    const long q = q0 + threadIdx.x;
+    int m = 0;
+    double dx = 0, dy = 0, dz = 0;
+    bool in = false;
+    if (q < nbox) {
+      kbr_point(G, s, q, m, dx, dy, dz);
+      in = dx * dx + dy * dy + dz * dz <= rc2;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, in);
+    if (lane == 0) wsum[warp] = __popc(bal);
+    __syncthreads();
+    int wo = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      wo += w < warp ? wsum[w] : 0;
+      tot += wsum[w];
+    }
+    const long i = base + wo + __popc(bal & ((1u << lane) - 1u));
+    if (in && i < off[a + 1]) {
+      mesh[i] = m;
+      ptatom[i] = a;
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      const int mm = min(2 * (int)(r / (2.0 * dl)), mxnl - 2);
+      const double d = 0.5 * (r / dl - (double)mm);
+      for (int l = 0; l < lmx; ++l) {
+        const int ch = l + lmx * it;
+        const double *tb = tabnl + (long)ch * (mxnl + 1);
+        const double t0 = tb[mm], t1 = tb[mm + 1], t2 = tb[mm + 2];
+        const double av = 2.0 * (t0 + t2 - 2.0 * t1);
+        const double f = d * ((d - 1.0) * av + t2 - t0) + t0;
+        vnl[i * lmx + l] = (T)(f * kbr_poly(poly[ch], dx, dy, dz));
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void k_kbr_line_count(const int *__restrict__ off, int natom, const int *__restrict__ mesh, int k1,
+                                 int *__restrict__ lcnt) {
+  const long tot = off[natom];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x)
+    atomicAdd(&lcnt[mesh[i] / k1], 1);
+}
+
+__global__ void k_kbr_line_fill(const int *__restrict__ off, int natom, const int *__restrict__ mesh,
+                                const int *__restrict__ ptatom, int k1, int *__restrict__ cursor,
+                                int4 *__restrict__ lent) {
+  const long tot = off[natom];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    const int m = mesh[i];
+    const int pos = atomicAdd(&cursor[m / k1], 1);
+    lent[pos] = make_int4(m % k1, (int)i, ptatom[i], 0);
+  }
+}
+
+// one thread per line: entries ordered by point index (insertion sort; lines are short)
+__global__ void k_kbr_line_sort(const int *__restrict__ loff, long nlines, int4 *__restrict__ lent) {
+  for (long l = blockIdx.x * (long)blockDim.x + threadIdx.x; l < nlines; l += (long)gridDim.x * blockDim.x) {
+    const int lo = loff[l], hi = loff[l + 1];
+    for (int i = lo + 1; i < hi; ++i) {
+      const int4 v = lent[i];
+      int j = i - 1;
+      while (j >= lo && lent[j].y > v.y) {
+        lent[j + 1] = lent[j];
+        --j;
+      }
+      lent[j + 1] = v;
+    }
+  }
+}
+
+void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm, const double *rcut, int *cnt,
+               int *off, cudaStream_t st) {
+  k_kbr_count<<<natom, 256, 0, st>>>(G, ityp, satm, rcut, cnt);
+  note_launch();
+  k_scan1<<<1, 1024, 0, st>>>(cnt, natom, off, nullptr);
+  note_launch();
+}
+
+template <typename T>
+void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
+              const double *dltnl, const double *tabnl, int mxnl, const int *poly, const int *off, long cap,
+              int *mesh, int *ptatom, T *vnl, cudaStream_t st) {
+  k_kbr_fill<T><<<natom, 256, 0, st>>>(G, lmx, ityp, satm, rcut, dltnl, tabnl, mxnl, poly, off, natom, cap, mesh,
+                                       ptatom, vnl);
+  note_launch();
+}
+template void kbr_fill<float>(const KbrGeom &, int, int, const int *, const double *, const double *,
+                              const double *, const double *, int, const int *, const int *, long, int *, int *,
+                              float *, cudaStream_t);
+template void kbr_fill<double>(const KbrGeom &, int, int, const int *, const double *, const double *,
+                               const double *, const double *, int, const int *, const int *, long, int *, int *,
+                               double *, cudaStream_t);
+
+int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int k1, long nlines, int *lcnt,
+              int *loff, int *cursor, int4 *lent, cudaStream_t st) {
+  if (cudaMemsetAsync(lcnt, 0, sizeof(int) * nlines, st) != cudaSuccess) return 1;
+  k_kbr_line_count<<<148 * 4, 256, 0, st>>>(off, natom, mesh, k1, lcnt);
+  note_launch();
+  k_scan1<<<1, 1024, 0, st>>>(lcnt, nlines, loff, cursor);
+  note_launch();
+  k_kbr_line_fill<<<148 * 4, 256, 0, st>>>(off, natom, mesh, ptatom, k1, cursor, lent);
+  note_launch();
+  k_kbr_line_sort<<<(unsigned)std::min<long>(148 * 4, (nlines + 127) / 128), 128, 0, st>>>(loff, nlines, lent);
+  note_launch();
+  return 0;
+}
 
 }  // namespace qx

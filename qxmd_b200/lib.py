@@ -25,7 +25,7 @@ QX_ERR = {1: "ARG", 2: "CUDA", 3: "NOTPD", 4: "EIG", 5: "STATE"}
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [
     "qx_last_error", "qx_version", "qx_launch_count", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
-    "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g",
+    "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g", "qx_set_kb_r_builder", "qx_build_kb_r", "qx_get_kb_r",
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
@@ -95,6 +95,10 @@ def lib(build_if_missing: bool = True):
         "qx_set_kb_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _ip, _ip, _dp, _ip], C.c_int),
         "qx_build_kb_g": ([_ctx, C.c_int, _ip, _dp], C.c_int),
         "qx_get_kb_g": ([_ctx, _dp, _dp], C.c_int),
+        "qx_set_kb_r_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _ip, _dp, C.c_double, _dp],
+                                C.c_int),
+        "qx_build_kb_r": ([_ctx, C.c_int, _ip, _dp], C.c_int),
+        "qx_get_kb_r": ([_ctx, C.POINTER(C.c_int), _vp, _vp, _vp], C.c_int),
         "qx_set_kb_r": ([_ctx, C.c_int, C.c_int, _ip, _ip, _dp, _dp, C.c_double], C.c_int),
         "qx_set_nlmode": ([_ctx, C.c_int], C.c_int),
         "qx_set_occ": ([_ctx, _dp, C.c_double], C.c_int),
@@ -354,6 +358,29 @@ class Context:
         vcl = np.zeros(nproj)
         _ck(self.L.qx_get_kb_g(self.h, tab, vcl), "qx_get_kb_g")
         return tab.T.copy(), vcl
+
+    def set_kb_r_builder(self, b: dict):
+        """qx_set_kb_r_builder from the dict of cell.kbr_builder_tables."""
+        _ck(self.L.qx_set_kb_r_builder(self.h, b["ntype"], 4, b["mxnl"], _f64(b["dltnl"]), _f64(b["rcut"]),
+                                       _f64(b["tabnl"]), np.ascontiguousarray(b["poly"], dtype=np.int32),
+                                       _f64(b["clalp"]), b["rdelv"], _f64(b["rba"])), "qx_set_kb_r_builder")
+
+    def build_kb_r(self, ityp, satm):
+        """qx_build_kb_r: the real-space KB tables of the geometry satm (natom, 3) fractional."""
+        satm = _f64(satm)
+        _ck(self.L.qx_build_kb_r(self.h, satm.shape[0], np.ascontiguousarray(ityp, dtype=np.int32), satm),
+            "qx_build_kb_r")
+
+    def get_kb_r(self, natom):
+        """(off (natom+1), mesh (npts), vnl (npts, 4)) read back from the device."""
+        n = C.c_int(0)
+        _ck(self.L.qx_get_kb_r(self.h, C.byref(n), None, None, None), "qx_get_kb_r")
+        off = np.zeros(natom + 1, dtype=np.int32)
+        mesh = np.zeros(max(n.value, 1), dtype=np.int32)
+        vnl = np.zeros((max(n.value, 1), 4))
+        _ck(self.L.qx_get_kb_r(self.h, C.byref(n), off.ctypes.data, mesh.ctypes.data, vnl.ctypes.data),
+            "qx_get_kb_r")
+        return off, mesh[: n.value], vnl[: n.value]
 
     def set_force_tables(self):
         """qx_set_force_tables from the system's geometry (one species)."""

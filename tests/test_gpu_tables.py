@@ -1,8 +1,10 @@
-"""G-space KB tables built on the device (qx_set_kb_builder once per cell,
-qx_build_kb_g once per geometry: setqlm nlkbpp.f90:2196-2247, setbgq
-nlkbpp.f90:2135-2187, phases of stscfn_pw pwlda.f90:5711-5850) against the
-oracle's restatement, and H|psi> after an MD-like move of the atoms that
-rebuilds the tables in place.
+"""KB tables built on the device against the oracle's restatement, and
+H|psi> after MD-like moves of the atoms that rebuild the tables in place:
+G space (qx_set_kb_builder once per cell, qx_build_kb_g once per geometry:
+setqlm nlkbpp.f90:2196-2247, setbgq nlkbpp.f90:2135-2187, phases of
+stscfn_pw pwlda.f90:5711-5850) and real space (qx_set_kb_r_builder,
+qx_build_kb_r: setnlc nlkbppr.f90:1010-1560, the points, values and x-line
+index that calnlc's kernels read).
 
 Tolerances: the FP64 table 1e-13 of its largest entry (the device cos/sin
 and fused multiply-adds against numpy); the FP32 table 2e-7 (one rounding);
@@ -15,7 +17,7 @@ import pytest
 import oracle
 from oracle import tables
 from qxmd_b200 import cell
-from qxmd_b200.lib import QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context
+from qxmd_b200.lib import QX_NL_GSPACE, QX_NL_RSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context
 
 from gpu_util import need_gpu, relerr
 
@@ -91,5 +93,76 @@ def test_build_kb_g_rejects_short_radial_table(si8):
         with pytest.raises(Exception) as e:
             ctx.set_kb_builder(b)
         assert "radial table too short" in str(e.value)
+    finally:
+        ctx.close()
+
+
+def _kbr_system(s, off, mesh, vnl, b):
+    kr = cell.KBReal(off=off, mesh=mesh, vnl=vnl, clalp=b["clalp"], rdelv=b["rdelv"])
+    return dataclasses.replace(s, kb_r=kr)
+
+
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_build_kb_r_matches_oracle_and_rebuilds_in_place(si8, si8_psi, prec):
+    """Points in the oracle's box order exactly, values within the table
+    tolerance, and real-space-KB H|psi> over three geometries."""
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
+    nat = si8.cell.natom
+    ctx = Context(si8, prec, QX_NL_RSPACE)
+    try:
+        ctx.set_kb_r_builder(b)
+        satm = b["satm"]
+        for step in range(3):
+            ctx.build_kb_r(b["ityp"], satm)
+            roff, rmesh, rvnl = tables.setnlc(b, b["ityp"], satm)
+            off, mesh, vnl = ctx.get_kb_r(nat)
+            assert np.array_equal(off, roff)
+            assert np.array_equal(mesh, rmesh)
+            assert np.max(np.abs(vnl - rvnl)) / np.max(np.abs(rvnl)) < TAB_TOL[prec]
+            ctx.put_psi(si8_psi)
+            ctx.enonloc()
+            hc = ctx.get_hpsi()
+            h = oracle.Ham(_kbr_system(si8, roff, rmesh, rvnl, b), QX_NL_RSPACE)
+            assert relerr(hc, h.hpsi(si8_psi)) < H_TOL[prec]
+            satm = _moved(satm, 20 + step)
+    finally:
+        ctx.close()
+
+
+def test_build_kb_r_grows_its_buffers(si8, si8_psi):
+    """A larger projector radius (4.0 -> 4.4 bohr, 33 % more points) outgrows
+    the first build's 25 % headroom: the buffers are reallocated and H|psi>
+    still matches the oracle."""
+    need_gpu()
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_RSPACE)
+    try:
+        npts = []
+        for rc in (4.0, 4.4):
+            b = cell.kbr_builder_tables(si8.gs, si8.cell, dataclasses.replace(si8.pp, rcut=rc))
+            ctx.set_kb_r_builder(b)
+            ctx.build_kb_r(b["ityp"], b["satm"])
+            roff, rmesh, rvnl = tables.setnlc(b, b["ityp"], b["satm"])
+            off, mesh, vnl = ctx.get_kb_r(si8.cell.natom)
+            assert np.array_equal(mesh, rmesh)
+            npts.append(mesh.size)
+            ctx.put_psi(si8_psi)
+            ctx.enonloc()
+            hc = ctx.get_hpsi()
+            h = oracle.Ham(_kbr_system(si8, roff, rmesh, rvnl, b), QX_NL_RSPACE)
+            assert relerr(hc, h.hpsi(si8_psi)) < H_TOL[QX_PREC_FP64]
+        assert npts[1] > 1.25 * npts[0]
+    finally:
+        ctx.close()
+
+
+def test_build_kb_r_rejects_sphere_wider_than_half_cell(si8):
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, dataclasses.replace(si8.pp, rcut=5.5))
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_RSPACE)
+    try:
+        with pytest.raises(Exception) as e:
+            ctx.set_kb_r_builder(b)
+        assert "wider than half the cell" in str(e.value)
     finally:
         ctx.close()
