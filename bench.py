@@ -277,8 +277,27 @@ def kb_build_timing(sys_, ctx, R, W, flush):
     nproj, ne = b["lmx"] * sys_.cell.natom, sys_.gs.nplwex
     nbytes = 4 * nproj * ne * (2 if ne % 4 else 1)
     ms = t / R
-    return {"ms_per_geometry": ms, "table_bytes_written": nbytes, "gb_per_s": nbytes / (ms * 1e-3) / 1e9,
-            "builds_timed": R}
+    out = {"ms_per_geometry": ms, "table_bytes_written": nbytes, "gb_per_s": nbytes / (ms * 1e-3) / 1e9,
+           "builds_timed": R}
+    # real-space tables (setnlc): point search, values, x-line index; one
+    # host read of the point count per build (buffer capacity check)
+    br = cell.kbr_builder_tables(sys_.gs, sys_.cell, sys_.pp)
+    ctx.set_kb_r_builder(br)
+    for g in geoms[:W]:
+        ctx.build_kb_r(br["ityp"], g)
+    ctx.sync()
+    t = 0.0
+    for g in geoms[W:]:
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.build_kb_r(br["ityp"], g)
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1)
+    npts = ctx.get_kb_r(sys_.cell.natom)[1].size
+    out["real_space"] = {"ms_per_geometry": t / R, "points": int(npts)}
+    return out
 
 
 def run_si512(args):
