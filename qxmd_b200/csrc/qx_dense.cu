@@ -874,8 +874,9 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
 //      re-orthogonalised against each other; per-thread work arrays are
 //      interleaved across threads so every access is coalesced;
 //  (4) k_wy_t + k_backtrans_wy: V = Q Z, one warp per column, the reflectors
-//      in compact-WY blocks of 8 (k_backtrans, one reflector at a time, for
-//      n > 256).
+//      in compact-WY blocks of 8; for n > 256 k_backtrans_tile, one CTA per 8
+//      columns held in shared memory, the same blocks (QX_BACKTRANS_TILE=0:
+//      k_backtrans, one warp per column and one reflector at a time).
 // Eigenpairs are ascending; each eigenvector's largest-magnitude component is
 // made positive (first index on ties).  Every loop is bounded.
 
@@ -1679,6 +1680,106 @@ __global__ void __launch_bounds__(128) k_backtrans_wy(const double *__restrict__
   }
 }
 
+// V(:, c) = Q Z(:, c) for n > 256: one CTA per BTC columns, the columns in
+// shared memory (row i's BTC entries side by side), thread t owning rows
+// i = t mod 256 for the whole run.  Per compact-WY block of WYB reflectors
+// (last to first): S = Y^T Z (WYB x BTC sums: per-thread partials, warp
+// shuffles, then across warps), U = T S, Z -= Y U; two barriers per block.
+// Then the sign convention of k_backtrans, one warp per column.
+constexpr int BTC = 8;
+__global__ void __launch_bounds__(256) k_backtrans_tile(const double *__restrict__ Z, const double *__restrict__ HV,
+                                                        const double *__restrict__ Tm, int n,
+                                                        double *__restrict__ V) {
+  extern __shared__ double zt[];   // n * BTC
+  __shared__ double red[8][WYB * BTC];
+  __shared__ double Us[WYB * BTC];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int c0 = blockIdx.x * BTC, nc = min(BTC, n - c0);
+  for (long q = t; q < (long)n * BTC; q += blockDim.x) {
+    const int i = (int)(q / BTC), cc = (int)(q - (long)i * BTC);
+    zt[q] = cc < nc ? Z[(long)(c0 + cc) * n + i] : 0.0;
+  }
+  __syncthreads();
+  const int nref = n - 2, nblk = (nref + WYB - 1) / WYB;
+  for (int blk = nblk - 1; blk >= 0; --blk) {
+    const int k0 = blk * WYB;
+    double acc[WYB][BTC];
+#pragma unroll
+    for (int j = 0; j < WYB; ++j)
+#pragma unroll
+      for (int cc = 0; cc < BTC; ++cc) acc[j][cc] = 0.0;
+    for (int i = t; i < n; i += 256) {
+      if (i <= k0) continue;
+      double z[BTC];
+#pragma unroll
+      for (int cc = 0; cc < BTC; ++cc) z[cc] = zt[(long)i * BTC + cc];
+#pragma unroll
+      for (int j = 0; j < WYB; ++j) {
+        const int k = k0 + j;
+        const double y = (k < nref && i > k) ? HV[(long)k * n + i] : 0.0;
+#pragma unroll
+        for (int cc = 0; cc < BTC; ++cc) acc[j][cc] += y * z[cc];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < WYB; ++j)
+#pragma unroll
+      for (int cc = 0; cc < BTC; ++cc) {
+        double v = acc[j][cc];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][j * BTC + cc] = v;
+      }
+    __syncthreads();
+    if (t < WYB * BTC) {
+      // S(j, cc) summed over the warps, then U = T S (T upper triangular)
+      const int i = t / BTC, cc = t - (t / BTC) * BTC;
+      const double *T = Tm + (long)blk * WYB * WYB;
+      double u = 0.0;
+      for (int j = i; j < WYB; ++j) {
+        double sj = 0.0;
+        for (int w = 0; w < 8; ++w) sj += red[w][j * BTC + cc];
+        u += T[i * WYB + j] * sj;
+      }
+      Us[i * BTC + cc] = u;
+    }
+    __syncthreads();
+    for (int i = t; i < n; i += 256) {
+      if (i <= k0) continue;
+      double d[BTC];
+#pragma unroll
+      for (int cc = 0; cc < BTC; ++cc) d[cc] = 0.0;
+#pragma unroll
+      for (int j = 0; j < WYB; ++j) {
+        const int k = k0 + j;
+        const double y = (k < nref && i > k) ? HV[(long)k * n + i] : 0.0;
+#pragma unroll
+        for (int cc = 0; cc < BTC; ++cc) d[cc] += y * Us[j * BTC + cc];
+      }
+#pragma unroll
+      for (int cc = 0; cc < BTC; ++cc) zt[(long)i * BTC + cc] -= d[cc];
+    }
+  }
+  __syncthreads();
+  if (warp < nc) {
+    const int cc = warp;
+    double mx = -1.0, zk = 0.0;
+    int km = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double v = zt[(long)i * BTC + cc];
+      if (fabs(v) > mx) { mx = fabs(v); km = i; zk = v; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double m2 = __shfl_xor_sync(0xffffffffu, mx, o);
+      const int k2 = __shfl_xor_sync(0xffffffffu, km, o);
+      const double z2 = __shfl_xor_sync(0xffffffffu, zk, o);
+      if (m2 > mx || (m2 == mx && k2 < km)) { mx = m2; km = k2; zk = z2; }
+    }
+    const double sg = zk < 0.0 ? -1.0 : 1.0;
+    for (int i = lane; i < n; i += 32) V[(long)(c0 + cc) * n + i] = sg * zt[(long)i * BTC + cc];
+  }
+}
+
 // The cooperative tridiagonalisation when the matrix fits the shared memory
 // of the GPU's CTAs (one per SM) and cooperative launch is available; false
 // if it was not launched.  Scratch in vp (7n doubles): v (2n), p (n), the
@@ -1743,6 +1844,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   if (!attr) {
     cudaFuncSetAttribute(k_sytrd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRD_SMEM_MAX);
     cudaFuncSetAttribute(k_backtrans, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_backtrans_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(k_invit<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
@@ -1760,10 +1862,12 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
     k_sytrd<false><<<1, TRD_T, 0, st>>>(A, n, d, e, HV, tau, vp);
   }
   note_launch();
-  // T of the WY blocks (n <= 256): on the side stream when one is given
+  // T of the WY blocks: on the side stream when one is given
   double *Tm = ws + 6 * (long)n * NT;   // (n/WYB + 1) WYB^2 doubles, inside the work size
-  const bool fork = n <= 256 && n >= 2 && side && evf && evj;
-  if (n <= 256 && n >= 2) {
+  static const bool tile_bt = !getenv("QX_BACKTRANS_TILE") || atoi(getenv("QX_BACKTRANS_TILE")) != 0;
+  const bool need_t = n >= 2 && (n <= 256 || tile_bt);
+  const bool fork = need_t && side && evf && evj;
+  if (need_t) {
     const int nblk = (n - 2 + WYB - 1) / WYB;
     cudaStream_t ts = st;
     if (fork) {
@@ -1800,7 +1904,13 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   } else {
     const size_t bt = sizeof(double) * 8 * (size_t)n;
     if (bt > 200 * 1024) { set_error("syev: n=%d too large for the back-transformation", n); return 1; }
-    k_backtrans<<<(n + 7) / 8, 256, bt, st>>>(Z, HV, tau, n, V); note_launch();
+    if (tile_bt) {
+      if (fork) cudaStreamWaitEvent(st, evj, 0);
+      k_backtrans_tile<<<(n + BTC - 1) / BTC, 256, sizeof(double) * BTC * (size_t)n, st>>>(Z, HV, Tm, n, V);
+    } else {
+      k_backtrans<<<(n + 7) / 8, 256, bt, st>>>(Z, HV, tau, n, V);
+    }
+    note_launch();
   }
   return 0;
 }

@@ -4,7 +4,9 @@ Gram-Schmidt through the blocked FP64 Cholesky and triangular inverse
 eigen-decomposition + rotation (untryt2/untryhc2, eigen.f90:1171-1451),
 against the oracle.  nb = 160 is the Si64 band count (matrix in one CTA's
 registers); nb = 200 exceeds one SM and runs on the cooperative kernels that
-spread the columns over one CTA per SM.
+spread the columns over one CTA per SM; nb = 300 also takes the
+back-transformation that keeps 8 eigenvector columns per CTA in shared
+memory.
 
 Tolerances: FP64 1e-10 (orthonormalised bands), eigenvalues 1e-10 relative;
 mixed precision (FP32 bands, 3xTF32 tensor-core contractions, FP64
@@ -58,7 +60,7 @@ def test_schmidt_reports_first_bad_pivot_in_later_block(si8, nb, bad):
         ctx.close()
 
 
-@pytest.mark.parametrize("nb", [48, 160, 200])
+@pytest.mark.parametrize("nb", [48, 160, 200, 300])
 @pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
 def test_untryt_many_blocks(si8, nb, prec):
     need_gpu()
