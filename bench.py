@@ -173,15 +173,16 @@ def cpu_sample(sys_, nb_apps, nthreads=1):
 
 
 def run_profile_step(args):
-    """W + K mixed-precision SCF iterations of the workload and nothing else,
-    printing the library's launch counts so that an ncu capture can skip the
-    set-up and warm-up launches (-s) and take exactly the timed ones (-c)."""
+    """W + K mixed-precision SCF iterations of the workload (the Si512 cell
+    with --si512) and nothing else, printing the library's launch counts so
+    that an ncu capture can skip the set-up and warm-up launches (-s) and
+    take exactly the timed ones (-c)."""
     import torch
 
     from qxmd_b200 import cell
     from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED, launch_count
     torch.cuda.set_device(0)
-    sys_ = cell.si64()
+    sys_ = cell.si512() if args.si512 else cell.si64()
     ctx = Context(sys_, QX_PREC_FP64 if args.sequential else QX_PREC_MIXED, QX_NL_GSPACE)
     ctx.put_psi(cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband))
     ctx.schmidt()
