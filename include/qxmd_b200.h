@@ -118,14 +118,17 @@ int qx_set_kb_r(qx_ctx *ctx, int natom, int lmx, const int *off, const int *mesh
 /* The real-space tables built on the device, for MD steps (setnlc
  * nlkbppr.f90:1010-1560).  Once per cell: ntype species of lmx = 4 channels,
  * radial tables tabnl((mxnl + 1), 4 * ntype) at r = k * dltnl(it), projector
- * radius rcut(ntype), poly(4 * ntype): the real solid-harmonic polynomial
+ * radius rcut(ntype), dtabnl (nullable, same shape): g'(r)/r of each radial
+ * table g, for the projector gradients of the forces (tbfnl of fnnlcl2),
+ * poly(4 * ntype): the real solid-harmonic polynomial
  * that multiplies each channel's radial value (0: 1; 1-3: x, y, z; 4-8: xy,
  * yz, zx, x^2 - y^2, 3z^2 - r^2 of the displacement from the atom), clalp(4)
  * KB energies, rdelv the volume per grid point, rba(3, 3) the lattice
  * vectors as columns (row-major here: rba[3 * x + j] = component x of
  * vector j).  The sphere must fit in half the cell along every axis. */
 int qx_set_kb_r_builder(qx_ctx *ctx, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
-                        const double *tabnl, const int *poly, const double *clalp, double rdelv, const double *rba);
+                        const double *tabnl, const double *dtabnl, const int *poly, const double *clalp, double rdelv,
+                        const double *rba);
 /* Once per geometry: the points of every atom (species ityp(natom), 0-based,
  * fractional coordinates satm(3, natom)) within its projector radius, their
  * projector values, and the x-line index of the real-space KB kernels.  The
@@ -274,11 +277,20 @@ int qx_set_force_tables(qx_ctx *ctx, int natom, int ntype, const int *ityp, cons
  *     4 sum_n occ_n sum_l vclalp_l <beta|psi_n> sum_{G != 0} G (beta_re psi_im - beta_im psi_re).
  * The ion-ion (Ewald) term is geometry only and stays with the caller. */
 int qx_forces(qx_ctx *ctx, double *floc, double *fnl);
+/* Real-space KB forces (Ry/bohr, (3, natom)) of the current psi (fnnlcl2,
+ * nlkbppr.f90:2024-3120): F_a = 2 sum_n occ_n / Omega sum_l clalp_l P_l D_l,
+ * P_l = rdelv sum_points vnl_l psi_n, D_l = rdelv sum_points grad vnl_l psi_n,
+ * psi_n(r) from the inverse FFT passes; needs the tables of qx_build_kb_r
+ * with the gradient table (dtabnl) given to qx_set_kb_r_builder. */
+int qx_forces_nl_r(qx_ctx *ctx, double *fnl);
 
 /* ---- drop-in shims with the reference's host-array arguments ----------- */
 /* kbnlpp_frc2 (nlkbpp.f90:1878): fnlc(3, natom) += the G-space KB forces of
  * cgjr(nplwex, nband) with the occupations of qx_set_occ. */
 int qxgpu_kbnlpp_frc2(qx_ctx *ctx, const double *cgjr, double *fnlc);
+/* fnnlcl2 (nlkbppr.f90:2024): fnlc(3, natom) += the real-space KB forces of
+ * cgjr(nplwex, nband) (tables of qx_build_kb_r with gradients). */
+int qxgpu_fnnlcl2(qx_ctx *ctx, const double *cgjr, double *fnlc);
 /* hcnonloc: rhcr(nplwex, nb) += local (+ real-space KB) H products of cgjr. */
 int qxgpu_hcnonloc(qx_ctx *ctx, const double *cgjr, double *rhcr, int nb);
 /* hckbpp_g (nlkbpp.f90:1284-1393): rhcr += G-space KB products of cgjr. */

@@ -389,14 +389,17 @@ def kbr_builder_tables(gs: GSphere, cell: Cell, pp: ModelPP, dl: float = 0.002) 
     """Arguments of qx_set_kb_r_builder / qx_build_kb_r for the model
     pseudopotential (one species): radial tables on r = k dl (s: A_s
     exp(-r^2/2 sig^2) Y_00; p: A_p exp(-r^2/2 sig^2) Y_1, times the
-    displacement component through poly 1-3), the projector radius, the KB
+    displacement component through poly 1-3) and their g'(r)/r tables for the
+    force gradients, the projector radius, the KB
     energies and the volume per grid point; plus the geometry."""
     mxnl = 2 * int(pp.rcut / (2.0 * dl)) + 6
     r = np.arange(mxnl + 1) * dl
     ex = np.exp(-0.5 * r * r / pp.sig ** 2)
     tabnl = np.ascontiguousarray(np.stack([pp.a_s * ex * Y00] + [pp.a_p * ex * Y1] * 3))
+    # g'(r)/r of the Gaussian radial parts: -g(r)/sig^2
+    dtabnl = np.ascontiguousarray(-tabnl / pp.sig ** 2)
     satm = np.ascontiguousarray(np.linalg.solve(gs.rba, cell.pos.T).T)
-    return dict(ntype=1, mxnl=mxnl, dltnl=np.array([dl]), rcut=np.array([pp.rcut]), tabnl=tabnl,
+    return dict(ntype=1, mxnl=mxnl, dltnl=np.array([dl]), rcut=np.array([pp.rcut]), tabnl=tabnl, dtabnl=dtabnl,
                 poly=np.arange(4, dtype=np.int32), clalp=np.array([pp.e_s, pp.e_p, pp.e_p, pp.e_p]),
                 rdelv=gs.rvol / gs.kfft0, rba=np.ascontiguousarray(gs.rba, dtype=np.float64),
                 grid=tuple(gs.grid), ityp=np.zeros(cell.natom, dtype=np.int32), satm=satm)

@@ -146,6 +146,11 @@ struct qx_ctx {
       *d_kbr_cursor = nullptr;
   int4 *d_kbr_lent = nullptr;
   void *d_kbr_vnl = nullptr, *d_kbr_sumr = nullptr, *d_kbr_bufR = nullptr;
+  double *d_kbr_dtab = nullptr;   // g'(r)/r tables (optional)
+  void *d_kbr_dvnl = nullptr;     // projector gradients per point (with d_kbr_dtab)
+  long kbr_dvnl_cap = 0;
+  double *d_kbr_fpart = nullptr, *d_kbr_fout = nullptr;
+  long kbr_fpart_n = 0;
   bool have_kbr_builder = false;
   bool defer = false;
   struct ScfGraph {
@@ -807,8 +812,8 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
 }
 
 extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
-                                   const double *tabnl, const int *poly, const double *clalp, double rdelv,
-                                   const double *rba) {
+                                   const double *tabnl, const double *dtabnl, const int *poly, const double *clalp,
+                                   double rdelv, const double *rba) {
   if (!c || ntype <= 0 || lmx != 4 || mxnl < 2 || !dltnl || !rcut || !tabnl || !poly || !clalp || !rba ||
       !(rdelv > 0.0)) {
     set_error("qx_set_kb_r_builder: bad arguments (lmx must be 4)");
@@ -856,6 +861,12 @@ extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, cons
   CK(cudaMemcpyAsync(c->d_kbr_dl, dltnl, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_kbr_rcut, rcut, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_kbr_tab, tabnl, sizeof(double) * (size_t)(mxnl + 1) * nchan, cudaMemcpyHostToDevice, c->st));
+  c->d_kbr_dtab = nullptr;
+  if (dtabnl) {
+    TRY(dalloc(c, &c->d_kbr_dtab, sizeof(double) * (size_t)(mxnl + 1) * nchan));
+    CK(cudaMemcpyAsync(c->d_kbr_dtab, dtabnl, sizeof(double) * (size_t)(mxnl + 1) * nchan, cudaMemcpyHostToDevice,
+                       c->st));
+  }
   CK(cudaMemcpyAsync(c->d_kbr_poly, poly, sizeof(int) * nchan, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(pl.d_kb_clalp, clalp, sizeof(double) * lmx, cudaMemcpyHostToDevice, c->st));
   drop_scf_graphs(c);
@@ -908,14 +919,18 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
     c->kbr_cap = cap;
     moved = true;
   }
+  if (c->d_kbr_dtab && c->kbr_dvnl_cap < c->kbr_cap) {
+    TRY(dalloc(c, &c->d_kbr_dvnl, ts * 12 * (size_t)c->kbr_cap));
+    c->kbr_dvnl_cap = c->kbr_cap;
+  }
   if (c->prec == QX_PREC_FP64)
     kbr_fill<double>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
-                     c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh, c->d_kbr_ptatom,
-                     (double *)c->d_kbr_vnl, c->st);
+                     c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
+                     c->d_kbr_ptatom, (double *)c->d_kbr_vnl, (double *)c->d_kbr_dvnl, c->st);
   else
     kbr_fill<float>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
-                    c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh, c->d_kbr_ptatom,
-                    (float *)c->d_kbr_vnl, c->st);
+                    c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
+                    c->d_kbr_ptatom, (float *)c->d_kbr_vnl, (float *)c->d_kbr_dvnl, c->st);
   if (kbr_lines(c->d_kbr_off, natom, c->d_kbr_mesh, c->d_kbr_ptatom, pl.k1, nlines, c->d_kbr_lcnt, c->d_kbr_loff,
                 c->d_kbr_cursor, c->d_kbr_lent, c->st)) {
     set_error("qx_build_kb_r: memset failed");
@@ -2013,6 +2028,53 @@ extern "C" int qx_forces(qx_ctx *c, double *floc, double *fnl) {
   if (!c) return QX_ERR_ARG;
   if (!c->have_ftab || !c->have_occ) { set_error("qx_forces: call qx_set_force_tables and qx_set_occ first"); return QX_ERR_STATE; }
   return c->prec == QX_PREC_FP64 ? forces_impl<double>(c, floc, fnl) : forces_impl<float>(c, floc, fnl);
+}
+
+// Real-space KB forces of the current psi (fnnlcl2, nlkbppr.f90:2024-3120),
+// from the tables of qx_build_kb_r with the gradient table given.
+template <typename T>
+static int fnl_r_impl(qx_ctx *c, double *fnl) {
+  const Plan &pl = c->pl;
+  const int natom = pl.natom;
+  const long need = (long)c->npair_all * natom * 3;
+  if (need > c->kbr_fpart_n) {
+    TRY(dalloc(c, &c->d_kbr_fpart, sizeof(double) * need));
+    TRY(dalloc(c, &c->d_kbr_fout, sizeof(double) * 3 * (size_t)natom));
+    c->kbr_fpart_n = need;
+  }
+  PipeParams P = base_params(c);
+  for (int p0 = 0; p0 < c->npair_all; p0 += pl.chunk) {
+    P.pair0 = p0;
+    const int npl = std::min(pl.chunk, c->npair_all - p0);
+    P.npair = p0 + npl;
+    TRY(launch_fnl_r_chunk<T>(pl, P, npl, (const T *)c->psi, c->ne, (const T *)c->d_kbr_dvnl, c->d_wocc,
+                              c->d_kbr_fpart, c->st));
+    CKL();
+  }
+  fnl_r_sum(c->d_kbr_fpart, c->npair_all, natom, c->d_kbr_fout, c->st);
+  CKL();
+  CK(cudaMemcpyAsync(fnl, c->d_kbr_fout, sizeof(double) * 3 * natom, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+extern "C" int qx_forces_nl_r(qx_ctx *c, double *fnl) {
+  if (!c || !fnl) { set_error("qx_forces_nl_r: null"); return QX_ERR_ARG; }
+  if (!c->have_occ) { set_error("qx_forces_nl_r: occupations not set"); return QX_ERR_STATE; }
+  if (!c->have_kbr || !c->d_kbr_dvnl || c->pl.d_kb_mesh != c->d_kbr_mesh) {
+    set_error("qx_forces_nl_r: real-space tables with gradients (qx_set_kb_r_builder with dtabnl, qx_build_kb_r) needed");
+    return QX_ERR_STATE;
+  }
+  return c->prec == QX_PREC_FP64 ? fnl_r_impl<double>(c, fnl) : fnl_r_impl<float>(c, fnl);
+}
+
+extern "C" int qxgpu_fnnlcl2(qx_ctx *c, const double *cgjr, double *fnlc) {
+  if (!c || !cgjr || !fnlc) return QX_ERR_ARG;
+  TRY(qx_put_psi(c, cgjr));
+  std::vector<double> f(3 * (size_t)std::max(c->pl.natom, 1));
+  TRY(qx_forces_nl_r(c, f.data()));
+  for (int i = 0; i < 3 * c->pl.natom; ++i) fnlc[i] += f[i];
+  return QX_OK;
 }
 
 extern "C" int qxgpu_kbnlpp_frc2(qx_ctx *c, const double *cgjr, double *fnlc) {

@@ -475,6 +475,74 @@ __global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typen
   }
 }
 
+// Real-space KB force of one (atom, band pair) (fnnlcl2, nlkbppr.f90:2024-3120):
+// for each band b of the pair, P_l = rdelv sum_points vnl_l psi_b and
+// D_l = rdelv sum_points grad vnl_l psi_b (gradient with respect to the
+// point), then F_a += 2 occ_b / Omega sum_l clalp_l P_l D_l; one partial per
+// pair in fpart[(pair * natom + atom) * 3 + dim] (summed over pairs in a
+// fixed order afterwards).  wocc = occ / Omega.
+template <typename T>
+__global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typename c2t<T>::type *__restrict__ R,
+                                                       const int *__restrict__ off, const int *__restrict__ mesh,
+                                                       const T *__restrict__ vnl, const T *__restrict__ dvnl,
+                                                       const double *__restrict__ clalp, double rdelv, int natom,
+                                                       const double *__restrict__ wocc,
+                                                       double *__restrict__ fpart) {
+  typedef typename c2t<T>::type C;
+  const int at = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= pair_count(P)) return;
+  const long n = (long)P.k1 * P.k2 * P.k3;
+  const C *Rp = R + (long)pl * n;
+  double acc[32];   // P[band][l] (8), then D[band][l][dim] (24)
+#pragma unroll
+  for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+  for (int mm = off[at] + threadIdx.x; mm < off[at + 1]; mm += blockDim.x) {
+    const C z = Rp[mesh[mm]];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const double v = (double)vnl[(long)mm * 4 + l];
+      acc[l] += v * (double)z.x;
+      acc[4 + l] += v * (double)z.y;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double g = (double)dvnl[((long)mm * 4 + l) * 3 + d];
+        acc[8 + l * 3 + d] += g * (double)z.x;
+        acc[20 + l * 3 + d] += g * (double)z.y;
+      }
+    }
+  }
+  __shared__ double red[QX_THREADS / 32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    const double sq = block_sum(acc[q], red);
+    if (threadIdx.x == 0) acc[q] = sq;
+  }
+  if (threadIdx.x == 0) {
+    const int b[2] = {P.pairs[2 * p], P.pairs[2 * p + 1]};
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int h = 0; h < 2; ++h) {
+      if (b[h] < 0) continue;
+      const double w = 2.0 * wocc[b[h]] * rdelv * rdelv;
+      for (int l = 0; l < 4; ++l)
+        for (int d = 0; d < 3; ++d) f[d] += w * clalp[l] * acc[4 * h + l] * acc[8 + 12 * h + l * 3 + d];
+    }
+    double *o = fpart + ((long)p * natom + at) * 3;
+    o[0] = f[0];
+    o[1] = f[1];
+    o[2] = f[2];
+  }
+}
+
+// fnl[atom * 3 + dim] = sum over pairs of fpart, in pair order
+__global__ void k_fnl_r_sum(const double *__restrict__ fpart, int npair, int natom, double *__restrict__ fnl) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= natom * 3) return;
+  double s = 0.0;
+  for (int p = 0; p < npair; ++p) s += fpart[(long)p * natom * 3 + q];
+  fnl[q] = s;
+}
+
 // sumr(l, atom) = rdelv * clalp_l * sum_points vnl_l * psi(point), both bands
 // of the pair at once (real part band A, imaginary part band B).
 template <typename T>
@@ -785,6 +853,39 @@ int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin,
   return 0;
 }
 
+// psi(r) of a chunk of band pairs (z, y, x inverse passes into bufR) and the
+// real-space KB force partials of every (atom, pair).
+template <typename T>
+int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const T *dvnl,
+                       const double *wocc, double *fpart, cudaStream_t st) {
+  typedef typename c2t<T>::type C;
+  const size_t cs = sizeof(C);
+  Bufs<T> &bf = pl.bufs<T>();
+  const FftTabs<T> g1 = tabs<T>(pl, 0), g2 = tabs<T>(pl, 1), g3 = tabs<T>(pl, 2);
+  dim3 gz(P.P2, npl);
+  if (!(sizeof(T) == sizeof(float) &&
+        launch_zcols_inv_f32(P, npl, (const float *)cin, ldc, (float2 *)bf.bufA, st) == 0)) {
+    k_zinv<T><<<gz, QX_THREADS, fft_smem(P.L3, P.P1 | 1, cs), st>>>(P, cin, ldc, bf.bufA, g3); note_launch();
+  }
+  dim3 gy(P.k3, npl);
+  k_ypass<T, +1><<<gy, QX_THREADS, fft_smem(P.L2, P.P1, cs), st>>>(P, bf.bufA, bf.bufB, g2); note_launch();
+  const int nlines = pl.xlines<T>();
+  const int nch = (P.k2 + nlines - 1) / nlines;
+  dim3 gx(P.k3 * nch, npl);
+  k_xinv_r<T><<<gx, QX_THREADS, fft_smem(P.L1, nlines | 1, cs), st>>>(P, bf.bufB, bf.bufR, nlines, nch, g1);
+  note_launch();
+  dim3 ga(pl.natom, npl);
+  k_fnl_r<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
+                                        pl.rdelv, pl.natom, wocc, fpart);
+  note_launch();
+  return 0;
+}
+
+void fnl_r_sum(const double *fpart, int npair, int natom, double *fnl, cudaStream_t st) {
+  k_fnl_r_sum<<<(natom * 3 + 127) / 128, 128, 0, st>>>(fpart, npair, natom, fnl);
+  note_launch();
+}
+
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st) {
   typedef typename c2t<T>::type C;
@@ -874,6 +975,10 @@ template int launch_rho_chunk<float>(const Plan &, const PipeParams &, int, cons
                                      double *, int, cudaStream_t);
 template int launch_rho_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, const double *,
                                       double *, int, cudaStream_t);
+template int launch_fnl_r_chunk<float>(const Plan &, const PipeParams &, int, const float *, long, const float *,
+                                       const double *, double *, cudaStream_t);
+template int launch_fnl_r_chunk<double>(const Plan &, const PipeParams &, int, const double *, long, const double *,
+                                        const double *, double *, cudaStream_t);
 template int launch_full_fft<float>(const Plan &, float2 *, int, double, cudaStream_t);
 template int launch_full_fft<double>(const Plan &, double2 *, int, double, cudaStream_t);
 template void set_fft_smem_limits<float>(size_t);

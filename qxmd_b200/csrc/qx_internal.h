@@ -98,6 +98,11 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
 template <typename T>
 int launch_rho_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const double *wocc,
                      double *rho, int accumulate, cudaStream_t st);
+// real-space KB force partials of a chunk of band pairs (fpart: npair x natom x 3)
+template <typename T>
+int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, const T *dvnl,
+                       const double *wocc, double *fpart, cudaStream_t st);
+void fnl_r_sum(const double *fpart, int npair, int natom, double *fnl, cudaStream_t st);
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
 template <typename T> void set_fft_smem_limits(size_t bytes);
@@ -191,8 +196,8 @@ void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm,
                int *off, cudaStream_t st);
 template <typename T>
 void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
-              const double *dltnl, const double *tabnl, int mxnl, const int *poly, const int *off, long cap,
-              int *mesh, int *ptatom, T *vnl, cudaStream_t st);
+              const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl, const int *poly,
+              const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st);
 int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int k1, long nlines, int *lcnt,
               int *loff, int *cursor, int4 *lent, cudaStream_t st);
 

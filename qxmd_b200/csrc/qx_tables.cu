@@ -192,12 +192,38 @@ __global__ void __launch_bounds__(1024) k_scan1(const int *__restrict__ in, long
   if (t == 1023) out[n] = part[1023];
 }
 
+// gradient of the polynomial of kbr_poly
+__device__ __forceinline__ void kbr_dpoly(int c, double x, double y, double z, double &gx, double &gy, double &gz) {
+  gx = gy = gz = 0.0;
+  switch (c) {
+    case 0: break;
+    case 1: gx = 1.0; break;
+    case 2: gy = 1.0; break;
+    case 3: gz = 1.0; break;
+    case 4: gx = y; gy = x; break;
+    case 5: gy = z; gz = y; break;
+    case 6: gx = z; gz = x; break;
+    case 7: gx = 2.0 * x; gy = -2.0 * y; break;
+    default: gx = -2.0 * x; gy = -2.0 * y; gz = 4.0 * z; break;
+  }
+}
+
+__device__ __forceinline__ double kbr_interp(const double *tb, int mm, double d) {
+  const double t0 = tb[mm], t1 = tb[mm + 1], t2 = tb[mm + 2];
+  const double av = 2.0 * (t0 + t2 - 2.0 * t1);
+  return d * ((d - 1.0) * av + t2 - t0) + t0;
+}
+
+// dvnl (optional): the gradient of each projector with respect to the point,
+// grad (g(r) P(d)) = (g'(r)/r) P(d) d + g(r) grad P(d), from the table
+// dtabnl of g'(r)/r; dvnl[(i * lmx + l) * 3 + dim].
 template <typename T>
 __global__ void k_kbr_fill(KbrGeom G, int lmx, const int *__restrict__ ityp, const double *__restrict__ satm,
                            const double *__restrict__ rcut, const double *__restrict__ dltnl,
-                           const double *__restrict__ tabnl, int mxnl, const int *__restrict__ poly,
-                           const int *__restrict__ off, int natom, long cap, int *__restrict__ mesh,
-                           int *__restrict__ ptatom, T *__restrict__ vnl) {
+                           const double *__restrict__ tabnl, const double *__restrict__ dtabnl, int mxnl,
+                           const int *__restrict__ poly, const int *__restrict__ off, int natom, long cap,
+                           int *__restrict__ mesh, int *__restrict__ ptatom, T *__restrict__ vnl,
+                           T *__restrict__ dvnl) {
   if (off[natom] > cap) return;   // the host grows the buffers and launches again
   const int a = blockIdx.x, it = ityp[a];
   const double *s = satm + 3 * a;
@@ -234,11 +260,17 @@ __global__ void k_kbr_fill(KbrGeom G, int lmx, const int *__restrict__ ityp, con
       const double d = 0.5 * (r / dl - (double)mm);
       for (int l = 0; l < lmx; ++l) {
         const int ch = l + lmx * it;
-        const double *tb = tabnl + (long)ch * (mxnl + 1);
-        const double t0 = tb[mm], t1 = tb[mm + 1], t2 = tb[mm + 2];
-        const double av = 2.0 * (t0 + t2 - 2.0 * t1);
-        const double f = d * ((d - 1.0) * av + t2 - t0) + t0;
-        vnl[i * lmx + l] = (T)(f * kbr_poly(poly[ch], dx, dy, dz));
+        const double f = kbr_interp(tabnl + (long)ch * (mxnl + 1), mm, d);
+        const double pv = kbr_poly(poly[ch], dx, dy, dz);
+        vnl[i * lmx + l] = (T)(f * pv);
+        if (dvnl) {
+          const double fd = kbr_interp(dtabnl + (long)ch * (mxnl + 1), mm, d);
+          double gx, gy, gz;
+          kbr_dpoly(poly[ch], dx, dy, dz, gx, gy, gz);
+          dvnl[(i * lmx + l) * 3 + 0] = (T)(fd * pv * dx + f * gx);
+          dvnl[(i * lmx + l) * 3 + 1] = (T)(fd * pv * dy + f * gy);
+          dvnl[(i * lmx + l) * 3 + 2] = (T)(fd * pv * dz + f * gz);
+        }
       }
     }
     __syncthreads();
@@ -291,18 +323,18 @@ void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm,
 
 template <typename T>
 void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
-              const double *dltnl, const double *tabnl, int mxnl, const int *poly, const int *off, long cap,
-              int *mesh, int *ptatom, T *vnl, cudaStream_t st) {
-  k_kbr_fill<T><<<natom, 256, 0, st>>>(G, lmx, ityp, satm, rcut, dltnl, tabnl, mxnl, poly, off, natom, cap, mesh,
-                                       ptatom, vnl);
+              const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl, const int *poly,
+              const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st) {
+  k_kbr_fill<T><<<natom, 256, 0, st>>>(G, lmx, ityp, satm, rcut, dltnl, tabnl, dtabnl, mxnl, poly, off, natom, cap,
+                                       mesh, ptatom, vnl, dtabnl ? dvnl : nullptr);
   note_launch();
 }
 template void kbr_fill<float>(const KbrGeom &, int, int, const int *, const double *, const double *,
-                              const double *, const double *, int, const int *, const int *, long, int *, int *,
-                              float *, cudaStream_t);
+                              const double *, const double *, const double *, int, const int *, const int *, long,
+                              int *, int *, float *, float *, cudaStream_t);
 template void kbr_fill<double>(const KbrGeom &, int, int, const int *, const double *, const double *,
-                               const double *, const double *, int, const int *, const int *, long, int *, int *,
-                               double *, cudaStream_t);
+                               const double *, const double *, const double *, int, const int *, const int *, long,
+                               int *, int *, double *, double *, cudaStream_t);
 
 int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int k1, long nlines, int *lcnt,
               int *loff, int *cursor, int4 *lent, cudaStream_t st) {

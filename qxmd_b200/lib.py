@@ -26,6 +26,7 @@ QX_ERR = {1: "ARG", 2: "CUDA", 3: "NOTPD", 4: "EIG", 5: "STATE"}
 EXPORTS = [
     "qx_last_error", "qx_version", "qx_launch_count", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
     "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g", "qx_set_kb_r_builder", "qx_build_kb_r", "qx_get_kb_r",
+    "qx_forces_nl_r", "qxgpu_fnnlcl2",
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
     "qx_sync", "qx_hpsi", "qx_ekinetic", "qx_enonloc", "qx_hmatrix", "qx_gradres", "qx_untryt",
@@ -95,8 +96,10 @@ def lib(build_if_missing: bool = True):
         "qx_set_kb_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _ip, _ip, _dp, _ip], C.c_int),
         "qx_build_kb_g": ([_ctx, C.c_int, _ip, _dp], C.c_int),
         "qx_get_kb_g": ([_ctx, _dp, _dp], C.c_int),
-        "qx_set_kb_r_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _ip, _dp, C.c_double, _dp],
+        "qx_set_kb_r_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _vp, _ip, _dp, C.c_double, _dp],
                                 C.c_int),
+        "qx_forces_nl_r": ([_ctx, _dp], C.c_int),
+        "qxgpu_fnnlcl2": ([_ctx, _dp, _dp], C.c_int),
         "qx_build_kb_r": ([_ctx, C.c_int, _ip, _dp], C.c_int),
         "qx_get_kb_r": ([_ctx, C.POINTER(C.c_int), _vp, _vp, _vp], C.c_int),
         "qx_set_kb_r": ([_ctx, C.c_int, C.c_int, _ip, _ip, _dp, _dp, C.c_double], C.c_int),
@@ -361,9 +364,17 @@ class Context:
 
     def set_kb_r_builder(self, b: dict):
         """qx_set_kb_r_builder from the dict of cell.kbr_builder_tables."""
+        dt = _f64(b["dtabnl"]) if b.get("dtabnl") is not None else None
         _ck(self.L.qx_set_kb_r_builder(self.h, b["ntype"], 4, b["mxnl"], _f64(b["dltnl"]), _f64(b["rcut"]),
-                                       _f64(b["tabnl"]), np.ascontiguousarray(b["poly"], dtype=np.int32),
+                                       _f64(b["tabnl"]), None if dt is None else dt.ctypes.data,
+                                       np.ascontiguousarray(b["poly"], dtype=np.int32),
                                        _f64(b["clalp"]), b["rdelv"], _f64(b["rba"])), "qx_set_kb_r_builder")
+
+    def forces_nl_r(self):
+        """Real-space KB forces (natom, 3) Ry/bohr of the current psi."""
+        f = np.zeros(3 * self.sys.cell.natom)
+        _ck(self.L.qx_forces_nl_r(self.h, f), "qx_forces_nl_r")
+        return f.reshape(-1, 3)
 
     def build_kb_r(self, ityp, satm):
         """qx_build_kb_r: the real-space KB tables of the geometry satm (natom, 3) fractional."""

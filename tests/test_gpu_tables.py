@@ -166,3 +166,48 @@ def test_build_kb_r_rejects_sphere_wider_than_half_cell(si8):
         assert "wider than half the cell" in str(e.value)
     finally:
         ctx.close()
+
+
+def _e_nl_r(s, b, satm, psi):
+    """sum_n occ_n <psi_n|V_NL psi_n> with the oracle's real-space tables
+    (setnlc restated) at the fractional coordinates satm."""
+    off, mesh, vnl = tables.setnlc(b, b["ityp"], satm)
+    sr = _kbr_system(s, off, mesh, vnl, b)
+    dh = oracle.Ham(sr, QX_NL_RSPACE).hpsi(psi) - oracle.Ham(sr, 0).hpsi(psi)
+    return sum(s.occ[n] * oracle.dot(psi[n], dh[n]) for n in range(min(s.occ.size, psi.shape[0])))
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-4), (QX_PREC_MIXED, 1e-4)])
+def test_real_space_kb_forces_match_energy_differences(si8, si8_psi, prec, tol):
+    """fnnlcl2 on the device (qx_forces_nl_r) against central differences
+    (h = 1e-3 bohr) of the oracle's real-space KB energy with the tables
+    rebuilt at each displaced geometry; tolerance relative to the largest
+    force component.  The force, like fnnlcl2's, differentiates over a fixed
+    point set; the energy differences also see grid points crossing the
+    projector radius, a term proportional to the projector's size there
+    (3e-4 of the force at 4.0 bohr, measured), so the test uses a 4.4 bohr
+    radius where the Gaussian projectors are 13 times smaller at the edge."""
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, dataclasses.replace(si8.pp, rcut=4.4))
+    satm = _moved(b["satm"], 3)
+    ctx = Context(si8, prec, QX_NL_RSPACE)
+    try:
+        ctx.set_kb_r_builder(b)
+        ctx.build_kb_r(b["ityp"], satm)
+        ctx.put_psi(si8_psi)
+        f = ctx.forces_nl_r()
+    finally:
+        ctx.close()
+    h = 1e-3
+    ainv = np.linalg.inv(si8.gs.rba)
+    fd = np.zeros((2, 3))
+    for k, a in enumerate((0, 5)):
+        for d in range(3):
+            ds = ainv[:, d] * h
+            sp, sm = satm.copy(), satm.copy()
+            sp[a] += ds
+            sm[a] -= ds
+            fd[k, d] = -(_e_nl_r(si8, b, sp, si8_psi) - _e_nl_r(si8, b, sm, si8_psi)) / (2 * h)
+    scale = np.max(np.abs(f))
+    assert scale > 1e-3
+    assert np.max(np.abs(f[[0, 5]] - fd)) / scale < tol
