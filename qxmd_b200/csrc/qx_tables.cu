@@ -297,18 +297,37 @@ __global__ void k_kbr_line_fill(const int *__restrict__ off, int natom, const in
   }
 }
 
-// one thread per line: entries ordered by point index (insertion sort; lines are short)
-__global__ void k_kbr_line_sort(const int *__restrict__ loff, long nlines, int4 *__restrict__ lent) {
-  for (long l = blockIdx.x * (long)blockDim.x + threadIdx.x; l < nlines; l += (long)gridDim.x * blockDim.x) {
-    const int lo = loff[l], hi = loff[l + 1];
-    for (int i = lo + 1; i < hi; ++i) {
-      const int4 v = lent[i];
-      int j = i - 1;
-      while (j >= lo && lent[j].y > v.y) {
-        lent[j + 1] = lent[j];
-        --j;
+// One block per line: entries ordered by point index.  Up to LSORT_MAX
+// entries go to shared memory and each lands at its rank (the count of
+// smaller point indices; indices are unique); a longer line is sorted by one
+// thread in place (insertion sort).
+constexpr int LSORT_MAX = 1024;
+__global__ void __launch_bounds__(128) k_kbr_line_sort(const int *__restrict__ loff, long nlines,
+                                                       int4 *__restrict__ lent) {
+  __shared__ int4 e[LSORT_MAX];
+  for (long l = blockIdx.x; l < nlines; l += gridDim.x) {
+    const int lo = loff[l], hi = loff[l + 1], m = hi - lo;
+    if (m <= 1) continue;   // uniform across the block
+    if (m <= LSORT_MAX) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) e[i] = lent[lo + i];
+      __syncthreads();
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int key = e[i].y;
+        int r = 0;
+        for (int j = 0; j < m; ++j) r += e[j].y < key ? 1 : 0;
+        lent[lo + r] = e[i];
       }
-      lent[j + 1] = v;
+      __syncthreads();
+    } else if (threadIdx.x == 0) {
+      for (int i = lo + 1; i < hi; ++i) {
+        const int4 v = lent[i];
+        int j = i - 1;
+        while (j >= lo && lent[j].y > v.y) {
+          lent[j + 1] = lent[j];
+          --j;
+        }
+        lent[j + 1] = v;
+      }
     }
   }
 }
@@ -345,7 +364,7 @@ int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int
   note_launch();
   k_kbr_line_fill<<<148 * 4, 256, 0, st>>>(off, natom, mesh, ptatom, k1, cursor, lent);
   note_launch();
-  k_kbr_line_sort<<<(unsigned)std::min<long>(148 * 4, (nlines + 127) / 128), 128, 0, st>>>(loff, nlines, lent);
+  k_kbr_line_sort<<<(unsigned)std::min<long>(148 * 16, nlines), 128, 0, st>>>(loff, nlines, lent);
   note_launch();
   return 0;
 }
