@@ -104,7 +104,10 @@ int qx_set_kb_builder(qx_ctx *ctx, int ntype, int lmx, int mxqlm, const double *
  * stscfn_pw pwlda.f90:5711-5850): eqlmr_ and vclalp of natom atoms of
  * species ityp(natom) (0-based) at fractional coordinates satm(3, natom),
  * projector j = l + lmx * a.  Reuses the table buffers when the projector
- * count is unchanged, so captured SCF-iteration graphs stay valid. */
+ * count is unchanged, so captured SCF-iteration graphs stay valid.  When
+ * force tables were set (qx_set_force_tables, same natom and projector
+ * count) their species, phases and KB derivative tables follow the new
+ * geometry too, so qx_forces needs no new qx_set_force_tables. */
 int qx_build_kb_g(qx_ctx *ctx, int natom, const int *ityp, const double *satm);
 /* Reads back the G-space KB tables in use (eqlmr_(nplwex, nproj), vclalp(nproj);
  * either pointer may be null), converted to double. */

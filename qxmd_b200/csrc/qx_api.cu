@@ -122,7 +122,7 @@ struct qx_ctx {
   // status, d_info[2] CG band applications) read once at the end, and the
   // whole iteration is captured as a graph per buffer arrangement
   // Hellmann-Feynman force tables (qx_set_force_tables)
-  int f_natom = 0, f_ntype = 0, f_n5 = 0, f_km[3] = {0, 0, 0}, f_ktot = 0;
+  int f_natom = 0, f_ntype = 0, f_n5 = 0, f_km[3] = {0, 0, 0}, f_ktot = 0, f_nproj = 0;
   int *d_ityp = nullptr, *d_ijk5 = nullptr, *d_ngabc = nullptr;
   double *d_satm = nullptr, *d_gvec5 = nullptr, *d_svco = nullptr, *d_gw = nullptr, *d_dcq = nullptr,
          *d_dsq = nullptr, *d_force = nullptr;
@@ -724,6 +724,19 @@ extern "C" int qx_build_kb_g(qx_ctx *c, int natom, const int *ityp, const double
                   c->pl.b32.vclalp, c->st);
   CKL();
   c->have_kbg = true;
+  // force tables of an earlier qx_set_force_tables follow the new geometry:
+  // species, phases and the KB derivative tables (the G-vector arrays and
+  // form factors do not depend on it)
+  if (c->have_ftab && c->f_natom == natom && c->f_nproj == nproj) {
+    CK(cudaMemcpyAsync(c->d_ityp, c->d_kb_ityp, sizeof(int) * natom, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_satm, c->d_kb_satm, sizeof(double) * 3 * natom, cudaMemcpyDeviceToDevice, c->st));
+    phase_tables(natom, c->d_satm, c->f_km[0], c->f_km[1], c->f_km[2], c->f_ktot, c->d_dcq, c->d_dsq, c->st);
+    if (c->prec == QX_PREC_FP64)
+      dtab_build<double>(nproj, ne / 2 - 1, c->pl.b64.kbg, c->d_gw, (double *)c->dtab, c->st);
+    else
+      dtab_build<float>(nproj, ne / 2 - 1, c->pl.b32.kbg, c->d_gw, (float *)c->dtab, c->st);
+    CKL();
+  }
   return QX_OK;
 }
 
@@ -1985,6 +1998,7 @@ extern "C" int qx_set_force_tables(qx_ctx *c, int natom, int ntype, const int *i
   c->f_ntype = ntype;
   c->f_n5 = n5;
   c->f_ktot = ktot;
+  c->f_nproj = np;
   for (int d = 0; d < 3; ++d) c->f_km[d] = km[d];
   phase_tables(natom, c->d_satm, km[0], km[1], km[2], ktot, c->d_dcq, c->d_dsq, c->st);
   if (c->prec == QX_PREC_FP64)

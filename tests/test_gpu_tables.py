@@ -211,3 +211,36 @@ def test_real_space_kb_forces_match_energy_differences(si8, si8_psi, prec, tol):
     scale = np.max(np.abs(f))
     assert scale > 1e-3
     assert np.max(np.abs(f[[0, 5]] - fd)) / scale < tol
+
+
+def test_build_kb_g_moves_the_force_tables(si8, si8_psi):
+    """After qx_set_force_tables at one geometry, qx_build_kb_g at another
+    carries the force path along (species, phases, KB derivative tables):
+    qx_forces then equals a context set up from scratch at the new geometry
+    with the analytic tables (1e-6 of the largest component: the tables
+    differ by the interpolation, 5e-9 of their largest entry)."""
+    need_gpu()
+    b = cell.kb_builder_tables(si8.gs, si8.cell, si8.pp)
+    satm = _moved(b["satm"], 30)
+    pos = satm @ si8.gs.rba.T
+    cb = dataclasses.replace(si8.cell, pos=pos)
+    kb, vcl = cell.kb_tables_g(si8.gs, cb, si8.pp)
+    sb = dataclasses.replace(si8, cell=cb, kb_g=kb, vclalp=vcl)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    try:
+        ctx.set_force_tables()
+        ctx.set_kb_builder(b)
+        ctx.build_kb_g(b["ityp"], satm)
+        ctx.put_psi(si8_psi)
+        fl, fn = ctx.forces()
+    finally:
+        ctx.close()
+    ref = Context(sb, QX_PREC_FP64, QX_NL_GSPACE)
+    try:
+        ref.set_force_tables()
+        ref.put_psi(si8_psi)
+        rl, rn = ref.forces()
+    finally:
+        ref.close()
+    assert np.max(np.abs(fl - rl)) / np.max(np.abs(rl)) < 1e-10
+    assert np.max(np.abs(fn - rn)) / np.max(np.abs(rn)) < 1e-6
