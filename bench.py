@@ -298,6 +298,20 @@ def kb_build_timing(sys_, ctx, R, W, flush):
         t += e0.elapsed_time(e1)
     npts = ctx.get_kb_r(sys_.cell.natom)[1].size
     out["real_space"] = {"ms_per_geometry": t / R, "points": int(npts)}
+    # real-space KB forces (fnnlcl2) of all bands on these tables: psi(r) by
+    # the inverse passes, then the projector and gradient sums per atom
+    ctx.put_psi(cell.random_wavefunctions(sys_.gs.nplwex, ctx.nb))
+    ctx.forces_nl_r()
+    t = 0.0
+    for _ in range(R):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.forces_nl_r()
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1)
+    out["real_space"]["forces_ms"] = t / R
     return out
 
 

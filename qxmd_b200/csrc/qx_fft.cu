@@ -486,12 +486,16 @@ __global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typena
                                                        const int *__restrict__ off, const int *__restrict__ mesh,
                                                        const T *__restrict__ vnl, const T *__restrict__ dvnl,
                                                        const double *__restrict__ clalp, double rdelv, int natom,
-                                                       const double *__restrict__ wocc,
+                                                       const double *__restrict__ wocc, int npl, int ppb,
                                                        double *__restrict__ fpart) {
   typedef typename c2t<T>::type C;
   const int at = blockIdx.x;
-  const int pl = blockIdx.y, p = P.pair0 + pl;
-  if (p >= pair_count(P)) return;
+  // ppb pairs of the chunk per block, one after another, so that the atom's
+  // table slice is read from cache after the first
+  const int pend = min(npl, (int)(blockIdx.y + 1) * ppb);
+  for (int pl = blockIdx.y * ppb; pl < pend; ++pl) {
+  const int p = P.pair0 + pl;
+  if (p >= pair_count(P)) break;   // uniform across the block
   const long n = (long)P.k1 * P.k2 * P.k3;
   const C *Rp = R + (long)pl * n;
   double acc[32];   // P[band][l] (8), then D[band][l][dim] (24)
@@ -512,13 +516,26 @@ __global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typena
       }
     }
   }
-  __shared__ double red[QX_THREADS / 32];
+  // the 32 sums: warp shuffles, then one pass over the warps' partials
+  __shared__ double red[QX_THREADS / 32][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < 32; ++q) {
-    const double sq = block_sum(acc[q], red);
-    if (threadIdx.x == 0) acc[q] = sq;
+    double v = acc[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][q] = v;
   }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+    red[0][threadIdx.x] = v;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = red[0][q];
     const int b[2] = {P.pairs[2 * p], P.pairs[2 * p + 1]};
     double f[3] = {0.0, 0.0, 0.0};
     for (int h = 0; h < 2; ++h) {
@@ -531,6 +548,8 @@ __global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typena
     o[0] = f[0];
     o[1] = f[1];
     o[2] = f[2];
+  }
+  __syncthreads();
   }
 }
 
@@ -874,9 +893,12 @@ int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *ci
   dim3 gx(P.k3 * nch, npl);
   k_xinv_r<T><<<gx, QX_THREADS, fft_smem(P.L1, nlines | 1, cs), st>>>(P, bf.bufB, bf.bufR, nlines, nch, g1);
   note_launch();
-  dim3 ga(pl.natom, npl);
+  // about two blocks per SM: pairs split over gy groups of ppb
+  const int gyf = std::max(1, std::min(npl, (2 * 148 + pl.natom - 1) / pl.natom));
+  const int ppb = (npl + gyf - 1) / gyf;
+  dim3 ga(pl.natom, (npl + ppb - 1) / ppb);
   k_fnl_r<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
-                                        pl.rdelv, pl.natom, wocc, fpart);
+                                        pl.rdelv, pl.natom, wocc, npl, ppb, fpart);
   note_launch();
   return 0;
 }
