@@ -893,8 +893,8 @@ int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *ci
   dim3 gx(P.k3 * nch, npl);
   k_xinv_r<T><<<gx, QX_THREADS, fft_smem(P.L1, nlines | 1, cs), st>>>(P, bf.bufB, bf.bufR, nlines, nch, g1);
   note_launch();
-  // about two blocks per SM: pairs split over gy groups of ppb
-  const int gyf = std::max(1, std::min(npl, (2 * 148 + pl.natom - 1) / pl.natom));
+  // about four blocks per SM: pairs split over gy groups of ppb
+  const int gyf = std::max(1, std::min(npl, (4 * 148 + pl.natom - 1) / pl.natom));
   const int ppb = (npl + gyf - 1) / gyf;
   dim3 ga(pl.natom, (npl + ppb - 1) / ppb);
   k_fnl_r<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
