@@ -41,14 +41,29 @@ PULAY_ASLH, PULAY_Q0, PULAY_ITRATN, PULAY_CMETRIC = 0.8, 0.8, 10, 20.0
 # FP32 H|psi> pass of this workload (ncu, --profile-hpsi; the capture command
 # is listed with the figures in the profiles directory)
 HPSI_PASS_DRAM_BYTES = 69812480
+# What limits the pipeline (ncu on the plane pass, the largest of its
+# kernels): its DRAM traffic is a fraction of the algorithmic bytes because
+# the z-transformed planes stay in L2, so it is not HBM-bound; it is bound by
+# latency at low occupancy.
+PIPELINE_LIMITER = ("latency, not HBM: DRAM traffic is 0.17x the algorithmic bytes (planes stay in the 126 MB L2); "
+                    "plane pass k_plane at 18.75% warp occupancy, 34.8% issue active, stalls led by barrier "
+                    "and long scoreboard")
 # FP64 SCF iterations of the refinement sweep after the mixed solution converged
 REFINE_ITERS = 3
 UNIT = "iter/s"
 WORKLOAD = "Si64 diamond 2x2x2, Gamma, Ecut 16 Ry / 64 Ry, 54^3 grid, 160 bands, G-space KB"
-# Average CG H|psi> band applications per SCF iteration of this workload after
-# the warm-up iterations (measured on the device path), used to scale the
-# reference arm's band-application rate to SCF iterations.
-CG_BAPPS_PER_ITER = 250
+DATA = "synthetic (seeded Si64 cell, model pseudopotential)"
+# SCF iterations of the CPU oracle in the cpu_baseline sample (after as many
+# untimed ones): about 10 s on 16 host threads
+CPU_SAMPLE_WARMUP, CPU_SAMPLE_ITERS = 2, 3
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def workload_config(sys_, ws):
+    """The workload as both arms name it."""
+    return {"workload": WORKLOAD, "bands": sys_.nband, "nplwex": sys_.gs.nplwex, "grid": list(sys_.gs.grid),
+            "parallelism": "replicas" if ws > 1 else "single",
+            "l2": "256 MB buffer written between timed iterations (device arm)"}
 
 
 def parse():
@@ -159,19 +174,6 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_sample(sys_, nb_apps, nthreads=1):
-    """Oracle (CPU FP64 restatement) band-application rate and dense-part
-    time on this workload: returns (band-apps/s, dense seconds)."""
-    import oracle
-    from qxmd_b200 import cell
-    ham = oracle.Ham(sys_, 1)
-    c = cell.random_wavefunctions(sys_.gs.nplwex, nb_apps)
-    t = time.perf_counter()
-    ham.hpsi(c)
-    rate = nb_apps / (time.perf_counter() - t)
-    return rate
-
-
 def run_profile_step(args):
     """W + K mixed-precision SCF iterations of the workload (the Si512 cell
     with --si512) and nothing else, printing the library's launch counts so
@@ -229,24 +231,33 @@ def run_profile_hpsi(args):
 
 
 def accuracy(acc, natom, iters):
-    """Total-energy and eigenvalue deviations of each path from the plain
-    FP64 path after the same number of SCF iterations from the same start."""
-    ref = acc["fp64"]
-    out = {"iterations": iters, "etot_fp64_ry": ref["etot"], "resid_fp64": ref["resid"],
-           "detot_last_fp64_ry": ref["detot_last"]}
-    for name in ("mixed", "mixed_refined", "fp64_batched"):
+    """Total energy, eigenvalues and forces of every path after `iters` SCF
+    iterations from the same start, against the CPU FP64 oracle run to
+    self-consistency over the same iteration count on the same inputs (the
+    fixture tests/golden/si64_scf.npz, made by tests/golden/make_fixtures.py).
+    Energies Ha/atom, eigenvalues Ha, forces Ha/bohr (local + KB terms; the
+    Ewald term is geometry only and the same everywhere)."""
+    g = np.load(os.path.join(GOLDEN, "si64_scf.npz"))
+    e_or, eig_or, f_or = float(g["etot"][-1]), g["eig"], g["floc"] + g["fnl"]
+    nocc = int(g["noband"])
+    out = {"reference": "CPU FP64 oracle after the same iteration count (self-consistent: residual "
+                        f"{float(g['resid'][-1]):.1e}, last energy change "
+                        f"{abs(float(g['etot'][-1] - g['etot'][-2])):.1e} Ry)",
+           "iterations": iters, "etot_oracle_ry": e_or}
+    for name in ("mixed", "fp64", "fp64_batched", "mixed_refined"):
         a = acc[name]
-        d = abs(a["etot"] - ref["etot"])
         out[name] = {"etot_ry": a["etot"], "resid": a["resid"], "detot_last_ry": a["detot_last"],
-                     "err_ha_per_atom": 0.5 * d / natom,
-                     "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - ref["eig"]))),
-                     "force_max_abs_err_ha_per_bohr": 0.5 * float(np.max(np.abs(a["force"] - ref["force"])))}
+                     "err_ha_per_atom": 0.5 * abs(a["etot"] - e_or) / natom,
+                     "eig_occ_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"][:nocc] - eig_or[:nocc]))),
+                     "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - eig_or))),
+                     "force_max_abs_err_ha_per_bohr": 0.5 * float(np.max(np.abs(a["force"] - f_or)))}
     out["mixed_refined"]["fp64_iterations"] = REFINE_ITERS
     out["mixed_refined"]["ms"] = acc["mixed_refined"]["ms"]
     out["err_ha_per_atom"] = out["mixed"]["err_ha_per_atom"]
     out["force_err_ha_per_bohr"] = out["mixed"]["force_max_abs_err_ha_per_bohr"]
-    out["force_max_abs_fp64_ha_per_bohr"] = 0.5 * float(np.max(np.abs(ref["force"])))
-    out["force_terms"] = "local pseudopotential (flocal_g) + G-space KB (kbnlpp_frc2); the ion-ion term is identical in all paths"
+    out["force_max_abs_oracle_ha_per_bohr"] = 0.5 * float(np.max(np.abs(f_or)))
+    out["gates"] = {"err_ha_per_atom": 1e-6, "force_err_ha_per_bohr": 1e-4}
+    out["force_terms"] = "local pseudopotential (flocal_g) + G-space KB (kbnlpp_frc2)"
     return out
 
 
@@ -591,13 +602,14 @@ def run_ours(args):
     N, ne = sys_.gs.kfft0, sys_.gs.nplwex
     bytes_per_bapp = 4 * N * 4 + 2 * ne * 4
     achieved = bytes_per_bapp * sys_.nband / (mixed["fft_pipeline_ms"] * 1e-3) / 1e9
+    fft_flops_pass = 5.0 * N * math.log2(N) * sys_.nband     # two complex transforms per band pair
     line = {
         "metric": METRIC, "value": mixed["value"], "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
         "ms_per_step": mixed["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded Si64 cell, model pseudopotential)",
-        "config": {"workload": WORKLOAD, "bands": sys_.nband, "nplwex": ne, "grid": list(sys_.gs.grid),
-                   "precision": "mixed", "parallelism": "replicas" if ws > 1 else "single",
-                   "l2": "256 MB buffer written between timed iterations", "autotune": tune_report},
+        "vs_baseline": None, "dtype": "f32+f64", "data": DATA,
+        "config": workload_config(sys_, ws),
+        "precision": "mixed: FP32 FFTs and H|psi>, 3xTF32 tensor-core contractions, FP64 Cholesky/eigen/density",
+        "autotune": tune_report,
         "hpsi_band_apps_per_s": mixed["hpsi_band_apps_per_s"],
         "fp64": {"path": "plain FP64 drop-in, one-rank band order (sequential CG, one graph launch per sweep)",
                  "value": fp64["value"], "ms_per_step": fp64["ms_per_step"],
@@ -615,23 +627,29 @@ def run_ours(args):
         "eig_clusters": mixed["eig_clusters"],
         "e2e": mixed["e2e"],
         "gpu_launches": mixed["launches"],
-        "roofline": {"kernel": "H|psi> FFT pipeline (zinv, y, xvx, y, zfwd, unpack), FP32",
+        "roofline": {"kernel": "H|psi> FFT pipeline (z inverse, plane pass, z forward), FP32",
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_band_app": bytes_per_bapp,
-                     # DRAM read + write of one all-band pass (four launches),
-                     # from the ncu capture of this workload
+                     # DRAM read + write of one all-band pass, from the ncu
+                     # capture of this workload
                      "traffic": HPSI_PASS_DRAM_BYTES, "traffic_unit": "bytes per 160-band pass",
-                     "algorithmic_bytes_per_pass": bytes_per_bapp * sys_.nband},
+                     "algorithmic_bytes_per_pass": bytes_per_bapp * sys_.nband,
+                     "fft_pipeline_ms": mixed["fft_pipeline_ms"],
+                     "dram_gbs": HPSI_PASS_DRAM_BYTES / (mixed["fft_pipeline_ms"] * 1e-3) / 1e9,
+                     "fp32_tflops": fft_flops_pass / (mixed["fft_pipeline_ms"] * 1e-3) / 1e12,
+                     "limiter": PIPELINE_LIMITER},
         "clocks": mixed["clocks"],
     }
     if ws == 1 and rank == 0:
-        rate = cpu_sample(sys_, 8)
-        bapps = sys_.nband + mixed["cg_bapps_per_iter"]
-        line["cpu_baseline"] = {"value": rate / bapps, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"8 H|psi> band-applications of this workload on the FP64 oracle "
-                                          f"({rate:.2f}/s, 1 thread) scaled by {bapps:.0f} band-applications "
-                                          f"per SCF iteration; dense band-space work not included"}
+        times, ncg = oracle_scf_timing(sys_, psi0, CPU_SAMPLE_WARMUP, CPU_SAMPLE_ITERS, host_cores())
+        v = 1.0 / float(np.mean(times))
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": host_cores(), "kind": "port",
+                                "sample": f"SCF iterations {CPU_SAMPLE_WARMUP + 1}-"
+                                          f"{CPU_SAMPLE_WARMUP + CPU_SAMPLE_ITERS} of this workload from the "
+                                          f"same start on the FP64 CPU oracle (whole iterations, "
+                                          f"{np.mean(ncg):.0f} CG band applications each), "
+                                          f"{host_cores()} host threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -639,49 +657,65 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def _ref_worker(args):
+def oracle_scf_timing(sys_, psi0, W, K, threads):
+    """W untimed then K timed SCF iterations of the FP64 CPU oracle (the
+    restatement of pwlda_md's iteration: potential, H|psi> of all bands,
+    H_sub, Jacobi diagonalisation and rotation, batched eigen_BKL, schmidt2,
+    softchg, Pulay mixing) from the same start as the device path, on
+    `threads` host threads.  Returns the per-iteration wall times (s) and the
+    CG band applications of the timed iterations."""
     import oracle
-    from qxmd_b200 import cell
-    seed, nb = args
-    sys_ = cell.si64(with_ewald=False)
-    ham = oracle.Ham(sys_, 1)
-    c = cell.random_wavefunctions(sys_.gs.nplwex, nb, seed=25.0 + seed)
-    t = time.perf_counter()
-    ham.hpsi(c)
-    return nb, time.perf_counter() - t
+    from oracle.scf import ScfState
+    oracle.set_threads(threads)
+    psi, _, rc = oracle.schmidt(psi0)
+    if rc:
+        raise RuntimeError("oracle schmidt failed on the start wavefunctions")
+    st = ScfState(sys_, psi, nlmode=1, mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0, pulay=PULAY_ITRATN,
+                  cmetric=PULAY_CMETRIC)
+    noband = int(sys_.cell.nel // 2)
+    for _ in range(W):
+        st.iteration(noband=noband)
+    times, ncg = [], []
+    for _ in range(K):
+        t = time.perf_counter()
+        r = st.iteration(noband=noband)
+        times.append(time.perf_counter() - t)
+        ncg.append(r["ncg_hpsi"])
+    return times, ncg
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def run_reference(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    """The reference arm: QXMD's own CPU build cannot be compiled on this image
+    (Fortran, FFTW and MPI are absent), so this times the CPU restatement of
+    the same iteration (the oracle) on all host threads, one SCF iteration per
+    step, on this workload from the same start."""
     rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import multiprocessing as mp
-    ncores = os.cpu_count() or 1
-    ctxm = mp.get_context("spawn")
     from qxmd_b200 import cell
-    sys_ = cell.si64(with_ewald=False)
-    bapps_iter = sys_.nband + CG_BAPPS_PER_ITER
-    times = []
-    with ctxm.Pool(ncores) as pool:
-        for step in range(args.warmup + args.steps):
-            t = time.perf_counter()
-            out = pool.map(_ref_worker, [(step * ncores + i, 1) for i in range(ncores)])
-            dt = time.perf_counter() - t
-            if step >= args.warmup:
-                times.append((sum(o[0] for o in out), dt))
-    nb_done = sum(x[0] for x in times)
-    tt = sum(x[1] for x in times)
-    rate = nb_done / tt
-    v = rate / bapps_iter
+    sys_ = cell.si64()
+    psi0 = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
+    ncores = host_cores()
+    times, ncg = oracle_scf_timing(sys_, psi0, args.warmup, args.steps, ncores)
+    ms = 1e3 * float(np.mean(times))
+    v = 1e3 / ms
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": "fp64"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+            "config": workload_config(sys_, ws),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
-                             "sample": f"each step: {ncores} Si64 H|psi> band-applications in parallel on the "
-                                       f"FP64 oracle ({rate:.2f} band-apps/s), scaled by {bapps_iter} "
-                                       f"band-applications per SCF iteration"},
+                             "sample": f"timed SCF iterations {args.warmup + 1}-{args.warmup + args.steps} of this "
+                                       f"workload on the FP64 CPU oracle (restatement of the reference "
+                                       f"iteration, batched CG, {np.mean(ncg):.0f} CG band applications per "
+                                       f"iteration), {ncores} host threads"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

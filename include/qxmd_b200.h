@@ -186,7 +186,12 @@ int qx_hmatrix(qx_ctx *ctx, double *hsub);
  * every GPU loading this library holds until exit.  Returns QX_ERR_ARG for
  * nb > QX_HMATRIX_STATIC_MAX_NB (two nb x nb partials must fit).  The first
  * call on each device looks up that array's device address (with the device
- * current) and should come before any stream capture.  All calls share the
+ * current) and should come before any stream capture.  Under CUDA's lazy
+ * module loading (the default) the array is reserved when its code module
+ * first loads on a device, which in a program that calls only this entry
+ * point is that first call: a caller that sizes and locks its memory pool at
+ * start-up should make one call then (or run with CUDA_MODULE_LOADING=EAGER,
+ * which reserves it when the library loads).  All calls share the
  * one array and it keeps the last call's partials; each call writes every
  * partial it reads, so nothing needs clearing, but calls that overlap on the
  * GPU (other streams, other host threads) race on it.  Enqueued on `stream`

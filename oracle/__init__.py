@@ -29,9 +29,12 @@ def build(force: bool = False) -> str:
     if not force and os.path.exists(_SO) and os.path.getmtime(_SO) >= os.path.getmtime(src):
         return _SO
     os.makedirs(os.path.dirname(_SO), exist_ok=True)
-    # -ffp-contract=off keeps every multiply and add as written.
-    subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11",
-                           "-ffp-contract=off", "-o", _SO, src, "-lm"])
+    # -ffp-contract=off keeps every multiply and add as written; -fopenmp
+    # runs the band loops on host threads (results independent of the count).
+    tmp = _SO + ".tmp"
+    subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-std=c11", "-fopenmp",
+                           "-ffp-contract=off", "-o", tmp, src, "-lm"])
+    os.replace(tmp, _SO)
     return _SO
 
 
@@ -88,7 +91,18 @@ def lib():
         L.orc_rotate.argtypes = [_dp, C.c_int, C.c_int, _dp]
         L.orc_softchg.argtypes = [C.POINTER(_Ham), _dp, C.c_int, _dp, C.c_double, _dp]
         L.orc_xclda.argtypes = [_dp, C.c_long, C.c_double, _dp, C.c_void_p, _dp]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_get_threads.restype = C.c_int
     return _lib
+
+
+def set_threads(n: int) -> None:
+    """Host threads of the oracle's band loops (results do not depend on it)."""
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
 
 
 def _f64(a):

@@ -9,7 +9,10 @@ numpy (FP64) from the reference:
   table): for every band n, projector l of atom a,
   fsl = sum_{g >= 1} (beta(2g) psi(2g+1) - beta(2g+1) psi(2g)) G(g),
   F_a += 2 * fsl * slmir * occ_n * 2 * vclalp_l, slmir = <beta|psi> with the
-  KB metric 2 sum - b0 c0 - 2 b1 c1 (hckbpp_ib_g, nlkbpp.f90:1678-1713).
+  KB metric 2 sum - b0 c0 - 2 b1 c1 (hckbpp_ib_g, nlkbpp.f90:1678-1713);
+* fnnlcl2 (nlkbppr.f90:2024-3120): real-space KB on the projector points of
+  setnlc, F_a = 2 sum_n occ_n / Omega sum_l clalp_l P_l D_l with P_l and its
+  gradient sum D_l over the fixed point set.
 
 The ion-ion term is qxmd_b200.cell.ewald_forces.  PARITY UNPINNED (see
 qxmd_oracle.c); the sum of the three terms is pinned by central differences
@@ -67,6 +70,31 @@ def floc_g(t: dict, rho_r: np.ndarray, grid) -> np.ndarray:
         zs = sc12 * c3 + cc12 * s3
         ftmp = t["svco"][g] * (r[g].real * zs + r[g].imag * zc)
         f[a] = 2.0 * (ftmp[:, None] * t["gvec5"][g]).sum(axis=0)
+    return f
+
+
+def fnl_r(off: np.ndarray, mesh: np.ndarray, vnl: np.ndarray, dvnl: np.ndarray, clalp: np.ndarray,
+          rdelv: float, rvol: float, psir: np.ndarray, occ: np.ndarray) -> np.ndarray:
+    """fnnlcl2 (nlkbppr.f90:2024-3120): real-space KB forces (natom, 3) Ry/bohr
+    on a fixed point set.  For band n with psi_n(r) (psir (nb, kfft0), the
+    unscaled inverse transform wvg2r) and atom a:
+      sumr_l = clalp_l P_l,  P_l = rdelv sum_points vnl_l psi_n  (svsumr of calnlc),
+      sumxr_l = D_l = rdelv sum_points grad vnl_l psi_n,
+      F_a += sum_l sumr_l sumxr_l * 2 occ_n / Omega       (nlkbppr.f90:3025-3043).
+    vnl (npts, 4) and dvnl (npts, 4, 3) from oracle.tables.setnlc(grad=True)."""
+    nat = off.size - 1
+    lmx = vnl.shape[1]
+    f = np.zeros((nat, 3))
+    for n in range(psir.shape[0]):
+        if abs(occ[n]) <= 1e-15:
+            continue
+        w = 2.0 * occ[n] / rvol
+        for a in range(nat):
+            sl = slice(off[a], off[a + 1])
+            ps = psir[n, mesh[sl]]
+            p = rdelv * (ps @ vnl[sl])                               # (lmx,)
+            dd = rdelv * np.einsum("p,plx->lx", ps, dvnl[sl])       # (lmx, 3)
+            f[a] += w * ((clalp[:lmx] * p)[:, None] * dd).sum(axis=0)
     return f
 
 

@@ -20,8 +20,30 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef double complex cplx;
+
+/* Host threads of the band-parallel loops.  Every parallel loop below gives
+ * each output element to one thread and keeps the serial order of its sums,
+ * so results do not depend on the thread count. */
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
+}
+
+int orc_get_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
 
 /* ------------------------------------------------------------------------ */
 /* Mixed-radix complex FFT (recursive decimation in time, any factorisation). */
@@ -196,6 +218,7 @@ void orc_hpsi1(const orc_ham *h, const double *c, double *hc) {
 }
 
 void orc_hpsi(const orc_ham *h, const double *c, double *hc, int nb) {
+#pragma omp parallel for schedule(dynamic, 1)
   for (int b = 0; b < nb; ++b) orc_hpsi1(h, c + (long)b * h->nplwex, hc + (long)b * h->nplwex);
 }
 
@@ -243,15 +266,14 @@ typedef struct {
  * one rank, where later bands see the updated lower bands.
  * lhcunt=.true., lortho=.false.: rhcr holds H*gdcr on entry.
  * Outputs eig, bzan (final residual) and nriter per band. */
-void orc_eigen_bkl(const orc_ham *h, const orc_cgparm *pm, int nb, double *gdcr,
-                   double *rhcr, const double *ekib, double *eig, double *bzan, int *nriter) {
+/* The CG steps of one band ib (the body of the band loop of eigen_BKL,
+ * eigen.f90:283-776) against the snapshot snap of bands 0..ib-1; work arrays
+ * prcd, gnk, hnk (ne) and prod (ib). */
+static void bkl_band(const orc_ham *h, const orc_cgparm *pm, int ib, double *gdcr, double *rhcr,
+                     const double *ekib, const double *snap, double *eig, double *bzan, int *nriter,
+                     double *prcd, double *gnk, double *hnk, double *prod) {
   int ne = h->nplwex;
-  double *snap = malloc(sizeof(double) * ne * (long)nb);
-  for (long i = 0; i < (long)ne * nb; ++i)
-    snap[i] = pm->ccreal4 ? (double)(float)gdcr[i] : gdcr[i];
-  double *prcd = malloc(sizeof(double) * ne), *gnk = malloc(sizeof(double) * ne),
-         *hnk = malloc(sizeof(double) * ne), *prod = malloc(sizeof(double) * (nb + 1));
-  for (int ib = 0; ib < nb; ++ib) {
+  {
     double *x = gdcr + (long)ib * ne, *hx = rhcr + (long)ib * ne;
     prpcg(ekib[ib], h->dkgnrm, ne, prcd);
     double e = orc_dot(x, hx, ne);
@@ -328,10 +350,39 @@ void orc_eigen_bkl(const orc_ham *h, const orc_cgparm *pm, int nb, double *gdcr,
     eig[ib] = e;
     if (bzan) bzan[ib] = zansa;
     if (nriter) nriter[ib] = iter;
-    if (pm->sequential)
-      for (int i = 0; i < ne; ++i) snap[(long)ib * ne + i] = pm->ccreal4 ? (double)(float)x[i] : x[i];
   }
-  free(snap); free(prcd); free(gnk); free(hnk); free(prod);
+}
+
+/* eigen_BKL for all bands (see bkl_band).  In the one-band-per-rank order
+ * every band reads only the entry snapshot, so the bands run in parallel;
+ * the one-rank order is serial. */
+void orc_eigen_bkl(const orc_ham *h, const orc_cgparm *pm, int nb, double *gdcr,
+                   double *rhcr, const double *ekib, double *eig, double *bzan, int *nriter) {
+  int ne = h->nplwex;
+  double *snap = malloc(sizeof(double) * ne * (long)nb);
+  for (long i = 0; i < (long)ne * nb; ++i)
+    snap[i] = pm->ccreal4 ? (double)(float)gdcr[i] : gdcr[i];
+  if (pm->sequential) {
+    double *prcd = malloc(sizeof(double) * ne), *gnk = malloc(sizeof(double) * ne),
+           *hnk = malloc(sizeof(double) * ne), *prod = malloc(sizeof(double) * (nb + 1));
+    for (int ib = 0; ib < nb; ++ib) {
+      bkl_band(h, pm, ib, gdcr, rhcr, ekib, snap, eig, bzan, nriter, prcd, gnk, hnk, prod);
+      const double *x = gdcr + (long)ib * ne;
+      for (int i = 0; i < ne; ++i) snap[(long)ib * ne + i] = pm->ccreal4 ? (double)(float)x[i] : x[i];
+    }
+    free(prcd); free(gnk); free(hnk); free(prod);
+  } else {
+#pragma omp parallel
+    {
+      double *prcd = malloc(sizeof(double) * ne), *gnk = malloc(sizeof(double) * ne),
+             *hnk = malloc(sizeof(double) * ne), *prod = malloc(sizeof(double) * (nb + 1));
+#pragma omp for schedule(dynamic, 1)
+      for (int ib = 0; ib < nb; ++ib)
+        bkl_band(h, pm, ib, gdcr, rhcr, ekib, snap, eig, bzan, nriter, prcd, gnk, hnk, prod);
+      free(prcd); free(gnk); free(hnk); free(prod);
+    }
+  }
+  free(snap);
 }
 
 /* rsdecmp + rsinvcd (schmidt.f90:428-544): Cholesky S = L L^T then L^-1, both
@@ -383,28 +434,35 @@ int orc_cholinv(double *s, int n) {
  * the lower-triangular L^-1 is left in linv (n x n, column-major) if given. */
 int orc_schmidt(double *c, int ne, int nb, double *linv) {
   double *s = calloc((long)nb * nb, sizeof(double));
+#pragma omp parallel for schedule(dynamic, 1)
   for (int i = 0; i < nb; ++i)
     for (int j = 0; j <= i; ++j) s[(long)j * nb + i] = orc_dot(c + (long)j * ne, c + (long)i * ne, ne);
   int rc = orc_cholinv(s, nb);
   if (rc) { free(s); return rc; }
-  double *buf = malloc(sizeof(double) * ne);
+  /* the in-place update of schmidt.f90:284-313 runs ib downwards so that
+   * column ib still reads the old columns jb <= ib; writing into a copy gives
+   * the same sums and lets the columns run in parallel */
+  double *out = malloc(sizeof(double) * (long)ne * nb);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int ib = nb - 1; ib >= 0; --ib) {
+    double *buf = out + (long)ib * ne;
     for (int i = 0; i < ne; ++i) buf[i] = 0.0;
     for (int jb = 0; jb <= ib; ++jb) {
       double p = s[(long)jb * nb + ib];
       const double *cj = c + (long)jb * ne;
       for (int i = 0; i < ne; ++i) buf[i] += p * cj[i];
     }
-    memcpy(c + (long)ib * ne, buf, sizeof(double) * ne);
   }
+  memcpy(c, out, sizeof(double) * (long)ne * nb);
   if (linv) memcpy(linv, s, sizeof(double) * nb * nb);
-  free(s); free(buf);
+  free(s); free(out);
   return 0;
 }
 
 /* hmatrix2 (engrad.f90:845-956): H(jb,ib) = <c_jb|hc_ib>, symmetric fill,
  * eig(ib) = H(ib,ib). */
 void orc_hmatrix(const double *c, const double *hc, int ne, int nb, double *hm, double *eig) {
+#pragma omp parallel for schedule(dynamic, 1)
   for (int ib = 0; ib < nb; ++ib)
     for (int jb = 0; jb <= ib; ++jb) {
       double p = orc_dot(hc + (long)ib * ne, c + (long)jb * ne, ne);
@@ -508,6 +566,7 @@ int orc_jacobi(double *a, int n, double *w, double *v, int maxsweep) {
 /* untrycore (eigen.f90:1456-1514): C <- C*U for C (ne x nb), U (nb x nb). */
 void orc_rotate(double *c, int ne, int nb, const double *u) {
   double *out = malloc(sizeof(double) * (long)ne * nb);
+#pragma omp parallel for schedule(static)
   for (int ib = 0; ib < nb; ++ib)
     for (int i = 0; i < ne; ++i) {
       double s = 0.0;
@@ -522,12 +581,28 @@ void orc_rotate(double *c, int ne, int nb, const double *u) {
 void orc_softchg(const orc_ham *h, const double *c, int nb, const double *occ, double rvol,
                  double *rho) {
   long n = (long)h->k1 * h->k2 * h->k3;
-  double *psir = malloc(sizeof(double) * n);
+  /* bands in chunks: psi(r) of a chunk in parallel, then every grid point
+   * sums its chunk in band order, which keeps the serial order of the sums */
+  int chunk = 2 * orc_get_threads();
+  if (chunk > nb) chunk = nb;
+  if (chunk < 1) chunk = 1;
+  double *psir = malloc(sizeof(double) * n * chunk);
   for (long i = 0; i < n; ++i) rho[i] = 0.0;
-  for (int b = 0; b < nb; ++b) {
-    orc_wvg2r(c + (long)b * h->nplwex, h->nplw, h->ijk_pos, h->ijk_neg, h->k1, h->k2, h->k3, psir);
-    double f = occ[b] / rvol;
-    for (long i = 0; i < n; ++i) rho[i] += psir[i] * psir[i] * f;
+  for (int b0 = 0; b0 < nb; b0 += chunk) {
+    int m = nb - b0 < chunk ? nb - b0 : chunk;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < m; ++k)
+      orc_wvg2r(c + (long)(b0 + k) * h->nplwex, h->nplw, h->ijk_pos, h->ijk_neg, h->k1, h->k2, h->k3,
+                psir + (long)k * n);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+      double r = rho[i];
+      for (int k = 0; k < m; ++k) {
+        double p = psir[(long)k * n + i];
+        r += p * p * (occ[b0 + k] / rvol);
+      }
+      rho[i] = r;
+    }
   }
   free(psir);
 }

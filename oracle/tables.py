@@ -85,20 +85,33 @@ def _poly(c: int, x, y, z):
     return [np.ones_like(x), x, y, z, x * y, y * z, z * x, x * x - y * y, 3 * z * z - (x * x + y * y + z * z)][c]
 
 
+def _poly_grad(c: int, x, y, z):
+    """Gradient (npts, 3) of the solid-harmonic polynomial of _poly."""
+    o, z0 = np.ones_like(x), np.zeros_like(x)
+    g = [(z0, z0, z0), (o, z0, z0), (z0, o, z0), (z0, z0, o), (y, x, z0), (z0, z, y), (z, z0, x),
+         (2 * x, -2 * y, z0), (-2 * x, -2 * y, 4 * z)][c]
+    return np.stack(g, axis=1)
+
+
 def box_halfwidths(rba: np.ndarray, grid, rmax: float):
     binv = np.linalg.inv(rba)
     return [int(rmax * np.linalg.norm(binv[i]) * grid[i] + 0.5) + 1 for i in range(3)]
 
 
-def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray):
+def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
     """(off (natom+1), mesh (npts), vnl (npts, 4)) in box order; b is the dict
-    of qxmd_b200.cell.kbr_builder_tables."""
+    of qxmd_b200.cell.kbr_builder_tables.  With grad, also dvnl (npts, 4, 3):
+    the gradient of each projector value with respect to the displacement d
+    of the point from its atom, as fnnlcl2 builds it from the radial table
+    and its derivative table (nlkbppr.f90:2200-2240):
+    grad(g(r) P(d)) = (g'(r)/r) d P(d) + g(r) grad P(d), both radial tables
+    interpolated by the three-point formula of setqlm."""
     k = np.array(b["grid"])
     nd = box_halfwidths(b["rba"], b["grid"], float(np.max(b["rcut"])))
     o3, o2, o1 = np.meshgrid(np.arange(-nd[2], nd[2] + 1), np.arange(-nd[1], nd[1] + 1),
                              np.arange(-nd[0], nd[0] + 1), indexing="ij")
     o = np.stack([o1.ravel(), o2.ravel(), o3.ravel()], axis=1)
-    offs, meshes, vals = [0], [], []
+    offs, meshes, vals, grads = [0], [], [], []
     for a in range(satm.shape[0]):
         it = int(ityp[a])
         s = satm[a]
@@ -116,5 +129,19 @@ def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray):
             ch = l + 4 * it
             v[:, l] = setqlm(r, b["dltnl"][it], b["tabnl"][ch], _poly(int(b["poly"][ch]), d[:, 0], d[:, 1], d[:, 2]))
         vals.append(v)
+        if grad:
+            gv = np.empty((r.size, 4, 3))
+            one = np.ones_like(r)
+            for l in range(4):
+                ch = l + 4 * it
+                c = int(b["poly"][ch])
+                g = setqlm(r, b["dltnl"][it], b["tabnl"][ch], one)
+                dg = setqlm(r, b["dltnl"][it], b["dtabnl"][ch], one)
+                p = _poly(c, d[:, 0], d[:, 1], d[:, 2])
+                gv[:, l, :] = (dg * p)[:, None] * d + g[:, None] * _poly_grad(c, d[:, 0], d[:, 1], d[:, 2])
+            grads.append(gv)
         offs.append(offs[-1] + r.size)
-    return np.asarray(offs, dtype=np.int32), np.concatenate(meshes), np.concatenate(vals, axis=0)
+    out = (np.asarray(offs, dtype=np.int32), np.concatenate(meshes), np.concatenate(vals, axis=0))
+    if grad:
+        out = out + (np.concatenate(grads, axis=0),)
+    return out

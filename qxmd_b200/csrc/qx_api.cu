@@ -186,6 +186,31 @@ static void drop_scf_graphs(qx_ctx *c) {
   c->scf_graphs.clear();
 }
 
+// Frees a context buffer that a new one replaces (a table that grew, a
+// projector or atom count that changed), so that memory does not pile up over
+// an MD run: waits for the context's streams (kernels in flight may still
+// read it), drops every captured graph (they hold its address) and takes it
+// off the context's list.  p may be null.
+static int dfree(qx_ctx *c, void *p) {
+  if (!p) return 0;
+  CK(cudaStreamSynchronize(c->st));
+  if (c->st2) CK(cudaStreamSynchronize(c->st2));
+  drop_scf_graphs(c);
+  if (c->seq_exec) { cudaGraphExecDestroy(c->seq_exec); c->seq_exec = nullptr; }
+  if (c->seq_graph) { cudaGraphDestroy(c->seq_graph); c->seq_graph = nullptr; }
+  auto it = std::find(c->allocs.begin(), c->allocs.end(), p);
+  if (it != c->allocs.end()) c->allocs.erase(it);
+  CK(cudaFree(p));
+  return 0;
+}
+// dfree(*p), then a new buffer of `bytes` into *p.
+template <typename P>
+static int dregrow(qx_ctx *c, P **p, size_t bytes) {
+  TRY(dfree(c, (void *)*p));
+  *p = nullptr;
+  return dalloc(c, p, bytes);
+}
+
 extern "C" const char *qx_last_error(void) { return g_err; }
 extern "C" int qx_version(void) { return 1; }
 extern "C" long qx_launch_count(void) { return g_launches.load(); }
@@ -519,8 +544,7 @@ extern "C" int qx_destroy(qx_ctx *c) {
 // on demand and kept, so repeated transfers allocate nothing.
 static int stage(qx_ctx *c, long n, double **out) {
   if (c->stage_len < n) {
-    if (c->d_stage) CK(cudaStreamSynchronize(c->st));
-    TRY(dalloc(c, &c->d_stage, sizeof(double) * n));
+    TRY(dregrow(c, &c->d_stage, sizeof(double) * n));
     c->stage_len = n;
   }
   *out = c->d_stage;
@@ -593,30 +617,39 @@ static const T *kbg_operand(const qx_ctx *c, long *ld) {
 extern "C" int qx_set_kb_g(qx_ctx *c, int nproj, const double *eqlmr, const double *vclalp) {
   if (!c || nproj <= 0 || !eqlmr || !vclalp) { set_error("qx_set_kb_g: bad arguments"); return QX_ERR_ARG; }
   const size_t ts = c->tsize();
-  void *kbg = nullptr, *vcl = nullptr, *proj = nullptr;
-  TRY(dalloc(c, &kbg, ts * (size_t)nproj * c->ne));
-  TRY(dalloc(c, &vcl, ts * nproj));
-  TRY(dalloc(c, &proj, ts * (size_t)nproj * c->nb));
+  void *kbg = c->prec == QX_PREC_FP64 ? (void *)c->pl.b64.kbg : (void *)c->pl.b32.kbg;
+  void *vcl = c->prec == QX_PREC_FP64 ? (void *)c->pl.b64.vclalp : (void *)c->pl.b32.vclalp;
+  void *proj = c->proj;
+  if (!c->have_kbg || c->pl.nproj != nproj) {
+    // a new projector count: new buffers (the old ones freed); the same count
+    // (a new geometry) rewrites the tables in place, so captured SCF graphs
+    // stay valid
+    TRY(dregrow(c, &kbg, ts * (size_t)nproj * c->ne));
+    TRY(dregrow(c, &vcl, ts * nproj));
+    TRY(dregrow(c, &proj, ts * (size_t)nproj * c->nb));
+    TRY(dfree(c, c->kbgp));
+    c->kbgp = nullptr;
+    c->kbgp_ld = 0;
+    c->pl.nproj = nproj;
+    drop_scf_graphs(c);
+    TRY(tcpad_reserve(c, (long)nproj + c->nb));
+    if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
+    else {
+      c->pl.b32.kbg = (float *)kbg;
+      c->pl.b32.vclalp = (float *)vcl;
+      if (c->ne & 3) {
+        c->kbgp_ld = (c->ne + 3) & ~3L;
+        TRY(dalloc(c, &c->kbgp, sizeof(float) * (size_t)nproj * c->kbgp_ld));
+      }
+    }
+    c->proj = proj;
+  }
   TRY(up(c, kbg, eqlmr, (long)nproj * c->ne));
   TRY(up(c, vcl, vclalp, nproj));
-  c->pl.nproj = nproj;
-  drop_scf_graphs(c);
-  TRY(tcpad_reserve(c, (long)nproj + c->nb));
-  c->kbgp = nullptr;
-  c->kbgp_ld = 0;
-  if (c->prec == QX_PREC_FP64) { c->pl.b64.kbg = (double *)kbg; c->pl.b64.vclalp = (double *)vcl; }
-  else {
-    c->pl.b32.kbg = (float *)kbg;
-    c->pl.b32.vclalp = (float *)vcl;
-    if (c->ne & 3) {
-      const long ldp = (c->ne + 3) & ~3L;
-      TRY(dalloc(c, &c->kbgp, sizeof(float) * (size_t)nproj * ldp));
-      pad_rows_f32((const float *)kbg, c->ne, c->ne, nproj, c->kbgp, ldp, c->st);
-      CKL();
-      c->kbgp_ld = ldp;
-    }
+  if (c->kbgp) {
+    pad_rows_f32((const float *)kbg, c->ne, c->ne, nproj, c->kbgp, c->kbgp_ld, c->st);
+    CKL();
   }
-  c->proj = proj;
   c->have_kbg = true;
   return QX_OK;
 }
@@ -682,11 +715,16 @@ extern "C" int qx_build_kb_g(qx_ctx *c, int natom, const int *ityp, const double
   const int lmx = c->kb_lmx, nproj = lmx * natom, ne = c->ne;
   const size_t ts = c->tsize();
   if (!c->have_kbg || c->pl.nproj != nproj) {
-    // first build (or a new projector count): the tables of qx_set_kb_g
-    void *kbg = nullptr, *vcl = nullptr, *proj = nullptr;
-    TRY(dalloc(c, &kbg, ts * (size_t)nproj * ne));
-    TRY(dalloc(c, &vcl, ts * nproj));
-    TRY(dalloc(c, &proj, ts * (size_t)nproj * c->nb));
+    // first build (or a new projector count): the tables of qx_set_kb_g,
+    // replacing (and freeing) any earlier ones
+    void *kbg = c->have_kbg ? (c->prec == QX_PREC_FP64 ? (void *)c->pl.b64.kbg : (void *)c->pl.b32.kbg) : nullptr;
+    void *vcl = c->have_kbg ? (c->prec == QX_PREC_FP64 ? (void *)c->pl.b64.vclalp : (void *)c->pl.b32.vclalp)
+                            : nullptr;
+    void *proj = c->have_kbg ? c->proj : nullptr;
+    TRY(dregrow(c, &kbg, ts * (size_t)nproj * ne));
+    TRY(dregrow(c, &vcl, ts * nproj));
+    TRY(dregrow(c, &proj, ts * (size_t)nproj * c->nb));
+    TRY(dfree(c, c->kbgp));
     c->pl.nproj = nproj;
     drop_scf_graphs(c);
     TRY(tcpad_reserve(c, (long)nproj + c->nb));
@@ -704,10 +742,10 @@ extern "C" int qx_build_kb_g(qx_ctx *c, int natom, const int *ityp, const double
     c->proj = proj;
   }
   if (natom > c->kb_natom_cap) {
-    TRY(dalloc(c, &c->d_kb_ityp, sizeof(int) * natom));
-    TRY(dalloc(c, &c->d_kb_satm, sizeof(double) * 3 * natom));
-    TRY(dalloc(c, &c->d_kb_dcq, sizeof(double) * (size_t)natom * c->kb_ktot));
-    TRY(dalloc(c, &c->d_kb_dsq, sizeof(double) * (size_t)natom * c->kb_ktot));
+    TRY(dregrow(c, &c->d_kb_ityp, sizeof(int) * natom));
+    TRY(dregrow(c, &c->d_kb_satm, sizeof(double) * 3 * natom));
+    TRY(dregrow(c, &c->d_kb_dcq, sizeof(double) * (size_t)natom * c->kb_ktot));
+    TRY(dregrow(c, &c->d_kb_dsq, sizeof(double) * (size_t)natom * c->kb_ktot));
     c->kb_natom_cap = natom;
   }
   CK(cudaMemcpyAsync(c->d_kb_ityp, ityp, sizeof(int) * natom, cudaMemcpyHostToDevice, c->st));
@@ -901,11 +939,11 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
   const long nlines = (long)pl.k2 * pl.k3;
   bool moved = false;   // a table buffer was (re)allocated: captured graphs hold stale pointers
   if (natom != c->kbr_natom) {
-    TRY(dalloc(c, &c->d_kbr_ityp, sizeof(int) * natom));
-    TRY(dalloc(c, &c->d_kbr_satm, sizeof(double) * 3 * natom));
-    TRY(dalloc(c, &c->d_kbr_cnt, sizeof(int) * natom));
-    TRY(dalloc(c, &c->d_kbr_off, sizeof(int) * (natom + 1)));
-    TRY(dalloc(c, &c->d_kbr_sumr, 2 * ts * (size_t)pl.chunk * natom * 4));
+    TRY(dregrow(c, &c->d_kbr_ityp, sizeof(int) * natom));
+    TRY(dregrow(c, &c->d_kbr_satm, sizeof(double) * 3 * natom));
+    TRY(dregrow(c, &c->d_kbr_cnt, sizeof(int) * natom));
+    TRY(dregrow(c, &c->d_kbr_off, sizeof(int) * (natom + 1)));
+    TRY(dregrow(c, &c->d_kbr_sumr, 2 * ts * (size_t)pl.chunk * natom * 4));
     c->kbr_natom = natom;
     moved = true;
   }
@@ -925,15 +963,15 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
   CK(cudaStreamSynchronize(c->st));
   if (total > c->kbr_cap) {
     const long cap = (long)(total * 1.25) + 64;
-    TRY(dalloc(c, &c->d_kbr_mesh, sizeof(int) * cap));
-    TRY(dalloc(c, &c->d_kbr_ptatom, sizeof(int) * cap));
-    TRY(dalloc(c, &c->d_kbr_lent, sizeof(int4) * cap));
-    TRY(dalloc(c, &c->d_kbr_vnl, ts * 4 * (size_t)cap));
+    TRY(dregrow(c, &c->d_kbr_mesh, sizeof(int) * cap));
+    TRY(dregrow(c, &c->d_kbr_ptatom, sizeof(int) * cap));
+    TRY(dregrow(c, &c->d_kbr_lent, sizeof(int4) * cap));
+    TRY(dregrow(c, &c->d_kbr_vnl, ts * 4 * (size_t)cap));
     c->kbr_cap = cap;
     moved = true;
   }
   if (c->d_kbr_dtab && c->kbr_dvnl_cap < c->kbr_cap) {
-    TRY(dalloc(c, &c->d_kbr_dvnl, ts * 12 * (size_t)c->kbr_cap));
+    TRY(dregrow(c, &c->d_kbr_dvnl, ts * 12 * (size_t)c->kbr_cap));
     c->kbr_dvnl_cap = c->kbr_cap;
   }
   if (c->prec == QX_PREC_FP64)
@@ -2052,8 +2090,8 @@ static int fnl_r_impl(qx_ctx *c, double *fnl) {
   const int natom = pl.natom;
   const long need = (long)c->npair_all * natom * 3;
   if (need > c->kbr_fpart_n) {
-    TRY(dalloc(c, &c->d_kbr_fpart, sizeof(double) * need));
-    TRY(dalloc(c, &c->d_kbr_fout, sizeof(double) * 3 * (size_t)natom));
+    TRY(dregrow(c, &c->d_kbr_fpart, sizeof(double) * need));
+    TRY(dregrow(c, &c->d_kbr_fout, sizeof(double) * 3 * (size_t)natom));
     c->kbr_fpart_n = need;
   }
   PipeParams P = base_params(c);

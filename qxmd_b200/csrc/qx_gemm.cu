@@ -305,9 +305,10 @@ extern "C" int qx_hmatrix_static(const double *c, const double *hc, int nplwex, 
   double *W = nullptr;
   int rc = scratch_address(&W);
   if (rc) return rc;
-  // Split K into at least two partials (so the scratch is always the
-  // reduction path), enough of them to give about two CTAs per SM, each at
-  // least 128 deep, as many as the scratch holds.
+  // Split K into partials: enough of them to give about two CTAs per SM, each
+  // at least 128 deep, as many as the scratch holds (two or more asked for;
+  // when nplwex <= BK the chunk rounds up to the whole of K, a single partial
+  // and no scratch).  At nb = 1024 the two partials fill the scratch exactly.
   const int tiles_m = (nb + qx::BM - 1) / qx::BM;
   const long tiles = (long)tiles_m * tiles_m;
   const long cap = (long)(QX_HMATRIX_STATIC_SCRATCH_BYTES / (sizeof(double) * (size_t)nb * nb));

@@ -82,3 +82,50 @@ def test_total_force_matches_scf_energy_derivative(si8, si8_psi):
         s = cell.build_system(moved(si8, ia, ax, sgn * d), 12.0, 48.0, 16)
         e.append(converge(s)[1]["etot"])
     assert f[ia, ax] == pytest.approx(-(e[0] - e[1]) / (2 * d), abs=2e-5)
+
+
+def _kbr_energy(s, b, off, mesh, vnl, psir):
+    """sum_n occ_n / Omega sum_l clalp_l P_l^2, P_l = rdelv sum vnl_l psi_n(r)."""
+    e = 0.0
+    for n in range(psir.shape[0]):
+        for a in range(off.size - 1):
+            sl = slice(off[a], off[a + 1])
+            p = b["rdelv"] * (psir[n, mesh[sl]] @ vnl[sl])
+            e += s.occ[n] / s.gs.rvol * float(np.sum(b["clalp"] * p * p))
+    return e
+
+
+def test_real_space_kb_force_matches_fixed_point_derivative(si8, si8_psi):
+    """fnnlcl2 restated (oracle.forces.fnl_r) against central differences of
+    the real-space KB energy over the SAME point set, the projector values
+    recomputed at the moved atom (what fnnlcl2 differentiates).  The two differ
+    only by the tables' interpolation (derivative table against the
+    derivative of the interpolated table) and the h^2 term: 1e-6 of the
+    largest component."""
+    import dataclasses
+    from oracle import tables
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
+    off, mesh, vnl, dvnl = tables.setnlc(b, b["ityp"], b["satm"], grad=True)
+    psir = np.array([oracle.wvg2r(si8.gs, c) for c in si8_psi])
+    f = of.fnl_r(off, mesh, vnl, dvnl, b["clalp"], b["rdelv"], si8.gs.rvol, psir, si8.occ)
+    k = np.array(si8.gs.grid)
+    h = 1e-4
+    for a, ax in [(0, 0), (2, 1), (5, 2), (7, 0)]:
+        sl = slice(off[a], off[a + 1])
+        m = mesh[sl]
+        n = np.stack([m % k[0], (m // k[0]) % k[1], m // (k[0] * k[1])], axis=1)
+        e = []
+        for sgn in (1, -1):
+            satm = b["satm"].copy()
+            satm[a] += sgn * h * np.linalg.inv(si8.gs.rba)[:, ax]
+            df = n / k - satm[a]
+            df -= np.round(df)
+            d = df @ si8.gs.rba.T
+            r = np.sqrt(np.einsum("ij,ij->i", d, d))
+            v2 = vnl.copy()
+            for l in range(4):
+                v2[sl, l] = tables.setqlm(r, b["dltnl"][0], b["tabnl"][l], tables._poly(l, d[:, 0], d[:, 1], d[:, 2]))
+            e.append(_kbr_energy(si8, b, off, mesh, v2, psir))
+        fd = -(e[0] - e[1]) / (2 * h)
+        assert f[a, ax] == pytest.approx(fd, abs=1e-6 * np.max(np.abs(f)))
+    assert np.max(np.abs(f)) > 1e-3

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 import oracle
+from oracle import forces as oforces
 from oracle import tables
 from qxmd_b200 import cell
 from qxmd_b200.lib import QX_NL_GSPACE, QX_NL_RSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context
@@ -211,6 +212,32 @@ def test_real_space_kb_forces_match_energy_differences(si8, si8_psi, prec, tol):
     scale = np.max(np.abs(f))
     assert scale > 1e-3
     assert np.max(np.abs(f[[0, 5]] - fd)) / scale < tol
+
+
+@pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-10), (QX_PREC_MIXED, 1e-4)])
+@pytest.mark.parametrize("nb", [16, 15])
+def test_real_space_kb_forces_match_restated_fnnlcl2(si8, si8_psi, prec, tol, nb):
+    """qx_forces_nl_r against the oracle's restatement of fnnlcl2
+    (oracle.forces.fnl_r) on the same point set and gradient tables, every
+    atom and component, relative to the largest component; 15 bands take the
+    odd-band path of the pair kernels (the last pair has one band)."""
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
+    satm = _moved(b["satm"], 5)
+    off, mesh, vnl, dvnl = tables.setnlc(b, b["ityp"], satm, grad=True)
+    psi = si8_psi[:nb]
+    occ = si8.occ[:nb]
+    psir = np.array([oracle.wvg2r(si8.gs, c) for c in psi])
+    ref = oforces.fnl_r(off, mesh, vnl, dvnl, b["clalp"], b["rdelv"], si8.gs.rvol, psir, occ)
+    ctx = Context(si8, prec, QX_NL_RSPACE, nband=nb)
+    try:
+        ctx.set_kb_r_builder(b)
+        ctx.build_kb_r(b["ityp"], satm)
+        ctx.put_psi(psi)
+        f = ctx.forces_nl_r()
+    finally:
+        ctx.close()
+    assert np.max(np.abs(f - ref)) / np.max(np.abs(ref)) < tol
 
 
 def test_build_kb_g_moves_the_force_tables(si8, si8_psi):

@@ -67,6 +67,29 @@ def test_hmatrix_static_matches_context_path(which):
         ctx.close()
 
 
+def test_hmatrix_static_at_the_largest_band_count():
+    """nb = 1024, the most the scratch takes: its two split-K partials fill
+    the 16 MiB exactly.  Small random operands, checked against an FP64
+    matmul with the Gamma-point metric 2 sum - c(1) hc(1), twice in a row."""
+    need_gpu()
+    torch = pytest.importorskip("torch")
+    nb, ne = 1024, 2048
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    for _ in range(2):
+        c = torch.randn((nb, ne), dtype=torch.float64, device="cuda", generator=gen)
+        hc = torch.randn((nb, ne), dtype=torch.float64, device="cuda", generator=gen)
+        out = torch.full((nb, nb), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        _ck(lib().qx_hmatrix_static(c.data_ptr(), hc.data_ptr(), ne, nb, out.data_ptr(), None), "qx_hmatrix_static")
+        torch.cuda.synchronize()
+        # column-major hsub(j, i) sits at out[i, j] of the row-major tensor:
+        # [i, j] = <c_j|hc_i>
+        got = out.cpu().numpy()
+        ref = (2.0 * hc @ c.t() - torch.outer(hc[:, 0], c[:, 0])).cpu().numpy()
+        assert np.all(np.isfinite(got))
+        assert relerr(got, ref) < TOL
+
+
 def test_hmatrix_static_rejects_oversize():
     need_gpu()
     torch = pytest.importorskip("torch")
