@@ -57,6 +57,8 @@ DATA = "synthetic (seeded Si64 cell, model pseudopotential)"
 # untimed ones): about 10 s on 16 host threads
 CPU_SAMPLE_WARMUP, CPU_SAMPLE_ITERS = 2, 3
 GOLDEN = os.path.join(ROOT, "tests", "golden")
+# TDDFT-FSSH workload: 32 adiabatic states, 1 fs MD steps, 100 steps
+FSSH_STATES, FSSH_DT_FS, FSSH_MD_STEPS, FSSH_SCF_PER_STEP, FSSH_SEED = 32, 1.0, 100, 4, 20240.0
 
 
 def workload_config(sys_, ws):
@@ -231,22 +233,24 @@ def run_profile_hpsi(args):
 
 
 def accuracy(acc, natom, iters):
-    """Total energy, eigenvalues and forces of every path after `iters` SCF
-    iterations from the same start, against the CPU FP64 oracle run to
-    self-consistency over the same iteration count on the same inputs (the
+    """Total energy, eigenvalues and forces of every path after at least
+    `iters` SCF iterations from the same start (each path's count is given),
+    against the CPU FP64 oracle run to self-consistency in `iters` iterations
+    on the same inputs (the
     fixture tests/golden/si64_scf.npz, made by tests/golden/make_fixtures.py).
     Energies Ha/atom, eigenvalues Ha, forces Ha/bohr (local + KB terms; the
     Ewald term is geometry only and the same everywhere)."""
     g = np.load(os.path.join(GOLDEN, "si64_scf.npz"))
     e_or, eig_or, f_or = float(g["etot"][-1]), g["eig"], g["floc"] + g["fnl"]
     nocc = int(g["noband"])
-    out = {"reference": "CPU FP64 oracle after the same iteration count (self-consistent: residual "
+    out = {"reference": f"CPU FP64 oracle after {g['etot'].size} iterations (self-consistent: residual "
                         f"{float(g['resid'][-1]):.1e}, last energy change "
                         f"{abs(float(g['etot'][-1] - g['etot'][-2])):.1e} Ry)",
            "iterations": iters, "etot_oracle_ry": e_or}
     for name in ("mixed", "fp64", "fp64_batched", "mixed_refined"):
         a = acc[name]
-        out[name] = {"etot_ry": a["etot"], "resid": a["resid"], "detot_last_ry": a["detot_last"],
+        out[name] = {"iterations": a["iterations"], "etot_ry": a["etot"], "resid": a["resid"],
+                     "detot_last_ry": a["detot_last"],
                      "err_ha_per_atom": 0.5 * abs(a["etot"] - e_or) / natom,
                      "eig_occ_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"][:nocc] - eig_or[:nocc]))),
                      "eig_max_abs_err_ha": 0.5 * float(np.max(np.abs(a["eig"] - eig_or))),
@@ -450,6 +454,81 @@ def run_batch(K, W):
             "launch": "one stream and one captured SCF-iteration graph per cell, all enqueued before any is read"}
 
 
+def run_fssh_md(nmd=FSSH_MD_STEPS, nscf=FSSH_SCF_PER_STEP):
+    """TDDFT-FSSH on Si64 (32 adiabatic states around the gap, 1 fs MD
+    steps): after the ground state is converged, every MD step moves the
+    atoms by seeded 300 K Maxwell-Boltzmann velocities (constant: the MD
+    integrator is the host's), rebuilds the KB projector table and the local
+    potential on the device (qx_build_kb_g, qx_build_vloc), runs nscf SCF
+    iterations from the previous step's state, then one surface-hopping step
+    (qx_fssh_step: overlap of the two steps' wavefunctions on the tensor cores,
+    couplings, FP64 RK4 density matrices over 1033 substeps, hop).  Device
+    time per MD step and of the FSSH part alone."""
+    import torch
+
+    from qxmd_b200 import cell
+    from qxmd_b200.lib import CgParm, Context, FsshParm, QX_NL_GSPACE, QX_PREC_MIXED
+    sys_ = cell.si64()
+    noband = int(sys_.cell.nel // 2)
+    b = cell.kb_builder_tables(sys_.gs, sys_.cell, sys_.pp)
+    ctx = Context(sys_, QX_PREC_MIXED, QX_NL_GSPACE)
+    ctx.put_psi(cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband))
+    ctx.schmidt()
+    ctx.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+    ctx.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
+    ctx.set_force_tables()
+    ctx.set_kb_builder(b)
+    ctx.scf_rho_from_psi()
+    parm = CgParm.defaults(noband)
+    for _ in range(30):
+        ctx.scf_iteration(parm)
+    # 300 K Maxwell-Boltzmann velocities in Rydberg units (hbar = 1, mass unit
+    # 2 m_e, energy Ry), constant over the run
+    rng = np.random.default_rng(7)
+    kt = 300.0 * 6.333623e-6                                    # Ry
+    mass = 28.0855 * 1822.888486 / 2.0                          # Si mass in units of 2 m_e
+    vel = rng.standard_normal((sys_.cell.natom, 3)) * math.sqrt(kt / mass)
+    vel -= vel.mean(axis=0)
+    dtmd = FSSH_DT_FS * 20.670687                                # fs -> Rydberg time (hbar / Ry)
+    b0, nst = noband - FSSH_STATES // 2, FSSH_STATES
+    occ = np.array([2.0] * (FSSH_STATES // 2) + [0.0] * (FSSH_STATES // 2))
+    ctx.fssh_init(FsshParm(b0=b0, nstate=nst, dtmd=dtmd, dttddft=0.02, boltzmann=1, treq=kt, hop=1,
+                           seed=FSSH_SEED), occ)
+    pos = sys_.cell.pos.copy()
+    ainv = np.linalg.inv(sys_.gs.rba)
+    tot = fs = 0.0
+    hops = 0
+    occ_last = occ
+    for step in range(nmd):
+        pos = pos + vel * dtmd
+        satm = pos @ ainv.T
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        ctx.build_kb_g(b["ityp"], satm)
+        ctx.build_vloc()
+        for _ in range(nscf):
+            ctx.scf_launch(parm)
+        e1.record()
+        tr, occ_last, _ = ctx.fssh_step()
+        e2.record()
+        torch.cuda.synchronize()
+        r = ctx.scf_result()
+        tot += e0.elapsed_time(e2)
+        fs += e1.elapsed_time(e2)
+        hops += tr is not None
+    dnr, _, _, _ = ctx.fssh_state()
+    ctx.close()
+    trace_dev = float(np.max(np.abs(np.trace(dnr, axis1=1, axis2=2) - 1.0)))
+    return {"metric": "TDDFT-FSSH MD steps/s", "value": nmd / (tot * 1e-3), "unit": "MD step/s",
+            "workload": f"Si64, {nst} adiabatic states (bands {b0}-{b0 + nst - 1}), dt {FSSH_DT_FS} fs, "
+                        f"{nmd} MD steps, {nscf} SCF iterations per step, 300 K velocities",
+            "ms_per_md_step": tot / nmd, "fssh_ms_per_step": fs / nmd,
+            "substeps_per_md_step": int(dtmd / 0.02), "hops": hops,
+            "electrons_in_window": float(occ_last.sum()), "etot_last_ry": r["etot"], "resid_last": r["resid"],
+            "max_trace_dev": trace_dev,
+            "precision": "mixed SCF and overlap (3xTF32); FP64 density-matrix propagation and hops"}
+
+
 def run_ours(args):
     import torch
 
@@ -565,12 +644,15 @@ def run_ours(args):
     acc = {}
     for name, _, _ in variants:
         ctx, parm = ctxs[name]
-        outs = [ctx.scf_iteration(parm) for _ in range(max(0, args.accuracy_iters - res[name]["iters_done"]))]
+        # at least accuracy_iters iterations, two of them here so that the
+        # last energy change is known
+        nmore = max(2, args.accuracy_iters - res[name]["iters_done"])
+        outs = [ctx.scf_iteration(parm) for _ in range(nmore)]
         ctx.sync()
         last = outs[-1] if outs else None
         ctx.set_force_tables()
         fl, fn = ctx.forces()
-        acc[name] = {"force": fl + fn,
+        acc[name] = {"force": fl + fn, "iterations": res[name]["iters_done"] + nmore,
                      "etot": last["etot"] if last else res[name]["etot_last"],
                      "resid": last["resid"] if last else None,
                      "detot_last": abs(outs[-1]["etot"] - outs[-2]["etot"]) if len(outs) > 1 else None,
@@ -588,7 +670,8 @@ def run_ours(args):
             torch.cuda.synchronize()
             ref_ctx.set_force_tables()
             rl, rn = ref_ctx.forces()
-            acc["mixed_refined"] = {"force": rl + rn, "etot": routs[-1]["etot"], "resid": routs[-1]["resid"],
+            acc["mixed_refined"] = {"force": rl + rn, "iterations": acc["mixed"]["iterations"] + REFINE_ITERS,
+                                    "etot": routs[-1]["etot"], "resid": routs[-1]["resid"],
                                     "detot_last": abs(routs[-1]["etot"] - routs[-2]["etot"]),
                                     "eig": ref_ctx.get_eig(), "ms": e0.elapsed_time(e1)}
             ref_ctx.close()
@@ -598,6 +681,7 @@ def run_ours(args):
     kb_ctx.close()
     mixed, fp64, fp64b = res["mixed"], res["fp64"], res["fp64_batched"]
     batch = run_batch(K, W) if ws == 1 else None
+    fssh = run_fssh_md() if ws == 1 else None
     hbm, peak_kind = peaks()
     N, ne = sys_.gs.kfft0, sys_.gs.nplwex
     bytes_per_bapp = 4 * N * 4 + 2 * ne * 4
@@ -619,6 +703,7 @@ def run_ours(args):
                          "value": fp64b["value"], "ms_per_step": fp64b["ms_per_step"],
                          "cg_bapps_per_iter": fp64b["cg_bapps_per_iter"]},
         "batch48": batch,
+        "fssh_md": fssh,
         "kb_tables": kb_tables,
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "mixed_over_fp64_batched": mixed["value"] / fp64b["value"],

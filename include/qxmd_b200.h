@@ -155,8 +155,9 @@ int qx_get_rho(qx_ctx *ctx, double *rho);
 int qx_put_rho(qx_ctx *ctx, const double *rho);
 int qx_get_glocal(qx_ctx *ctx, double *glocal);
 /* Device pointers of the resident arrays: 0 psi, 1 hpsi, 2 rho_in (double),
- * 3 rho_out (double), 4 eig (double).  psi/hpsi are double or float by
- * precision. */
+ * 3 rho_out (double), 4 eig (double), 5 the local pseudopotential of
+ * qx_scf_init / qx_build_vloc (double, kfft0).  psi/hpsi are double or float
+ * by precision. */
 void *qx_dev_ptr(qx_ctx *ctx, int which);
 int qx_sync(qx_ctx *ctx);
 
@@ -262,6 +263,47 @@ int qx_tddft_store(qx_ctx *ctx);
  * contexts.  The FP64 amplitude propagation and hops stay with the caller. */
 int qx_tddft_overlap(qx_ctx *ctx, double *aij);
 
+/* ---- TDDFT-FSSH surface hopping (tddft_fssh_dm, tddft_fssh.f90:1989-2402) -- */
+/* Density-matrix representation, one spin channel, no decoherence branch
+ * (lfssh_dish = .false.).  The states are the band window b0 .. b0+nstate-1
+ * (the reference's noband = noccmx states); each occupied state with a
+ * not-full neighbour within nupdn = 3 carries a 7 x 7 complex density
+ * matrix, integrated over each MD step in FP64 by RK4 in int(dtmd/dttddft)
+ * substeps with the couplings d(k, j) = -(A(k, j) - A(j, k)) / (2 dtmd) of the
+ * overlap A(k, j) = <psi_k(t)|psi_j(t+dt)> (tddft_fssh.f90:2098); then the hop
+ * probabilities and one Park-Miller draw (rnd00, funcs.f90:1673-1689) decide
+ * at most one transition (tddft_fssh.f90:2219-2366).  Times in Rydberg units
+ * (1 fs = 20.67), energies in Ry. */
+#define QX_FSSH_MAX_STATES 1024
+typedef struct {
+  int b0, nstate;      /* first band of the window, number of states        */
+  double dtmd;         /* MD step                                           */
+  double dttddft;      /* electronic substep (reference default 0.02)       */
+  int boltzmann;       /* lfssh_boltzmn: exp(-(e_news - e_s)/treq) on hops one state up */
+  double treq;         /* temperature (Ry) of that factor                   */
+  int hop;             /* lfssh_switch: accept transitions                  */
+  double seed;         /* rseed_fssh: state of rnd00 (0 < seed < 2147483647) */
+} qx_fssh_parm;
+/* Starts the surface hopping: density matrices set to the pure state,
+ * accumulated probabilities cleared, occupations occ(nstate) of the window,
+ * and the current psi kept as the previous step's wavefunctions. */
+int qx_fssh_init(qx_ctx *ctx, const qx_fssh_parm *p, const double *occ);
+/* One MD step.  phis (nullable): the overlap A as nstate x nstate column-major
+ * host array (a caller that reorders crossing states, as
+ * tddft_fssh_set_matrix2 does, passes its own); null: the overlap of the kept
+ * previous psi with the current psi on the device (tensor cores in mixed
+ * contexts), after which the current psi is kept for the next step.  eig
+ * (nullable): the window's eigenvalues, else the context's current ones.
+ * Outputs (nullable): occ(nstate) after the step, *transition = s * nstate +
+ * news of an accepted hop or -1, bkl(7, nstate): the hop probability of
+ * state s to s + iud at bkl[s * 7 + iud + 3]. */
+int qx_fssh_step(qx_ctx *ctx, const double *phis, const double *eig, double *occ, int *transition, double *bkl);
+/* Reads the state: dnr, dni (7, 7, nstate) with rho(j, k) of state s at
+ * [(s * 7 + j + 3) * 7 + k + 3]; accum(nstate, nstate) with the accumulated
+ * probability of s -> news at [news + s * nstate]; *rndx the rnd00 state.
+ * Any pointer may be null. */
+int qx_fssh_state(qx_ctx *ctx, double *dnr, double *dni, double *accum, double *rndx);
+
 /* ---- Hellmann-Feynman forces (force.f90:5-860 terms floc and fnlc) ------ */
 /* Geometry tables, set once per geometry after the KB tables (qx_set_kb_g)
  * and qx_scf_init:
@@ -277,6 +319,14 @@ int qx_tddft_overlap(qx_ctx *ctx, double *aij);
 int qx_set_force_tables(qx_ctx *ctx, int natom, int ntype, const int *ityp, const double *satm, int n5,
                         const int *ijk5, const int *ngabc, const double *gvec5, const double *svco,
                         const double *gw);
+/* The local pseudopotential of the current geometry on the device, in place
+ * of the one given to qx_scf_init (vlocal_g, nlkbpp.f90:862-1036):
+ * v(r) = sum_G V(G) e^{iG.r} over the density sphere,
+ * V(G) = (1/Omega) sum_a svco(G, ityp_a) e^{-iG.R_a}, from the form factors and
+ * phases of qx_set_force_tables (a later qx_build_kb_g moves the phases to its
+ * geometry).  Together with qx_build_kb_g this moves every geometry table of
+ * an SCF iteration without a host upload, for MD steps. */
+int qx_build_vloc(qx_ctx *ctx);
 /* Forces (Ry/bohr, (3, natom) each) of the current psi and its density
  * rho = sum occ/Omega |psi|^2:
  *   floc: local pseudopotential in G space (flocal_g, nlkbpp.f90:1037-1120),

@@ -91,6 +91,11 @@ def lib():
         L.orc_rotate.argtypes = [_dp, C.c_int, C.c_int, _dp]
         L.orc_softchg.argtypes = [C.POINTER(_Ham), _dp, C.c_int, _dp, C.c_double, _dp]
         L.orc_xclda.argtypes = [_dp, C.c_long, C.c_double, _dp, C.c_void_p, _dp]
+        L.orc_fssh_dm.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                  _dp, _dp, _dp, _dp, C.POINTER(C.c_double), C.c_void_p]
+        L.orc_fssh_dm.restype = C.c_int
+        L.orc_rnd00.argtypes = [C.POINTER(C.c_double)]
+        L.orc_rnd00.restype = C.c_double
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
     return _lib
@@ -107,6 +112,40 @@ def get_threads() -> int:
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Fssh:
+    """State of tddft_fssh_dm (tddft_fssh.f90:1989-2402) for a window of nst
+    states: density matrices dn (nst, 7, 7) complex (initially 1 at the centre),
+    accumulated probabilities accum[news, s], occupations and the rnd00 state."""
+
+    def __init__(self, occ, seed, dtmd, dttddft=0.02, boltzmann=True, treq=0.0019, hop=True):
+        self.nst = len(occ)
+        self.dnr = np.zeros((self.nst, 7, 7))
+        self.dni = np.zeros((self.nst, 7, 7))
+        self.dnr[:, 3, 3] = 1.0
+        self.accum = np.zeros((self.nst, self.nst), order="F")
+        self.occ = np.array(occ, dtype=np.float64)
+        self.rndx = C.c_double(seed)
+        self.dtmd, self.dttddft, self.boltz, self.treq, self.hop = dtmd, dttddft, boltzmann, treq, hop
+
+    def step(self, phis, eig):
+        """One MD step; phis[k, j] = <psi_k(t)|psi_j(t+dt)>.  Returns
+        (transition: None or (s, news), bkl (nst, 7))."""
+        bkl = np.zeros((self.nst, 7))
+        acc = np.ascontiguousarray(self.accum.T)          # [s, news] row-major = (news, s) column-major
+        ph = np.ascontiguousarray(np.asarray(phis, dtype=np.float64).T)   # column-major phis(k, j)
+        t = lib().orc_fssh_dm(self.nst, ph, _f64(eig), self.dtmd, self.dttddft, int(self.boltz), self.treq,
+                              int(self.hop), self.dnr, self.dni, acc, self.occ, C.byref(self.rndx),
+                              bkl.ctypes.data)
+        self.accum = acc.T.copy()
+        return (None if t < 0 else divmod(t, self.nst)), bkl
+
+
+def rnd00(rndx: float, n: int):
+    """n successive draws of the Park-Miller rnd00 from state rndx."""
+    x = C.c_double(rndx)
+    return np.array([lib().orc_rnd00(C.byref(x)) for _ in range(n)])
 
 
 class Ham:

@@ -634,3 +634,138 @@ void orc_xclda(const double *rho, long n, double rdelv, double *vexc, double *ee
   }
   for (int i = 0; i < 4; ++i) en4[i] = s[i] * 2.0 * rdelv;
 }
+
+/* ------------------------------------------------------------------------ */
+/* TDDFT-FSSH in the density-matrix representation: tddft_fssh_dm
+ * (tddft_fssh.f90:1989-2402) for one spin channel (nspnmx = 1), without the
+ * decoherence branch (lfssh_dish = .false.).  States s = 0..nst-1 of a band
+ * window (noband = noccmx = nst); phis(k, j) = <psi_k(t)|psi_j(t+dt)> at
+ * phis[k + j*nst]; eig(nst) in Ry.  Per state s a (2*3+1)^2 complex density
+ * matrix dn[s][j+3][k+3] (nupdn = 3) is integrated by RK4 over
+ * nstep = int(dtmd/dttddft) substeps; then the hop probabilities and one
+ * Park-Miller draw (rnd00, funcs.f90:1673-1689) decide a transition.
+ * Every expression keeps the reference's evaluation order (left to right).
+ * accum(news, s) at accum[news + s*nst]; bkl_out[s*7 + iud+3] the hop
+ * probability of each pair (0 where none).  Returns -1, or s*nst + news of
+ * the accepted transition. */
+#define FS_N 3
+#define FS_W 7
+static double rnd00(double *rndx) {
+  const double rnda = 16807.0, rndm = 0.2147483647e10;
+  double rnd = rnda * *rndx;
+  *rndx = fmod(rnd, rndm);
+  return *rndx / rndm;
+}
+
+double orc_rnd00(double *rndx) { return rnd00(rndx); }
+
+int orc_fssh_dm(int nst, const double *phis, const double *eig, double dtmd, double dttddft, int boltz,
+                double treq, int hop, double *dnr, double *dni, double *accum, double *occ_rec, double *rndx,
+                double *bkl_out) {
+#define PH(k, j) phis[(long)(k) + (long)(j) * nst]
+#define DKJ(k, j) (-(PH(k, j) - PH(j, k)) / 2.0 / dtmd)
+#define DR(s, j, k) dnr[((long)(s) * FS_W + (j) + FS_N) * FS_W + (k) + FS_N]
+#define DI(s, j, k) dni[((long)(s) * FS_W + (j) + FS_N) * FS_W + (k) + FS_N]
+  double rn = rnd00(rndx);
+  double *occ_store = malloc(sizeof(double) * nst);
+  double *probinteg = calloc((size_t)nst * FS_W, sizeof(double));
+  memcpy(occ_store, occ_rec, sizeof(double) * nst);
+  const double rkc[4] = {0.0, dttddft / 2.0, dttddft / 2.0, dttddft};
+  const int nstep = (int)(dtmd / dttddft);
+  double kr[4][FS_W][FS_W], ki[4][FS_W][FS_W], dmtr[FS_W][FS_W], dmti[FS_W][FS_W];
+  for (int s = 0; s < nst; ++s) {
+    int ldm = 0;
+    if (occ_store[s] > 0.5)
+      for (int iud = -FS_N; iud <= FS_N; ++iud) {
+        int ns = s + iud;
+        if (ns < 0 || ns >= nst || ns == s) continue;
+        if (occ_store[ns] > 1.5) continue;
+        ldm = 1;
+      }
+    if (!ldm) continue;
+    const int n1 = -FS_N > -s ? -FS_N : -s, n2 = FS_N < nst - 1 - s ? FS_N : nst - 1 - s;
+    for (int i = 0; i < nstep; ++i) {
+      /* stage 1 from dn itself (tddft_fssh.f90:2126-2141) */
+      for (int kb = n1; kb <= n2; ++kb)
+        for (int jb = n1; jb <= n2; ++jb) {
+          const int k = s + kb, j = s + jb;
+          double r = (eig[j] - eig[k]) * DI(s, jb, kb);
+          double m = -(eig[j] - eig[k]) * DR(s, jb, kb);
+          for (int lb = n1; lb <= n2; ++lb) {
+            const int l = s + lb;
+            r = r - DR(s, jb, lb) * DKJ(l, k) + DR(s, lb, kb) * DKJ(j, l);
+            m = m - DI(s, jb, lb) * DKJ(l, k) + DI(s, lb, kb) * DKJ(j, l);
+          }
+          kr[0][jb + FS_N][kb + FS_N] = r;
+          ki[0][jb + FS_N][kb + FS_N] = m;
+        }
+      /* stages 2-4 (2143-2166) */
+      for (int irk = 1; irk < 4; ++irk) {
+        for (int kb = n1; kb <= n2; ++kb)
+          for (int jb = n1; jb <= n2; ++jb) {
+            dmtr[jb + FS_N][kb + FS_N] = DR(s, jb, kb) + rkc[irk] * kr[irk - 1][jb + FS_N][kb + FS_N];
+            dmti[jb + FS_N][kb + FS_N] = DI(s, jb, kb) + rkc[irk] * ki[irk - 1][jb + FS_N][kb + FS_N];
+          }
+        for (int kb = n1; kb <= n2; ++kb)
+          for (int jb = n1; jb <= n2; ++jb) {
+            const int k = s + kb, j = s + jb;
+            double r = (eig[j] - eig[k]) * dmti[jb + FS_N][kb + FS_N];
+            double m = -(eig[j] - eig[k]) * dmtr[jb + FS_N][kb + FS_N];
+            for (int lb = n1; lb <= n2; ++lb) {
+              const int l = s + lb;
+              r = r - dmtr[jb + FS_N][lb + FS_N] * DKJ(l, k) + dmtr[lb + FS_N][kb + FS_N] * DKJ(j, l);
+              m = m - dmti[jb + FS_N][lb + FS_N] * DKJ(l, k) + dmti[lb + FS_N][kb + FS_N] * DKJ(j, l);
+            }
+            kr[irk][jb + FS_N][kb + FS_N] = r;
+            ki[irk][jb + FS_N][kb + FS_N] = m;
+          }
+      }
+      /* RK4 update (2168-2177) */
+      for (int kb = n1; kb <= n2; ++kb)
+        for (int jb = n1; jb <= n2; ++jb) {
+          const int a = jb + FS_N, b = kb + FS_N;
+          DR(s, jb, kb) = DR(s, jb, kb) + (kr[0][a][b] + 2.0 * kr[1][a][b] + 2.0 * kr[2][a][b] + kr[3][a][b]) *
+                                              dttddft / 6.0;
+          DI(s, jb, kb) = DI(s, jb, kb) + (ki[0][a][b] + 2.0 * ki[1][a][b] + 2.0 * ki[2][a][b] + ki[3][a][b]) *
+                                              dttddft / 6.0;
+        }
+      /* transition probability integral (2179-2188) */
+      for (int iud = -FS_N; iud <= FS_N; ++iud) {
+        int ns = s + iud;
+        if (ns < 0 || ns >= nst || ns == s) continue;
+        probinteg[(long)s * FS_W + iud + FS_N] += DR(s, iud, 0) / DR(s, 0, 0);
+      }
+    }
+  }
+  /* probabilities and the hop (2219-2366) */
+  int trans = -1;
+  double probsum = 0.0;
+  if (bkl_out) for (long i = 0; i < (long)nst * FS_W; ++i) bkl_out[i] = 0.0;
+  for (int s = 0; s < nst; ++s) {
+    if (!(occ_store[s] > 0.5)) continue;
+    for (int iud = -FS_N; iud <= FS_N; ++iud) {
+      int ns = s + iud;
+      if (ns < 0 || ns >= nst || ns == s) continue;
+      if (occ_store[ns] > 1.5) continue;
+      double boltzmn = (boltz && iud == 1) ? exp(-(eig[ns] - eig[s]) / treq) : 1.0;
+      double bkl0 = 2.0 * DKJ(ns, s) * dttddft * probinteg[(long)s * FS_W + iud + FS_N];
+      double bkl = bkl0 * boltzmn;
+      if (bkl_out) bkl_out[(long)s * FS_W + iud + FS_N] = bkl;
+      if (bkl > 0.0) accum[(long)ns + (long)s * nst] += bkl;
+      double pb = bkl > 0.0 ? bkl : 0.0;
+      if (hop && probsum <= rn && rn < probsum + pb) {
+        trans = s * nst + ns;
+        occ_rec[s] = occ_rec[s] - 1.0;
+        occ_rec[ns] = occ_rec[ns] + 1.0;
+      }
+      probsum = probsum + pb;
+    }
+  }
+  free(occ_store);
+  free(probinteg);
+  return trans;
+#undef PH
+#undef DKJ
+#undef DR
+#undef DI
+}

@@ -128,6 +128,14 @@ struct qx_ctx {
          *d_dsq = nullptr, *d_force = nullptr;
   void *prev = nullptr;    // wavefunctions of the previous MD step (gdcr_rec), context precision
   bool have_prev = false;
+  // TDDFT-FSSH state of the band window (qx_fssh.cu)
+  qx_fssh_parm fs{};
+  bool have_fssh = false;
+  int fs_cap = 0;
+  double *d_fs_dnr = nullptr, *d_fs_dni = nullptr, *d_fs_pint = nullptr, *d_fs_bkl = nullptr,
+         *d_fs_accum = nullptr, *d_fs_occ = nullptr, *d_fs_occ0 = nullptr, *d_fs_rndx = nullptr,
+         *d_fs_A = nullptr, *d_fs_eig = nullptr;
+  int *d_fs_trans = nullptr;
   void *dtab = nullptr;    // 3 nproj x nplwex derivative tables (context precision)
   void *dproj = nullptr;   // 3 nproj x nb
   bool have_ftab = false;
@@ -1100,6 +1108,7 @@ extern "C" void *qx_dev_ptr(qx_ctx *c, int which) {
     case 1: return c->hpsi;
     case 2: return c->d_rho_in;
     case 3: return c->d_rho_out;
+    case 5: return c->d_vloc;
     case 4: return c->d_eig;
     default: return nullptr;
   }
@@ -1981,6 +1990,123 @@ extern "C" int qx_tddft_overlap(qx_ctx *c, double *aij) {
   if (!c) return QX_ERR_ARG;
   if (!c->have_prev) { set_error("qx_tddft_overlap: call qx_tddft_store at the previous step first"); return QX_ERR_STATE; }
   return c->prec == QX_PREC_FP64 ? tddft_overlap_impl<double>(c, aij) : tddft_overlap_impl<float>(c, aij);
+}
+
+// ---------------------------------------------------------------------------
+// Local pseudopotential of the current geometry (vlocal_g, nlkbpp.f90:862-1036)
+extern "C" int qx_build_vloc(qx_ctx *c) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_ftab || !c->scf_ready || !c->have_occ) {
+    set_error("qx_build_vloc: call qx_set_occ, qx_scf_init and qx_set_force_tables first");
+    return QX_ERR_STATE;
+  }
+  const long n = c->pl.n;
+  CK(cudaMemsetAsync(c->d_zg, 0, sizeof(double2) * n, c->st));
+  vloc_g(c->f_n5, c->f_natom, c->d_ijk5, c->d_ngabc, c->d_svco, c->d_ityp, c->d_dcq, c->d_dsq, c->f_km[0],
+         c->f_km[1], c->f_km[2], c->f_ktot, c->rvol, c->pl.k1, c->pl.k2, c->pl.k3, c->d_zg, c->st);
+  CKL();
+  TRY(launch_full_fft<double>(c->pl, c->d_zg, +1, 1.0, c->st));
+  real_part(c->d_zg, c->d_vloc, n, c->st);
+  CKL();
+  return QX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TDDFT-FSSH surface hopping (tddft_fssh_dm, tddft_fssh.f90:1989-2402)
+namespace qx {
+void fssh_init(int nst, double *dnr, double *dni, double *accum, cudaStream_t st);
+void fssh_step(int nst, const double *A, const double *eig, double dtmd, double dttddft, int boltz, double treq,
+               int hop, double *dnr, double *dni, const double *occ_store, double *occ_rec, double *probinteg,
+               double *accum, double *rndx, double *bkl, int *trans, cudaStream_t st);
+}  // namespace qx
+
+extern "C" int qx_fssh_init(qx_ctx *c, const qx_fssh_parm *p, const double *occ) {
+  if (!c || !p || !occ) { set_error("qx_fssh_init: bad arguments"); return QX_ERR_ARG; }
+  const int nst = p->nstate;
+  if (nst < 2 || nst > QX_FSSH_MAX_STATES || p->b0 < 0 || p->b0 + nst > c->nb) {
+    set_error("qx_fssh_init: window b0 = %d, nstate = %d outside 2..%d states within %d bands", p->b0, nst,
+              QX_FSSH_MAX_STATES, c->nb);
+    return QX_ERR_ARG;
+  }
+  if (!(p->dtmd > 0.0) || !(p->dttddft > 0.0) || p->dtmd / p->dttddft > 1.0e7 ||
+      (p->boltzmann && !(p->treq > 0.0)) || !(p->seed > 0.0) || !(p->seed < 2147483647.0)) {
+    set_error("qx_fssh_init: need dtmd, dttddft > 0 with dtmd/dttddft <= 1e7, treq > 0 with the Boltzmann factor, "
+              "0 < seed < 2147483647");
+    return QX_ERR_ARG;
+  }
+  if (nst > c->fs_cap) {
+    TRY(dregrow(c, &c->d_fs_dnr, sizeof(double) * 49 * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_dni, sizeof(double) * 49 * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_pint, sizeof(double) * 7 * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_bkl, sizeof(double) * 7 * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_accum, sizeof(double) * (size_t)nst * nst));
+    TRY(dregrow(c, &c->d_fs_occ, sizeof(double) * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_occ0, sizeof(double) * (size_t)nst));
+    TRY(dregrow(c, &c->d_fs_A, sizeof(double) * (size_t)nst * nst));
+    TRY(dregrow(c, &c->d_fs_eig, sizeof(double) * (size_t)nst));
+    if (!c->d_fs_rndx) TRY(dalloc(c, &c->d_fs_rndx, sizeof(double)));
+    if (!c->d_fs_trans) TRY(dalloc(c, &c->d_fs_trans, sizeof(int)));
+    c->fs_cap = nst;
+  }
+  c->fs = *p;
+  fssh_init(nst, c->d_fs_dnr, c->d_fs_dni, c->d_fs_accum, c->st);
+  CKL();
+  CK(cudaMemcpyAsync(c->d_fs_occ, occ, sizeof(double) * nst, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_fs_rndx, &p->seed, sizeof(double), cudaMemcpyHostToDevice, c->st));
+  TRY(qx_tddft_store(c));
+  CK(cudaStreamSynchronize(c->st));
+  c->have_fssh = true;
+  return QX_OK;
+}
+
+template <typename T>
+static int fssh_overlap(qx_ctx *c) {
+  const int nst = c->fs.nstate, b0 = c->fs.b0;
+  T *m = (T *)c->mat_t;
+  // A(k, j) = <prev_(b0+k)|psi_(b0+j)> with the Gamma metric (tddft_fssh_cal_matrix)
+  const T *pv = (const T *)c->prev + (size_t)b0 * c->ne, *ps = (const T *)c->psi + (size_t)b0 * c->ne;
+  TRY(gemm<T>(true, false, nst, nst, c->ne, (T)1, pv, c->ne, ps, c->ne, (T)0, m, nst, 1, nullptr, nullptr, c->st,
+              c->gws, c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes));
+  convert<T, double>(m, c->d_fs_A, (long)nst * nst, c->st);
+  CKL();
+  return 0;
+}
+
+extern "C" int qx_fssh_step(qx_ctx *c, const double *phis, const double *eig, double *occ, int *transition,
+                            double *bkl) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_fssh) { set_error("qx_fssh_step: qx_fssh_init first"); return QX_ERR_STATE; }
+  const qx_fssh_parm &p = c->fs;
+  const int nst = p.nstate;
+  if (phis) {
+    CK(cudaMemcpyAsync(c->d_fs_A, phis, sizeof(double) * (size_t)nst * nst, cudaMemcpyHostToDevice, c->st));
+  } else {
+    TRY(c->prec == QX_PREC_FP64 ? fssh_overlap<double>(c) : fssh_overlap<float>(c));
+    TRY(qx_tddft_store(c));   // psi(t + dt) becomes the previous step's
+  }
+  if (eig) CK(cudaMemcpyAsync(c->d_fs_eig, eig, sizeof(double) * nst, cudaMemcpyHostToDevice, c->st));
+  else CK(cudaMemcpyAsync(c->d_fs_eig, c->d_eig + p.b0, sizeof(double) * nst, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_fs_occ0, c->d_fs_occ, sizeof(double) * nst, cudaMemcpyDeviceToDevice, c->st));
+  fssh_step(nst, c->d_fs_A, c->d_fs_eig, p.dtmd, p.dttddft, p.boltzmann, p.treq, p.hop, c->d_fs_dnr, c->d_fs_dni,
+            c->d_fs_occ0, c->d_fs_occ, c->d_fs_pint, c->d_fs_accum, c->d_fs_rndx, c->d_fs_bkl, c->d_fs_trans, c->st);
+  CKL();
+  if (occ) CK(cudaMemcpyAsync(occ, c->d_fs_occ, sizeof(double) * nst, cudaMemcpyDeviceToHost, c->st));
+  if (transition) CK(cudaMemcpyAsync(transition, c->d_fs_trans, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  if (bkl) CK(cudaMemcpyAsync(bkl, c->d_fs_bkl, sizeof(double) * 7 * (size_t)nst, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return QX_OK;
+}
+
+extern "C" int qx_fssh_state(qx_ctx *c, double *dnr, double *dni, double *accum, double *rndx) {
+  if (!c) return QX_ERR_ARG;
+  if (!c->have_fssh) { set_error("qx_fssh_state: qx_fssh_init first"); return QX_ERR_STATE; }
+  const size_t nst = c->fs.nstate;
+  if (dnr) CK(cudaMemcpyAsync(dnr, c->d_fs_dnr, sizeof(double) * 49 * nst, cudaMemcpyDeviceToHost, c->st));
+  if (dni) CK(cudaMemcpyAsync(dni, c->d_fs_dni, sizeof(double) * 49 * nst, cudaMemcpyDeviceToHost, c->st));
+  if (accum) CK(cudaMemcpyAsync(accum, c->d_fs_accum, sizeof(double) * nst * nst, cudaMemcpyDeviceToHost, c->st));
+  if (rndx) CK(cudaMemcpyAsync(rndx, c->d_fs_rndx, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return QX_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -42,6 +42,56 @@ __global__ void k_phase_tables(int natom, const double *__restrict__ satm, int k
   }
 }
 
+// vlocal_g (nlkbpp.f90:862-1036): V(G) = (1/Omega) sum_a svco(G, type of a)
+// (cos G.R_a, -sin G.R_a) on the density half sphere, written at +G and, as
+// its conjugate, at -G of the full complex grid (zeroed before); one thread
+// per G, atoms summed in order.
+__global__ void k_vloc_g(int n5, int natom, const int *__restrict__ ijk5, const int *__restrict__ ngabc,
+                         const double *__restrict__ svco, const int *__restrict__ ityp, const double *__restrict__ dcq,
+                         const double *__restrict__ dsq, int km1, int km2, int km3, int ktot, double rvolr, int k1n,
+                         int k2n, int k3n, double2 *__restrict__ zg) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n5) return;
+  const int k1 = ngabc[3 * g], k2 = ngabc[3 * g + 1], k3 = ngabc[3 * g + 2];
+  double re = 0.0, im = 0.0;
+  for (int a = 0; a < natom; ++a) {
+    const double *c1 = dcq + (long)a * ktot + km1, *s1 = dsq + (long)a * ktot + km1;
+    const double *c2 = dcq + (long)a * ktot + 2 * km1 + 1 + km2, *s2 = dsq + (long)a * ktot + 2 * km1 + 1 + km2;
+    const double *c3 = dcq + (long)a * ktot + 2 * km1 + 2 * km2 + 2 + km3,
+                 *s3 = dsq + (long)a * ktot + 2 * km1 + 2 * km2 + 2 + km3;
+    const double cc12 = c1[k1] * c2[k2] - s1[k1] * s2[k2];
+    const double sc12 = s1[k1] * c2[k2] + c1[k1] * s2[k2];
+    const double zc = cc12 * c3[k3] - sc12 * s3[k3];
+    const double zs = sc12 * c3[k3] + cc12 * s3[k3];
+    const double sv = svco[(long)ityp[a] * n5 + g] * rvolr;
+    re += sv * zc;
+    im -= sv * zs;
+  }
+  zg[ijk5[g]] = make_double2(re, im);
+  if (g > 0) {
+    const int m1 = (k1n - k1 % k1n) % k1n, m2 = (k2n - k2 % k2n) % k2n, m3 = (k3n - k3 % k3n) % k3n;
+    zg[m1 + (long)k1n * (m2 + (long)k2n * m3)] = make_double2(re, -im);
+  }
+}
+
+__global__ void k_real_part(const double2 *__restrict__ z, double *__restrict__ out, long n) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    out[i] = z[i].x;
+}
+
+void real_part(const double2 *z, double *out, long n, cudaStream_t st) {
+  k_real_part<<<4 * 148, 256, 0, st>>>(z, out, n);
+  note_launch();
+}
+
+void vloc_g(int n5, int natom, const int *ijk5, const int *ngabc, const double *svco, const int *ityp,
+            const double *dcq, const double *dsq, int km1, int km2, int km3, int ktot, double rvol, int k1, int k2,
+            int k3, double2 *zg, cudaStream_t st) {
+  k_vloc_g<<<(n5 + 255) / 256, 256, 0, st>>>(n5, natom, ijk5, ngabc, svco, ityp, dcq, dsq, km1, km2, km3, ktot,
+                                             1.0 / rvol, k1, k2, k3, zg);
+  note_launch();
+}
+
 // One block per atom: the three components of floc, G = 0 excluded.
 __global__ void __launch_bounds__(FT) k_floc(int n5, const int *__restrict__ ijk5, const int *__restrict__ ngabc,
                                              const double *__restrict__ gvec5, const double *__restrict__ svco,

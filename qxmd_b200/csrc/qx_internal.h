@@ -173,6 +173,10 @@ void phase_tables(int natom, const double *satm, int km1, int km2, int km3, int 
 void floc_g(int natom, int n5, const int *ijk5, const int *ngabc, const double *gvec5, const double *svco,
             const int *ityp, const double2 *rhog, const double *dcq, const double *dsq, int km1, int km2, int km3,
             int ktot, double *floc, cudaStream_t st);
+void real_part(const double2 *z, double *out, long n, cudaStream_t st);
+void vloc_g(int n5, int natom, const int *ijk5, const int *ngabc, const double *svco, const int *ityp,
+            const double *dcq, const double *dsq, int km1, int km2, int km3, int ktot, double rvol, int k1, int k2,
+            int k3, double2 *zg, cudaStream_t st);
 template <typename T>
 void dtab_build(int nproj, int nplw, const T *kbg, const double *gw, T *dtab, cudaStream_t st);
 template <typename T>

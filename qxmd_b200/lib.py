@@ -35,6 +35,7 @@ EXPORTS = [
     "qxgpu_kbnlpp_frc2",
     "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
+    "qx_fssh_init", "qx_fssh_step", "qx_fssh_state", "qx_build_vloc",
 ]
 
 
@@ -57,6 +58,13 @@ class CgParm(C.Structure):
                  roughfeig=0.3, threinn=0.0, wdinner=0.9, ccreal4=0, sequential=0)
         p.update(kw)
         return cls(**p)
+
+
+class FsshParm(C.Structure):
+    """qx_fssh_parm: band window, MD step and substep (Rydberg time units),
+    Boltzmann factor and its temperature (Ry), hops on/off, rnd00 seed."""
+    _fields_ = [("b0", C.c_int), ("nstate", C.c_int), ("dtmd", C.c_double), ("dttddft", C.c_double),
+                ("boltzmann", C.c_int), ("treq", C.c_double), ("hop", C.c_int), ("seed", C.c_double)]
 
 
 class ScfOut(C.Structure):
@@ -148,6 +156,10 @@ def lib(build_if_missing: bool = True):
         "qxgpu_untryt": ([_ctx, _dp, _dp, _vp], C.c_int),
         "qxgpu_softchg": ([_ctx, _dp, _dp], C.c_int),
         "qxgpu_rfft3": ([_ctx, C.c_int, _dp, _dp], C.c_int),
+        "qx_fssh_init": ([_ctx, C.POINTER(FsshParm), _dp], C.c_int),
+        "qx_build_vloc": ([_ctx], C.c_int),
+        "qx_fssh_step": ([_ctx, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "qx_fssh_state": ([_ctx, _vp, _vp, _vp, _vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -342,6 +354,36 @@ class Context:
         _ck(self.L.qx_tddft_overlap(self.h, out), "qx_tddft_overlap")
         return out.T.copy()   # column-major (i + j nband) -> [i, j]
 
+    def fssh_init(self, parm: FsshParm, occ):
+        """qx_fssh_init: start surface hopping on the band window of parm."""
+        self._fssh_n = parm.nstate
+        _ck(self.L.qx_fssh_init(self.h, C.byref(parm), _f64(occ)), "qx_fssh_init")
+
+    def fssh_step(self, phis=None, eig=None):
+        """qx_fssh_step; phis[k, j] = <psi_k(t)|psi_j(t+dt)> (None: the device
+        overlap of the kept and the current psi).  Returns (transition None or
+        (s, news), occ (nstate), bkl (nstate, 7))."""
+        n = getattr(self, "_fssh_n", 1)
+        ph = None if phis is None else np.ascontiguousarray(np.asarray(phis, dtype=np.float64).T)
+        ev = None if eig is None else _f64(eig)
+        occ = np.zeros(n)
+        tr = C.c_int(-1)
+        bkl = np.zeros((n, 7))
+        _ck(self.L.qx_fssh_step(self.h, None if ph is None else ph.ctypes.data,
+                                None if ev is None else ev.ctypes.data, occ.ctypes.data, C.addressof(tr),
+                                bkl.ctypes.data), "qx_fssh_step")
+        return (None if tr.value < 0 else divmod(tr.value, n)), occ, bkl
+
+    def fssh_state(self):
+        """(dnr, dni (nstate, 7, 7), accum[news, s], rndx)."""
+        n = self._fssh_n
+        dnr, dni = np.zeros((n, 7, 7)), np.zeros((n, 7, 7))
+        acc = np.zeros((n, n))
+        r = C.c_double()
+        _ck(self.L.qx_fssh_state(self.h, dnr.ctypes.data, dni.ctypes.data, acc.ctypes.data, C.addressof(r)),
+            "qx_fssh_state")
+        return dnr, dni, acc.T.copy(), r.value
+
     def set_kb_builder(self, b: dict):
         """qx_set_kb_builder from the dict of cell.kb_builder_tables."""
         _ck(self.L.qx_set_kb_builder(self.h, b["ntype"], b["lmx"], b["mxqlm"], _f64(b["dlqlm"]), _f64(b["tbqlm"]),
@@ -400,6 +442,10 @@ class Context:
                                        _f64(t["satm"]), t["n5"], np.ascontiguousarray(t["ijk5"], dtype=np.int32),
                                        np.ascontiguousarray(t["ngabc"], dtype=np.int32), _f64(t["gvec5"]),
                                        _f64(t["svco"]), _f64(t["gw"])), "qx_set_force_tables")
+
+    def build_vloc(self):
+        """qx_build_vloc: the local pseudopotential of the force tables' geometry."""
+        _ck(self.L.qx_build_vloc(self.h), "qx_build_vloc")
 
     def forces(self):
         """(floc, fnl) of the current psi, each (natom, 3) Ry/bohr."""

@@ -20,7 +20,7 @@ from oracle import tables
 from qxmd_b200 import cell
 from qxmd_b200.lib import QX_NL_GSPACE, QX_NL_RSPACE, QX_PREC_FP64, QX_PREC_MIXED, Context
 
-from gpu_util import need_gpu, relerr
+from gpu_util import device_array, need_gpu, relerr
 
 pytestmark = pytest.mark.gpu
 TAB_TOL = {QX_PREC_FP64: 1e-13, QX_PREC_MIXED: 2e-7}
@@ -271,3 +271,31 @@ def test_build_kb_g_moves_the_force_tables(si8, si8_psi):
         ref.close()
     assert np.max(np.abs(fl - rl)) / np.max(np.abs(rl)) < 1e-10
     assert np.max(np.abs(fn - rn)) / np.max(np.abs(rn)) < 1e-6
+
+
+def test_build_vloc_matches_host_potential_after_moves(si8):
+    """qx_build_vloc (vlocal_g, nlkbpp.f90:862-1036) at the set-up geometry
+    and after qx_build_kb_g moved the atoms: the device potential against
+    the host's v(r) = sum_G V(G) e^{iG.r} of the same geometry (1e-12 of its
+    largest value: recurrence phases against direct cosines)."""
+    need_gpu()
+    torch = pytest.importorskip("torch")
+    b = cell.kb_builder_tables(si8.gs, si8.cell, si8.pp)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    try:
+        ctx.scf_init()
+        ctx.set_force_tables()
+        ctx.set_kb_builder(b)
+        satm = b["satm"]
+        for step in range(3):
+            if step:
+                satm = _moved(satm, 60 + step)
+                ctx.build_kb_g(b["ityp"], satm)
+            ctx.build_vloc()
+            ctx.sync()
+            got = device_array(torch, ctx.dev_ptr(5), si8.gs.kfft0)
+            moved = dataclasses.replace(si8.cell, pos=satm @ si8.gs.rba.T)
+            ref = cell.vloc_grid(si8.gs, moved, si8.pp)
+            assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-12
+    finally:
+        ctx.close()
