@@ -50,6 +50,8 @@ PIPELINE_LIMITER = ("latency, not HBM: DRAM traffic is 0.17x the algorithmic byt
                     "and long scoreboard")
 # FP64 SCF iterations of the refinement sweep after the mixed solution converged
 REFINE_ITERS = 3
+# iteration cap of the Si512 run to self-consistency
+SI512_MAX_ITERS = 80
 UNIT = "iter/s"
 WORKLOAD = "Si64 diamond 2x2x2, Gamma, Ecut 16 Ry / 64 Ry, 54^3 grid, 160 bands, G-space KB"
 DATA = "synthetic (seeded Si64 cell, model pseudopotential)"
@@ -340,7 +342,7 @@ def run_si512(args):
     from qxmd_b200 import cell
     from qxmd_b200.lib import Context, QX_NL_GSPACE, QX_PREC_FP64, QX_PREC_MIXED
     t0 = time.perf_counter()
-    sys_ = cell.si512()
+    sys_ = cell.si512(with_ewald=True)
     setup_s = time.perf_counter() - t0
     psi = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -393,6 +395,60 @@ def run_si512(args):
     out["scf_mixed"] = {"value": R / (t / 1e3), "unit": "iter/s", "ms_per_iter": t / R,
                         "cg_bapps_per_iter": nh / R, "etot_last_ry": r["etot"],
                         "iterations_before": max(1, args.warmup)}
+    # on to self-consistency (|dE| < 1e-8 Ry between iterations), then the
+    # FP64 refinement sweep of the converged mixed state, both timed
+    done = max(1, args.warmup) + R
+    hist, t_conv, e_prev = [], 0.0, r["etot"]
+    for _ in range(SI512_MAX_ITERS - done):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = ctx.scf_iteration(parm)
+        e1.record()
+        torch.cuda.synchronize()
+        t_conv += e0.elapsed_time(e1)
+        done += 1
+        hist.append((r["etot"], r["resid"]))
+        if abs(r["etot"] - e_prev) < 1e-8:
+            break
+        e_prev = r["etot"]
+    conv = {"iterations": done, "converged": abs(r["etot"] - e_prev) < 1e-8, "etot_ry": r["etot"],
+            "etot_ry_per_atom": r["etot"] / sys_.cell.natom, "resid": r["resid"],
+            "detot_last_ry": abs(r["etot"] - e_prev), "ms_after_timed": t_conv,
+            "etot_history_ry": [h[0] for h in hist[-6:]], "resid_history": [h[1] for h in hist[-6:]]}
+    ref = Context(sys_, QX_PREC_FP64, QX_NL_GSPACE)
+    ref.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+    ref.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
+    ref.refine_from(ctx)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    routs = [ref.scf_iteration(CgParm.defaults(int(sys_.cell.nel // 2))) for _ in range(REFINE_ITERS)]
+    e1.record()
+    torch.cuda.synchronize()
+    conv["fp64_refinement"] = {"iterations": REFINE_ITERS, "ms": e0.elapsed_time(e1),
+                               "etot_ry": routs[-1]["etot"], "resid": routs[-1]["resid"],
+                               "mixed_minus_fp64_ha_per_atom": 0.5 * (r["etot"] - routs[-1]["etot"]) / sys_.cell.natom,
+                               "detot_last_ry": abs(routs[-1]["etot"] - routs[-2]["etot"])}
+    ref.close()
+    # the same cutoffs (12/48 Ry) on the smaller cells: the energy per atom
+    # approaches the Si512 value as the Gamma-point sampling of the larger
+    # cells improves
+    trend = {}
+    for name, s in (("si8", cell.si8()), ("si64_12ry", cell.build_system(cell.diamond_si((2, 2, 2), seed=2),
+                                                                         12.0, 48.0, 160))):
+        c = Context(s, QX_PREC_MIXED, QX_NL_GSPACE)
+        c.put_psi(cell.random_wavefunctions(s.gs.nplwex, s.nband))
+        c.schmidt()
+        c.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+        c.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
+        c.scf_rho_from_psi()
+        p = CgParm.defaults(int(s.cell.nel // 2))
+        e = [c.scf_iteration(p)["etot"] for _ in range(40)]
+        trend[name] = {"etot_ry_per_atom": e[-1] / s.cell.natom, "detot_last_ry": abs(e[-1] - e[-2])}
+        c.close()
+    trend["si512"] = {"etot_ry_per_atom": r["etot"] / sys_.cell.natom}
+    conv["energy_per_atom_12ry"] = trend
+    out["scf_to_convergence"] = conv
     out["kb_tables"] = kb_build_timing(sys_, ctx, max(3, args.steps), max(3, args.warmup), flush)
     ctx.close()
     print(json.dumps(out), flush=True)
@@ -454,6 +510,45 @@ def run_batch(K, W):
             "launch": "one stream and one captured SCF-iteration graph per cell, all enqueued before any is read"}
 
 
+def run_rspace(sys_, psi0, K, W, iters, flush):
+    """The same SCF iteration with real-space KB projectors (calnlc, the
+    reference's default for Si), mixed precision: K timed iterations after W,
+    then on to `iters` in all, the self-consistent energy and occupied
+    eigenvalues against the oracle's (tests/golden/si64_scf_rspace.npz)."""
+    import torch
+
+    from qxmd_b200.lib import CgParm, Context, QX_NL_RSPACE, QX_PREC_MIXED
+    ctx = Context(sys_, QX_PREC_MIXED, QX_NL_RSPACE)
+    ctx.put_psi(psi0)
+    ctx.schmidt()
+    ctx.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+    ctx.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
+    ctx.scf_rho_from_psi()
+    parm = CgParm.defaults(int(sys_.cell.nel // 2))
+    for _ in range(W):
+        ctx.scf_iteration(parm)
+    t = 0.0
+    for _ in range(K):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.scf_iteration(parm)
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1)
+    outs = [ctx.scf_iteration(parm) for _ in range(max(2, iters - W - K))]
+    eig = ctx.get_eig()
+    ctx.close()
+    g = np.load(os.path.join(GOLDEN, "si64_scf_rspace.npz"))
+    nocc = int(g["noband"])
+    return {"path": "mixed, real-space KB (calnlc), projector points from setnlc's rule",
+            "value": K / (t * 1e-3), "unit": UNIT, "ms_per_step": t / K,
+            "accuracy": {"iterations": W + K + len(outs), "etot_ry": outs[-1]["etot"],
+                         "etot_oracle_ry": float(g["etot"][-1]),
+                         "err_ha_per_atom": 0.5 * abs(outs[-1]["etot"] - float(g["etot"][-1])) / sys_.cell.natom,
+                         "eig_occ_max_abs_err_ha": 0.5 * float(np.max(np.abs(eig[:nocc] - g["eig"][:nocc])))}}
+
+
 def run_fssh_md(nmd=FSSH_MD_STEPS, nscf=FSSH_SCF_PER_STEP):
     """TDDFT-FSSH on Si64 (32 adiabatic states around the gap, 1 fs MD
     steps): after the ground state is converged, every MD step moves the
@@ -506,6 +601,7 @@ def run_fssh_md(nmd=FSSH_MD_STEPS, nscf=FSSH_SCF_PER_STEP):
         e0.record()
         ctx.build_kb_g(b["ityp"], satm)
         ctx.build_vloc()
+        ctx.scf_rho_from_psi()          # the new step's SCF starts from rho(psi), mixing history restarted
         for _ in range(nscf):
             ctx.scf_launch(parm)
         e1.record()
@@ -682,6 +778,7 @@ def run_ours(args):
     mixed, fp64, fp64b = res["mixed"], res["fp64"], res["fp64_batched"]
     batch = run_batch(K, W) if ws == 1 else None
     fssh = run_fssh_md() if ws == 1 else None
+    rspace = run_rspace(sys_, psi0, K, W, args.accuracy_iters, flush)
     hbm, peak_kind = peaks()
     N, ne = sys_.gs.kfft0, sys_.gs.nplwex
     bytes_per_bapp = 4 * N * 4 + 2 * ne * 4
@@ -704,6 +801,7 @@ def run_ours(args):
                          "cg_bapps_per_iter": fp64b["cg_bapps_per_iter"]},
         "batch48": batch,
         "fssh_md": fssh,
+        "mixed_rspace": rspace,
         "kb_tables": kb_tables,
         "mixed_over_fp64": mixed["value"] / fp64["value"],
         "mixed_over_fp64_batched": mixed["value"] / fp64b["value"],

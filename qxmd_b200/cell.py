@@ -477,7 +477,6 @@ def ewald_energy(cell: Cell, gs: GSphere, eta: float | None = None) -> float:
     nat = cell.natom
     if eta is None:
         eta = (math.sqrt(math.pi) * nat ** (1 / 6) / vol ** (1 / 3)) ** 2
-    from math import erfc
     # real space
     rc = 6.0 / math.sqrt(eta)
     nmax = [int(math.ceil(rc / np.linalg.norm(a[:, i]))) + 1 for i in range(3)]
@@ -488,12 +487,12 @@ def ewald_energy(cell: Cell, gs: GSphere, eta: float | None = None) -> float:
             for k in range(-nmax[2], nmax[2] + 1):
                 shifts.append(a @ np.array([i, j, k], dtype=np.float64))
     shifts = np.array(shifts)
-    for ia in range(nat):
-        d = cell.pos[ia] - cell.pos + 0.0
-        for s in shifts:
-            rr = np.linalg.norm(d + s, axis=1)
-            m = (rr > 1e-10) & (rr < rc)
-            er += np.sum(np.array([erfc(math.sqrt(eta) * x) for x in rr[m]]) / rr[m])
+    from scipy.special import erfc as verfc
+    d = cell.pos[:, None, :] - cell.pos[None, :, :]
+    for s in shifts:
+        rr = np.linalg.norm(d + s, axis=2)
+        m = (rr > 1e-10) & (rr < rc)
+        er += float(np.sum(verfc(math.sqrt(eta) * rr[m]) / rr[m]))
     er *= 0.5 * z * z
     # reciprocal space over the density sphere (half sphere, x2)
     g2 = gs.recnrm[1:]

@@ -56,7 +56,11 @@ __device__ __forceinline__ bool fs_active(const double *occ, int nst, int s) {
 }
 
 // One warp per state s: lane e < 49 owns rho(a - 3, b - 3) with
-// (a, b) = (e / 7, e % 7), lanes 0..16 also e + 32.
+// (a, b) = (e / 7, e % 7), lanes 0..16 also e + 32.  The couplings of an
+// element's row a and column b and its energy difference stay in registers
+// for the whole MD step; the stage matrix is shared through shared memory,
+// zero outside the window (the zero couplings there add exact zeros, so the
+// sums equal those over the window alone).
 __global__ void __launch_bounds__(32) k_fssh_prop(int nst, const double *A, const double *eig, double dtmd,
                                                  double dttddft, double *dnr, double *dni, const double *occ_store,
                                                  double *probinteg) {
@@ -70,61 +74,59 @@ __global__ void __launch_bounds__(32) k_fssh_prop(int nst, const double *A, cons
     const int a = e / FW, b = e % FW;
     const bool ok = a - FN >= n1 && a - FN <= n2 && b - FN >= n1 && b - FN <= n2;
     D[a][b] = ok ? dkj(A, nst, s + a - FN, s + b - FN, dtmd) : 0.0;
+    Sr[a][b] = 0.0;
+    Si[a][b] = 0.0;
   }
   if (lane < FW) E[lane] = (lane - FN >= n1 && lane - FN <= n2) ? eig[s + lane - FN] : 0.0;
-  // own elements
+  __syncwarp();
+  // own elements, their couplings and energy differences
   int ea[2], eb[2];
   bool own[2];
-  double dr[2], di[2];
+  double dr[2], di[2], de[2], drow[2][FW], dcol[2][FW];
   double *gr = dnr + (long)s * FW * FW, *gi = dni + (long)s * FW * FW;
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const int e = lane + 32 * t;
-    ea[t] = e / FW;
+    ea[t] = min(e / FW, FW - 1);
     eb[t] = e % FW;
     own[t] = e < FW * FW && ea[t] - FN >= n1 && ea[t] - FN <= n2 && eb[t] - FN >= n1 && eb[t] - FN <= n2;
     dr[t] = own[t] ? gr[e] : 0.0;
     di[t] = own[t] ? gi[e] : 0.0;
+    de[t] = sub(E[ea[t]], E[eb[t]]);
+#pragma unroll
+    for (int l = 0; l < FW; ++l) {
+      drow[t][l] = D[ea[t]][l];   // d(j, l)
+      dcol[t][l] = D[l][eb[t]];   // d(l, k)
+    }
   }
   const double rkc[4] = {0.0, dvd(dttddft, 2.0), dvd(dttddft, 2.0), dttddft};
   const int nstep = (int)(dtmd / dttddft);
-  const int l0 = n1 + FN, l1 = n2 + FN;
   // probability integrals of the neighbours this lane owns (elements (iud + 3, 3))
   bool pown[2];
   double pint[2] = {0.0, 0.0};
 #pragma unroll
   for (int t = 0; t < 2; ++t) pown[t] = own[t] && eb[t] == FN && ea[t] != FN;
-  __syncwarp();
   for (int step = 0; step < nstep; ++step) {
     double kr[4][2], ki[4][2];
 #pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if (own[t]) { Sr[ea[t]][eb[t]] = dr[t]; Si[ea[t]][eb[t]] = di[t]; }
-    __syncwarp();
-#pragma unroll
     for (int irk = 0; irk < 4; ++irk) {
-      if (irk > 0) {
-        __syncwarp();   // every lane has read the previous stage input
+      __syncwarp();   // every lane has read the previous stage input
 #pragma unroll
-        for (int t = 0; t < 2; ++t)
-          if (own[t]) {
-            Sr[ea[t]][eb[t]] = add(dr[t], mul(rkc[irk], kr[irk - 1][t]));
-            Si[ea[t]][eb[t]] = add(di[t], mul(rkc[irk], ki[irk - 1][t]));
-          }
-        __syncwarp();
-      }
+      for (int t = 0; t < 2; ++t)
+        if (own[t]) {
+          Sr[ea[t]][eb[t]] = irk == 0 ? dr[t] : add(dr[t], mul(rkc[irk], kr[irk - 1][t]));
+          Si[ea[t]][eb[t]] = irk == 0 ? di[t] : add(di[t], mul(rkc[irk], ki[irk - 1][t]));
+        }
+      __syncwarp();
 #pragma unroll
       for (int t = 0; t < 2; ++t) {
-        kr[irk][t] = 0.0;
-        ki[irk][t] = 0.0;
-        if (!own[t]) continue;
         const int a = ea[t], b = eb[t];
-        const double de = sub(E[a], E[b]);
-        double r = mul(de, Si[a][b]);
-        double m = mul(-de, Sr[a][b]);
-        for (int l = l0; l <= l1; ++l) {
-          r = add(sub(r, mul(Sr[a][l], D[l][b])), mul(Sr[l][b], D[a][l]));
-          m = add(sub(m, mul(Si[a][l], D[l][b])), mul(Si[l][b], D[a][l]));
+        double r = mul(de[t], Si[a][b]);
+        double m = mul(-de[t], Sr[a][b]);
+#pragma unroll
+        for (int l = 0; l < FW; ++l) {
+          r = add(sub(r, mul(Sr[a][l], dcol[t][l])), mul(Sr[l][b], drow[t][l]));
+          m = add(sub(m, mul(Si[a][l], dcol[t][l])), mul(Si[l][b], drow[t][l]));
         }
         kr[irk][t] = r;
         ki[irk][t] = m;
@@ -147,7 +149,6 @@ __global__ void __launch_bounds__(32) k_fssh_prop(int nst, const double *A, cons
 #pragma unroll
     for (int t = 0; t < 2; ++t)
       if (pown[t]) pint[t] = add(pint[t], dvd(Sr[ea[t]][FN], Sr[FN][FN]));
-    __syncwarp();
   }
 #pragma unroll
   for (int t = 0; t < 2; ++t)

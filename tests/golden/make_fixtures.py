@@ -17,6 +17,8 @@ that the GPU parity tests and bench.py's accuracy block compare against:
   cmetric 20) to self-consistency: total energy, residual and CG work per
   iteration, the final eigenvalues and the Hellmann-Feynman forces (local
   flocal_g + G-space KB kbnlpp_frc2 + Ewald).
+* si64_scf_rspace.npz -- the same iteration with real-space KB projectors
+  (calnlc, the reference's default for Si) to self-consistency.
 * batch_cells.npz -- three cells of the 48-cell batch with different grids
   (21^3, 42x21x21, 25^3) iterated the same way to self-consistency.
 * si512_hpsi.npz  -- H|psi> of four LCG bands of Si512 (96^3 grid, 2048
@@ -71,11 +73,11 @@ def low_g(rho: np.ndarray, gs, n: int = NLOWG) -> np.ndarray:
     return z[gs.ijk_pos[:n]]
 
 
-def scf_to_convergence(s, iters: int, noband: int):
+def scf_to_convergence(s, iters: int, noband: int, nlmode: int = 1):
     psi = cell.random_wavefunctions(s.gs.nplwex, s.nband)
     psi, _, rc = oracle.schmidt(psi)
     assert rc == 0
-    st = ScfState(s, psi, nlmode=1, mixbeta=ASLH, kerker_q0=Q0, pulay=ITRATN, cmetric=CMETRIC)
+    st = ScfState(s, psi, nlmode=nlmode, mixbeta=ASLH, kerker_q0=Q0, pulay=ITRATN, cmetric=CMETRIC)
     out = []
     for it in range(iters):
         r = st.iteration(noband=noband)
@@ -119,6 +121,18 @@ def make_si64_scf():
                 eewald=s.eewald)
 
 
+def make_si64_scf_rspace():
+    """The Si64 iteration with real-space KB projectors (calnlc, QXMD's
+    default for Si) to self-consistency: energies per iteration and the final
+    eigenvalues."""
+    s = cell.si64()
+    noband = int(s.cell.nel // 2)
+    st, out = scf_to_convergence(s, SI64_ITERS, noband, nlmode=2)
+    return dict(etot=np.array([r["etot"] for r in out]), resid=np.array([r["resid"] for r in out]),
+                ncg_hpsi=np.array([r["ncg_hpsi"] for r in out], dtype=np.int32), eig=out[-1]["eig"],
+                natom=s.cell.natom, noband=noband)
+
+
 def make_batch_cells():
     d = {"cells": np.array(BATCH_CELLS, dtype=np.int32), "iters": BATCH_ITERS}
     for i in BATCH_CELLS:
@@ -141,7 +155,8 @@ def make_si512_hpsi():
                 hpsi_chk=np.stack([gamma_dot(hc, vv[None, :]) for vv in v]), hpsi_head=hc[:, :1024])
 
 
-MAKERS = {"si64_start": make_si64_start, "si64_scf": make_si64_scf, "batch_cells": make_batch_cells,
+MAKERS = {"si64_start": make_si64_start, "si64_scf": make_si64_scf, "si64_scf_rspace": make_si64_scf_rspace,
+          "batch_cells": make_batch_cells,
           "si512_hpsi": make_si512_hpsi}
 
 

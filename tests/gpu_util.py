@@ -17,6 +17,6 @@ def device_array(torch, ptr, n, typestr="<f8"):
     """Host copy of n elements at a device pointer of this library (read
     through the CUDA array interface)."""
     class _View:
-        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), True), "version": 3}
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False), "version": 3}
     torch.cuda.synchronize()
     return torch.as_tensor(_View(), device="cuda").cpu().numpy()

@@ -146,6 +146,34 @@ def test_si64_scf_against_fixture(si64, prec, sequential):
 
 
 @pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_si64_scf_rspace_against_fixture(si64, prec):
+    """The same 40 iterations with real-space KB projectors (calnlc, the
+    reference's default for Si): self-consistent energy per atom and
+    occupied eigenvalues against the oracle's."""
+    need_gpu()
+    from qxmd_b200.lib import QX_NL_RSPACE
+    g = golden("si64_scf_rspace")
+    s = si64
+    ctx = Context(s, prec, QX_NL_RSPACE)
+    try:
+        ctx.put_psi(cell.random_wavefunctions(s.gs.nplwex, s.nband))
+        ctx.schmidt()
+        ctx.scf_init(**PULAY)
+        ctx.scf_mixing(10, 20.0)
+        ctx.scf_rho_from_psi()
+        p = CgParm.defaults(int(g["noband"]))
+        e = [ctx.scf_iteration(p)["etot"] for _ in range(g["etot"].size)]
+        if prec == QX_PREC_FP64:
+            assert relerr(np.array(e[:4]), g["etot"][:4]) < 1e-9
+        de, _, deig = GATE[prec]
+        assert abs(e[-1] - g["etot"][-1]) / int(g["natom"]) < de
+        nocc = int(g["noband"])
+        assert np.max(np.abs(ctx.get_eig()[:nocc] - g["eig"][:nocc])) < deig
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
 def test_batch_cells_against_fixture(prec):
     """Three cells of the batch, each on its own stream and enqueued before any
     is read, iterated to self-consistency."""
