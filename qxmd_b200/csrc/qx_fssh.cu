@@ -55,111 +55,81 @@ __device__ __forceinline__ bool fs_active(const double *occ, int nst, int s) {
   return any;
 }
 
-// One warp per state s: lane e < 49 owns rho(a - 3, b - 3) with
-// (a, b) = (e / 7, e % 7), lanes 0..16 also e + 32.  The couplings of an
-// element's row a and column b and its energy difference stay in registers
-// for the whole MD step; the stage matrix is shared through shared memory,
-// zero outside the window (the zero couplings there add exact zeros, so the
-// sums equal those over the window alone).
-__global__ void __launch_bounds__(32) k_fssh_prop(int nst, const double *A, const double *eig, double dtmd,
-                                                 double dttddft, double *dnr, double *dni, const double *occ_store,
-                                                 double *probinteg) {
+// One CTA of 128 threads per state s: thread t < 98 owns the real (t even) or
+// imaginary (t odd) part of rho(a - 3, b - 3), (a, b) = (e / 7, e % 7),
+// e = t / 2.  Each thread carries one chain of the reference's sum, in the
+// reference's order.  The couplings of the element's row a and column b and
+// its energy difference stay in registers for the whole MD step; the RK
+// stage matrices go through two shared buffers in turn, so one barrier per
+// stage suffices.  Outside the window the matrices are zero and the
+// couplings too: the extra terms add exact zeros, so the sums equal those
+// over the window alone.
+constexpr int FT_PROP = 128;
+__global__ void __launch_bounds__(FT_PROP) k_fssh_prop(int nst, const double *A, const double *eig, double dtmd,
+                                                      double dttddft, double *dnr, double *dni,
+                                                      const double *occ_store, double *probinteg) {
   const int s = blockIdx.x;
-  const int lane = threadIdx.x;
-  __shared__ double D[FW][FW], E[FW], Sr[FW][FW], Si[FW][FW];
-  if (lane < FW) probinteg[(long)s * FW + lane] = 0.0;
+  const int t = threadIdx.x;
+  __shared__ double D[FW][FW], E[FW];
+  __shared__ double S[2][2][FW][FW];   // [buffer][re, im][a][b]
+  if (t < FW) probinteg[(long)s * FW + t] = 0.0;
   if (!fs_active(occ_store, nst, s)) return;
   const int n1 = max(-FN, -s), n2 = min(FN, nst - 1 - s);
-  for (int e = lane; e < FW * FW; e += 32) {
-    const int a = e / FW, b = e % FW;
+  if (t < FW * FW) {
+    const int a = t / FW, b = t % FW;
     const bool ok = a - FN >= n1 && a - FN <= n2 && b - FN >= n1 && b - FN <= n2;
     D[a][b] = ok ? dkj(A, nst, s + a - FN, s + b - FN, dtmd) : 0.0;
-    Sr[a][b] = 0.0;
-    Si[a][b] = 0.0;
   }
-  if (lane < FW) E[lane] = (lane - FN >= n1 && lane - FN <= n2) ? eig[s + lane - FN] : 0.0;
-  __syncwarp();
-  // own elements, their couplings and energy differences
-  int ea[2], eb[2];
-  bool own[2];
-  double dr[2], di[2], de[2], drow[2][FW], dcol[2][FW];
-  double *gr = dnr + (long)s * FW * FW, *gi = dni + (long)s * FW * FW;
+  for (int i = t; i < 2 * 2 * FW * FW; i += FT_PROP) (&S[0][0][0][0])[i] = 0.0;
+  if (t < FW) E[t] = (t - FN >= n1 && t - FN <= n2) ? eig[s + t - FN] : 0.0;
+  __syncthreads();
+  const int e = min(t >> 1, FW * FW - 1), part = t & 1;
+  const int a = e / FW, b = e % FW;
+  const bool own = t < 2 * FW * FW && a - FN >= n1 && a - FN <= n2 && b - FN >= n1 && b - FN <= n2;
+  double *g = (part ? dni : dnr) + (long)s * FW * FW + e;
+  double dv = own ? *g : 0.0;
+  const double de = part ? -sub(E[a], E[b]) : sub(E[a], E[b]);
+  double drow[FW], dcol[FW];
 #pragma unroll
-  for (int t = 0; t < 2; ++t) {
-    const int e = lane + 32 * t;
-    ea[t] = min(e / FW, FW - 1);
-    eb[t] = e % FW;
-    own[t] = e < FW * FW && ea[t] - FN >= n1 && ea[t] - FN <= n2 && eb[t] - FN >= n1 && eb[t] - FN <= n2;
-    dr[t] = own[t] ? gr[e] : 0.0;
-    di[t] = own[t] ? gi[e] : 0.0;
-    de[t] = sub(E[ea[t]], E[eb[t]]);
-#pragma unroll
-    for (int l = 0; l < FW; ++l) {
-      drow[t][l] = D[ea[t]][l];   // d(j, l)
-      dcol[t][l] = D[l][eb[t]];   // d(l, k)
-    }
+  for (int l = 0; l < FW; ++l) {
+    drow[l] = D[a][l];   // d(j, l)
+    dcol[l] = D[l][b];   // d(l, k)
   }
   const double rkc[4] = {0.0, dvd(dttddft, 2.0), dvd(dttddft, 2.0), dttddft};
   const int nstep = (int)(dtmd / dttddft);
-  // probability integrals of the neighbours this lane owns (elements (iud + 3, 3))
-  bool pown[2];
-  double pint[2] = {0.0, 0.0};
-#pragma unroll
-  for (int t = 0; t < 2; ++t) pown[t] = own[t] && eb[t] == FN && ea[t] != FN;
+  // probability integral of the neighbour owned here (real part of element (iud + 3, 3))
+  const bool pown = own && part == 0 && b == FN && a != FN;
+  double pint = 0.0;
+  if (own) S[0][part][a][b] = dv;
+  __syncthreads();
   for (int step = 0; step < nstep; ++step) {
-    double kr[4][2], ki[4][2];
+    double k[4];
 #pragma unroll
     for (int irk = 0; irk < 4; ++irk) {
-      __syncwarp();   // every lane has read the previous stage input
+      const int cur = irk & 1;
+      // real part: (e_j - e_k) Im rho + sum_l (-Re rho(j, l) d(l, k) + Re rho(l, k) d(j, l));
+      // imaginary part: -(e_j - e_k) Re rho + the same sum over Im rho
+      const double(*X)[FW] = S[cur][part];
+      double r = mul(de, S[cur][1 - part][a][b]);
 #pragma unroll
-      for (int t = 0; t < 2; ++t)
-        if (own[t]) {
-          Sr[ea[t]][eb[t]] = irk == 0 ? dr[t] : add(dr[t], mul(rkc[irk], kr[irk - 1][t]));
-          Si[ea[t]][eb[t]] = irk == 0 ? di[t] : add(di[t], mul(rkc[irk], ki[irk - 1][t]));
+      for (int l = 0; l < FW; ++l) r = add(sub(r, mul(X[a][l], dcol[l])), mul(X[l][b], drow[l]));
+      k[irk] = r;
+      if (own) {
+        if (irk < 3) {
+          S[1 - cur][part][a][b] = add(dv, mul(rkc[irk + 1], r));
+        } else {
+          // RK4 update: rho + (k1 + 2 k2 + 2 k3 + k4) dttddft / 6 (tddft_fssh.f90:2168-2177)
+          const double sm = add(add(add(k[0], mul(2.0, k[1])), mul(2.0, k[2])), k[3]);
+          dv = add(dv, dvd(mul(sm, dttddft), 6.0));
+          S[0][part][a][b] = dv;
         }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int a = ea[t], b = eb[t];
-        double r = mul(de[t], Si[a][b]);
-        double m = mul(-de[t], Sr[a][b]);
-#pragma unroll
-        for (int l = 0; l < FW; ++l) {
-          r = add(sub(r, mul(Sr[a][l], dcol[t][l])), mul(Sr[l][b], drow[t][l]));
-          m = add(sub(m, mul(Si[a][l], dcol[t][l])), mul(Si[l][b], drow[t][l]));
-        }
-        kr[irk][t] = r;
-        ki[irk][t] = m;
       }
+      __syncthreads();
     }
-    // RK4 update: rho + (k1 + 2 k2 + 2 k3 + k4) dttddft / 6 (tddft_fssh.f90:2168-2177)
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if (own[t]) {
-        const double sr = add(add(add(kr[0][t], mul(2.0, kr[1][t])), mul(2.0, kr[2][t])), kr[3][t]);
-        const double si = add(add(add(ki[0][t], mul(2.0, ki[1][t])), mul(2.0, ki[2][t])), ki[3][t]);
-        dr[t] = add(dr[t], dvd(mul(sr, dttddft), 6.0));
-        di[t] = add(di[t], dvd(mul(si, dttddft), 6.0));
-      }
-    __syncwarp();
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if (own[t]) Sr[ea[t]][eb[t]] = dr[t];
-    __syncwarp();
-#pragma unroll
-    for (int t = 0; t < 2; ++t)
-      if (pown[t]) pint[t] = add(pint[t], dvd(Sr[ea[t]][FN], Sr[FN][FN]));
+    if (pown) pint = add(pint, dvd(S[0][0][a][FN], S[0][0][FN][FN]));
   }
-#pragma unroll
-  for (int t = 0; t < 2; ++t)
-    if (own[t]) {
-      const int e = lane + 32 * t;
-      gr[e] = dr[t];
-      gi[e] = di[t];
-    }
-#pragma unroll
-  for (int t = 0; t < 2; ++t)
-    if (pown[t]) probinteg[(long)s * FW + ea[t]] = pint[t];
+  if (own) *g = dv;
+  if (pown) probinteg[(long)s * FW + a] = pint;
 }
 
 // Park-Miller rnd00: rndx <- mod(16807 rndx, 2147483647), rn = rndx / 2147483647.
@@ -220,7 +190,7 @@ void fssh_init(int nst, double *dnr, double *dni, double *accum, cudaStream_t st
 void fssh_step(int nst, const double *A, const double *eig, double dtmd, double dttddft, int boltz, double treq,
                int hop, double *dnr, double *dni, const double *occ_store, double *occ_rec, double *probinteg,
                double *accum, double *rndx, double *bkl, int *trans, cudaStream_t st) {
-  k_fssh_prop<<<nst, 32, 0, st>>>(nst, A, eig, dtmd, dttddft, dnr, dni, occ_store, probinteg);
+  k_fssh_prop<<<nst, FT_PROP, 0, st>>>(nst, A, eig, dtmd, dttddft, dnr, dni, occ_store, probinteg);
   note_launch();
   k_fssh_hop<<<1, 32, 0, st>>>(nst, A, eig, dtmd, dttddft, boltz, treq, hop, probinteg, occ_store, occ_rec, accum,
                                rndx, bkl, trans);
