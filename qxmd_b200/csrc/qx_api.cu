@@ -224,21 +224,19 @@ extern "C" int qx_version(void) { return 1; }
 extern "C" long qx_launch_count(void) { return g_launches.load(); }
 
 // ---------------------------------------------------------------------------
-static bool factor_len(int n, FftLen &L) {
-  L.n = n;
-  L.nstage = 0;
-  int m = n;
-  // largest radices first: fewer passes through shared memory
-  const int rad[8] = {9, 8, 7, 6, 5, 4, 3, 2};
-  while (m > 1) {
-    int r = 0;
-    for (int c : rad)
-      if (m % c == 0) { r = c; break; }
-    if (!r || L.nstage >= 8) return false;
-    L.radix[L.nstage++] = r;
-    m /= r;
+// The stage plan of a length from an explicit radix sequence (product n,
+// each 2..9, at most 8 stages) and the layout of its stage tables.
+static bool plan_len(int n, const int *radix, int nstage, FftLen &L) {
+  if (nstage < 0 || nstage > 8) return false;
+  long prod = 1;
+  for (int s = 0; s < nstage; ++s) {
+    if (radix[s] < 2 || radix[s] > 9) return false;
+    prod *= radix[s];
   }
-  // stage table layout
+  if (prod != n) return false;
+  L.n = n;
+  L.nstage = nstage;
+  for (int s = 0; s < nstage; ++s) L.radix[s] = radix[s];
   int ns = 1, st = 0, ob = 0;
   for (int s = 0; s < L.nstage; ++s) {
     const int R = L.radix[s], nr = n / R;
@@ -251,6 +249,38 @@ static bool factor_len(int n, FftLen &L) {
   L.nst = st;
   L.nob = ob;
   return true;
+}
+
+static bool factor_len(int n, FftLen &L) {
+  int m = n, nst = 0, radix[8];
+  // largest radices first: fewer passes through shared memory (the default
+  // plan; qx_autotune may pick another)
+  const int rad[8] = {9, 8, 7, 6, 5, 4, 3, 2};
+  while (m > 1) {
+    int r = 0;
+    for (int c : rad)
+      if (m % c == 0) { r = c; break; }
+    if (!r || nst >= 8) return false;
+    radix[nst++] = r;
+    m /= r;
+  }
+  return plan_len(n, radix, nst, L);
+}
+
+// Every ordered factorisation of n into radices 2..9 with at most maxst
+// stages (the autotuner's candidate plans).
+static void radix_plans(int n, int maxst, std::vector<std::vector<int>> &out, std::vector<int> &cur) {
+  if (n == 1) {
+    if (!cur.empty()) out.push_back(cur);
+    return;
+  }
+  if ((int)cur.size() >= maxst) return;
+  for (int r = 9; r >= 2; --r)
+    if (n % r == 0) {
+      cur.push_back(r);
+      radix_plans(n / r, maxst, out, cur);
+      cur.pop_back();
+    }
 }
 
 // Stage output bases (precision independent) of the three lengths.
@@ -295,6 +325,11 @@ static int upload_tw(qx_ctx *c) {
     }
   }
   C *dp = nullptr, *ds = nullptr;
+  // a new plan replaces the tables of the old one
+  TRY(dfree(c, pl.bufs<T>().tw));
+  TRY(dfree(c, pl.bufs<T>().stw));
+  pl.bufs<T>().tw = nullptr;
+  pl.bufs<T>().stw = nullptr;
   TRY(dalloc(c, &dp, sizeof(C) * base.size()));
   TRY(dalloc(c, &ds, sizeof(C) * std::max<size_t>(stg.size(), 1)));
   CK(cudaMemcpy(dp, base.data(), sizeof(C) * base.size(), cudaMemcpyHostToDevice));
@@ -378,6 +413,20 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
     set_error("qx_create: cannot write FFT roots to the device: %s", cudaGetErrorString(cudaGetLastError()));
     delete c;
     return QX_ERR_CUDA;
+  }
+  // QX_FFT_PLAN = "r1xr2x...": that radix sequence for every axis whose
+  // length it multiplies to (tests pin the stage kernels on chosen plans)
+  if (const char *fp = getenv("QX_FFT_PLAN")) {
+    int rad[8], nr = 0;
+    for (const char *q = fp; *q && nr < 8;) {
+      rad[nr++] = atoi(q);
+      while (*q && *q != 'x') ++q;
+      if (*q == 'x') ++q;
+    }
+    for (int d = 0; d < 3; ++d) {
+      FftLen L;
+      if (plan_len(pl.L[d].n, rad, nr, L)) pl.L[d] = L;
+    }
   }
   pl.tw_off[0] = 0; pl.tw_off[1] = k1; pl.tw_off[2] = k1 + k2;
   pl.stw_off[0] = 0; pl.stw_off[1] = pl.L[0].nst; pl.stw_off[2] = pl.L[0].nst + pl.L[1].nst;
@@ -1873,11 +1922,103 @@ static int time_ms(cudaStream_t st, const std::function<int()> &f, int reps, flo
   return 0;
 }
 
+// Applies the radix plans L[0..2] of the three grid lengths and rebuilds what
+// depends on them: the table offsets, the stage output bases and the
+// twiddles of every precision the context holds (the old tables are freed
+// and captured graphs dropped).  QX_ERR_ARG, with nothing changed, when the
+// plans' shared-memory tiles would exceed 227 KB.
+static int replan_fft(qx_ctx *c, const FftLen L[3]) {
+  Plan &pl = c->pl;
+  Plan trial = pl;
+  for (int d = 0; d < 3; ++d) trial.L[d] = L[d];
+  const size_t need64 = fft_smem_need<double>(trial), need32 = fft_smem_need<float>(trial);
+  if (need64 > 227 * 1024 || (c->prec == QX_PREC_MIXED && need32 > 227 * 1024)) return QX_ERR_ARG;
+  CK(cudaStreamSynchronize(c->st));
+  if (c->st2) CK(cudaStreamSynchronize(c->st2));
+  for (int d = 0; d < 3; ++d) pl.L[d] = L[d];
+  pl.stw_off[0] = 0; pl.stw_off[1] = pl.L[0].nst; pl.stw_off[2] = pl.L[0].nst + pl.L[1].nst;
+  pl.sob_off[0] = 0; pl.sob_off[1] = pl.L[0].nob; pl.sob_off[2] = pl.L[0].nob + pl.L[1].nob;
+  std::vector<int> sob;
+  for (int d = 0; d < 3; ++d) stage_bases(pl.L[d], sob);
+  TRY(dregrow(c, &pl.d_sob, sizeof(int) * std::max<size_t>(sob.size(), 1)));
+  if (!sob.empty()) CK(cudaMemcpy(pl.d_sob, sob.data(), sizeof(int) * sob.size(), cudaMemcpyHostToDevice));
+  if (c->prec == QX_PREC_MIXED) {
+    TRY(upload_tw<float>(c));
+    set_fft_smem_limits<float>(need32);
+  }
+  TRY(upload_tw<double>(c));
+  set_fft_smem_limits<double>(need64);
+  drop_scf_graphs(c);
+  if (c->seq_exec) { cudaGraphExecDestroy(c->seq_exec); c->seq_exec = nullptr; }
+  if (c->seq_graph) { cudaGraphDestroy(c->seq_graph); c->seq_graph = nullptr; }
+  CKL();
+  return QX_OK;
+}
+
+static std::string plan_str(const FftLen &L) {
+  std::string s;
+  for (int i = 0; i < L.nstage; ++i) s += (i ? "x" : "") + std::to_string(L.radix[i]);
+  return s;
+}
+
 extern "C" int qx_autotune(qx_ctx *c, char *report, int report_len) {
   if (!c) return QX_ERR_ARG;
   std::string rep;
   char buf[256];
   const int nb = c->nb, ne = c->ne, np = c->pl.nproj;
+  // FFT radix plans of the shared-memory stage kernels: for each distinct
+  // grid length, every ordered factorisation into radices 2..9 of at most
+  // four stages (fewest stages first, at most 16), timed on one H|psi> pass
+  // of this context plus an FP64 full-grid transform pair (the density side),
+  // the other lengths held at their current plans
+  if (c->have_glocal) {
+    auto measure = [&](float *ms) -> int {
+      float m1 = 0.f, m2 = 0.f;
+      TRY(time_ms(c->st, [&]() { return qx_hpsi(c, c->psi, c->tmp, nb, QX_HPSI_KINETIC); }, 3, &m1));
+      if (c->d_zg)
+        TRY(time_ms(c->st, [&]() {
+          TRY(launch_full_fft<double>(c->pl, c->d_zg, -1, 1.0, c->st));
+          return launch_full_fft<double>(c->pl, c->d_zg, +1, 1.0, c->st);
+        }, 3, &m2));
+      *ms = m1 + m2;
+      return 0;
+    };
+    const int lens[3] = {c->pl.k1, c->pl.k2, c->pl.k3};
+    bool done_len[3] = {false, false, false};
+    for (int d = 0; d < 3; ++d) {
+      if (done_len[d]) continue;
+      const int n = lens[d];
+      std::vector<std::vector<int>> cands;
+      std::vector<int> cur;
+      radix_plans(n, 4, cands, cur);
+      std::stable_sort(cands.begin(), cands.end(),
+                       [](const std::vector<int> &x, const std::vector<int> &y) { return x.size() < y.size(); });
+      if (cands.size() > 16) cands.resize(16);
+      FftLen best[3] = {c->pl.L[0], c->pl.L[1], c->pl.L[2]};
+      float tbest = 0.f;
+      TRY(measure(&tbest));
+      const float tdef = tbest;
+      for (const auto &cd : cands) {
+        FftLen L[3] = {c->pl.L[0], c->pl.L[1], c->pl.L[2]};
+        bool ok = true;
+        for (int e = 0; e < 3; ++e)
+          if (lens[e] == n) ok = ok && plan_len(n, cd.data(), (int)cd.size(), L[e]);
+        if (!ok || replan_fft(c, L) != QX_OK) continue;
+        float t = 0.f;
+        TRY(measure(&t));
+        if (t < tbest) {
+          tbest = t;
+          for (int e = 0; e < 3; ++e) best[e] = L[e];
+        }
+      }
+      TRY(replan_fft(c, best));
+      for (int e = 0; e < 3; ++e)
+        if (lens[e] == n) done_len[e] = true;
+      snprintf(buf, sizeof(buf), "FFT length %d: %zu plans, %s (%.1f us; default %.1f us); ", n, cands.size() + 1,
+               plan_str(best[d]).c_str(), tbest * 1e3, tdef * 1e3);
+      rep += buf;
+    }
+  }
   if (c->prec == QX_PREC_MIXED && tc_enabled()) {
     struct Shape { bool ta, tb; int M, N, K, gamma; const void *A; long lda; const void *B; long ldb; float beta; long ldc; const char *what; };
     std::vector<Shape> shapes = {
@@ -1888,26 +2029,34 @@ extern "C" int qx_autotune(qx_ctx *c, char *report, int report_len) {
       shapes.push_back({true, false, np, nb, ne, 2, c->pl.b32.kbg, ne, c->psi, ne, 0.f, np, "K^T C"});
       shapes.push_back({false, false, ne, nb, np, 0, c->pl.b32.kbg, ne, c->proj, np, 1.f, ne, "K P"});
     }
+    // tile width x K split per contraction shape
     const int cand[] = {1, 2, 3, 4, 6, 8, 12, 16, 24, 32, 48};
+    const int tiles[] = {64, 80, 96, 128};
     for (const Shape &sh : shapes) {
       const int nkb = (sh.K + 31) / 32;
       float best = 1e30f;
-      int bests = 1;
-      for (int ns : cand) {
-        if (ns > nkb || (size_t)ns * sh.M * sh.N * sizeof(float) > c->gws_bytes) continue;
-        float ms = 0.f;
-        tc_split_force = ns;
-        const int r = time_ms(c->st, [&]() {
-          return gemm<float>(sh.ta, sh.tb, sh.M, sh.N, sh.K, 1.f, (const float *)sh.A, sh.lda, (const float *)sh.B,
-                             sh.ldb, sh.beta, (float *)c->tmp, sh.ldc, sh.gamma, nullptr, nullptr, c->st, c->gws,
-                             c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes);
-        }, 3, &ms);
-        tc_split_force = 0;
-        TRY(r);
-        if (ms < best) { best = ms; bests = ns; }
+      int bests = 1, bestt = 0;
+      for (int bn : tiles) {
+        if (!tc_tile_valid(sh.tb, bn)) continue;
+        for (int ns : cand) {
+          if (ns > nkb || (size_t)ns * sh.M * sh.N * sizeof(float) > c->gws_bytes) continue;
+          float ms = 0.f;
+          tc_split_force = ns;
+          tc_tile_force = bn;
+          const int r = time_ms(c->st, [&]() {
+            return gemm<float>(sh.ta, sh.tb, sh.M, sh.N, sh.K, 1.f, (const float *)sh.A, sh.lda, (const float *)sh.B,
+                               sh.ldb, sh.beta, (float *)c->tmp, sh.ldc, sh.gamma, nullptr, nullptr, c->st, c->gws,
+                               c->gws_bytes, nullptr, c->tcpad, c->tcpad_bytes);
+          }, 3, &ms);
+          tc_split_force = 0;
+          tc_tile_force = 0;
+          TRY(r);
+          if (ms < best) { best = ms; bests = ns; bestt = bn; }
+        }
       }
-      tc_split_store(sh.ta, sh.tb, sh.M, sh.N, sh.K, sh.gamma, bests);
-      snprintf(buf, sizeof(buf), "%s %dx%dx%d: K split %d (%.1f us); ", sh.what, sh.M, sh.N, sh.K, bests, best * 1e3);
+      tc_split_store(sh.ta, sh.tb, sh.M, sh.N, sh.K, sh.gamma, bests, bestt);
+      snprintf(buf, sizeof(buf), "%s %dx%dx%d: tile %d, K split %d (%.1f us); ", sh.what, sh.M, sh.N, sh.K, bestt,
+               bests, best * 1e3);
       rep += buf;
     }
   }

@@ -152,9 +152,11 @@ void pad_rows_f32(const float *src, long ld, long inner, long rows, float *dst, 
 int tc_error_take();
 // autotuner hooks of the tensor-core GEMM: a per-shape K-split table and a
 // per-thread override used while timing candidates
-extern thread_local int tc_split_force;
+extern thread_local int tc_split_force, tc_tile_force;
 int tc_split_lookup(bool ta, bool tb, int M, int N, int K, int gamma);
-void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit);
+int tc_tile_lookup(bool ta, bool tb, int M, int N, int K, int gamma);
+void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit, int tile);
+bool tc_tile_valid(bool tb, int bn);
 
 // qx_dense.cu (FP64, nb x nb)
 // work: >= 32*33 + n doubles, used when S does not fit shared memory.

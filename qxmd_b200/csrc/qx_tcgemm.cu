@@ -573,19 +573,31 @@ static bool atmem_enabled() {
 
 bool tc_enabled() { return tc::enabled(); }
 
-// K-split factors chosen by the autotuner, per shape (process-wide: contexts
-// of equal sizes share them), and the override the autotuner times with.
+// K-split factors and tile widths chosen by the autotuner, per shape
+// (process-wide: contexts of equal sizes share them), and the overrides the
+// autotuner times with.
 static std::mutex g_split_mu;
-static std::map<std::array<long, 6>, int> g_split;
+static std::map<std::array<long, 6>, std::array<int, 2>> g_split;   // {nsplit, tile width}
 thread_local int tc_split_force = 0;
+thread_local int tc_tile_force = 0;
 int tc_split_lookup(bool ta, bool tb, int M, int N, int K, int gamma) {
   std::lock_guard<std::mutex> lk(g_split_mu);
   auto it = g_split.find({(long)ta, (long)tb, M, N, K, gamma});
-  return it == g_split.end() ? 0 : it->second;
+  return it == g_split.end() ? 0 : it->second[0];
 }
-void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit) {
+int tc_tile_lookup(bool ta, bool tb, int M, int N, int K, int gamma) {
   std::lock_guard<std::mutex> lk(g_split_mu);
-  g_split[{(long)ta, (long)tb, M, N, K, gamma}] = nsplit;
+  auto it = g_split.find({(long)ta, (long)tb, M, N, K, gamma});
+  return it == g_split.end() ? 0 : it->second[1];
+}
+void tc_split_store(bool ta, bool tb, int M, int N, int K, int gamma, int nsplit, int tile) {
+  std::lock_guard<std::mutex> lk(g_split_mu);
+  g_split[{(long)ta, (long)tb, M, N, K, gamma}] = {nsplit, tile};
+}
+// Tile widths the kernel is built for: K-major B takes any multiple of 16
+// (64, 80, 128 here), MN-major B multiples of 32 (64, 96, 128).
+bool tc_tile_valid(bool tb, int bn) {
+  return tb ? (bn == 64 || bn == 96 || bn == 128) : (bn == 64 || bn == 80 || bn == 128);
 }
 
 namespace tc {
@@ -657,11 +669,20 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
   }
   const bool a_mn = !ta, b_mn = tb;
   const int tm = (M + BM - 1) / BM, nkb = (K + BK - 1) / BK;
-  // 80-wide tiles for K-major B, 96-wide (three 32-column chunks) for MN-major B
-  const int bn = b_mn ? 96 : 80;
-  const int tn = (N + bn - 1) / bn;
   CUtensorMap ma, mb;
   const bool atm = tc::atmem_enabled();
+  // tile width: 80 for K-major B, 96 (three 32-column chunks) for MN-major
+  // B, unless the autotuner measured another for this shape (A in tensor
+  // memory only)
+  int bn = b_mn ? 96 : 80;
+  {
+    // QX_TC_TILE forces a width for every shape where it is valid (tests)
+    const char *env = getenv("QX_TC_TILE");
+    const int want = tc_tile_force > 0 ? tc_tile_force
+                                       : (env && atoi(env) > 0 ? atoi(env) : tc_tile_lookup(ta, tb, M, N, K, gamma));
+    if (atm && want > 0 && tc_tile_valid(tb, want)) bn = want;
+  }
+  const int tn = (N + bn - 1) / bn;
   if (!(a_mn ? tc::make_map(&ma, A, M, K, lda, 32, atm ? 0 : 2) : tc::make_map(&ma, A, K, M, lda, BM, 1))) return -1;
   if (!(b_mn ? tc::make_map(&mb, B, N, K, ldb, 32, 2) : tc::make_map(&mb, B, K, N, ldb, bn, 1))) return -1;
   // split K until the grid covers the SMs, at least 8 k-blocks a split, or
@@ -683,12 +704,24 @@ int tc_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float *A, 
                rowscale};
   dim3 g(tm, tn, nsplit);
   int rc;
-  if (bn == 96) {
-    if (a_mn) rc = tc::launch_tc<true, true, 96>(atm, ma, mb, a, g, st);
-    else rc = tc::launch_tc<false, true, 96>(atm, ma, mb, a, g, st);
+  if (b_mn) {
+    switch (bn) {
+      case 64: rc = a_mn ? tc::launch_tc<true, true, 64, true>(ma, mb, a, g, st)
+                         : tc::launch_tc<false, true, 64, true>(ma, mb, a, g, st); break;
+      case 128: rc = a_mn ? tc::launch_tc<true, true, 128, true>(ma, mb, a, g, st)
+                          : tc::launch_tc<false, true, 128, true>(ma, mb, a, g, st); break;
+      default: rc = a_mn ? tc::launch_tc<true, true, 96>(atm, ma, mb, a, g, st)
+                         : tc::launch_tc<false, true, 96>(atm, ma, mb, a, g, st);
+    }
   } else {
-    if (a_mn) rc = tc::launch_tc<true, false, 80>(atm, ma, mb, a, g, st);
-    else rc = tc::launch_tc<false, false, 80>(atm, ma, mb, a, g, st);
+    switch (bn) {
+      case 64: rc = a_mn ? tc::launch_tc<true, false, 64, true>(ma, mb, a, g, st)
+                         : tc::launch_tc<false, false, 64, true>(ma, mb, a, g, st); break;
+      case 128: rc = a_mn ? tc::launch_tc<true, false, 128, true>(ma, mb, a, g, st)
+                          : tc::launch_tc<false, false, 128, true>(ma, mb, a, g, st); break;
+      default: rc = a_mn ? tc::launch_tc<true, false, 80>(atm, ma, mb, a, g, st)
+                         : tc::launch_tc<false, false, 80>(atm, ma, mb, a, g, st);
+    }
   }
   if (rc) return rc;
   if (nsplit > 1)

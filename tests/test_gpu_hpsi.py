@@ -121,3 +121,55 @@ def test_plane_pass_lengths(monkeypatch, ecutdens, n):
         out[mode] = ctx.get_hpsi()
         assert relerr(out[mode], ref) < TOL[QX_PREC_MIXED]
     assert relerr(out["1"], out["0"]) < TOL[QX_PREC_MIXED]
+
+
+@pytest.mark.parametrize("plan", ["2x3x4", "3x8", "4x6", "6x4", "8x3", "2x2x2x3", "3x2x2x2"])
+def test_fft_radix_plans(si8, si8_psi, monkeypatch, plan):
+    """Every stage kernel on a forced radix plan of the 24-point axes
+    (QX_FFT_PLAN, the plans the autotuner chooses among): FP64 H|psi> and the
+    FP64 full-grid transforms of the density against the oracle, and the
+    mixed path's H|psi>."""
+    need_gpu()
+    monkeypatch.setenv("QX_FFT_PLAN", plan)
+    ref = oracle.Ham(si8, QX_NL_GSPACE).hpsi(si8_psi)
+    for prec in (QX_PREC_FP64, QX_PREC_MIXED):
+        ctx = Context(si8, prec, QX_NL_GSPACE)
+        ctx.put_psi(si8_psi)
+        ctx.enonloc()
+        assert relerr(ctx.get_hpsi(), ref) < TOL[prec]
+        ctx.close()
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(si8.gs.kfft0)
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_GSPACE)
+    fx, fy = ctx.rfft3_host(1, x, np.zeros_like(x))
+    k1, k2, k3 = si8.gs.grid
+    z = np.fft.fftn(x.reshape(k3, k2, k1)).ravel() / x.size
+    assert relerr(fx + 1j * fy, z) < 1e-13
+    ctx.close()
+
+
+@pytest.mark.parametrize("tile", ["64", "128"])
+def test_tensor_core_tile_widths(monkeypatch, tile):
+    """The contractions on the other tile widths the autotuner may pick
+    (QX_TC_TILE forces one wherever it is valid): Si64 H|psi> with the G-space
+    KB contractions, H_sub and Gram-Schmidt, mixed against FP64."""
+    need_gpu()
+    s = cell.si64(with_ewald=False)
+    c = cell.random_wavefunctions(s.gs.nplwex, s.nband)
+    c, _, rc = oracle.schmidt(c)
+    assert rc == 0
+    out = {}
+    for prec in (QX_PREC_FP64, QX_PREC_MIXED):
+        if prec == QX_PREC_MIXED:
+            monkeypatch.setenv("QX_TC_TILE", tile)
+        ctx = Context(s, prec, QX_NL_GSPACE)
+        ctx.put_psi(c)
+        ctx.enonloc()
+        hc = ctx.get_hpsi()
+        hs = ctx.hmatrix()
+        q = ctx.schmidt_host(c + 0.01 * np.roll(c, 1, axis=0))
+        out[prec] = (hc, hs, q)
+        ctx.close()
+    monkeypatch.delenv("QX_TC_TILE")
+    for a, b in zip(out[QX_PREC_MIXED], out[QX_PREC_FP64]):
+        assert relerr(a, b) < 5e-5

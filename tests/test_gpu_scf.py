@@ -121,3 +121,33 @@ def test_autotune_then_refine_to_fp64(si8, si8_psi):
     fine.refine_from(mixed)
     efine = [fine.scf_iteration(p)["etot"] for _ in range(3)][-1]
     assert abs(efine - e64) / si8.cell.natom < 2e-9        # Ry/atom, FP64 level
+
+
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_autotune_plans_keep_results(si8, si8_psi, prec):
+    """qx_autotune picks an FFT radix plan per grid length (and, mixed, a
+    tile width and K split per contraction shape); afterwards H|psi> still
+    matches the oracle and SCF iterations match an untuned context's."""
+    need_gpu()
+    p = CgParm.defaults(16)
+    res = []
+    for tune in (False, True):
+        ctx = Context(si8, prec, QX_NL_GSPACE)
+        ctx.put_psi(si8_psi)
+        ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)
+        ctx.scf_mixing(10, 20.0)
+        if tune:
+            report = ctx.autotune()
+            assert "FFT length 24" in report
+            if prec == QX_PREC_MIXED:
+                assert "tile" in report
+        ctx.put_psi(si8_psi)
+        ctx.enonloc()
+        ref = oracle.Ham(si8, QX_NL_GSPACE).hpsi(si8_psi)
+        tol = 1e-11 if prec == QX_PREC_FP64 else 2e-5
+        assert np.max(np.abs(ctx.get_hpsi() - ref)) / np.max(np.abs(ref)) < tol
+        ctx.scf_rho_from_psi()
+        res.append([ctx.scf_iteration(p)["etot"] for _ in range(4)])
+        ctx.close()
+    tol = 1e-9 if prec == QX_PREC_FP64 else 1e-4
+    np.testing.assert_allclose(res[1], res[0], rtol=tol)
