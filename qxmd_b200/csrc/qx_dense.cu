@@ -776,7 +776,7 @@ static bool cholinv_grid(double *S, int n, double *work, int *d_info, cudaStream
   const int nq = (n + G - 1) / G;
   const size_t sm = sizeof(double) * ((size_t)nq * n + (size_t)n);
   if (sm > 200 * 1024) return false;
-  static size_t sm_set = 48 * 1024;   // per process: only ever raised
+  static size_t sm_set = 0;   // per process: set at the first call, then only ever raised
   if (sm > sm_set) {
     if (cudaFuncSetAttribute(k_cholinv_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
       return false;
@@ -825,7 +825,10 @@ int cholinv(double *S, int n, double *work, int *d_info, cudaStream_t st) {
   const size_t pbytes = sizeof(double) * ((size_t)(n | 1) * n + 2 * (size_t)n + (size_t)PB * n);
   const size_t rbytes = sizeof(double) * (size_t)(n | 1) * n;
   if (n <= 160 && cholinv_registers_enabled()) {
-    static size_t rset = 48 * 1024;   // per process: only ever raised
+    // per process, only ever raised; the first call always sets it (the
+    // kernels' static shared buffers count against the 48 KB default, so a
+    // dynamic size below 48 KB can still need the opt-in)
+    static size_t rset = 0;
     if (rbytes > rset) {
       // exactly what this size needs: with the kernels' static buffers the
       // opt-in ceiling is below the 227 KB of a CTA
@@ -1797,7 +1800,7 @@ static bool sytrd_grid(double *A, int n, double *d, double *e, double *HV, doubl
   const int nq = (n + G - 1) / G;
   const size_t sm = sizeof(double) * ((size_t)nq * n + 2 * (size_t)n);
   if (sm > 200 * 1024 || 3L * n + G + 2 + 1 > 7L * n) return false;
-  static size_t sm_set = 48 * 1024;   // per process: only ever raised
+  static size_t sm_set = 0;   // per process: set at the first call, then only ever raised
   if (sm > sm_set) {
     if (cudaFuncSetAttribute(k_sytrd_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
       return false;
@@ -1886,7 +1889,7 @@ int syev(double *A, int n, double *w, double *V, double *work, int *d_info, cuda
   }
   // one warp per eigenvalue, one warp per block: spread over the SMs
   const size_t bsm = sizeof(double) * 2 * (size_t)n;
-  static size_t bsm_set = 48 * 1024;   // per process: only ever raised (contexts of several sizes coexist)
+  static size_t bsm_set = 0;   // per process: set at the first call, then only ever raised (contexts of several sizes coexist)
   if (bsm > bsm_set) {
     cudaFuncSetAttribute(k_bisect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm);
     bsm_set = bsm;

@@ -43,3 +43,26 @@ def test_concurrent_cells_match_sequential():
             conc[k].append(ctx.scf_result()["etot"])
     for a, b in zip(seq, conc):
         assert a == b
+
+
+def test_small_cell_first_in_a_fresh_process():
+    """A batch cell's Gram-Schmidt and SCF iteration as the first dense calls
+    of a process (the shared-memory opt-in of the register Cholesky must not
+    depend on a larger cell having run before)."""
+    need_gpu()
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from qxmd_b200 import cell\n"
+            "from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_MIXED\n"
+            "s = cell.batch_cell(0)\n"
+            "ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE)\n"
+            "ctx.put_psi(cell.random_wavefunctions(s.gs.nplwex, s.nband))\n"
+            "ctx.schmidt()\n"
+            "ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)\n"
+            "ctx.scf_rho_from_psi()\n"
+            "print(ctx.scf_iteration(CgParm.defaults(int(s.cell.nel // 2)))['etot'])\n") % root
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
