@@ -47,9 +47,9 @@ HPSI_PASS_DRAM_BYTES = 69812480
 # kernels): its DRAM traffic is a fraction of the algorithmic bytes because
 # the z-transformed planes stay in L2, so it is not HBM-bound; it is bound by
 # latency at low occupancy.
-PIPELINE_LIMITER = ("latency, not HBM: DRAM traffic is 0.17x the algorithmic bytes (planes stay in the 126 MB L2); "
-                    "plane pass k_plane at 18.75% warp occupancy, 34.8% issue active, stalls led by barrier "
-                    "and long scoreboard")
+PIPELINE_LIMITER = ("latency, not HBM: DRAM traffic is 0.17x the algorithmic bytes (the pruned transforms keep "
+                    "only the z-transformed planes); plane pass k_plane at 18.6% achieved occupancy (128 "
+                    "registers), 34.9% issue active, FMA pipe 27%, stalls led by barrier, wait and long scoreboard")
 # FP64 SCF iterations of the refinement sweep after the mixed solution converged
 REFINE_ITERS = 3
 # iteration caps of the Si512 run to self-consistency and of its FP64 sweep
