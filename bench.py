@@ -657,7 +657,7 @@ def run_ours(args):
 
     from qxmd_b200 import cell
     from qxmd_b200.lib import (CgParm, Context, QX_HPSI_KINETIC, QX_NL_GSPACE, QX_PREC_FP64,
-                               QX_PREC_MIXED, launch_count)
+                               QX_PREC_MIXED, gemm_fallbacks, launch_count)
     ws, rank, local = dist_setup(args)
     sys_ = cell.si64()
     psi0 = cell.random_wavefunctions(sys_.gs.nplwex, sys_.nband)
@@ -686,7 +686,7 @@ def run_ours(args):
         barrier(ws)
         if name == "mixed":
             clocks.start()
-        n0 = launch_count()
+        n0, f0 = launch_count(), gemm_fallbacks()
         tot_ms, outs = 0.0, []
         for _ in range(K):
             flush.zero_()
@@ -697,11 +697,13 @@ def run_ours(args):
             torch.cuda.synchronize()
             tot_ms += e0.elapsed_time(e1)
         launches = launch_count() - n0
+        fallbacks = gemm_fallbacks() - f0
         if name == "mixed":
             clk = clocks.stop()
         barrier(ws)
         tmax = max_over_ranks(tot_ms, ws)
         r = {"ms_per_step": tmax / K, "value": ws * K / (tmax / 1e3), "launches": launches,
+             "fp32_gemm_fallbacks_per_step": fallbacks / K,
              "etot_last": outs[-1]["etot"], "cg_bapps_per_iter": float(np.mean([o["ncg_hpsi"] for o in outs])),
              "eig_clusters": float(np.mean([o["eig_clusters"] for o in outs]))}
         r["iters_done"] = W + K
@@ -837,6 +839,7 @@ def run_ours(args):
         "eig_clusters": mixed["eig_clusters"],
         "e2e": mixed["e2e"],
         "gpu_launches": mixed["launches"],
+        "fp32_gemm_fallbacks_per_step": mixed["fp32_gemm_fallbacks_per_step"],
         "roofline": {"kernel": "H|psi> FFT pipeline (z inverse, plane pass, z forward), FP32",
                      "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,

@@ -73,6 +73,10 @@ const char *qx_last_error(void);
 int qx_version(void);
 /* Number of kernels this library has launched in the process (all contexts). */
 long qx_launch_count(void);
+/* FP32 band contractions in the process that ran on the CUDA-core GEMM
+ * instead of the tensor cores (a column map or device column count, or
+ * operands outside the TMA rules that could not be restaged). */
+long qx_gemm_fallbacks(void);
 
 /* ---- set-up (module state of the reference, uploaded once per geometry) -- */
 

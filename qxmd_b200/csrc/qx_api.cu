@@ -166,6 +166,7 @@ struct qx_ctx {
     cudaGraphExec_t exec = nullptr;
     void *psi = nullptr, *hpsi = nullptr, *tmp = nullptr;   // pointer arrangement after the iteration
     long launches = 0;
+    long fallbacks = 0;   // FP32 contractions on the CUDA-core GEMM per replay
   };
   std::vector<ScfGraph> scf_graphs;
   std::vector<void *> allocs;
@@ -1817,10 +1818,11 @@ static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
     CK(cudaStreamBeginCapture(c->cap_st, cudaStreamCaptureModeThreadLocal));
     cudaStream_t user = c->st;
     c->st = c->cap_st;
-    const long l0 = g_launches.load();
+    const long l0 = g_launches.load(), f0 = fp32_gemm_fallbacks();
     const int r = scf_body<T>(c, p);
-    const long nl = g_launches.load() - l0;
+    const long nl = g_launches.load() - l0, nf = fp32_gemm_fallbacks() - f0;
     g_launches.fetch_sub(nl);
+    fp32_gemm_fallbacks_add(-nf);
     c->st = user;
     cudaGraph_t graph = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(c->cap_st, &graph);
@@ -1834,6 +1836,7 @@ static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
     e.key = key;
     e.psi = c->psi; e.hpsi = c->hpsi; e.tmp = c->tmp;
     e.launches = nl;
+    e.fallbacks = nf;
     const cudaError_t ei = cudaGraphInstantiate(&e.exec, graph, 0);
     cudaGraphDestroy(graph);
     c->psi = psi0; c->hpsi = hpsi0; c->tmp = tmp0;
@@ -1847,6 +1850,7 @@ static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
   }
   CK(cudaGraphLaunch(g->exec, c->st));
   g_launches.fetch_add(g->launches);
+  fp32_gemm_fallbacks_add(g->fallbacks);
   c->psi = g->psi; c->hpsi = g->hpsi; c->tmp = g->tmp;
   c->pulay_reset = false;
   c->have_glocal = true;

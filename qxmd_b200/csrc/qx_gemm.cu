@@ -5,6 +5,7 @@
 // (schmidt.f90:284-313).  The Gamma-point half-sphere metric
 // 2*sum - x(1)*y(1) is applied in the epilogue.
 #include <algorithm>
+#include <atomic>
 
 #include "qx_internal.h"
 #include "qx_cg.h"
@@ -195,11 +196,19 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
 // runs on the CUDA-core kernel above.  Split K when the output has too few
 // tiles to fill the GPU and the caller provides a workspace of at least
 // nsplit*M*N elements.
+// FP32 contractions that ran on the CUDA-core kernel instead of the tensor
+// cores (a column map, a device column count or operands outside the TMA
+// rules), counted for qx_gemm_fallbacks().
+static std::atomic<long> g_fp32_fallbacks{0};
+long fp32_gemm_fallbacks() { return g_fp32_fallbacks.load(); }
+void fp32_gemm_fallbacks_add(long n) { g_fp32_fallbacks.fetch_add(n); }
+
 template <typename T>
 int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, const T *B, long ldb, T beta, T *C,
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes,
          const T *rowscale, void *pad, size_t pad_bytes) {
   if (M <= 0 || N <= 0) return 0;
+  if (sizeof(T) == sizeof(float) && K > 0 && (colmap || ncol_dev || !tc_enabled())) ++g_fp32_fallbacks;
   if (rowscale && beta != (T)0) { set_error("gemm: a row scale needs beta = 0"); return 1; }
   if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0) {
     const int r = tc_gemm(ta, tb, M, N, K, (float)alpha, (const float *)A, lda, (const float *)B, ldb, (float)beta,
@@ -209,6 +218,7 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
       set_error("tensor-core GEMM launch failed: %s", cudaGetErrorString(cudaGetLastError()));
       return 2;
     }
+    if (tc_enabled()) ++g_fp32_fallbacks;   // operands outside the TMA rules
   }
   dim3 g((M + BM - 1) / BM, (N + BN - 1) / BN);
   const long tiles = (long)g.x * g.y;
@@ -291,6 +301,8 @@ int scratch_address(double **out) {
   return QX_OK;
 }
 }  // namespace
+
+extern "C" long qx_gemm_fallbacks(void) { return qx::fp32_gemm_fallbacks(); }
 
 extern "C" int qx_hmatrix_static(const double *c, const double *hc, int nplwex, int nb, double *hsub, void *stream) {
   if (!c || !hc || !hsub || nplwex <= 0 || nb <= 0) {

@@ -150,6 +150,9 @@ bool tc_enabled();
 void pad_rows_f32(const float *src, long ld, long inner, long rows, float *dst, long ldp, cudaStream_t st);
 // Error code left by a tensor-core GEMM whose bounded wait ran out (0: none); clears it.
 int tc_error_take();
+// FP32 contractions that ran on the CUDA-core kernel (qx_gemm.cu)
+long fp32_gemm_fallbacks();
+void fp32_gemm_fallbacks_add(long n);   // graph capture and replay accounting
 // autotuner hooks of the tensor-core GEMM: a per-shape K-split table and a
 // per-thread override used while timing candidates
 extern thread_local int tc_split_force, tc_tile_force;

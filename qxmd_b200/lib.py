@@ -35,7 +35,7 @@ EXPORTS = [
     "qxgpu_kbnlpp_frc2",
     "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
-    "qx_fssh_init", "qx_fssh_step", "qx_fssh_state", "qx_build_vloc",
+    "qx_fssh_init", "qx_fssh_step", "qx_fssh_state", "qx_build_vloc", "qx_gemm_fallbacks",
 ]
 
 
@@ -158,6 +158,7 @@ def lib(build_if_missing: bool = True):
         "qxgpu_rfft3": ([_ctx, C.c_int, _dp, _dp], C.c_int),
         "qx_fssh_init": ([_ctx, C.POINTER(FsshParm), _dp], C.c_int),
         "qx_build_vloc": ([_ctx], C.c_int),
+        "qx_gemm_fallbacks": ([], C.c_long),
         "qx_fssh_step": ([_ctx, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "qx_fssh_state": ([_ctx, _vp, _vp, _vp, _vp], C.c_int),
     }
@@ -167,6 +168,11 @@ def lib(build_if_missing: bool = True):
         f.restype = res
     _lib = L
     return L
+
+
+def gemm_fallbacks() -> int:
+    """FP32 contractions so far that ran on the CUDA-core GEMM (qx_gemm_fallbacks)."""
+    return int(lib().qx_gemm_fallbacks())
 
 
 def launch_count() -> int:
