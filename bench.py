@@ -103,6 +103,45 @@ def peaks():
         return 6650.0, "fallback"
 
 
+# FP64 peak of a B200 at its maximum SM clock: 148 SMs x 64 FP64 FMA lanes a
+# clock x 2 flops (no FP64 figure is measured alongside the HBM and bf16 peaks)
+FP64_FLOPS_PER_CLOCK = 148 * 64 * 2
+SM_MAX_MHZ = 1965.0
+
+
+def band_matrix_timing(ctx, sys_, R, flush, sm_max_mhz=None):
+    """The band matrix <psi_j|H psi_i> of an FP64 context alone (qx_hmatrix
+    with no host copy: one FP64 GEMM of nband x nband x nplwex, split over K,
+    the reduction of its partial sums and the symmetrisation), device-timed
+    over R calls with L2 flushed between them; throughput against the FP64
+    peak at the maximum SM clock."""
+    import torch
+    _hm(ctx)
+    t = 0.0
+    for _ in range(R):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _hm(ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        t += e0.elapsed_time(e1)
+    ms = t / R
+    nb, ne = sys_.nband, sys_.gs.nplwex
+    flops = 2.0 * nb * nb * ne
+    peak = FP64_FLOPS_PER_CLOCK * (sm_max_mhz or SM_MAX_MHZ) * 1e6 / 1e12
+    tf = flops / (ms * 1e-3) / 1e12
+    return {"kernels": "k_dgemm (FP64 DMMA tensor cores, split-K) + k_gemm_reduce + k_symmetrize", "shape_mnk": [nb, nb, ne],
+            "ms": ms, "tflops": tf, "peak_tflops": peak, "frac": tf / peak,
+            "peak_kind": "nominal FP64 at max SM clock (148 SMs x 64 FMA/clock x 2)"}
+
+
+def _hm(ctx):
+    rc = ctx.L.qx_hmatrix(ctx.h, None)
+    if rc:
+        raise RuntimeError(f"qx_hmatrix failed ({rc})")
+
+
 class Clocks:
     """nvidia-smi sampler for the timed region."""
 
@@ -369,6 +408,8 @@ def run_si512(args):
             torch.cuda.synchronize()
             t += e0.elapsed_time(e1)
         out[name] = {"value": sys_.nband * R / (t / 1e3), "ms_per_pass": t / R}
+        if name == "fp64":
+            out[name]["band_matrix_gemm"] = band_matrix_timing(ctx, sys_, R, flush)
         ctx.close()
     out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     # whole SCF iterations of the mixed path from the random start (Pulay
@@ -736,6 +777,8 @@ def run_ours(args):
             torch.cuda.synchronize()
             t += e0.elapsed_time(e1)
         r["fft_pipeline_ms"] = t / R
+        if name == "fp64":
+            r["band_matrix"] = band_matrix_timing(ctx, sys_, R, flush)
         if name == "mixed":
             # end to end through the host-array API: H2D psi (pinned), one
             # iteration, D2H psi, rho, eigenvalues
@@ -824,7 +867,8 @@ def run_ours(args):
         "fp64": {"path": "plain FP64 drop-in, one-rank band order (sequential CG, one graph launch per sweep)",
                  "value": fp64["value"], "ms_per_step": fp64["ms_per_step"],
                  "hpsi_band_apps_per_s": fp64["hpsi_band_apps_per_s"],
-                 "cg_bapps_per_iter": fp64["cg_bapps_per_iter"], "gpu_launches": fp64["launches"]},
+                 "cg_bapps_per_iter": fp64["cg_bapps_per_iter"], "gpu_launches": fp64["launches"],
+                 "band_matrix_gemm": fp64["band_matrix"]},
         "fp64_batched": {"path": "FP64, all bands at once (one band per rank order)",
                          "value": fp64b["value"], "ms_per_step": fp64b["ms_per_step"],
                          "cg_bapps_per_iter": fp64b["cg_bapps_per_iter"]},

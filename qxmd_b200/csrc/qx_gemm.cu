@@ -1,4 +1,5 @@
-// Tiled CUDA-core GEMM for the band and projector contractions:
+// GEMMs of the band and projector contractions (CUDA-core kernel for FP32
+// with a column map, FP64 tensor-core kernel for FP64):
 // S = C^T C (schmidt.f90:190-237), H_sub = C^T HC (engrad.f90:869-895),
 // <beta|psi> and its back-application (nlkbpp.f90:1678-1713), subgs3
 // (engrad.f90:1122-1142), C*U (eigen.f90:1482-1510) and C*L^-T
@@ -191,11 +192,302 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
   note_launch();
 }
 
-// FP32 without a column map goes to the tensor-core kernel (qx_tcgemm.cu)
-// when the operands meet its TMA rules; everything else, and all FP64 work,
-// runs on the CUDA-core kernel above.  Split K when the output has too few
-// tiles to fill the GPU and the caller provides a workspace of at least
-// nsplit*M*N elements.
+// Dispatch (gemm<T> below): FP32 without a column map goes to the tensor-core
+// kernel (qx_tcgemm.cu) when the operands meet its TMA rules; all FP64 work
+// goes to the DMMA kernel k_dgemm; the rest (FP32 with a column map or
+// operands outside the TMA rules) runs on the CUDA-core kernel above.  Split
+// K when the output has too few tiles to fill the GPU and the caller
+// provides a workspace of at least nsplit*M*N elements.
+// ---------------------------------------------------------------------------
+// FP64 contractions on the FP64 tensor cores: mma.sync m8n8k4 (DMMA, 256
+// FMAs a warp instruction; the FP64 FMA pipe of a B200 measures about 10 %
+// below it, and DFMA kernels are bound by instruction issue long before).
+// A CTA owns a TM x TM output tile, warps arranged WGM x WGN, each warp a
+// (TM / WGM) x (TM / WGN) block of 8 x 8 DMMA fragments.  k-blocks of DKB
+// are staged in shared memory by cp.async, DST deep (DST - 1 blocks in
+// flight while one is multiplied; one barrier a k-block).  Each operand
+// keeps its global layout in shared memory:
+//   k-contiguous (A transposed, B not): [row][DKB + 2]; a lane reads the
+//     double2 at k-pair q (its index in its quad) of row g (its quad), one
+//     16-byte load serving two DMMAs; the odd pitch in 16-byte units puts
+//     the 32 lanes' loads in the fewest shared-memory wavefronts;
+//   row-contiguous (A not transposed, B transposed): [k][TM + 2]; a lane
+//     reads k = 2q + h of row g, two scalar loads.
+// DMMA k-index q of both operands holds k = 2q + h in the h-th DMMA of a
+// k-pair, so the products pair up and the sum runs over all k.  TM = 128
+// (8 warps of 64 x 32) for large outputs, TM = 64 (4 warps of 32 x 32, more
+// CTAs an SM) where 128-wide tiles would mostly be padding, e.g. the
+// 160 x 160 band matrices.  colmap / ncol_dev as in k_gemm (output column n
+// is stored column colmap[n] of B and C; columns from *ncol_dev on are not
+// computed).  Split-K partials W[z][n][m] as k_gemm's.
+constexpr int DKB = 16, DST = 3;
+
+__device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc, bool live) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(live ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// doubles of one operand's k-block in shared memory
+template <int TM, bool KMAJ>
+constexpr int dop_size() {
+  return KMAJ ? TM * (DKB + 2) : DKB * (TM + 2);
+}
+template <int TM, bool TA, bool TB>
+constexpr size_t dgemm_smem() {
+  return sizeof(double) * DST * (size_t)(dop_size<TM, TA>() + dop_size<TM, !TB>());
+}
+
+template <int TM, int WGM, int WGN, bool TA, bool TB, bool SPLIT>
+__global__ void __launch_bounds__(32 * WGM *WGN) k_dgemm(int M, int N, int K, double alpha,
+                                                          const double *__restrict__ A, long lda,
+                                                          const double *__restrict__ B, long ldb, double beta,
+                                                          double *__restrict__ Cm, long ldc, int gamma,
+                                                          const int *__restrict__ colmap,
+                                                          const int *__restrict__ ncol_dev, int kchunk,
+                                                          double *__restrict__ W) {
+  constexpr int NT = 32 * WGM * WGN, MF = TM / WGM / 8, NF = TM / WGN / 8;
+  constexpr int KP = DKB + 2, MP = TM + 2, L = TM * DKB / NT;   // L: elements a thread stages per operand
+  constexpr int SA = dop_size<TM, TA>(), SST = SA + dop_size<TM, !TB>();
+  extern __shared__ __align__(16) double dsm[];
+  const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TM;
+  if (n0 >= Nact) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp % WGM, wn = warp / WGM, g = lane >> 2, q = lane & 3;
+  const int kb = SPLIT ? blockIdx.z * kchunk : 0;
+  const int ke = SPLIT ? min(K, kb + kchunk) : K;
+  const int nk = (ke - kb + DKB - 1) / DKB;
+  // the rows a thread stages are the same in every k-block: source row
+  // offsets once (B through the column map), then only k moves
+  long aoff[L], boff[L];
+  unsigned alive = 0, blive = 0;
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    const int e = tid + NT * i;
+    const int ra = TA ? e / DKB : e % TM, rb = TB ? e % TM : e / DKB;
+    const int gm = m0 + ra, gn = n0 + rb;
+    if (gm < M) alive |= 1u << i;
+    if (gn < Nact) blive |= 1u << i;
+    aoff[i] = gm < M ? (TA ? (long)gm * lda : (long)gm) : 0;
+    const long cn = gn < Nact ? (colmap ? (long)colmap[gn] : (long)gn) : 0;
+    boff[i] = TB ? cn : cn * ldb;
+  }
+  auto stage = [&](int blk) {
+    double *S = dsm + (blk % DST) * SST;
+    const int k0 = kb + blk * DKB;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const int e = tid + NT * i;
+      {
+        const int r = TA ? e / DKB : e % TM, k = TA ? e % DKB : e / TM;
+        const bool live = ((alive >> i) & 1) && k0 + k < ke;
+        const double *src = live ? (TA ? A + aoff[i] + k0 + k : A + aoff[i] + (long)(k0 + k) * lda) : A;
+        cp_async8(TA ? S + r * KP + k : S + k * MP + r, src, live);
+      }
+      {
+        const int r = TB ? e % TM : e / DKB, k = TB ? e / TM : e % DKB;
+        const bool live = ((blive >> i) & 1) && k0 + k < ke;
+        const double *src = live ? (TB ? B + boff[i] + (long)(k0 + k) * ldb : B + boff[i] + k0 + k) : B;
+        cp_async8(TB ? S + SA + k * MP + r : S + SA + r * KP + k, src, live);
+      }
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < DST - 1; ++s) {
+    if (s < nk) stage(s);
+    cp_async_commit();
+  }
+  double acc[MF][NF][2];
+#pragma unroll
+  for (int i = 0; i < MF; ++i)
+#pragma unroll
+    for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  for (int it = 0; it < nk; ++it) {
+    cp_async_wait<DST - 2>();   // this thread's copies of block it are in
+    __syncthreads();            // everyone's are, and block it - 1 is consumed
+    if (it + DST - 1 < nk) stage(it + DST - 1);
+    cp_async_commit();
+    const double *As = dsm + (it % DST) * SST, *Bs = As + SA;
+#pragma unroll
+    for (int kp = 0; kp < DKB; kp += 8) {
+      double a[MF][2], b[NF][2];
+#pragma unroll
+      for (int f = 0; f < MF; ++f) {
+        const int row = wm * (TM / WGM) + 8 * f + g;
+        if (TA) {
+          const double2 v = *reinterpret_cast<const double2 *>(As + row * KP + kp + 2 * q);
+          a[f][0] = v.x;
+          a[f][1] = v.y;
+        } else {
+          a[f][0] = As[(kp + 2 * q) * MP + row];
+          a[f][1] = As[(kp + 2 * q + 1) * MP + row];
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const int col = wn * (TM / WGN) + 8 * f + g;
+        if (!TB) {
+          const double2 v = *reinterpret_cast<const double2 *>(Bs + col * KP + kp + 2 * q);
+          b[f][0] = v.x;
+          b[f][1] = v.y;
+        } else {
+          b[f][0] = Bs[(kp + 2 * q) * MP + col];
+          b[f][1] = Bs[(kp + 2 * q + 1) * MP + col];
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int i = 0; i < MF; ++i)
+#pragma unroll
+          for (int j = 0; j < NF; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i][h], b[j][h]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int i = 0; i < MF; ++i) {
+    const int gm = m0 + wm * (TM / WGM) + 8 * i + g;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int gn = n0 + wn * (TM / WGN) + 8 * j + 2 * q + c;
+        if (gn >= Nact) continue;
+        if (SPLIT) {
+          W[((long)blockIdx.z * N + gn) * M + gm] = acc[i][j][c];
+          continue;
+        }
+        const long cn = colmap ? colmap[gn] : gn;
+        double v = acc[i][j][c];
+        if (gamma) {
+          const double a0 = TA ? A[(long)gm * lda] : A[gm];
+          const double b0 = TB ? B[cn] : B[cn * ldb];
+          v = 2.0 * v - a0 * b0;
+          if (gamma == 2) {
+            const double a1 = TA ? A[(long)gm * lda + 1] : A[lda + gm];
+            const double b1 = TB ? B[ldb + cn] : B[cn * ldb + 1];
+            v -= 2.0 * a1 * b1;
+          }
+        }
+        double *c_ = Cm + cn * ldc + gm;
+        *c_ = (beta == 0.0) ? alpha * v : alpha * v + beta * *c_;
+      }
+  }
+}
+
+// QX_DGEMM=0 keeps every FP64 contraction on k_gemm (read at every call).
+static bool dgemm_enabled() {
+  const char *e = getenv("QX_DGEMM");
+  return !(e && e[0] == '0');
+}
+
+// Dynamic shared-memory opt-in of one k_dgemm shape and its resident CTAs an
+// SM, once per device.
+template <int TM, int WGM, int WGN, bool TA, bool TB>
+static int dgemm_prepare() {
+  static std::atomic<int> per_sm[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    set_error("k_dgemm: no current device");
+    return 0;
+  }
+  const int known = per_sm[dev].load();
+  if (known > 0) return known;
+  constexpr int smem = (int)dgemm_smem<TM, TA, TB>();
+  const cudaError_t e1 =
+      cudaFuncSetAttribute(k_dgemm<TM, WGM, WGN, TA, TB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const cudaError_t e2 =
+      cudaFuncSetAttribute(k_dgemm<TM, WGM, WGN, TA, TB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  int n = 0;
+  const cudaError_t e3 =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dgemm<TM, WGM, WGN, TA, TB, true>, 32 * WGM * WGN, smem);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || n < 1) {
+    set_error("k_dgemm: shared-memory opt-in of %d bytes failed: %s", smem,
+              cudaGetErrorString(e1 ? e1 : e2 ? e2 : e3));
+    return 0;
+  }
+  per_sm[dev].store(n);
+  return n;
+}
+
+template <int TM, int WGM, int WGN, bool TA, bool TB>
+static int launch_dgemm_tm(int M, int N, int K, double alpha, const double *A, long lda, const double *B, long ldb,
+                           double beta, double *C, long ldc, int gamma, const int *colmap, const int *ncol_dev,
+                           void *ws, size_t ws_bytes, cudaStream_t st) {
+  constexpr int NT = 32 * WGM * WGN;
+  const int per_sm = dgemm_prepare<TM, WGM, WGN, TA, TB>();
+  if (per_sm < 1) return 2;
+  dim3 g((M + TM - 1) / TM, (N + TM - 1) / TM);
+  const long tiles = (long)g.x * g.y, slots = 148L * per_sm;
+  // The fewest K-splits (each at least 64 deep, all partials in the
+  // workspace, at most four waves) whose CTAs fill 90 % of the waves they
+  // take, else the best-filling count.
+  auto fill = [&](long ctas) { return (double)ctas / (double)(((ctas + slots - 1) / slots) * slots); };
+  int nsplit = 1, kchunk = K;
+  if (ws && K >= 128 && fill(tiles) < 0.9) {
+    long cap = std::min<long>((4 * slots + tiles - 1) / tiles, (K + 63) / 64);
+    cap = std::min<long>(cap, (long)(ws_bytes / ((size_t)M * N * sizeof(double))));
+    double best = fill(tiles);
+    for (int n = 2; n <= cap; ++n) {
+      const int kc = ((K + n - 1) / n + DKB - 1) / DKB * DKB, ns = (K + kc - 1) / kc;
+      const double f = fill(tiles * ns);
+      if (f > best + 1e-9) {
+        best = f;
+        nsplit = ns;
+        kchunk = kc;
+      }
+      if (f >= 0.9) break;
+    }
+  }
+  constexpr size_t smem = dgemm_smem<TM, TA, TB>();
+  if (nsplit <= 1) {
+    k_dgemm<TM, WGM, WGN, TA, TB, false><<<g, NT, smem, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma,
+                                                              colmap, ncol_dev, K, nullptr);
+    note_launch();
+    return 0;
+  }
+  g.z = nsplit;
+  k_dgemm<TM, WGM, WGN, TA, TB, true><<<g, NT, smem, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma,
+                                                           colmap, ncol_dev, kchunk, (double *)ws);
+  note_launch();
+  const long mn = (long)M * N;
+  k_gemm_reduce<double, TA, TB><<<(int)((mn + 31) / 32), RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C,
+                                                                       ldc, gamma, colmap, ncol_dev,
+                                                                       (const double *)ws, nullptr);
+  note_launch();
+  return 0;
+}
+
+// 128-wide tiles unless they would cover more than 15 % more padded area
+// than 64-wide ones.
+static int dgemm_tile(int M, int N) {
+  const long a128 = (long)((M + 127) / 128) * ((N + 127) / 128) * 128 * 128;
+  const long a64 = (long)((M + 63) / 64) * ((N + 63) / 64) * 64 * 64;
+  return a128 * 100 <= a64 * 115 ? 128 : 64;
+}
+
+template <bool TA, bool TB>
+static int launch_dgemm(int M, int N, int K, double alpha, const double *A, long lda, const double *B, long ldb,
+                        double beta, double *C, long ldc, int gamma, const int *colmap, const int *ncol_dev, void *ws,
+                        size_t ws_bytes, cudaStream_t st) {
+  if (dgemm_tile(M, N) == 128)
+    return launch_dgemm_tm<128, 2, 4, TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev,
+                                              ws, ws_bytes, st);
+  return launch_dgemm_tm<64, 2, 2, TA, TB>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, ws,
+                                           ws_bytes, st);
+}
+
 // FP32 contractions that ran on the CUDA-core kernel instead of the tensor
 // cores (a column map, a device column count or operands outside the TMA
 // rules), counted for qx_gemm_fallbacks().
@@ -219,6 +511,26 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
       return 2;
     }
     if (tc_enabled()) ++g_fp32_fallbacks;   // operands outside the TMA rules
+  }
+  if (sizeof(T) == sizeof(double) && K > 0 && dgemm_enabled()) {
+    const double *Ad = (const double *)A, *Bd = (const double *)B;
+    double *Cd = (double *)C;
+    int r;
+    if (ta && tb)
+      r = launch_dgemm<true, true>(M, N, K, alpha, Ad, lda, Bd, ldb, beta, Cd, ldc, gamma, colmap, ncol_dev, ws,
+                                   ws_bytes, st);
+    else if (ta)
+      r = launch_dgemm<true, false>(M, N, K, alpha, Ad, lda, Bd, ldb, beta, Cd, ldc, gamma, colmap, ncol_dev, ws,
+                                    ws_bytes, st);
+    else if (tb)
+      r = launch_dgemm<false, true>(M, N, K, alpha, Ad, lda, Bd, ldb, beta, Cd, ldc, gamma, colmap, ncol_dev, ws,
+                                    ws_bytes, st);
+    else
+      r = launch_dgemm<false, false>(M, N, K, alpha, Ad, lda, Bd, ldb, beta, Cd, ldc, gamma, colmap, ncol_dev, ws,
+                                     ws_bytes, st);
+    if (r) return r;
+    if (rowscale) scale_rows<T>(M, N, C, ldc, rowscale, colmap, ncol_dev, st);
+    return 0;
   }
   dim3 g((M + BM - 1) / BM, (N + BN - 1) / BN);
   const long tiles = (long)g.x * g.y;
