@@ -143,17 +143,53 @@ def _hm(ctx):
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and clock-event-reason sampler for the timed region: an NVML
+    thread every 5 ms (the timed regions here are tens of milliseconds), else
+    nvidia-smi every 200 ms.  Reads only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.sm, self.bits, self.stop_flag = [], 0, threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        self.bits |= int(get_reasons(h))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.005)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -162,6 +198,13 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            reasons = sorted(nm for nm, bit in self.REASONS.items() if self.bits & bit)
+            sm = self.sm
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.mx,
+                    "reasons": reasons, "samples": len(sm), "sampler": "nvml 5 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -185,7 +228,7 @@ class Clocks:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "sampler": "nvidia-smi 200 ms"}
 
 
 def dist_setup(args):

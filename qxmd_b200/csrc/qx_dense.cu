@@ -566,9 +566,21 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
   const int ld = n | 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int r0 = warp * NR;
-  for (long q = tid; q < (long)n * n; q += W * 32) {
-    const int j = (int)(q / n), i = (int)(q - (long)j * n);
-    stg[(long)j * ld + i] = Sg[q];
+  // global to shared by cp.async: every copy of a thread in flight at once,
+  // none through registers; element q = j n + i, stepped by the block size
+  // without a division
+  {
+    int j = tid / n, i = tid - j * n;
+    for (long q = tid; q < (long)n * n; q += W * 32) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(stg + (long)j * ld + i);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(Sg + q) : "memory");
+      i += W * 32;
+      while (i >= n) {
+        i -= n;
+        ++j;
+      }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
   __syncthreads();
   double a[NR][NC];
@@ -671,9 +683,16 @@ __global__ void __launch_bounds__(W * 32, 1) k_cholinv_rg(double *__restrict__ S
     }
   }
   __syncthreads();
-  for (long q = tid; q < (long)n * n; q += W * 32) {
-    const int j = (int)(q / n), i = (int)(q - (long)j * n);
-    Sg[q] = stg[(long)j * ld + i];
+  {
+    int j = tid / n, i = tid - j * n;
+    for (long q = tid; q < (long)n * n; q += W * 32) {
+      Sg[q] = stg[(long)j * ld + i];
+      i += W * 32;
+      while (i >= n) {
+        i -= n;
+        ++j;
+      }
+    }
   }
   if (tid == 0) *info = 0;
 }
