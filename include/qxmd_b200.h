@@ -136,6 +136,17 @@ int qx_set_kb_r(qx_ctx *ctx, int natom, int lmx, const int *off, const int *mesh
 int qx_set_kb_r_builder(qx_ctx *ctx, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
                         const double *tabnl, const double *dtabnl, const int *poly, const double *clalp, double rdelv,
                         const double *rba);
+/* Per-channel projector radii (rmxnlc(la, it) of setnlc nlkbppr.f90:1405-1431,
+ * which gives each angular channel la its own point list, numsnl(la, i) points
+ * of meshnl): rcl(4, ntype), rcl[l + 4 * it] the radius of the channel of
+ * projector l of species it, each in (0, rcut(it)]; the species radius given
+ * to qx_set_kb_r_builder must be the largest of its channels'.  The device
+ * keeps one list per atom, the points within rcut(it), and a projector is zero
+ * (value and gradient) beyond its own channel's radius, so that calnlc's
+ * per-channel sums and fnnlcl2's are reproduced exactly (the added terms are
+ * zeros).  Until this is called every channel has the species radius.  Takes
+ * effect at the next qx_build_kb_r. */
+int qx_set_kb_r_channel_radii(qx_ctx *ctx, const double *rcl);
 /* Once per geometry: the points of every atom (species ityp(natom), 0-based,
  * fractional coordinates satm(3, natom)) within its projector radius, their
  * projector values, and the x-line index of the real-space KB kernels.  The

@@ -100,7 +100,8 @@ def box_halfwidths(rba: np.ndarray, grid, rmax: float):
 
 def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
     """(off (natom+1), mesh (npts), vnl (npts, 4)) in box order; b is the dict
-    of qxmd_b200.cell.kbr_builder_tables.  With grad, also dvnl (npts, 4, 3):
+    of qxmd_b200.cell.kbr_builder_tables, with optional per-projector channel
+    radii b["rcut_l"] (4 * ntype, each at most the species radius b["rcut"]).  With grad, also dvnl (npts, 4, 3):
     the gradient of each projector value with respect to the displacement d
     of the point from its atom, as fnnlcl2 builds it from the radial table
     and its derivative table (nlkbppr.f90:2200-2240):
@@ -124,10 +125,17 @@ def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
         w = n % k
         meshes.append((w[:, 0] + k[0] * (w[:, 1] + k[1] * w[:, 2])).astype(np.int32))
         r = np.sqrt(r2[sel])
+        # projector l belongs to the channel of radius rcut_l[ch] (rmxnlc of
+        # nlkbppr.f90:1405-1431): zero at the points outside it, so that the
+        # sums over the species sphere equal the sums over each channel's list
+        rl2 = r2[sel]
+        inside = [rl2 <= (b["rcut_l"][l + 4 * it] ** 2 if b.get("rcut_l") is not None else np.inf)
+                  for l in range(4)]
         v = np.empty((r.size, 4))
         for l in range(4):
             ch = l + 4 * it
             v[:, l] = setqlm(r, b["dltnl"][it], b["tabnl"][ch], _poly(int(b["poly"][ch]), d[:, 0], d[:, 1], d[:, 2]))
+            v[:, l] = np.where(inside[l], v[:, l], 0.0)
         vals.append(v)
         if grad:
             gv = np.empty((r.size, 4, 3))
@@ -139,6 +147,7 @@ def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
                 dg = setqlm(r, b["dltnl"][it], b["dtabnl"][ch], one)
                 p = _poly(c, d[:, 0], d[:, 1], d[:, 2])
                 gv[:, l, :] = (dg * p)[:, None] * d + g[:, None] * _poly_grad(c, d[:, 0], d[:, 1], d[:, 2])
+                gv[:, l, :] = np.where(inside[l][:, None], gv[:, l, :], 0.0)
             grads.append(gv)
         offs.append(offs[-1] + r.size)
     out = (np.asarray(offs, dtype=np.int32), np.concatenate(meshes), np.concatenate(vals, axis=0))

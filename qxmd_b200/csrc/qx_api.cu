@@ -154,6 +154,8 @@ struct qx_ctx {
       *d_kbr_cursor = nullptr;
   int4 *d_kbr_lent = nullptr;
   void *d_kbr_vnl = nullptr, *d_kbr_sumr = nullptr, *d_kbr_bufR = nullptr;
+  double *d_kbr_rcl = nullptr;    // radius of each projector's channel (lmx * ntype)
+  std::vector<double> kbr_rcut_h; // species radii (the largest channel's)
   double *d_kbr_dtab = nullptr;   // g'(r)/r tables (optional)
   void *d_kbr_dvnl = nullptr;     // projector gradients per point (with d_kbr_dtab)
   long kbr_dvnl_cap = 0;
@@ -969,6 +971,16 @@ extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, cons
   TRY(dalloc(c, &pl.d_kb_clalp, sizeof(double) * lmx));
   CK(cudaMemcpyAsync(c->d_kbr_dl, dltnl, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_kbr_rcut, rcut, sizeof(double) * ntype, cudaMemcpyHostToDevice, c->st));
+  // every channel at the species radius until qx_set_kb_r_channel_radii
+  {
+    std::vector<double> rcl((size_t)nchan);
+    for (int it = 0; it < ntype; ++it)
+      for (int l = 0; l < lmx; ++l) rcl[l + lmx * it] = rcut[it];
+    TRY(dregrow(c, &c->d_kbr_rcl, sizeof(double) * nchan));
+    CK(cudaMemcpyAsync(c->d_kbr_rcl, rcl.data(), sizeof(double) * nchan, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));   // rcl is a host temporary
+    c->kbr_rcut_h.assign(rcut, rcut + ntype);
+  }
   CK(cudaMemcpyAsync(c->d_kbr_tab, tabnl, sizeof(double) * (size_t)(mxnl + 1) * nchan, cudaMemcpyHostToDevice, c->st));
   c->d_kbr_dtab = nullptr;
   if (dtabnl) {
@@ -984,6 +996,24 @@ extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, cons
   c->kbr_mxnl = mxnl;
   pl.rdelv = rdelv;
   c->have_kbr_builder = true;
+  return QX_OK;
+}
+
+extern "C" int qx_set_kb_r_channel_radii(qx_ctx *c, const double *rcl) {
+  if (!c || !rcl) { set_error("qx_set_kb_r_channel_radii: bad arguments"); return QX_ERR_ARG; }
+  if (!c->have_kbr_builder) { set_error("qx_set_kb_r_channel_radii: qx_set_kb_r_builder first"); return QX_ERR_STATE; }
+  const int ntype = c->kbr_ntype, lmx = 4;
+  for (int it = 0; it < ntype; ++it)
+    for (int l = 0; l < lmx; ++l) {
+      const double r = rcl[l + lmx * it];
+      if (!(r > 0.0) || r > c->kbr_rcut_h[it]) {
+        set_error("qx_set_kb_r_channel_radii: radius %g of projector %d, species %d, outside (0, %g] (the species "
+                  "radius of qx_set_kb_r_builder)", r, l, it, c->kbr_rcut_h[it]);
+        return QX_ERR_ARG;
+      }
+    }
+  CK(cudaMemcpyAsync(c->d_kbr_rcl, rcl, sizeof(double) * lmx * ntype, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
   return QX_OK;
 }
 
@@ -1033,11 +1063,11 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
     c->kbr_dvnl_cap = c->kbr_cap;
   }
   if (c->prec == QX_PREC_FP64)
-    kbr_fill<double>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
+    kbr_fill<double>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
                      c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
                      c->d_kbr_ptatom, (double *)c->d_kbr_vnl, (double *)c->d_kbr_dvnl, c->st);
   else
-    kbr_fill<float>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_dl, c->d_kbr_tab,
+    kbr_fill<float>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
                     c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
                     c->d_kbr_ptatom, (float *)c->d_kbr_vnl, (float *)c->d_kbr_dvnl, c->st);
   if (kbr_lines(c->d_kbr_off, natom, c->d_kbr_mesh, c->d_kbr_ptatom, pl.k1, nlines, c->d_kbr_lcnt, c->d_kbr_loff,

@@ -205,8 +205,8 @@ void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm,
                int *off, cudaStream_t st);
 template <typename T>
 void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
-              const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl, const int *poly,
-              const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st);
+              const double *rcl, const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl,
+              const int *poly, const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st);
 int kbr_lines(const int *off, int natom, const int *mesh, const int *ptatom, int k1, long nlines, int *lcnt,
               int *loff, int *cursor, int4 *lent, cudaStream_t st);
 

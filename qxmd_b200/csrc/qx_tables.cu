@@ -216,10 +216,16 @@ __device__ __forceinline__ double kbr_interp(const double *tb, int mm, double d)
 
 // dvnl (optional): the gradient of each projector with respect to the point,
 // grad (g(r) P(d)) = (g'(r)/r) P(d) d + g(r) grad P(d), from the table
-// dtabnl of g'(r)/r; dvnl[(i * lmx + l) * 3 + dim].
+// dtabnl of g'(r)/r; dvnl[(i * lmx + l) * 3 + dim].  rcl[l + lmx * it]: the
+// radius of projector l's angular channel (rmxnlc of setnlc,
+// nlkbppr.f90:1405-1431); the atom's points are those within the species
+// radius rcut (the largest channel's), and a projector is zero, value and
+// gradient, at the points beyond its own channel's radius, so each channel
+// sums over exactly the points of its own list in setnlc.
 template <typename T>
 __global__ void k_kbr_fill(KbrGeom G, int lmx, const int *__restrict__ ityp, const double *__restrict__ satm,
-                           const double *__restrict__ rcut, const double *__restrict__ dltnl,
+                           const double *__restrict__ rcut, const double *__restrict__ rcl,
+                           const double *__restrict__ dltnl,
                            const double *__restrict__ tabnl, const double *__restrict__ dtabnl, int mxnl,
                            const int *__restrict__ poly, const int *__restrict__ off, int natom, long cap,
                            int *__restrict__ mesh, int *__restrict__ ptatom, T *__restrict__ vnl,
@@ -258,13 +264,15 @@ __global__ void k_kbr_fill(KbrGeom G, int lmx, const int *__restrict__ ityp, con
       const double r = sqrt(dx * dx + dy * dy + dz * dz);
       const int mm = min(2 * (int)(r / (2.0 * dl)), mxnl - 2);
       const double d = 0.5 * (r / dl - (double)mm);
+      const double r2 = dx * dx + dy * dy + dz * dz;
       for (int l = 0; l < lmx; ++l) {
         const int ch = l + lmx * it;
-        const double f = kbr_interp(tabnl + (long)ch * (mxnl + 1), mm, d);
+        const bool inl = r2 <= rcl[ch] * rcl[ch];
+        const double f = inl ? kbr_interp(tabnl + (long)ch * (mxnl + 1), mm, d) : 0.0;
         const double pv = kbr_poly(poly[ch], dx, dy, dz);
         vnl[i * lmx + l] = (T)(f * pv);
         if (dvnl) {
-          const double fd = kbr_interp(dtabnl + (long)ch * (mxnl + 1), mm, d);
+          const double fd = inl ? kbr_interp(dtabnl + (long)ch * (mxnl + 1), mm, d) : 0.0;
           double gx, gy, gz;
           kbr_dpoly(poly[ch], dx, dy, dz, gx, gy, gz);
           dvnl[(i * lmx + l) * 3 + 0] = (T)(fd * pv * dx + f * gx);
@@ -342,16 +350,16 @@ void kbr_count(const KbrGeom &G, int natom, const int *ityp, const double *satm,
 
 template <typename T>
 void kbr_fill(const KbrGeom &G, int natom, int lmx, const int *ityp, const double *satm, const double *rcut,
-              const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl, const int *poly,
-              const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st) {
-  k_kbr_fill<T><<<natom, 256, 0, st>>>(G, lmx, ityp, satm, rcut, dltnl, tabnl, dtabnl, mxnl, poly, off, natom, cap,
-                                       mesh, ptatom, vnl, dtabnl ? dvnl : nullptr);
+              const double *rcl, const double *dltnl, const double *tabnl, const double *dtabnl, int mxnl,
+              const int *poly, const int *off, long cap, int *mesh, int *ptatom, T *vnl, T *dvnl, cudaStream_t st) {
+  k_kbr_fill<T><<<natom, 256, 0, st>>>(G, lmx, ityp, satm, rcut, rcl, dltnl, tabnl, dtabnl, mxnl, poly, off, natom,
+                                       cap, mesh, ptatom, vnl, dtabnl ? dvnl : nullptr);
   note_launch();
 }
-template void kbr_fill<float>(const KbrGeom &, int, int, const int *, const double *, const double *,
+template void kbr_fill<float>(const KbrGeom &, int, int, const int *, const double *, const double *, const double *,
                               const double *, const double *, const double *, int, const int *, const int *, long,
                               int *, int *, float *, float *, cudaStream_t);
-template void kbr_fill<double>(const KbrGeom &, int, int, const int *, const double *, const double *,
+template void kbr_fill<double>(const KbrGeom &, int, int, const int *, const double *, const double *, const double *,
                                const double *, const double *, const double *, int, const int *, const int *, long,
                                int *, int *, double *, double *, cudaStream_t);
 

@@ -25,7 +25,7 @@ QX_ERR = {1: "ARG", 2: "CUDA", 3: "NOTPD", 4: "EIG", 5: "STATE"}
 # Every symbol the header declares (checked by the CPU test suite).
 EXPORTS = [
     "qx_last_error", "qx_version", "qx_launch_count", "qx_create", "qx_destroy", "qx_set_glocal", "qx_set_kb_g",
-    "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g", "qx_set_kb_r_builder", "qx_build_kb_r", "qx_get_kb_r",
+    "qx_set_kb_builder", "qx_build_kb_g", "qx_get_kb_g", "qx_set_kb_r_builder", "qx_set_kb_r_channel_radii", "qx_build_kb_r", "qx_get_kb_r",
     "qx_forces_nl_r", "qxgpu_fnnlcl2",
     "qx_set_kb_r", "qx_set_nlmode", "qx_set_occ", "qx_put_psi", "qx_get_psi", "qx_put_hpsi",
     "qx_get_hpsi", "qx_get_eig", "qx_get_rho", "qx_put_rho", "qx_get_glocal", "qx_dev_ptr",
@@ -104,6 +104,7 @@ def lib(build_if_missing: bool = True):
         "qx_set_kb_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _ip, _ip, _dp, _ip], C.c_int),
         "qx_build_kb_g": ([_ctx, C.c_int, _ip, _dp], C.c_int),
         "qx_get_kb_g": ([_ctx, _dp, _dp], C.c_int),
+        "qx_set_kb_r_channel_radii": ([_ctx, _dp], C.c_int),
         "qx_set_kb_r_builder": ([_ctx, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _vp, _ip, _dp, C.c_double, _dp],
                                 C.c_int),
         "qx_forces_nl_r": ([_ctx, _dp], C.c_int),
@@ -417,6 +418,12 @@ class Context:
                                        _f64(b["tabnl"]), None if dt is None else dt.ctypes.data,
                                        np.ascontiguousarray(b["poly"], dtype=np.int32),
                                        _f64(b["clalp"]), b["rdelv"], _f64(b["rba"])), "qx_set_kb_r_builder")
+        if b.get("rcut_l") is not None:
+            self.set_kb_r_channel_radii(b["rcut_l"])
+
+    def set_kb_r_channel_radii(self, rcl):
+        """qx_set_kb_r_channel_radii: rcl (4 * ntype,) radius of each projector's channel."""
+        _ck(self.L.qx_set_kb_r_channel_radii(self.h, _f64(rcl)), "qx_set_kb_r_channel_radii")
 
     def forces_nl_r(self):
         """Real-space KB forces (natom, 3) Ry/bohr of the current psi."""

@@ -131,6 +131,62 @@ def test_build_kb_r_matches_oracle_and_rebuilds_in_place(si8, si8_psi, prec):
         ctx.close()
 
 
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_build_kb_r_channel_radii_match_oracle(si8, si8_psi, prec):
+    """Per-channel projector radii (qx_set_kb_r_channel_radii; setnlc's
+    rmxnlc(la), nlkbppr.f90:1405-1431): an s channel at 0.8 of the p radius.
+    The points are the species sphere's, the s projector is zero beyond its
+    own radius (and nonzero somewhere inside it), the values match the
+    oracle's setnlc, and real-space H|psi> and the real-space KB forces match
+    the oracle (restated calnlc and fnnlcl2 on those tables)."""
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
+    rp = float(b["rcut"][0])
+    b = dict(b, rcut_l=np.array([0.8 * rp, rp, rp, rp]))
+    nat = si8.cell.natom
+    satm = _moved(b["satm"], 7)
+    roff, rmesh, rvnl, rdvnl = tables.setnlc(b, b["ityp"], satm, grad=True)
+    ctx = Context(si8, prec, QX_NL_RSPACE)
+    try:
+        ctx.set_kb_r_builder(b)
+        ctx.build_kb_r(b["ityp"], satm)
+        off, mesh, vnl = ctx.get_kb_r(nat)
+        assert np.array_equal(off, roff)
+        assert np.array_equal(mesh, rmesh)
+        assert np.max(np.abs(vnl - rvnl)) / np.max(np.abs(rvnl)) < TAB_TOL[prec]
+        zero_s = rvnl[:, 0] == 0.0
+        assert zero_s.any() and not zero_s.all()
+        assert np.all(vnl[zero_s, 0] == 0.0)
+        ctx.put_psi(si8_psi)
+        ctx.enonloc()
+        hc = ctx.get_hpsi()
+        h = oracle.Ham(_kbr_system(si8, roff, rmesh, rvnl, b), QX_NL_RSPACE)
+        assert relerr(hc, h.hpsi(si8_psi)) < H_TOL[prec]
+        f = ctx.forces_nl_r()
+    finally:
+        ctx.close()
+    psir = np.array([oracle.wvg2r(si8.gs, c) for c in si8_psi])
+    ref = oforces.fnl_r(roff, rmesh, rvnl, rdvnl, b["clalp"], b["rdelv"], si8.gs.rvol, psir, si8.occ[:si8_psi.shape[0]])
+    assert np.max(np.abs(f - ref)) / np.max(np.abs(ref)) < (1e-10 if prec == QX_PREC_FP64 else 1e-4)
+
+
+def test_channel_radii_rejected_beyond_species_radius(si8):
+    need_gpu()
+    b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
+    rp = float(b["rcut"][0])
+    ctx = Context(si8, QX_PREC_FP64, QX_NL_RSPACE)
+    try:
+        with pytest.raises(Exception) as e:
+            ctx.set_kb_r_channel_radii(np.array([rp, rp, rp, rp]))
+        assert "qx_set_kb_r_builder first" in str(e.value)
+        ctx.set_kb_r_builder(b)
+        with pytest.raises(Exception) as e:
+            ctx.set_kb_r_channel_radii(np.array([rp, 1.1 * rp, rp, rp]))
+        assert "outside" in str(e.value)
+    finally:
+        ctx.close()
+
+
 def test_build_kb_r_grows_its_buffers(si8, si8_psi):
     """A larger projector radius (4.0 -> 4.4 bohr, 33 % more points) outgrows
     the first build's 25 % headroom: the buffers are reallocated and H|psi>

@@ -69,3 +69,54 @@ def test_real_space_builder_matches_model_tables():
             got = vnl[off[a]:off[a + 1]][o]
             want = ref.vnl[ref.off[a]:ref.off[a + 1]][p]
             assert np.max(np.abs(got - want)) / scale < 1e-8
+
+
+def test_channel_radii_reproduce_calnlc_per_channel_lists():
+    """setnlc gives each angular channel its own point list, the points within
+    rmxnlc(la) (nlkbppr.f90:1405-1431), and calnlc sums each projector over
+    its channel's list (nlkbppr.f90:1812-1818, 1862-1868).  The device keeps
+    one list per atom (the species radius, the largest channel's) with each
+    projector zero beyond its own channel's radius.  Restated here both ways
+    for s and p channels of different radii: the nonzero part of the union
+    list is the channel list (same points, same order, same values), and the
+    projections sumr and the scattered rk agree to rounding."""
+    s = cell.si8(with_ewald=False)
+    b = cell.kbr_builder_tables(s.gs, s.cell, s.pp)
+    rp = float(b["rcut"][0])
+    rs = 0.8 * rp
+    itola = [0, 1, 1, 1]                  # projector l -> channel la (s, p, p, p)
+    rcl = np.array([rs, rp, rp, rp])
+    off, mesh, vnl = tables.setnlc(dict(b, rcut_l=rcl), b["ityp"], b["satm"])
+    chan = {la: tables.setnlc(dict(b, rcut=np.array([rc])), b["ityp"], b["satm"]) for la, rc in ((0, rs), (1, rp))}
+    nat = s.cell.natom
+    assert chan[0][0][-1] < chan[1][0][-1]          # the s lists are strictly smaller
+    for a in range(nat):
+        u = slice(off[a], off[a + 1])
+        for l in range(4):
+            co, cm, cv = chan[itola[l]]
+            c = slice(co[a], co[a + 1])
+            keep = vnl[u, l] != 0.0
+            assert np.array_equal(mesh[u][keep], cm[c][cv[c, l] != 0.0])
+            assert np.array_equal(vnl[u, l][keep], cv[c, l][cv[c, l] != 0.0])
+    rng = np.random.default_rng(9)
+    eigv = rng.standard_normal(s.gs.kfft0)
+    scale = b["rdelv"] * b["clalp"]
+
+    def calnlc(lists_of):
+        sumr = np.zeros((nat, 4))
+        for a in range(nat):
+            for l in range(4):
+                o, m, v = lists_of(l)
+                sumr[a, l] = np.dot(v[o[a]:o[a + 1], l], eigv[m[o[a]:o[a + 1]]])
+        sumr *= scale
+        rk = np.zeros(s.gs.kfft0)
+        for a in range(nat):
+            for l in range(4):
+                o, m, v = lists_of(l)
+                np.add.at(rk, m[o[a]:o[a + 1]], v[o[a]:o[a + 1], l] * sumr[a, l])
+        return sumr, rk
+
+    sr, rr = calnlc(lambda l: chan[itola[l]])
+    su, ru = calnlc(lambda l: (off, mesh, vnl))
+    assert np.max(np.abs(su - sr)) <= 1e-13 * np.max(np.abs(sr))
+    assert np.max(np.abs(ru - rr)) <= 1e-13 * np.max(np.abs(rr))
