@@ -41,6 +41,9 @@ extern "C" {
 #define QX_HPSI_NONLOCAL 2
 #define QX_HPSI_ACCUMULATE 4
 
+/* Real-space KB: at most 9 projectors per atom (s, three p, five d). */
+#define QX_KBR_MAX_LMX 9
+
 typedef struct qx_ctx qx_ctx;
 
 /* Convergence controls of the CG band update; defaults of
@@ -119,17 +122,20 @@ int qx_get_kb_g(qx_ctx *ctx, double *eqlmr, double *vclalp);
 /* Real-space KB tables (setnlc nlkbppr.f90:1010-1768, used by calnlc
  * nlkbppr.f90:1773-1900): atom a owns points off[a]..off[a+1]-1 with
  * zero-based grid index mesh[] and projector values vnl[point*lmx + l];
- * clalp(lmx) = clalp_ncr; rdelv = volume per grid point.  lmx must be 4. */
+ * clalp(lmx) = clalp_ncr; rdelv = volume per grid point.  1 <= lmx <=
+ * QX_KBR_MAX_LMX; species with fewer projectors than lmx carry zero columns
+ * (the reference's lmx(it) differs by species; one stride serves all here). */
 int qx_set_kb_r(qx_ctx *ctx, int natom, int lmx, const int *off, const int *mesh, const double *vnl,
                 const double *clalp, double rdelv);
 /* The real-space tables built on the device, for MD steps (setnlc
- * nlkbppr.f90:1010-1560).  Once per cell: ntype species of lmx = 4 channels,
- * radial tables tabnl((mxnl + 1), 4 * ntype) at r = k * dltnl(it), projector
+ * nlkbppr.f90:1010-1560).  Once per cell: ntype species of lmx projectors each
+ * (1 <= lmx <= QX_KBR_MAX_LMX; s, p, d), radial tables tabnl((mxnl + 1),
+ * lmx * ntype) at r = k * dltnl(it), projector
  * radius rcut(ntype), dtabnl (nullable, same shape): g'(r)/r of each radial
  * table g, for the projector gradients of the forces (tbfnl of fnnlcl2),
- * poly(4 * ntype): the real solid-harmonic polynomial
+ * poly(lmx * ntype): the real solid-harmonic polynomial
  * that multiplies each channel's radial value (0: 1; 1-3: x, y, z; 4-8: xy,
- * yz, zx, x^2 - y^2, 3z^2 - r^2 of the displacement from the atom), clalp(4)
+ * yz, zx, x^2 - y^2, 3z^2 - r^2 of the displacement from the atom), clalp(lmx)
  * KB energies, rdelv the volume per grid point, rba(3, 3) the lattice
  * vectors as columns (row-major here: rba[3 * x + j] = component x of
  * vector j).  The sphere must fit in half the cell along every axis. */
@@ -138,7 +144,7 @@ int qx_set_kb_r_builder(qx_ctx *ctx, int ntype, int lmx, int mxnl, const double 
                         const double *rba);
 /* Per-channel projector radii (rmxnlc(la, it) of setnlc nlkbppr.f90:1405-1431,
  * which gives each angular channel la its own point list, numsnl(la, i) points
- * of meshnl): rcl(4, ntype), rcl[l + 4 * it] the radius of the channel of
+ * of meshnl): rcl(lmx, ntype), rcl[l + lmx * it] the radius of the channel of
  * projector l of species it, each in (0, rcut(it)]; the species radius given
  * to qx_set_kb_r_builder must be the largest of its channels'.  The device
  * keeps one list per atom, the points within rcut(it), and a projector is zero
@@ -154,7 +160,7 @@ int qx_set_kb_r_channel_radii(qx_ctx *ctx, const double *rcl);
  * are then dropped); otherwise they are reused in place. */
 int qx_build_kb_r(qx_ctx *ctx, int natom, const int *ityp, const double *satm);
 /* Reads back the real-space tables in use: *npts, and when not null
- * off(natom + 1), mesh(npts), vnl(4 * npts) (double). */
+ * off(natom + 1), mesh(npts), vnl(lmx * npts) (double). */
 int qx_get_kb_r(qx_ctx *ctx, int *npts, int *off, int *mesh, double *vnl);
 int qx_set_nlmode(qx_ctx *ctx, int mode);
 /* occ(nband) and the cell volume (softchg weights occ/rvol, chgdns.f90:421). */

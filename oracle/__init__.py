@@ -183,7 +183,7 @@ class Ham:
         h.kbg = k["kbg"].ctypes.data
         h.vclalp = k["vclalp"].ctypes.data
         h.natom = sys.cell.natom
-        h.lmx = sys.pp.lmx
+        h.lmx = int(k["vnl"].shape[1]) if k["vnl"].ndim == 2 else sys.pp.lmx   # projectors per point
         h.off = k["off"].ctypes.data
         h.mesh = k["mesh"].ctypes.data
         h.vnl = k["vnl"].ctypes.data

@@ -99,15 +99,17 @@ def box_halfwidths(rba: np.ndarray, grid, rmax: float):
 
 
 def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
-    """(off (natom+1), mesh (npts), vnl (npts, 4)) in box order; b is the dict
+    """(off (natom+1), mesh (npts), vnl (npts, lmx)) in box order; b is the dict
     of qxmd_b200.cell.kbr_builder_tables, with optional per-projector channel
-    radii b["rcut_l"] (4 * ntype, each at most the species radius b["rcut"]).  With grad, also dvnl (npts, 4, 3):
+    radii b["rcut_l"] (lmx * ntype, each at most the species radius b["rcut"]);
+    b["lmx"] projectors per atom (4 when absent).  With grad, also dvnl (npts, lmx, 3):
     the gradient of each projector value with respect to the displacement d
     of the point from its atom, as fnnlcl2 builds it from the radial table
     and its derivative table (nlkbppr.f90:2200-2240):
     grad(g(r) P(d)) = (g'(r)/r) d P(d) + g(r) grad P(d), both radial tables
     interpolated by the three-point formula of setqlm."""
     k = np.array(b["grid"])
+    lmx = int(b.get("lmx", 4))
     nd = box_halfwidths(b["rba"], b["grid"], float(np.max(b["rcut"])))
     o3, o2, o1 = np.meshgrid(np.arange(-nd[2], nd[2] + 1), np.arange(-nd[1], nd[1] + 1),
                              np.arange(-nd[0], nd[0] + 1), indexing="ij")
@@ -129,19 +131,19 @@ def setnlc(b: dict, ityp: np.ndarray, satm: np.ndarray, grad: bool = False):
         # nlkbppr.f90:1405-1431): zero at the points outside it, so that the
         # sums over the species sphere equal the sums over each channel's list
         rl2 = r2[sel]
-        inside = [rl2 <= (b["rcut_l"][l + 4 * it] ** 2 if b.get("rcut_l") is not None else np.inf)
-                  for l in range(4)]
-        v = np.empty((r.size, 4))
-        for l in range(4):
-            ch = l + 4 * it
+        inside = [rl2 <= (b["rcut_l"][l + lmx * it] ** 2 if b.get("rcut_l") is not None else np.inf)
+                  for l in range(lmx)]
+        v = np.empty((r.size, lmx))
+        for l in range(lmx):
+            ch = l + lmx * it
             v[:, l] = setqlm(r, b["dltnl"][it], b["tabnl"][ch], _poly(int(b["poly"][ch]), d[:, 0], d[:, 1], d[:, 2]))
             v[:, l] = np.where(inside[l], v[:, l], 0.0)
         vals.append(v)
         if grad:
-            gv = np.empty((r.size, 4, 3))
+            gv = np.empty((r.size, lmx, 3))
             one = np.ones_like(r)
-            for l in range(4):
-                ch = l + 4 * it
+            for l in range(lmx):
+                ch = l + lmx * it
                 c = int(b["poly"][ch])
                 g = setqlm(r, b["dltnl"][it], b["tabnl"][ch], one)
                 dg = setqlm(r, b["dltnl"][it], b["dtabnl"][ch], one)

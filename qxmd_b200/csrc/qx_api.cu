@@ -146,7 +146,7 @@ struct qx_ctx {
   bool have_kb_builder = false;
   // real-space table builder (qx_set_kb_r_builder, qx_build_kb_r)
   KbrGeom kbr_geom = {};
-  int kbr_ntype = 0, kbr_mxnl = 0, kbr_natom = 0;
+  int kbr_ntype = 0, kbr_mxnl = 0, kbr_natom = 0, kbr_lmx = 4;
   long kbr_cap = 0;
   double *d_kbr_dl = nullptr, *d_kbr_rcut = nullptr, *d_kbr_tab = nullptr, *d_kbr_satm = nullptr;
   int *d_kbr_poly = nullptr, *d_kbr_ityp = nullptr, *d_kbr_cnt = nullptr, *d_kbr_off = nullptr,
@@ -871,8 +871,8 @@ extern "C" int qx_get_kb_g(qx_ctx *c, double *eqlmr, double *vclalp) {
 
 extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const int *mesh, const double *vnl,
                            const double *clalp, double rdelv) {
-  if (!c || natom <= 0 || lmx != 4 || !off || !mesh || !vnl || !clalp) {
-    set_error("qx_set_kb_r: bad arguments (lmx must be 4)");
+  if (!c || natom <= 0 || lmx < 1 || lmx > QX_KBR_MAX_LMX || !off || !mesh || !vnl || !clalp) {
+    set_error("qx_set_kb_r: bad arguments (1 <= lmx <= %d)", QX_KBR_MAX_LMX);
     return QX_ERR_ARG;
   }
   Plan &pl = c->pl;
@@ -901,10 +901,11 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
   CK(cudaMemcpy(pl.d_line_off, loff.data(), sizeof(int) * (nlines + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(pl.d_line_ent, lent.data(), sizeof(int4) * lent.size(), cudaMemcpyHostToDevice));
   void *v = nullptr;
-  TRY(dalloc(c, &v, c->tsize() * (size_t)npts * 4));
-  TRY(up(c, v, vnl, (long)npts * 4));
+  TRY(dalloc(c, &v, c->tsize() * (size_t)npts * lmx));
+  TRY(up(c, v, vnl, (long)npts * lmx));
   pl.natom = natom;
   pl.npts = npts;
+  pl.kb_lmx = lmx;
   pl.rdelv = rdelv;
   drop_scf_graphs(c);
   // real-space line buffer and projection sums, per chunk
@@ -912,11 +913,11 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
   if (c->prec == QX_PREC_FP64) {
     pl.b64.kb_vnl = (double *)v;
     TRY(dalloc(c, &pl.b64.bufR, sizeof(double2) * ch * pl.n));
-    TRY(dalloc(c, &pl.b64.sumr, sizeof(double2) * ch * natom * 4));
+    TRY(dalloc(c, &pl.b64.sumr, sizeof(double2) * ch * natom * lmx));
   } else {
     pl.b32.kb_vnl = (float *)v;
     TRY(dalloc(c, &pl.b32.bufR, sizeof(float2) * ch * pl.n));
-    TRY(dalloc(c, &pl.b32.sumr, sizeof(float2) * ch * natom * 4));
+    TRY(dalloc(c, &pl.b32.sumr, sizeof(float2) * ch * natom * lmx));
   }
   c->have_kbr = true;
   return QX_OK;
@@ -925,9 +926,9 @@ extern "C" int qx_set_kb_r(qx_ctx *c, int natom, int lmx, const int *off, const 
 extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, const double *dltnl, const double *rcut,
                                    const double *tabnl, const double *dtabnl, const int *poly, const double *clalp,
                                    double rdelv, const double *rba) {
-  if (!c || ntype <= 0 || lmx != 4 || mxnl < 2 || !dltnl || !rcut || !tabnl || !poly || !clalp || !rba ||
-      !(rdelv > 0.0)) {
-    set_error("qx_set_kb_r_builder: bad arguments (lmx must be 4)");
+  if (!c || ntype <= 0 || lmx < 1 || lmx > QX_KBR_MAX_LMX || mxnl < 2 || !dltnl || !rcut || !tabnl || !poly ||
+      !clalp || !rba || !(rdelv > 0.0)) {
+    set_error("qx_set_kb_r_builder: bad arguments (1 <= lmx <= %d)", QX_KBR_MAX_LMX);
     return QX_ERR_ARG;
   }
   Plan &pl = c->pl;
@@ -992,6 +993,12 @@ extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, cons
   CK(cudaMemcpyAsync(pl.d_kb_clalp, clalp, sizeof(double) * lmx, cudaMemcpyHostToDevice, c->st));
   drop_scf_graphs(c);
   c->kbr_geom = G;
+  if (lmx != c->kbr_lmx) {   // table buffers sized per projector count: rebuilt at the next build
+    c->kbr_cap = 0;
+    c->kbr_dvnl_cap = 0;
+    c->kbr_natom = 0;
+    c->kbr_lmx = lmx;
+  }
   c->kbr_ntype = ntype;
   c->kbr_mxnl = mxnl;
   pl.rdelv = rdelv;
@@ -1002,7 +1009,7 @@ extern "C" int qx_set_kb_r_builder(qx_ctx *c, int ntype, int lmx, int mxnl, cons
 extern "C" int qx_set_kb_r_channel_radii(qx_ctx *c, const double *rcl) {
   if (!c || !rcl) { set_error("qx_set_kb_r_channel_radii: bad arguments"); return QX_ERR_ARG; }
   if (!c->have_kbr_builder) { set_error("qx_set_kb_r_channel_radii: qx_set_kb_r_builder first"); return QX_ERR_STATE; }
-  const int ntype = c->kbr_ntype, lmx = 4;
+  const int ntype = c->kbr_ntype, lmx = c->kbr_lmx;
   for (int it = 0; it < ntype; ++it)
     for (int l = 0; l < lmx; ++l) {
       const double r = rcl[l + lmx * it];
@@ -1031,7 +1038,7 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
     TRY(dregrow(c, &c->d_kbr_satm, sizeof(double) * 3 * natom));
     TRY(dregrow(c, &c->d_kbr_cnt, sizeof(int) * natom));
     TRY(dregrow(c, &c->d_kbr_off, sizeof(int) * (natom + 1)));
-    TRY(dregrow(c, &c->d_kbr_sumr, 2 * ts * (size_t)pl.chunk * natom * 4));
+    TRY(dregrow(c, &c->d_kbr_sumr, 2 * ts * (size_t)pl.chunk * natom * c->kbr_lmx));
     c->kbr_natom = natom;
     moved = true;
   }
@@ -1054,20 +1061,20 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
     TRY(dregrow(c, &c->d_kbr_mesh, sizeof(int) * cap));
     TRY(dregrow(c, &c->d_kbr_ptatom, sizeof(int) * cap));
     TRY(dregrow(c, &c->d_kbr_lent, sizeof(int4) * cap));
-    TRY(dregrow(c, &c->d_kbr_vnl, ts * 4 * (size_t)cap));
+    TRY(dregrow(c, &c->d_kbr_vnl, ts * c->kbr_lmx * (size_t)cap));
     c->kbr_cap = cap;
     moved = true;
   }
   if (c->d_kbr_dtab && c->kbr_dvnl_cap < c->kbr_cap) {
-    TRY(dregrow(c, &c->d_kbr_dvnl, ts * 12 * (size_t)c->kbr_cap));
+    TRY(dregrow(c, &c->d_kbr_dvnl, ts * 3 * c->kbr_lmx * (size_t)c->kbr_cap));
     c->kbr_dvnl_cap = c->kbr_cap;
   }
   if (c->prec == QX_PREC_FP64)
-    kbr_fill<double>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
+    kbr_fill<double>(G, natom, c->kbr_lmx, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
                      c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
                      c->d_kbr_ptatom, (double *)c->d_kbr_vnl, (double *)c->d_kbr_dvnl, c->st);
   else
-    kbr_fill<float>(G, natom, 4, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
+    kbr_fill<float>(G, natom, c->kbr_lmx, c->d_kbr_ityp, c->d_kbr_satm, c->d_kbr_rcut, c->d_kbr_rcl, c->d_kbr_dl, c->d_kbr_tab,
                     c->d_kbr_dtab, c->kbr_mxnl, c->d_kbr_poly, c->d_kbr_off, c->kbr_cap, c->d_kbr_mesh,
                     c->d_kbr_ptatom, (float *)c->d_kbr_vnl, (float *)c->d_kbr_dvnl, c->st);
   if (kbr_lines(c->d_kbr_off, natom, c->d_kbr_mesh, c->d_kbr_ptatom, pl.k1, nlines, c->d_kbr_lcnt, c->d_kbr_loff,
@@ -1096,6 +1103,7 @@ extern "C" int qx_build_kb_r(qx_ctx *c, int natom, const int *ityp, const double
   }
   pl.natom = natom;
   pl.npts = total;
+  pl.kb_lmx = c->kbr_lmx;
   if (moved) drop_scf_graphs(c);
   c->have_kbr = true;
   return QX_OK;
@@ -1111,9 +1119,9 @@ extern "C" int qx_get_kb_r(qx_ctx *c, int *npts, int *off, int *mesh, double *vn
   if (mesh) CK(cudaMemcpy(mesh, pl.d_kb_mesh, sizeof(int) * pl.npts, cudaMemcpyDeviceToHost));
   if (vnl) {
     if (c->prec == QX_PREC_FP64) {
-      CK(cudaMemcpy(vnl, pl.b64.kb_vnl, sizeof(double) * 4 * pl.npts, cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(vnl, pl.b64.kb_vnl, sizeof(double) * pl.kb_lmx * pl.npts, cudaMemcpyDeviceToHost));
     } else {
-      std::vector<float> h((size_t)4 * pl.npts);
+      std::vector<float> h((size_t)pl.kb_lmx * pl.npts);
       CK(cudaMemcpy(h.data(), pl.b32.kb_vnl, sizeof(float) * h.size(), cudaMemcpyDeviceToHost));
       for (size_t i = 0; i < h.size(); ++i) vnl[i] = h[i];
     }

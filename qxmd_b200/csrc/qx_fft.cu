@@ -480,15 +480,17 @@ __global__ void __launch_bounds__(QX_THREADS) k_xinv_r(PipeParams P, const typen
 // D_l = rdelv sum_points grad vnl_l psi_b (gradient with respect to the
 // point), then F_a += 2 occ_b / Omega sum_l clalp_l P_l D_l; one partial per
 // pair in fpart[(pair * natom + atom) * 3 + dim] (summed over pairs in a
-// fixed order afterwards).  wocc = occ / Omega.
-template <typename T>
+// fixed order afterwards).  wocc = occ / Omega.  lmx <= ML projectors per
+// point (ML = 4: s, p; ML = 9: s, p, d).
+template <typename T, int ML>
 __global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typename c2t<T>::type *__restrict__ R,
                                                        const int *__restrict__ off, const int *__restrict__ mesh,
                                                        const T *__restrict__ vnl, const T *__restrict__ dvnl,
                                                        const double *__restrict__ clalp, double rdelv, int natom,
-                                                       const double *__restrict__ wocc, int npl, int ppb,
+                                                       int lmx, const double *__restrict__ wocc, int npl, int ppb,
                                                        double *__restrict__ fpart) {
   typedef typename c2t<T>::type C;
+  constexpr int NQ = 8 * ML;   // P[band][l] (2 ML), then D[band][l][dim] (6 ML)
   const int at = blockIdx.x;
   // ppb pairs of the chunk per block, one after another, so that the atom's
   // table slice is read from cache after the first
@@ -498,51 +500,51 @@ __global__ void __launch_bounds__(QX_THREADS) k_fnl_r(PipeParams P, const typena
   if (p >= pair_count(P)) break;   // uniform across the block
   const long n = (long)P.k1 * P.k2 * P.k3;
   const C *Rp = R + (long)pl * n;
-  double acc[32];   // P[band][l] (8), then D[band][l][dim] (24)
+  double acc[NQ];
 #pragma unroll
-  for (int q = 0; q < 32; ++q) acc[q] = 0.0;
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
   for (int mm = off[at] + threadIdx.x; mm < off[at + 1]; mm += blockDim.x) {
     const C z = Rp[mesh[mm]];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const double v = (double)vnl[(long)mm * 4 + l];
+    for (int l = 0; l < ML; ++l) {
+      if (l >= lmx) break;   // uniform
+      const double v = (double)vnl[(long)mm * lmx + l];
       acc[l] += v * (double)z.x;
-      acc[4 + l] += v * (double)z.y;
+      acc[ML + l] += v * (double)z.y;
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const double g = (double)dvnl[((long)mm * 4 + l) * 3 + d];
-        acc[8 + l * 3 + d] += g * (double)z.x;
-        acc[20 + l * 3 + d] += g * (double)z.y;
+        const double g = (double)dvnl[((long)mm * lmx + l) * 3 + d];
+        acc[2 * ML + l * 3 + d] += g * (double)z.x;
+        acc[5 * ML + l * 3 + d] += g * (double)z.y;
       }
     }
   }
-  // the 32 sums: warp shuffles, then one pass over the warps' partials
-  __shared__ double red[QX_THREADS / 32][32];
+  // the NQ sums: warp shuffles, then one pass over the warps' partials
+  __shared__ double red[QX_THREADS / 32][NQ];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < 32; ++q) {
+  for (int q = 0; q < NQ; ++q) {
     double v = acc[q];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if (lane == 0) red[warp][q] = v;
   }
   __syncthreads();
-  if (threadIdx.x < 32) {
+  for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
     double v = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
-    red[0][threadIdx.x] = v;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][q];
+    red[0][q] = v;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = red[0][q];
+    const double *s = red[0];
     const int b[2] = {P.pairs[2 * p], P.pairs[2 * p + 1]};
     double f[3] = {0.0, 0.0, 0.0};
     for (int h = 0; h < 2; ++h) {
       if (b[h] < 0) continue;
       const double w = 2.0 * wocc[b[h]] * rdelv * rdelv;
-      for (int l = 0; l < 4; ++l)
-        for (int d = 0; d < 3; ++d) f[d] += w * clalp[l] * acc[4 * h + l] * acc[8 + 12 * h + l * 3 + d];
+      for (int l = 0; l < lmx; ++l)
+        for (int d = 0; d < 3; ++d) f[d] += w * clalp[l] * s[h * ML + l] * s[2 * ML + 3 * ML * h + l * 3 + d];
     }
     double *o = fpart + ((long)p * natom + at) * 3;
     o[0] = f[0];
@@ -563,12 +565,13 @@ __global__ void k_fnl_r_sum(const double *__restrict__ fpart, int npair, int nat
 }
 
 // sumr(l, atom) = rdelv * clalp_l * sum_points vnl_l * psi(point), both bands
-// of the pair at once (real part band A, imaginary part band B).
-template <typename T>
+// of the pair at once (real part band A, imaginary part band B); lmx <= ML
+// projectors per point.
+template <typename T, int ML>
 __global__ void __launch_bounds__(QX_THREADS) k_nlproj(PipeParams P, const typename c2t<T>::type *__restrict__ R,
                                                         const int *__restrict__ off, const int *__restrict__ mesh,
                                                         const T *__restrict__ vnl, const double *__restrict__ clalp,
-                                                        double rdelv, int natom,
+                                                        double rdelv, int natom, int lmx,
                                                         typename c2t<T>::type *__restrict__ sumr) {
   typedef typename c2t<T>::type C;
   const int at = blockIdx.x;
@@ -576,24 +579,27 @@ __global__ void __launch_bounds__(QX_THREADS) k_nlproj(PipeParams P, const typen
   if (p >= pair_count(P)) return;
   const long n = (long)P.k1 * P.k2 * P.k3;
   const C *Rp = R + (long)pl * n;
-  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double acc[2 * ML];
+#pragma unroll
+  for (int q = 0; q < 2 * ML; ++q) acc[q] = 0.0;
   for (int mm = off[at] + threadIdx.x; mm < off[at + 1]; mm += blockDim.x) {
     const C z = Rp[mesh[mm]];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) {
-      const double v = (double)vnl[(long)mm * 4 + l];
+    for (int l = 0; l < ML; ++l) {
+      if (l >= lmx) break;   // uniform
+      const double v = (double)vnl[(long)mm * lmx + l];
       acc[2 * l] += v * (double)z.x;
       acc[2 * l + 1] += v * (double)z.y;
     }
   }
   __shared__ double red[QX_THREADS / 32];
-  for (int l = 0; l < 8; ++l) {
+  for (int l = 0; l < 2 * lmx; ++l) {
     const double s = block_sum(acc[l], red);
     if (threadIdx.x == 0) acc[l] = s;
   }
   if (threadIdx.x == 0) {
-    C *o = sumr + ((long)pl * natom + at) * 4;
-    for (int l = 0; l < 4; ++l) {
+    C *o = sumr + ((long)pl * natom + at) * lmx;
+    for (int l = 0; l < lmx; ++l) {
       const double f = rdelv * clalp[l];
       o[l] = mk2<T>((T)(acc[2 * l] * f), (T)(acc[2 * l + 1] * f));
     }
@@ -603,13 +609,13 @@ __global__ void __launch_bounds__(QX_THREADS) k_nlproj(PipeParams P, const typen
 // Forward x pass for the real-space KB mode: V*psi + sum vnl*sumr, forward
 // x-FFT, keep the pruned part.  Line CSR `loff/lent` lists the projector
 // points of each line (i3*k2 + i2): {i1, point index, atom}.
-template <typename T>
+template <typename T, int ML>
 __global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typename c2t<T>::type *__restrict__ R,
                                                         typename c2t<T>::type *__restrict__ bufB,
                                                         const T *__restrict__ vloc, const int *__restrict__ loff,
                                                         const int4 *__restrict__ lent, const T *__restrict__ vnl,
                                                         const typename c2t<T>::type *__restrict__ sumr, int natom,
-                                                        int nlines, int nchunk,
+                                                        int lmx, int nlines, int nchunk,
                                                         FftTabs<T> gt1) {
   typedef typename c2t<T>::type C;
   const int i3 = blockIdx.x / nchunk, ch = blockIdx.x - i3 * nchunk;
@@ -631,16 +637,20 @@ __global__ void __launch_bounds__(QX_THREADS) k_xfwd_r(PipeParams P, const typen
     t0[i1 * ld + l] = z;
   }
   __syncthreads();
-  const C *S = sumr + (long)pl * natom * 4;
+  const C *S = sumr + (long)pl * natom * lmx;
   const int line0 = i3 * k2 + i20;
   for (int l = 0; l < nl; ++l) {
     for (int e = loff[line0 + l] + threadIdx.x; e < loff[line0 + l + 1]; e += blockDim.x) {
       const int4 en = lent[e];
-      const C *s = S + (long)en.z * 4;
-      const T *v = vnl + (long)en.y * 4;
+      const C *s = S + (long)en.z * lmx;
+      const T *v = vnl + (long)en.y * lmx;
       T ar = 0, ai = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) { ar += v[q] * s[q].x; ai += v[q] * s[q].y; }
+      for (int q = 0; q < ML; ++q) {
+        if (q >= lmx) break;   // uniform
+        ar += v[q] * s[q].x;
+        ai += v[q] * s[q].y;
+      }
       atomicAdd(&t0[en.x * ld + l].x, ar);
       atomicAdd(&t0[en.x * ld + l].y, ai);
     }
@@ -833,10 +843,19 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   if (nlmode == 2) {
     k_xinv_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.bufR, nlines, nch, g1); note_launch();
     dim3 ga(pl.natom, npl);
-    k_nlproj<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, pl.d_kb_clalp,
-                                           pl.rdelv, pl.natom, bf.sumr); note_launch();
-    k_xfwd_r<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufR, bf.bufB, bf.vloc, pl.d_line_off, pl.d_line_ent,
-                                             bf.kb_vnl, bf.sumr, pl.natom, nlines, nch, g1); note_launch();
+    if (pl.kb_lmx <= 4) {
+      k_nlproj<T, 4><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, pl.d_kb_clalp,
+                                                pl.rdelv, pl.natom, pl.kb_lmx, bf.sumr); note_launch();
+      k_xfwd_r<T, 4><<<gx, QX_THREADS, smx, st>>>(P, bf.bufR, bf.bufB, bf.vloc, pl.d_line_off, pl.d_line_ent,
+                                                  bf.kb_vnl, bf.sumr, pl.natom, pl.kb_lmx, nlines, nch, g1);
+      note_launch();
+    } else {
+      k_nlproj<T, 9><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, pl.d_kb_clalp,
+                                                pl.rdelv, pl.natom, pl.kb_lmx, bf.sumr); note_launch();
+      k_xfwd_r<T, 9><<<gx, QX_THREADS, smx, st>>>(P, bf.bufR, bf.bufB, bf.vloc, pl.d_line_off, pl.d_line_ent,
+                                                  bf.kb_vnl, bf.sumr, pl.natom, pl.kb_lmx, nlines, nch, g1);
+      note_launch();
+    }
   } else {
     k_xvx<T><<<gx, QX_THREADS, smx, st>>>(P, bf.bufB, bf.vloc, nlines, nch, g1); note_launch();
   }
@@ -897,8 +916,12 @@ int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *ci
   const int gyf = std::max(1, std::min(npl, (4 * 148 + pl.natom - 1) / pl.natom));
   const int ppb = (npl + gyf - 1) / gyf;
   dim3 ga(pl.natom, (npl + ppb - 1) / ppb);
-  k_fnl_r<T><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
-                                        pl.rdelv, pl.natom, wocc, npl, ppb, fpart);
+  if (pl.kb_lmx <= 4)
+    k_fnl_r<T, 4><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
+                                             pl.rdelv, pl.natom, pl.kb_lmx, wocc, npl, ppb, fpart);
+  else
+    k_fnl_r<T, 9><<<ga, QX_THREADS, 0, st>>>(P, bf.bufR, pl.d_kb_off, pl.d_kb_mesh, bf.kb_vnl, dvnl, pl.d_kb_clalp,
+                                             pl.rdelv, pl.natom, pl.kb_lmx, wocc, npl, ppb, fpart);
   note_launch();
   return 0;
 }
@@ -979,7 +1002,8 @@ void set_fft_smem_limits(size_t bytes) {
   cudaFuncSetAttribute(k_xvx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_zfwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_xinv_r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  cudaFuncSetAttribute(k_xfwd_r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xfwd_r<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k_xfwd_r<T, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_xrho<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_full_z<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaFuncSetAttribute(k_full_z<T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

@@ -69,8 +69,8 @@ struct Plan {
   // sphere z-columns (see PipeParams)
   int *d_col_ja = nullptr, *d_col_ig = nullptr;
   int ncol = 0;
-  // real-space KB
-  int natom = 0, npts = 0;
+  // real-space KB (kb_lmx projectors per point, at most 9: s, p, d)
+  int natom = 0, npts = 0, kb_lmx = 4;
   int *d_kb_off = nullptr, *d_kb_mesh = nullptr;
   double *d_kb_clalp = nullptr;
   double rdelv = 0.0;

@@ -225,7 +225,8 @@ class Context:
         _ck(L.qx_set_glocal(h, _f64(sys.vloc)), "qx_set_glocal")
         _ck(L.qx_set_kb_g(h, sys.kb_g.shape[1], _f64(sys.kb_g.T), _f64(sys.vclalp)), "qx_set_kb_g")
         kr = sys.kb_r
-        _ck(L.qx_set_kb_r(h, sys.cell.natom, 4, np.ascontiguousarray(kr.off, dtype=np.int32),
+        self._kbr_lmx = int(np.asarray(kr.vnl).shape[1])
+        _ck(L.qx_set_kb_r(h, sys.cell.natom, self._kbr_lmx, np.ascontiguousarray(kr.off, dtype=np.int32),
                           np.ascontiguousarray(kr.mesh, dtype=np.int32), _f64(kr.vnl), _f64(kr.clalp),
                           kr.rdelv), "qx_set_kb_r")
         _ck(L.qx_set_nlmode(h, nlmode), "qx_set_nlmode")
@@ -414,15 +415,17 @@ class Context:
     def set_kb_r_builder(self, b: dict):
         """qx_set_kb_r_builder from the dict of cell.kbr_builder_tables."""
         dt = _f64(b["dtabnl"]) if b.get("dtabnl") is not None else None
-        _ck(self.L.qx_set_kb_r_builder(self.h, b["ntype"], 4, b["mxnl"], _f64(b["dltnl"]), _f64(b["rcut"]),
+        lmx = int(b.get("lmx", 4))
+        _ck(self.L.qx_set_kb_r_builder(self.h, b["ntype"], lmx, b["mxnl"], _f64(b["dltnl"]), _f64(b["rcut"]),
                                        _f64(b["tabnl"]), None if dt is None else dt.ctypes.data,
                                        np.ascontiguousarray(b["poly"], dtype=np.int32),
                                        _f64(b["clalp"]), b["rdelv"], _f64(b["rba"])), "qx_set_kb_r_builder")
+        self._kbr_lmx = lmx
         if b.get("rcut_l") is not None:
             self.set_kb_r_channel_radii(b["rcut_l"])
 
     def set_kb_r_channel_radii(self, rcl):
-        """qx_set_kb_r_channel_radii: rcl (4 * ntype,) radius of each projector's channel."""
+        """qx_set_kb_r_channel_radii: rcl (lmx * ntype,) radius of each projector's channel."""
         _ck(self.L.qx_set_kb_r_channel_radii(self.h, _f64(rcl)), "qx_set_kb_r_channel_radii")
 
     def forces_nl_r(self):
@@ -438,12 +441,12 @@ class Context:
             "qx_build_kb_r")
 
     def get_kb_r(self, natom):
-        """(off (natom+1), mesh (npts), vnl (npts, 4)) read back from the device."""
+        """(off (natom+1), mesh (npts), vnl (npts, lmx)) read back from the device."""
         n = C.c_int(0)
         _ck(self.L.qx_get_kb_r(self.h, C.byref(n), None, None, None), "qx_get_kb_r")
         off = np.zeros(natom + 1, dtype=np.int32)
         mesh = np.zeros(max(n.value, 1), dtype=np.int32)
-        vnl = np.zeros((max(n.value, 1), 4))
+        vnl = np.zeros((max(n.value, 1), self._kbr_lmx))
         _ck(self.L.qx_get_kb_r(self.h, C.byref(n), off.ctypes.data, mesh.ctypes.data, vnl.ctypes.data),
             "qx_get_kb_r")
         return off, mesh[: n.value], vnl[: n.value]

@@ -170,6 +170,65 @@ def test_build_kb_r_channel_radii_match_oracle(si8, si8_psi, prec):
     assert np.max(np.abs(f - ref)) / np.max(np.abs(ref)) < (1e-10 if prec == QX_PREC_FP64 else 1e-4)
 
 
+def _with_channels(b, lmx):
+    """The model's builder tables with lmx projectors per atom: s only
+    (lmx 1) or s, three p and five d (lmx 9; the d radial part a Gaussian
+    like the others, times the d polynomials 4-8 of kbr_poly, KB energy
+    0.1 Ry), with channel radii 0.8 (s), 1.0 (p) and 0.9 (d) of the species
+    radius."""
+    rc = float(b["rcut"][0])
+    tab, dtab = b["tabnl"], b["dtabnl"]
+    if lmx == 1:
+        return dict(b, lmx=1, tabnl=tab[:1].copy(), dtabnl=dtab[:1].copy(), poly=np.zeros(1, dtype=np.int32),
+                    clalp=b["clalp"][:1].copy(), rcut_l=np.array([0.8 * rc]))
+    d = 0.6 * tab[1]
+    return dict(b, lmx=9, tabnl=np.ascontiguousarray(np.vstack([tab] + [d] * 5)),
+                dtabnl=np.ascontiguousarray(np.vstack([dtab] + [0.6 * dtab[1]] * 5)),
+                poly=np.arange(9, dtype=np.int32), clalp=np.concatenate([b["clalp"], [0.1] * 5]),
+                rcut_l=np.array([0.8 * rc] + [rc] * 3 + [0.9 * rc] * 5))
+
+
+@pytest.mark.parametrize("lmx", [1, 9])
+@pytest.mark.parametrize("prec", [QX_PREC_FP64, QX_PREC_MIXED])
+def test_build_kb_r_s_or_spd_channels_match_oracle(si8, si8_psi, prec, lmx):
+    """lmx other than 4 (the reference's lmx(it): 1 for s only, 9 for s, p,
+    d): the device tables against the oracle's setnlc, real-space H|psi>
+    against the oracle's calnlc through the builder and through host tables
+    (qx_set_kb_r), and the real-space KB forces against the restated
+    fnnlcl2."""
+    need_gpu()
+    b = _with_channels(cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp), lmx)
+    nat = si8.cell.natom
+    satm = _moved(b["satm"], 11)
+    roff, rmesh, rvnl, rdvnl = tables.setnlc(b, b["ityp"], satm, grad=True)
+    assert rvnl.shape[1] == lmx
+    sr = _kbr_system(si8, roff, rmesh, rvnl, b)
+    href = oracle.Ham(sr, QX_NL_RSPACE).hpsi(si8_psi)
+    ctx = Context(si8, prec, QX_NL_RSPACE)
+    try:
+        ctx.set_kb_r_builder(b)
+        ctx.build_kb_r(b["ityp"], satm)
+        off, mesh, vnl = ctx.get_kb_r(nat)
+        assert np.array_equal(off, roff) and np.array_equal(mesh, rmesh)
+        assert np.max(np.abs(vnl - rvnl)) / np.max(np.abs(rvnl)) < TAB_TOL[prec]
+        ctx.put_psi(si8_psi)
+        ctx.enonloc()
+        assert relerr(ctx.get_hpsi(), href) < H_TOL[prec]
+        f = ctx.forces_nl_r()
+    finally:
+        ctx.close()
+    psir = np.array([oracle.wvg2r(si8.gs, c) for c in si8_psi])
+    ref = oforces.fnl_r(roff, rmesh, rvnl, rdvnl, b["clalp"], b["rdelv"], si8.gs.rvol, psir, si8.occ[:si8_psi.shape[0]])
+    assert np.max(np.abs(f - ref)) / np.max(np.abs(ref)) < (1e-10 if prec == QX_PREC_FP64 else 1e-4)
+    ctx = Context(sr, prec, QX_NL_RSPACE)   # the same tables uploaded from the host
+    try:
+        ctx.put_psi(si8_psi)
+        ctx.enonloc()
+        assert relerr(ctx.get_hpsi(), href) < H_TOL[prec]
+    finally:
+        ctx.close()
+
+
 def test_channel_radii_rejected_beyond_species_radius(si8):
     need_gpu()
     b = cell.kbr_builder_tables(si8.gs, si8.cell, si8.pp)
