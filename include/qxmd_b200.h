@@ -252,6 +252,19 @@ int qx_scf_mixing(qx_ctx *ctx, int itratn, double cmetric);
  * Pulay history). */
 int qx_scf_rho_from_psi(qx_ctx *ctx);
 int qx_scf_iteration(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out);
+/* One SCF iteration on host arrays, for a host program that keeps gdcr on
+ * the host between iterations (pwlda_md's loop, S/pwlda.f90:1628-3700):
+ * psi_in (nplwex x nband, real*8) is uploaded while the iteration builds
+ * the potential from the density, which does not need it (null: keep the
+ * device wavefunctions), H|psi> waits for it, and the results are read back
+ * as soon as each is final, on a stream of their own: psi_out after
+ * schmidt2, while the density and the mixing still run; rho_out (kfft0, the
+ * output density of softchg) after softchg; eig_out (nband) at the end.  Any
+ * pointer may be null; page-locked host buffers let the copies overlap the
+ * iteration (pageable ones still work, synchronously).  psi_in and psi_out
+ * may be the same buffer.  Returns when every copy has landed. */
+int qx_scf_iteration_host(qx_ctx *ctx, const qx_cgparm *p, qx_scf_out *out, const double *psi_in, double *psi_out,
+                          double *rho_out, double *eig_out);
 /* The same iteration in two halves, for many cells at once: qx_scf_launch
  * enqueues it on the context's stream (graph replay, nothing waits);
  * qx_scf_result waits for that stream and reads the results.  Launching every

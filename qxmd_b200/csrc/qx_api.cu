@@ -111,6 +111,14 @@ struct qx_ctx {
   // FFT pipeline (fork / join events; captured as parallel graph branches)
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // host I/O of qx_scf_iteration_host: psi and rho are read back on io_st as
+  // soon as the iteration has made them final (events recorded inside it,
+  // captured as event-record nodes of the iteration graph)
+  cudaStream_t io_st = nullptr;
+  cudaEvent_t ev_psi_final = nullptr, ev_rho_final = nullptr;
+  cudaEvent_t ev_psi_in = nullptr;   // psi uploaded on io_st; the iteration waits for it before H|psi>
+  double *d_io = nullptr;
+  long io_len = 0;
   cudaGraph_t seq_graph = nullptr;
   cudaGraphExec_t seq_exec = nullptr;
   std::vector<char> seq_key;
@@ -577,6 +585,15 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
     TRY(upload_tw<double>(c));
     set_fft_smem_limits<double>(227 * 1024);
   }
+  // read-back stream and the events the iteration records for it
+  if (cudaStreamCreateWithFlags(&c->io_st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_psi_final, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_rho_final, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_psi_in, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("qx_create: stream or event creation failed");
+    qx_destroy(c);
+    return QX_ERR_CUDA;
+  }
   if (cudaGetLastError() != cudaSuccess) { set_error("qx_create: CUDA error during set-up"); qx_destroy(c); return QX_ERR_CUDA; }
 #undef FAIL
   *out = c;
@@ -594,6 +611,10 @@ extern "C" int qx_destroy(qx_ctx *c) {
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->io_st) cudaStreamDestroy(c->io_st);
+  if (c->ev_psi_final) cudaEventDestroy(c->ev_psi_final);
+  if (c->ev_rho_final) cudaEventDestroy(c->ev_rho_final);
+  if (c->ev_psi_in) cudaEventDestroy(c->ev_psi_in);
   for (void *p : c->allocs) cudaFree(p);
   delete c;
   return QX_OK;
@@ -1802,12 +1823,39 @@ static int scf_mix(qx_ctx *c) {
   return 0;
 }
 
+// Records ev on the iteration's stream; under capture as an event-record
+// node of the graph, so that each launch of the graph records it.
+static int mark_final(qx_ctx *c, cudaEvent_t ev) {
+  if (!ev) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->st, &cs));
+  if (cs == cudaStreamCaptureStatusActive)
+    CK(cudaEventRecordWithFlags(ev, c->st, cudaEventRecordExternal));
+  else
+    CK(cudaEventRecord(ev, c->st));
+  return 0;
+}
+
 // One SCF iteration in pwlda_md order with every status and summary left on
 // the device (c->defer): no host round trip between the first kernel and the
 // final read.
+// Makes the iteration's stream wait for ev (under capture an event-wait node
+// of the graph, so that each launch waits for the event's latest record).
+static int wait_mark(qx_ctx *c, cudaEvent_t ev) {
+  if (!ev) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->st, &cs));
+  if (cs == cudaStreamCaptureStatusActive)
+    CK(cudaStreamWaitEvent(c->st, ev, cudaEventWaitExternal));
+  else
+    CK(cudaStreamWaitEvent(c->st, ev, 0));
+  return 0;
+}
+
 template <typename T>
 static int scf_body(qx_ctx *c, const qx_cgparm *p) {
   TRY(scf_potential(c));
+  TRY(wait_mark(c, c->ev_psi_in));   // psi from the host, when qx_scf_iteration_host sent one
   TRY(qx_enonloc(c));
   TRY(qx_hmatrix(c, nullptr));
   TRY(gradres_impl<T>(c, nullptr, nullptr, nullptr));
@@ -1817,7 +1865,9 @@ static int scf_body(qx_ctx *c, const qx_cgparm *p) {
   CKL();
   TRY(qx_eigen(c, p, nullptr, nullptr));
   TRY(qx_schmidt(c));
+  TRY(mark_final(c, c->ev_psi_final));   // psi final: the read-back may start
   TRY(qx_softchg(c));
+  TRY(mark_final(c, c->ev_rho_final));   // rho_out final
   TRY(scf_mix(c));
   return 0;
 }
@@ -1937,6 +1987,54 @@ extern "C" int qx_scf_result(qx_ctx *c, qx_scf_out *out) {
 extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) {
   TRY(qx_scf_launch(c, p));
   return qx_scf_result(c, out);
+}
+
+extern "C" int qx_scf_iteration_host(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out, const double *psi_in,
+                                     double *psi_out, double *rho_out, double *eig_out) {
+  if (!c || !p) return QX_ERR_ARG;
+  const long n = (long)c->nb * c->ne;
+  if ((psi_out || psi_in) && c->prec != QX_PREC_FP64 && c->io_len < n) {   // sized before the launch
+    TRY(dregrow(c, &c->d_io, sizeof(double) * n));
+    c->io_len = n;
+  }
+  if (rho_out && !c->d_rho_out) { set_error("qx_scf_iteration_host: no density (qx_scf_init)"); return QX_ERR_STATE; }
+  if (psi_in) {
+    // upload on io_st while the iteration builds the potential, which does
+    // not read psi; the iteration waits for ev_psi_in before H|psi>.  io_st
+    // first waits for everything already on the context's stream (psi's
+    // previous readers).
+    CK(cudaEventRecord(c->ev_psi_in, c->st));
+    CK(cudaStreamWaitEvent(c->io_st, c->ev_psi_in, 0));
+    if (c->prec == QX_PREC_FP64) {
+      CK(cudaMemcpyAsync(c->psi, psi_in, sizeof(double) * n, cudaMemcpyHostToDevice, c->io_st));
+    } else {
+      CK(cudaMemcpyAsync(c->d_io, psi_in, sizeof(double) * n, cudaMemcpyHostToDevice, c->io_st));
+      convert<double, float>(c->d_io, (float *)c->psi, n, c->io_st);
+      CKL();
+    }
+    CK(cudaEventRecord(c->ev_psi_in, c->io_st));
+  }
+  TRY(qx_scf_launch(c, p));
+  if (psi_out) {
+    CK(cudaStreamWaitEvent(c->io_st, c->ev_psi_final, 0));
+    if (c->prec == QX_PREC_FP64) {
+      CK(cudaMemcpyAsync(psi_out, c->psi, sizeof(double) * n, cudaMemcpyDeviceToHost, c->io_st));
+    } else {
+      convert<float, double>((const float *)c->psi, c->d_io, n, c->io_st);
+      CKL();
+      CK(cudaMemcpyAsync(psi_out, c->d_io, sizeof(double) * n, cudaMemcpyDeviceToHost, c->io_st));
+    }
+  }
+  if (rho_out) {
+    CK(cudaStreamWaitEvent(c->io_st, c->ev_rho_final, 0));
+    CK(cudaMemcpyAsync(rho_out, c->d_rho_out, sizeof(double) * c->pl.n, cudaMemcpyDeviceToHost, c->io_st));
+  }
+  if (eig_out) CK(cudaMemcpyAsync(eig_out, c->d_eig, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+  const int r = qx_scf_result(c, out);
+  const cudaError_t e = cudaStreamSynchronize(c->io_st);
+  if (r) return r;
+  if (e != cudaSuccess) { set_error("qx_scf_iteration_host: read-back: %s", cudaGetErrorString(e)); return QX_ERR_CUDA; }
+  return QX_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -33,7 +33,7 @@ EXPORTS = [
     "qx_untryhc", "qx_eigen", "qx_hmatrix_static", "qx_schmidt", "qx_softchg", "qx_scf_init", "qx_scf_mixing", "qx_set_force_tables", "qx_forces",
     "qx_tddft_store", "qx_tddft_overlap", "qx_autotune", "qx_refine_from", "qx_scf_launch", "qx_scf_result",
     "qxgpu_kbnlpp_frc2",
-    "qx_scf_rho_from_psi", "qx_scf_iteration", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
+    "qx_scf_rho_from_psi", "qx_scf_iteration", "qx_scf_iteration_host", "qxgpu_hcnonloc", "qxgpu_hckbpp_g", "qxgpu_enonloc", "qxgpu_eigen",
     "qxgpu_schmidt", "qxgpu_hmatrix", "qxgpu_untryt", "qxgpu_softchg", "qxgpu_rfft3",
     "qx_fssh_init", "qx_fssh_step", "qx_fssh_state", "qx_build_vloc", "qx_gemm_fallbacks",
 ]
@@ -148,6 +148,7 @@ def lib(build_if_missing: bool = True):
         "qxgpu_kbnlpp_frc2": ([_ctx, _dp, _dp], C.c_int),
         "qx_scf_rho_from_psi": ([_ctx], C.c_int),
         "qx_scf_iteration": ([_ctx, C.POINTER(CgParm), C.POINTER(ScfOut)], C.c_int),
+        "qx_scf_iteration_host": ([_ctx, C.POINTER(CgParm), C.POINTER(ScfOut), _vp, _vp, _vp, _vp], C.c_int),
         "qxgpu_hcnonloc": ([_ctx, _dp, _dp, C.c_int], C.c_int),
         "qxgpu_hckbpp_g": ([_ctx, _dp, _dp, C.c_int], C.c_int),
         "qxgpu_enonloc": ([_ctx, _dp, _dp, _vp], C.c_int),
@@ -497,6 +498,22 @@ class Context:
     def scf_iteration(self, parm: CgParm) -> dict:
         out = ScfOut()
         _ck(self.L.qx_scf_iteration(self.h, C.byref(parm), C.byref(out)), "qx_scf_iteration")
+        return out.asdict()
+
+    def scf_iteration_host(self, parm: CgParm, psi_in=None, psi_out=None, rho_out=None, eig_out=None) -> dict:
+        """qx_scf_iteration_host on host float64 arrays (C-contiguous; the
+        outputs are written in place; None skips one)."""
+        def ptr(a, n, out):
+            if a is None:
+                return None
+            assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.size == n
+            assert not out or a.flags["WRITEABLE"]
+            return a.ctypes.data
+        n = self.nb * self.sys.gs.nplwex
+        out = ScfOut()
+        _ck(self.L.qx_scf_iteration_host(self.h, C.byref(parm), C.byref(out), ptr(psi_in, n, False),
+                                         ptr(psi_out, n, True), ptr(rho_out, self.sys.gs.kfft0, True),
+                                         ptr(eig_out, self.nb, True)), "qx_scf_iteration_host")
         return out.asdict()
 
     # -- drop-in shims (host arrays) ----------------------------------------

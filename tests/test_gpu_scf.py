@@ -93,6 +93,55 @@ def test_scf_graph_replay_matches_stream_launches(si8, si8_psi, monkeypatch):
         np.testing.assert_array_equal(ra, rb)
 
 
+@pytest.mark.parametrize("graph", ["1", "0"])
+@pytest.mark.parametrize("prec", [QX_PREC_MIXED, QX_PREC_FP64])
+def test_scf_iteration_host_matches_separate_calls(si8, si8_psi, prec, graph, monkeypatch):
+    """qx_scf_iteration_host (psi in, iteration, psi / rho / eigenvalues read
+    back as soon as each is final, on their own stream) against
+    qx_put_psi + qx_scf_iteration + qx_get_psi / qx_get_rho / qx_get_eig on a
+    twin context from the same state: identical numbers over four iterations,
+    graph replay and plain launches, one buffer for psi in and out, pageable
+    and page-locked host arrays, outputs left out."""
+    need_gpu()
+    import torch
+    monkeypatch.setenv("QX_GRAPH", graph)
+    p = CgParm.defaults(16)
+    ctxs = []
+    for _ in range(2):
+        ctx = Context(si8, prec, QX_NL_GSPACE)
+        ctx.put_psi(si8_psi)
+        ctx.scf_init(mixbeta=0.8, kerker_q0=0.8)
+        ctx.scf_mixing(10, 20.0)
+        ctx.scf_rho_from_psi()
+        ctxs.append(ctx)
+    a, b = ctxs
+    try:
+        nb, ne, n = a.nb, si8.gs.nplwex, si8.gs.kfft0
+        pin = lambda k: torch.empty(k, dtype=torch.float64).pin_memory().numpy()
+        for it in range(4):
+            start = a.get_psi()
+            ra = a.scf_iteration(p)
+            pa, rhoa, ea = a.get_psi(), a.get_rho(), a.get_eig()
+            if it < 2:   # page-locked, psi in and out in one buffer
+                buf, rho, eig = pin(nb * ne), pin(n), pin(nb)
+                buf[:] = start.ravel()
+                rb = b.scf_iteration_host(p, psi_in=buf, psi_out=buf, rho_out=rho, eig_out=eig)
+                pb = buf.reshape(nb, ne)
+            elif it == 2:   # pageable, device psi kept (no psi_in)
+                pb, rho, eig = np.empty((nb, ne)), np.empty(n), np.empty(nb)
+                rb = b.scf_iteration_host(p, psi_out=pb.reshape(-1), rho_out=rho, eig_out=eig)
+            else:           # outputs left out
+                rb = b.scf_iteration_host(p, psi_in=np.ascontiguousarray(start).reshape(-1))
+                pb, rho, eig = b.get_psi(), b.get_rho(), b.get_eig()
+            assert ra["etot"] == rb["etot"] and ra["ncg_hpsi"] == rb["ncg_hpsi"]
+            np.testing.assert_array_equal(pa, pb)
+            np.testing.assert_array_equal(rhoa, rho)
+            np.testing.assert_array_equal(ea, eig)
+    finally:
+        a.close()
+        b.close()
+
+
 def test_autotune_then_refine_to_fp64(si8, si8_psi):
     """The autotuner's choices keep the mixed path's numbers, and the FP64
     refinement sweep (qx_refine_from + 3 FP64 iterations) of a converged
