@@ -90,6 +90,139 @@ __global__ void __launch_bounds__(64, plane_minb(N)) k_plane(PipeParams P, float
 }
 
 // ---------------------------------------------------------------------------
+// The same fused y-x-y pass for longer lines (N = 2H, H a register-FFT length,
+// N > 64), two threads per line: lanes 2l and 2l + 1 of a warp own line l.
+// Backward transforms and the forward y transform by decimation in time:
+// thread h holds the samples x[2j + h], transforms them (H points), and one
+// butterfly exchange with its partner (shfl_xor 1) leaves it the outputs
+// X[k + hH], k < H, at positions out_pos(H, k).  The forward x transform
+// follows the potential multiply, when thread h holds the second half of the
+// line (y[k + hH]), so it runs by decimation in frequency: the exchange
+// stage first (a = y[k] + y[k+H] kept by h = 0, b = (y[k] - y[k+H]) w^k by
+// h = 1), then the H-point transform gives the outputs Y[2j + h].  Whole
+// warps run each phase (lanes without a line work on zeros and store
+// nothing), so every shuffle has its full mask.
+namespace pl2 {
+template <int SIGN, int N>
+__device__ __forceinline__ void dit_combine(float2 (&v)[N / 2], int h) {
+  constexpr int H = N / 2;
+  rf::static_for<0, H>([&](auto kc) {
+    constexpr int k = decltype(kc)::value, pk = rf::out_pos(H, k);
+    const float2 mine = v[pk];
+    float2 other;
+    other.x = __shfl_xor_sync(0xffffffffu, mine.x, 1);
+    other.y = __shfl_xor_sync(0xffffffffu, mine.y, 1);
+    const float2 e = h ? other : mine;
+    const float2 t = rf::twiddle<float, SIGN, k, N>(h ? mine : other);
+    v[pk] = h ? rf::sub(e, t) : rf::add(e, t);
+  });
+}
+// v[out_pos(H, k)] = y[k + hH] in; u[k] (natural order) = a[k] (h = 0) or
+// b[k] (h = 1) out, ready for the H-point transform.
+template <int SIGN, int N>
+__device__ __forceinline__ void dif_split(const float2 (&v)[N / 2], float2 (&u)[N / 2], int h) {
+  constexpr int H = N / 2;
+  rf::static_for<0, H>([&](auto kc) {
+    constexpr int k = decltype(kc)::value, pk = rf::out_pos(H, k);
+    const float2 mine = v[pk];
+    float2 other;
+    other.x = __shfl_xor_sync(0xffffffffu, mine.x, 1);
+    other.y = __shfl_xor_sync(0xffffffffu, mine.y, 1);
+    const float2 lo = h ? other : mine, hi = h ? mine : other;   // y[k], y[k + H]
+    u[k] = h ? rf::twiddle<float, SIGN, k, N>(rf::sub(lo, hi)) : rf::add(lo, hi);
+  });
+}
+}  // namespace pl2
+
+template <int N>
+__global__ void __launch_bounds__(2 * N) k_plane2(PipeParams P, float2 *__restrict__ bufA,
+                                                 const float *__restrict__ vloc) {
+  using rf::out_pos;
+  constexpr int H = N / 2;
+  const int i3 = blockIdx.x;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= (P.npair_dev ? *P.npair_dev : P.npair)) return;
+  const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
+  extern __shared__ float2 T[];   // [N][P1]
+  float2 *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
+  const int t = threadIdx.x, l = t >> 1, h = t & 1;
+  const bool warp_on_cols = (t & ~31) < 2 * P1;   // some lane of this warp owns a column
+  const float2 zero = make_float2(0.f, 0.f);
+
+  // (1) y backward, line = sphere column a = l
+  if (warp_on_cols) {
+    const bool on = l < P1;
+    float2 x[H];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const int i2 = 2 * j + h;
+      const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+      float2 v = zero;
+      if (on && j2 >= 0 && l >= P.row_lo[j2] && l <= P.row_hi[j2]) v = A[j2 * P1 + l];
+      x[j] = v;
+    }
+    rf::fft<float, +1, H>(x);
+    pl2::dit_combine<+1, N>(x, h);
+    if (on) {
+      rf::static_for<0, H>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        T[(k + h * H) * P1 + l] = x[out_pos(H, k)];
+      });
+    }
+  }
+  __syncthreads();
+  // (2) x backward, * V, x forward; line = grid row i2 = l (every thread has one)
+  {
+    float2 x[H];
+    float2 *row = T + l * P1;
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const int i1 = 2 * j + h;
+      float2 v = zero;
+      if (i1 <= m1) v = row[i1 + m1];
+      else if (i1 >= N - m1) v = row[i1 - N + m1];
+      x[j] = v;
+    }
+    rf::fft<float, +1, H>(x);
+    pl2::dit_combine<+1, N>(x, h);
+    const float *V = vloc + ((long)i3 * N + l) * N + h * H;
+    rf::static_for<0, H>([&](auto kc) {
+      constexpr int k = decltype(kc)::value, pk = out_pos(H, k);
+      const float vv = V[k];
+      x[pk] = make_float2(x[pk].x * vv, x[pk].y * vv);
+    });
+    float2 u[H];
+    pl2::dif_split<-1, N>(x, u, h);
+    rf::fft<float, -1, H>(u);
+    __syncthreads();   // every thread has read its row before any row is rewritten
+    rf::static_for<0, H>([&](auto jc) {
+      constexpr int j = decltype(jc)::value;
+      const int i1 = 2 * j + h;
+      if (i1 <= m1) row[i1 + m1] = u[out_pos(H, j)];
+      else if (i1 >= N - m1) row[i1 - N + m1] = u[out_pos(H, j)];
+    });
+  }
+  __syncthreads();
+  // (3) y forward, line = sphere column a = l; only rows inside the sphere are kept
+  if (warp_on_cols) {
+    const bool on = l < P1;
+    float2 x[H];
+#pragma unroll
+    for (int j = 0; j < H; ++j) x[j] = on ? T[(2 * j + h) * P1 + l] : zero;
+    rf::fft<float, -1, H>(x);
+    pl2::dit_combine<-1, N>(x, h);
+    if (on) {
+      rf::static_for<0, H>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        const int i2 = k + h * H;
+        const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+        if (j2 >= 0 && l >= P.row_lo[j2] && l <= P.row_hi[j2]) A[j2 * P1 + l] = x[out_pos(H, k)];
+      });
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The z transforms of the FP32 pipeline, one sphere z-column (j2, a) of one
 // band pair per thread with the whole line in registers (replacing the
 // shared-memory k_zinv / k_zfwd for the specialised lengths).  The column's
@@ -277,6 +410,78 @@ __global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__
   }
 }
 
+// The density pass for the two-threads-a-line lengths (see k_plane2): the
+// y and x backward transforms by decimation in time, thread h of row l then
+// adds the columns k + hH, k < H, of the row to the FP64 accumulation plane.
+template <int N>
+__global__ void __launch_bounds__(2 * N) k_rho_plane2(PipeParams P, const float2 *__restrict__ bufA,
+                                                     const double *__restrict__ wocc, double *__restrict__ part,
+                                                     int npl, int per_group) {
+  using rf::out_pos;
+  constexpr int H = N / 2;
+  const int i3 = blockIdx.x, grp = blockIdx.y;
+  const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
+  extern __shared__ double accs[];            // [N][N] FP64, then the [N][P1] complex tile
+  float2 *T = reinterpret_cast<float2 *>(accs + N * N);
+  const int t = threadIdx.x, l = t >> 1, h = t & 1;
+  const bool warp_on_cols = (t & ~31) < 2 * P1;
+  const float2 zero = make_float2(0.f, 0.f);
+  for (int i = t; i < N * N; i += 2 * N) accs[i] = 0.0;
+  const int np = min(npl, (P.npair_dev ? *P.npair_dev : P.npair) - P.pair0);
+  const int pl0 = grp * per_group, pl1 = min(np, pl0 + per_group);
+  for (int pl = pl0; pl < pl1; ++pl) {
+    const int p = P.pair0 + pl;
+    const float2 *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
+    if (warp_on_cols) {
+      const bool on = l < P1;
+      float2 x[H];
+#pragma unroll
+      for (int j = 0; j < H; ++j) {
+        const int i2 = 2 * j + h;
+        const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+        float2 v = zero;
+        if (on && j2 >= 0 && l >= P.row_lo[j2] && l <= P.row_hi[j2]) v = A[j2 * P1 + l];
+        x[j] = v;
+      }
+      rf::fft<float, +1, H>(x);
+      pl2::dit_combine<+1, N>(x, h);
+      if (on) {
+        rf::static_for<0, H>([&](auto kc) {
+          constexpr int k = decltype(kc)::value;
+          T[(k + h * H) * P1 + l] = x[out_pos(H, k)];
+        });
+      }
+    }
+    __syncthreads();
+    {
+      float2 x[H];
+      const float2 *row = T + l * P1;
+#pragma unroll
+      for (int j = 0; j < H; ++j) {
+        const int i1 = 2 * j + h;
+        float2 v = zero;
+        if (i1 <= m1) v = row[i1 + m1];
+        else if (i1 >= N - m1) v = row[i1 - N + m1];
+        x[j] = v;
+      }
+      rf::fft<float, +1, H>(x);
+      pl2::dit_combine<+1, N>(x, h);
+      const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+      const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
+      double *a = accs + l * N + h * H;
+      rf::static_for<0, H>([&](auto kc) {
+        constexpr int k = decltype(kc)::value, q = out_pos(H, k);
+        const double re = x[q].x, im = x[q].y;
+        a[k] += fa * re * re + fb * im * im;
+      });
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  double *dst = part + ((long)grp * P.k3 + i3) * N * N;
+  for (int i = t; i < N * N; i += 2 * N) dst[i] = accs[i];
+}
+
 // rho = [rho +] sum over groups of part (fixed order).
 // Sum of the RHO_GROUPS partial planes in group order (all loads of an
 // element issued together).
@@ -311,6 +516,26 @@ static int rho_launch(const PipeParams &P, int npl, const float2 *bufA, const do
   return 0;
 }
 
+template <int N>
+static int rho2_launch(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part, double *rho,
+                       int accumulate, cudaStream_t st) {
+  const size_t sm = sizeof(double) * (size_t)N * N + sizeof(float2) * (size_t)N * P.P1;
+  if (sm > 200 * 1024) return -1;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_rho_plane2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const int per_group = (npl + RHO_GROUPS - 1) / RHO_GROUPS;
+  dim3 g(P.k3, RHO_GROUPS);
+  k_rho_plane2<N><<<g, 2 * N, sm, st>>>(P, bufA, wocc, part, npl, per_group);
+  note_launch();
+  const long n = (long)P.k1 * P.k2 * P.k3;
+  k_rho_groups<<<148 * 4, 256, 0, st>>>(part, n, rho, accumulate);
+  note_launch();
+  return 0;
+}
+
 // Density of one chunk of pairs through the plane kernel; -1 if the grid has
 // no specialised length.  part: RHO_GROUPS * kfft0 doubles.
 int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part,
@@ -329,6 +554,7 @@ int launch_rho_plane_f32(const PipeParams &P, int npl, const float2 *bufA, const
     case 54: return rho_launch<54>(P, npl, bufA, wocc, part, rho, accumulate, st);
     case 60: return rho_launch<60>(P, npl, bufA, wocc, part, rho, accumulate, st);
     case 64: return rho_launch<64>(P, npl, bufA, wocc, part, rho, accumulate, st);
+    case 96: return rho2_launch<96>(P, npl, bufA, wocc, part, rho, accumulate, st);
     default: return -1;
   }
 }
@@ -337,6 +563,7 @@ bool plane_length_supported(int k1, int k2) {
   if (k1 != k2) return false;
   switch (k1) {
     case 20: case 24: case 27: case 30: case 32: case 36: case 40: case 45: case 48: case 54: case 60: case 64:
+    case 96:
       return true;
     default:
       return false;
@@ -357,6 +584,21 @@ static int plane_launch(const PipeParams &P, int npl, float2 *bufA, const float 
   return 0;
 }
 
+template <int N>
+static int plane2_launch(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st) {
+  const size_t sm = sizeof(float2) * (size_t)N * P.P1;
+  if (2 * P.P1 > 2 * N || sm > 100 * 1024) return -1;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_plane2<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    attr = true;
+  }
+  dim3 g(P.k3, npl);
+  k_plane2<N><<<g, 2 * N, sm, st>>>(P, bufA, vloc);
+  note_launch();
+  return 0;
+}
+
 // Launch the fused pass if this grid has a specialised length; -1 otherwise.
 int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st) {
   if (P.k1 != P.k2 || P.P1 > P.k1 || P.P2 > P.k2) return -1;
@@ -373,6 +615,7 @@ int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vl
     case 54: return plane_launch<54>(P, npl, bufA, vloc, st);
     case 60: return plane_launch<60>(P, npl, bufA, vloc, st);
     case 64: return plane_launch<64>(P, npl, bufA, vloc, st);
+    case 96: return plane2_launch<96>(P, npl, bufA, vloc, st);
     default: return -1;
   }
 }

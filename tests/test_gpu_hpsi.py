@@ -100,27 +100,36 @@ def test_hpsi_linearity_full_si64():
         assert oracle.dot(x[b], out[1][b]) == pytest.approx(oracle.dot(y[b], out[0][b]), rel=1e-10)
 
 
-@pytest.mark.parametrize("ecutdens,n", [(170.0, 45), (200.0, 48), (235.0, 54), (295.0, 60)])
+@pytest.mark.parametrize("ecutdens,n", [(170.0, 45), (200.0, 48), (235.0, 54), (295.0, 60), (760.0, 96)])
 def test_plane_pass_lengths(monkeypatch, ecutdens, n):
     """The fused FP32 plane pass on the larger specialised lengths (Si8 cells
     whose density cutoff gives an n^3 grid, wave cutoff ecutdens/4 so the
     sphere spans half the grid) against the oracle, and against the separate
-    y/x passes (QX_PLANE=0) on the same input."""
+    y/x passes (QX_PLANE=0) on the same input; the density pass (softchg)
+    the same way.  96 runs the two-threads-a-line kernels."""
     need_gpu()
     s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), ecutdens / 4.0, ecutdens, 4, with_ewald=False)
     assert tuple(s.gs.grid) == (n, n, n)
     c = cell.random_wavefunctions(s.gs.nplwex, 4)
     c /= np.sqrt(np.array([oracle.dot(x, x) for x in c]))[:, None]
-    ref = oracle.Ham(s, QX_NL_GSPACE).hpsi(c)
-    out = {}
+    h = oracle.Ham(s, QX_NL_GSPACE)
+    ref = h.hpsi(c)
+    rref = h.softchg(c, s.occ[:4])
+    out, rho = {}, {}
     for mode in ("1", "0"):
         monkeypatch.setenv("QX_PLANE", mode)
         ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, nband=4)
-        ctx.put_psi(c)
-        ctx.enonloc()
-        out[mode] = ctx.get_hpsi()
+        try:
+            ctx.put_psi(c)
+            ctx.enonloc()
+            out[mode] = ctx.get_hpsi()
+            rho[mode] = ctx.softchg_host(c)
+        finally:
+            ctx.close()
         assert relerr(out[mode], ref) < TOL[QX_PREC_MIXED]
+        assert relerr(rho[mode], rref) < TOL[QX_PREC_MIXED]
     assert relerr(out["1"], out["0"]) < TOL[QX_PREC_MIXED]
+    assert relerr(rho["1"], rho["0"]) < TOL[QX_PREC_MIXED]
 
 
 @pytest.mark.parametrize("plan", ["2x3x4", "3x8", "4x6", "6x4", "8x3", "2x2x2x3", "3x2x2x2"])
