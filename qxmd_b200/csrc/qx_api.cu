@@ -117,6 +117,9 @@ struct qx_ctx {
   cudaStream_t io_st = nullptr;
   cudaEvent_t ev_psi_final = nullptr, ev_rho_final = nullptr;
   cudaEvent_t ev_psi_in = nullptr;   // psi uploaded on io_st; the iteration waits for it before H|psi>
+  // set by the first qx_scf_iteration_host: only then do the iteration's
+  // graphs carry the event nodes (they slow the replay of many small graphs)
+  bool host_io = false;
   double *d_io = nullptr;
   long io_len = 0;
   cudaGraph_t seq_graph = nullptr;
@@ -1826,7 +1829,7 @@ static int scf_mix(qx_ctx *c) {
 // Records ev on the iteration's stream; under capture as an event-record
 // node of the graph, so that each launch of the graph records it.
 static int mark_final(qx_ctx *c, cudaEvent_t ev) {
-  if (!ev) return 0;
+  if (!ev || !c->host_io) return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(c->st, &cs));
   if (cs == cudaStreamCaptureStatusActive)
@@ -1842,7 +1845,7 @@ static int mark_final(qx_ctx *c, cudaEvent_t ev) {
 // Makes the iteration's stream wait for ev (under capture an event-wait node
 // of the graph, so that each launch waits for the event's latest record).
 static int wait_mark(qx_ctx *c, cudaEvent_t ev) {
-  if (!ev) return 0;
+  if (!ev || !c->host_io) return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(c->st, &cs));
   if (cs == cudaStreamCaptureStatusActive)
@@ -1885,7 +1888,7 @@ static bool scf_graphs_enabled() {
 template <typename T>
 static int scf_graph_launch(qx_ctx *c, const qx_cgparm *p) {
   const void *keyp[] = {c->psi, c->hpsi, c->tmp};
-  const int keyi[] = {c->pulay_reset ? 1 : 0, c->itratn, c->nlmode};
+  const int keyi[] = {c->pulay_reset ? 1 : 0, c->itratn, c->nlmode, c->host_io ? 1 : 0};
   std::vector<char> key(sizeof(keyp) + sizeof(keyi) + sizeof(qx_cgparm));
   memcpy(key.data(), keyp, sizeof(keyp));
   memcpy(key.data() + sizeof(keyp), keyi, sizeof(keyi));
@@ -1992,6 +1995,7 @@ extern "C" int qx_scf_iteration(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out) 
 extern "C" int qx_scf_iteration_host(qx_ctx *c, const qx_cgparm *p, qx_scf_out *out, const double *psi_in,
                                      double *psi_out, double *rho_out, double *eig_out) {
   if (!c || !p) return QX_ERR_ARG;
+  c->host_io = true;   // the iteration records and waits for the I/O events from now on
   const long n = (long)c->nb * c->ne;
   if ((psi_out || psi_in) && c->prec != QX_PREC_FP64 && c->io_len < n) {   // sized before the launch
     TRY(dregrow(c, &c->d_io, sizeof(double) * n));
