@@ -298,6 +298,59 @@ __global__ void __launch_bounds__(ZC_T) k_zcols_fwd(PipeParams P, const float2 *
   });
 }
 
+// The inverse z pass for the two-lanes-a-line lengths (N = 2H > 64): lanes
+// 2c and 2c + 1 own sphere z-column c, each gathers the coefficients of the
+// even or odd i3 and transforms them (H points), and the butterfly exchange
+// of k_plane2 completes the N-point transform.  Whole warps run (lanes past
+// the last column work on zeros and store nothing).
+template <int N>
+__global__ void __launch_bounds__(ZC_T) k_zcols_inv2(PipeParams P, const float *__restrict__ cin, long ldc,
+                                                      float2 *__restrict__ bufA) {
+  using rf::out_pos;
+  constexpr int H = N / 2;
+  const int q = (int)((blockIdx.x * ZC_T + threadIdx.x) >> 1), h = threadIdx.x & 1;
+  const int pl = blockIdx.y, p = P.pair0 + pl;
+  if (p >= (P.npair_dev ? *P.npair_dev : P.npair)) return;   // uniform in the block
+  const bool on = q < P.ncol;
+  const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+  const float *cA = cin + (long)bA * ldc;
+  const float *cB = bB >= 0 ? cin + (long)bB * ldc : nullptr;
+  float2 x[H];
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const int i3 = 2 * j + h;
+    const int code = on ? P.col_ig[i3 * P.ncol + q] : 0;
+    float2 z = make_float2(0.f, 0.f);
+    if (code != 0) {
+      const int ig = (code > 0 ? code : -code) - 1;
+      const float ra = cA[2 * ig], ia = ig ? cA[2 * ig + 1] : 0.f;
+      const float rb = cB ? cB[2 * ig] : 0.f, ib = (cB && ig) ? cB[2 * ig + 1] : 0.f;
+      if (code > 0) { z.x = ra - ib; z.y = ia + rb; }
+      else          { z.x = ra + ib; z.y = rb - ia; }
+    }
+    x[j] = z;
+  }
+  rf::fft<float, +1, H>(x);
+  pl2::dit_combine<+1, N>(x, h);
+  if (on) {
+    float2 *dst = bufA + (long)pl * N * P.P2 * P.P1 + P.col_ja[q];
+    rf::static_for<0, H>([&](auto kc) {
+      constexpr int k = decltype(kc)::value;
+      dst[(long)(k + h * H) * P.P2 * P.P1] = x[out_pos(H, k)];
+    });
+  }
+}
+
+template <int N>
+static int zcols2_launch(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, bool inv,
+                         cudaStream_t st) {
+  if (!inv) return -1;   // the forward z pass stays on the shared-memory kernel
+  dim3 g((2 * P.ncol + ZC_T - 1) / ZC_T, npl);
+  k_zcols_inv2<N><<<g, ZC_T, 0, st>>>(P, cin, ldc, bufA);
+  note_launch();
+  return 0;
+}
+
 template <int N>
 static int zcols_launch(const PipeParams &P, int npl, const float *cin, long ldc, float2 *bufA, const float2 *src,
                         float2 *zsph, bool inv, cudaStream_t st) {
@@ -330,6 +383,7 @@ static int zcols_dispatch(const PipeParams &P, int npl, const float *cin, long l
     case 54: return zcols_launch<54>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
     case 60: return zcols_launch<60>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
     case 64: return zcols_launch<64>(P, npl, cin, ldc, bufA, src, zsph, inv, st);
+    case 96: return zcols2_launch<96>(P, npl, cin, ldc, bufA, inv, st);
     default: return -1;
   }
 }

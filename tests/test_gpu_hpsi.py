@@ -105,8 +105,9 @@ def test_plane_pass_lengths(monkeypatch, ecutdens, n):
     """The fused FP32 plane pass on the larger specialised lengths (Si8 cells
     whose density cutoff gives an n^3 grid, wave cutoff ecutdens/4 so the
     sphere spans half the grid) against the oracle, and against the separate
-    y/x passes (QX_PLANE=0) on the same input; the density pass (softchg)
-    the same way.  96 runs the two-threads-a-line kernels."""
+    y/x passes and shared-memory z passes (QX_PLANE=0, QX_ZCOLS=0) on the
+    same input; the density pass (softchg) the same way.  96 runs the
+    two-threads-a-line kernels (plane, density and inverse z passes)."""
     need_gpu()
     s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), ecutdens / 4.0, ecutdens, 4, with_ewald=False)
     assert tuple(s.gs.grid) == (n, n, n)
@@ -118,6 +119,7 @@ def test_plane_pass_lengths(monkeypatch, ecutdens, n):
     out, rho = {}, {}
     for mode in ("1", "0"):
         monkeypatch.setenv("QX_PLANE", mode)
+        monkeypatch.setenv("QX_ZCOLS", mode)
         ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, nband=4)
         try:
             ctx.put_psi(c)
