@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--profile-step", action="store_true",
                     help="only the mixed-precision SCF iterations (warm-up, then --steps), no L2 flush, "
                          "no extra arms: the launch sequence profiled under ncu")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="W + K steps of the 48-cell batch and nothing else, printing launch counts for an ncu "
+                         "launch list")
     ap.add_argument("--si512", action="store_true",
                     help="only H|psi> band applications/s on the Si512 cell (1100 bands, 96^3 grid), mixed and FP64")
     ap.add_argument("--sequential", action="store_true",
@@ -292,6 +295,51 @@ def run_profile_step(args):
     print(json.dumps({"profile_step": True, "launches_before": n0, "launches_per_step": (launch_count() - n0) / max(1, args.steps),
                       "wall_ms_per_step": 1e3 * dt / max(1, args.steps), "etot": out["etot"]}), flush=True)
     ctx.close()
+
+
+def run_profile_batch(args):
+    """W + K steps of the 48-cell batch of run_batch (mixed precision, one
+    context and stream per cell, every cell's iteration enqueued before any is
+    read) and nothing else, printing the library's launch counts so that an
+    ncu launch list can skip the set-up and warm-up (-s) and take exactly the
+    timed steps (-c)."""
+    import torch
+
+    from qxmd_b200 import cell
+    from qxmd_b200.lib import CgParm, Context, QX_NL_GSPACE, QX_PREC_MIXED, launch_count
+    torch.cuda.set_device(0)
+    cells = [cell.batch_cell(i) for i in range(48)]
+    streams = [torch.cuda.Stream() for _ in cells]
+    ctxs, parms = [], []
+    for s, st in zip(cells, streams):
+        ctx = Context(s, QX_PREC_MIXED, QX_NL_GSPACE, stream=st.cuda_stream)
+        ctx.put_psi(cell.random_wavefunctions(s.gs.nplwex, s.nband))
+        ctx.schmidt()
+        ctx.scf_init(mixbeta=PULAY_ASLH, kerker_q0=PULAY_Q0)
+        ctx.scf_mixing(PULAY_ITRATN, PULAY_CMETRIC)
+        ctx.scf_rho_from_psi()
+        ctxs.append(ctx)
+        parms.append(CgParm.defaults(int(s.cell.nel // 2)))
+
+    def step():
+        for ctx, p in zip(ctxs, parms):
+            ctx.scf_launch(p)
+        return [ctx.scf_result() for ctx in ctxs]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    n0 = launch_count()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t
+    print(json.dumps({"profile_batch": True, "launches_before": n0,
+                      "launches_per_step": (launch_count() - n0) / max(1, args.steps),
+                      "wall_ms_per_step": 1e3 * dt / max(1, args.steps)}), flush=True)
+    for ctx in ctxs:
+        ctx.close()
 
 
 def run_profile_hpsi(args):
@@ -1029,6 +1077,8 @@ def main():
         run_profile_step(args)
     elif args.profile_hpsi:
         run_profile_hpsi(args)
+    elif args.profile_batch:
+        run_profile_batch(args)
     elif args.si512:
         run_si512(args)
     else:
