@@ -488,9 +488,22 @@ static int launch_dgemm(int M, int N, int K, double alpha, const double *A, long
                                            ws_bytes, st);
 }
 
+// FP32 contractions below this many flops (2 M N K) run on the CUDA-core
+// kernel: the tensor-core kernel's fixed cost per CTA (TMEM allocation,
+// barriers, pipeline fill, a TMEM drain per k-block) outweighs their work.
+// Measured on the 48-cell batch (all its contractions below 0.2 GFLOP) and
+// on Si64 (every contraction 0.48 GFLOP or more).  QX_TC_MIN_FLOPS overrides
+// it (read at every call).
+constexpr double TC_MIN_FLOPS_DEFAULT = 2.0e8;
+static double tc_min_flops() {
+  const char *e = getenv("QX_TC_MIN_FLOPS");
+  return e ? atof(e) : TC_MIN_FLOPS_DEFAULT;
+}
+
 // FP32 contractions that ran on the CUDA-core kernel instead of the tensor
 // cores (a column map, a device column count or operands outside the TMA
-// rules), counted for qx_gemm_fallbacks().
+// rules; not the small ones sent there by tc_min_flops), counted for
+// qx_gemm_fallbacks().
 static std::atomic<long> g_fp32_fallbacks{0};
 long fp32_gemm_fallbacks() { return g_fp32_fallbacks.load(); }
 void fp32_gemm_fallbacks_add(long n) { g_fp32_fallbacks.fetch_add(n); }
@@ -500,9 +513,11 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes,
          const T *rowscale, void *pad, size_t pad_bytes) {
   if (M <= 0 || N <= 0) return 0;
-  if (sizeof(T) == sizeof(float) && K > 0 && (colmap || ncol_dev || !tc_enabled())) ++g_fp32_fallbacks;
+  // small FP32 contractions run on the CUDA-core kernel by choice (not counted)
+  const bool small = sizeof(T) == sizeof(float) && 2.0 * (double)M * (double)N * (double)K < tc_min_flops();
+  if (sizeof(T) == sizeof(float) && K > 0 && !small && (colmap || ncol_dev || !tc_enabled())) ++g_fp32_fallbacks;
   if (rowscale && beta != (T)0) { set_error("gemm: a row scale needs beta = 0"); return 1; }
-  if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0) {
+  if (sizeof(T) == sizeof(float) && !colmap && !ncol_dev && K > 0 && !small) {
     const int r = tc_gemm(ta, tb, M, N, K, (float)alpha, (const float *)A, lda, (const float *)B, ldb, (float)beta,
                           (float *)C, ldc, gamma, st, ws, ws_bytes, (const float *)rowscale, pad, pad_bytes);
     if (r == 0) return 0;

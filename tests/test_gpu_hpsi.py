@@ -14,6 +14,18 @@ from qxmd_b200.lib import (Context, QX_NL_GSPACE, QX_NL_NONE, QX_NL_RSPACE, QX_P
 from gpu_util import need_gpu, relerr
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True, params=["size_threshold", "tensor_cores"])
+def fp32_contraction_path(request, monkeypatch):
+    """Every test here twice: FP32 contractions below QX_TC_MIN_FLOPS on the
+    CUDA-core kernel (the default, which sends this module's Si8 shapes
+    there), and all of them on the tensor cores (threshold 0)."""
+    if request.param == "tensor_cores":
+        monkeypatch.setenv("QX_TC_MIN_FLOPS", "0")
+    else:
+        monkeypatch.delenv("QX_TC_MIN_FLOPS", raising=False)
+    return request.param
 TOL = {QX_PREC_FP64: 1e-11, QX_PREC_MIXED: 2e-5}
 
 
