@@ -19,72 +19,89 @@ namespace qx {
 // where that needs no spills.
 constexpr int plane_minb(int n) { return n <= 54 ? 8 : 1; }
 
-template <int N>
+// QX_PLANE_PAIRS=0 keeps one z plane a CTA (read at every call).
+static bool plane_pairs_enabled() {
+  const char *e = getenv("QX_PLANE_PAIRS");
+  return !(e && e[0] == '0');
+}
+
+
+template <int N, int PL>
 __global__ void __launch_bounds__(64, plane_minb(N)) k_plane(PipeParams P, float2 *__restrict__ bufA, const float *__restrict__ vloc) {
   using rf::out_pos;
-  const int i3 = blockIdx.x;
+  // PL = 2: the CTA takes planes i3 and i3 + 1; the y phases give warp w the
+  // columns of plane w (P1 <= 32), the x phase runs the two planes' rows in
+  // turn.  PL = 1: one plane, the columns on threads 0 .. P1 - 1.
+  const int i3b = blockIdx.x * PL;
   const int pl = blockIdx.y, p = P.pair0 + pl;
   if (p >= (P.npair_dev ? *P.npair_dev : P.npair)) return;
   const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
-  extern __shared__ float2 T[];   // [N][P1]
-  float2 *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
+  const int npl_here = min(PL, P.k3 - i3b);   // planes this CTA owns (uniform)
+  extern __shared__ float2 T[];   // [PL][N][P1]
   const int t = threadIdx.x;
   const float2 zero = make_float2(0.f, 0.f);
+  // column phases: plane and column of this thread
+  const int cpl = (PL == 2) ? (t >> 5) : 0, col = (PL == 2) ? (t & 31) : t;
+  const bool col_on = col < P1 && cpl < npl_here;
+  float2 *A = bufA + ((long)pl * P.k3 + i3b + cpl) * P2 * P1;
+  float2 *Tc = T + (long)cpl * N * P1;
 
-  // (1) y backward, thread = sphere column a
-  if (t < P1) {
+  // (1) y backward, thread = sphere column a of its plane
+  if (col_on) {
     float2 x[N];
 #pragma unroll
     for (int i2 = 0; i2 < N; ++i2) {
       const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
       float2 v = zero;
-      if (j2 >= 0 && t >= P.row_lo[j2] && t <= P.row_hi[j2]) v = A[j2 * P1 + t];
+      if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) v = A[j2 * P1 + col];
       x[i2] = v;
     }
     rf::fft<float, +1, N>(x);
     rf::static_for<0, N>([&](auto ic) {
       constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
-      T[i2 * P1 + t] = x[q];
+      Tc[i2 * P1 + col] = x[q];
     });
   }
   __syncthreads();
-  // (2) x backward, * V, x forward; thread = grid row i2
-  if (t < N) {
-    float2 x[N];
-    float2 *row = T + t * P1;
+  // (2) x backward, * V, x forward; thread = grid row i2, plane after plane
+  for (int rp = 0; rp < npl_here; ++rp) {
+    if (t < N) {
+      float2 x[N];
+      float2 *row = T + ((long)rp * N + t) * P1;
 #pragma unroll
-    for (int i1 = 0; i1 < N; ++i1) {
-      float2 v = zero;
-      if (i1 <= m1) v = row[i1 + m1];
-      else if (i1 >= N - m1) v = row[i1 - N + m1];
-      x[i1] = v;
+      for (int i1 = 0; i1 < N; ++i1) {
+        float2 v = zero;
+        if (i1 <= m1) v = row[i1 + m1];
+        else if (i1 >= N - m1) v = row[i1 - N + m1];
+        x[i1] = v;
+      }
+      rf::fft<float, +1, N>(x);
+      const float *V = vloc + ((long)(i3b + rp) * N + t) * N;
+      float2 y[N];
+      rf::static_for<0, N>([&](auto ic) {
+        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+        const float vv = V[i1];
+        y[i1] = make_float2(x[q].x * vv, x[q].y * vv);
+      });
+      rf::fft<float, -1, N>(y);
+      rf::static_for<0, N>([&](auto ic) {
+        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+        if (i1 <= m1) row[i1 + m1] = y[q];
+        else if (i1 >= N - m1) row[i1 - N + m1] = y[q];
+      });
     }
-    rf::fft<float, +1, N>(x);
-    const float *V = vloc + ((long)i3 * N + t) * N;
-    float2 y[N];
-    rf::static_for<0, N>([&](auto ic) {
-      constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
-      const float vv = V[i1];
-      y[i1] = make_float2(x[q].x * vv, x[q].y * vv);
-    });
-    rf::fft<float, -1, N>(y);
-    rf::static_for<0, N>([&](auto ic) {
-      constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
-      if (i1 <= m1) row[i1 + m1] = y[q];
-      else if (i1 >= N - m1) row[i1 - N + m1] = y[q];
-    });
   }
   __syncthreads();
-  // (3) y forward, thread = sphere column a; only rows inside the sphere are kept
-  if (t < P1) {
+  // (3) y forward, thread = sphere column a of its plane; only rows inside the sphere are kept
+  if (col_on) {
     float2 x[N];
 #pragma unroll
-    for (int i2 = 0; i2 < N; ++i2) x[i2] = T[i2 * P1 + t];
+    for (int i2 = 0; i2 < N; ++i2) x[i2] = Tc[i2 * P1 + col];
     rf::fft<float, -1, N>(x);
     rf::static_for<0, N>([&](auto ic) {
       constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
       const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
-      if (j2 >= 0 && t >= P.row_lo[j2] && t <= P.row_hi[j2]) A[j2 * P1 + t] = x[q];
+      if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) A[j2 * P1 + col] = x[q];
     });
   }
 }
@@ -402,65 +419,73 @@ int launch_zcols_fwd_f32(const PipeParams &P, int npl, const float2 *bufA, float
 // owns one grid row).  The group's partial plane goes to part[group]; a
 // second kernel sums the groups in a fixed order, so the result is the same
 // from run to run.
-template <int N>
+template <int N, int PL>
 __global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__restrict__ bufA,
                                                   const double *__restrict__ wocc, double *__restrict__ part,
                                                   int npl, int per_group) {
   using rf::out_pos;
-  const int i3 = blockIdx.x, grp = blockIdx.y;
+  // PL = 2: planes i3 and i3 + 1, warp w taking plane w's columns in the y
+  // phase (P1 <= 32), the rows of the two planes in turn in the x phase.
+  const int i3b = blockIdx.x * PL, grp = blockIdx.y;
   const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
-  extern __shared__ double accs[];            // [N][N] FP64, then the [N][P1] complex tile
-  float2 *T = reinterpret_cast<float2 *>(accs + N * N);
+  const int npl_here = min(PL, P.k3 - i3b);
+  extern __shared__ double accs[];            // [PL][N][N] FP64, then the [PL][N][P1] complex tiles
+  float2 *T = reinterpret_cast<float2 *>(accs + PL * N * N);
   const int t = threadIdx.x;
   const float2 zero = make_float2(0.f, 0.f);
-  if (t < N)
-    for (int i1 = 0; i1 < N; ++i1) accs[t * N + i1] = 0.0;
+  const int cpl = (PL == 2) ? (t >> 5) : 0, col = (PL == 2) ? (t & 31) : t;
+  const bool col_on = col < P1 && cpl < npl_here;
+  float2 *Tc = T + (long)cpl * N * P1;
+  for (int i = t; i < PL * N * N; i += blockDim.x) accs[i] = 0.0;
   const int np = min(npl, (P.npair_dev ? *P.npair_dev : P.npair) - P.pair0);
   const int pl0 = grp * per_group, pl1 = min(np, pl0 + per_group);
   for (int pl = pl0; pl < pl1; ++pl) {
     const int p = P.pair0 + pl;
-    const float2 *A = bufA + ((long)pl * P.k3 + i3) * P2 * P1;
-    if (t < P1) {
+    const float2 *A = bufA + ((long)pl * P.k3 + i3b + cpl) * P2 * P1;
+    if (col_on) {
       float2 x[N];
 #pragma unroll
       for (int i2 = 0; i2 < N; ++i2) {
         const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
         float2 v = zero;
-        if (j2 >= 0 && t >= P.row_lo[j2] && t <= P.row_hi[j2]) v = A[j2 * P1 + t];
+        if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) v = A[j2 * P1 + col];
         x[i2] = v;
       }
       rf::fft<float, +1, N>(x);
       rf::static_for<0, N>([&](auto ic) {
         constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
-        T[i2 * P1 + t] = x[q];
+        Tc[i2 * P1 + col] = x[q];
       });
     }
     __syncthreads();
-    if (t < N) {
-      float2 x[N];
-      const float2 *row = T + t * P1;
+    const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
+    const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
+    for (int rp = 0; rp < npl_here; ++rp) {
+      if (t < N) {
+        float2 x[N];
+        const float2 *row = T + ((long)rp * N + t) * P1;
 #pragma unroll
-      for (int i1 = 0; i1 < N; ++i1) {
-        float2 v = zero;
-        if (i1 <= m1) v = row[i1 + m1];
-        else if (i1 >= N - m1) v = row[i1 - N + m1];
-        x[i1] = v;
+        for (int i1 = 0; i1 < N; ++i1) {
+          float2 v = zero;
+          if (i1 <= m1) v = row[i1 + m1];
+          else if (i1 >= N - m1) v = row[i1 - N + m1];
+          x[i1] = v;
+        }
+        rf::fft<float, +1, N>(x);
+        double *a = accs + ((long)rp * N + t) * N;
+        rf::static_for<0, N>([&](auto ic) {
+          constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+          const double re = x[q].x, im = x[q].y;
+          a[i1] += fa * re * re + fb * im * im;
+        });
       }
-      rf::fft<float, +1, N>(x);
-      const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
-      const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
-      double *a = accs + t * N;
-      rf::static_for<0, N>([&](auto ic) {
-        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
-        const double re = x[q].x, im = x[q].y;
-        a[i1] += fa * re * re + fb * im * im;
-      });
     }
     __syncthreads();
   }
-  if (t < N) {
-    double *dst = part + ((long)grp * P.k3 + i3) * N * N + (long)t * N;
-    for (int i1 = 0; i1 < N; ++i1) dst[i1] = accs[t * N + i1];
+  __syncthreads();
+  for (int rp = 0; rp < npl_here; ++rp) {
+    double *dst = part + ((long)grp * P.k3 + i3b + rp) * N * N;
+    for (int i = t; i < N * N; i += blockDim.x) dst[i] = accs[(long)rp * N * N + i];
   }
 }
 
@@ -554,15 +579,21 @@ __global__ void k_rho_groups(const double *__restrict__ part, long n, double *__
 template <int N>
 static int rho_launch(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part, double *rho,
                       int accumulate, cudaStream_t st) {
-  const size_t sm = sizeof(double) * (size_t)N * N + sizeof(float2) * (size_t)N * P.P1;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_rho_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_rho_plane<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_rho_plane<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 192 * 1024);
     attr = true;
   }
   const int per_group = (npl + RHO_GROUPS - 1) / RHO_GROUPS;
-  dim3 g(P.k3, RHO_GROUPS);
-  k_rho_plane<N><<<g, 64, sm, st>>>(P, bufA, wocc, part, npl, per_group);
+  const size_t sm1 = sizeof(double) * (size_t)N * N + sizeof(float2) * (size_t)N * P.P1;
+  if (P.P1 <= 32 && plane_pairs_enabled() && 2 * sm1 <= 192 * 1024) {
+    dim3 g((P.k3 + 1) / 2, RHO_GROUPS);
+    k_rho_plane<N, 2><<<g, 64, 2 * sm1, st>>>(P, bufA, wocc, part, npl, per_group);
+  } else {
+    dim3 g(P.k3, RHO_GROUPS);
+    k_rho_plane<N, 1><<<g, 64, sm1, st>>>(P, bufA, wocc, part, npl, per_group);
+  }
   note_launch();
   const long n = (long)P.k1 * P.k2 * P.k3;
   k_rho_groups<<<148 * 4, 256, 0, st>>>(part, n, rho, accumulate);
@@ -626,14 +657,21 @@ bool plane_length_supported(int k1, int k2) {
 
 template <int N>
 static int plane_launch(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st) {
-  const size_t sm = sizeof(float2) * (size_t)N * P.P1;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_plane<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_plane<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_plane<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     attr = true;
   }
-  dim3 g(P.k3, npl);
-  k_plane<N><<<g, 64, sm, st>>>(P, bufA, vloc);
+  if (P.P1 <= 32 && plane_pairs_enabled()) {   // two planes a CTA: warp w takes plane w's columns
+    const size_t sm = sizeof(float2) * 2 * (size_t)N * P.P1;
+    dim3 g((P.k3 + 1) / 2, npl);
+    k_plane<N, 2><<<g, 64, sm, st>>>(P, bufA, vloc);
+  } else {
+    const size_t sm = sizeof(float2) * (size_t)N * P.P1;
+    dim3 g(P.k3, npl);
+    k_plane<N, 1><<<g, 64, sm, st>>>(P, bufA, vloc);
+  }
   note_launch();
   return 0;
 }
