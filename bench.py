@@ -42,14 +42,15 @@ PULAY_ASLH, PULAY_Q0, PULAY_ITRATN, PULAY_CMETRIC = 0.8, 0.8, 10, 20.0
 # dram__bytes_read.sum + dram__bytes_write.sum over the four launches of one
 # FP32 H|psi> pass of this workload (ncu, --profile-hpsi; the capture command
 # is listed with the figures in the profiles directory)
-HPSI_PASS_DRAM_BYTES = 69812480
+HPSI_PASS_DRAM_BYTES = 69974016
 # What limits the pipeline (ncu on the plane pass, the largest of its
 # kernels): its DRAM traffic is a fraction of the algorithmic bytes because
 # the z-transformed planes stay in L2, so it is not HBM-bound; it is bound by
 # latency at low occupancy.
 PIPELINE_LIMITER = ("latency, not HBM: DRAM traffic is 0.17x the algorithmic bytes (the pruned transforms keep "
-                    "only the z-transformed planes); plane pass k_plane at 18.6% achieved occupancy (128 "
-                    "registers), 34.9% issue active, FMA pipe 27%, stalls led by barrier, wait and long scoreboard")
+                    "only the z-transformed planes); plane pass k_plane (two z planes a CTA) at 22.7% achieved "
+                    "occupancy (128 registers), 41.4% issue active, FMA pipe 36%, stalls led by long scoreboard, "
+                    "instruction fetch and wait")
 # FP64 SCF iterations of the refinement sweep after the mixed solution converged
 REFINE_ITERS = 3
 # iteration caps of the Si512 run to self-consistency and of its FP64 sweep
