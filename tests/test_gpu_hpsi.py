@@ -112,7 +112,8 @@ def test_hpsi_linearity_full_si64():
         assert oracle.dot(x[b], out[1][b]) == pytest.approx(oracle.dot(y[b], out[0][b]), rel=1e-10)
 
 
-@pytest.mark.parametrize("ecutdens,n", [(170.0, 45), (200.0, 48), (235.0, 54), (295.0, 60), (760.0, 96)])
+@pytest.mark.parametrize("ecutdens,n", [(40.0, 21), (55.0, 25), (152.5, 42), (170.0, 45), (200.0, 48),
+                                          (217.5, 49), (235.0, 54), (295.0, 60), (760.0, 96)])
 def test_plane_pass_lengths(monkeypatch, ecutdens, n):
     """The fused FP32 plane pass on the larger specialised lengths (Si8 cells
     whose density cutoff gives an n^3 grid, wave cutoff ecutdens/4 so the
