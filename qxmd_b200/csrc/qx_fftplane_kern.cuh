@@ -24,81 +24,96 @@ namespace qx {
 // where that needs no spills.
 constexpr int plane_minb(int n) { return n <= 54 ? 8 : 1; }
 
-template <int N, int PL>
-__global__ void __launch_bounds__(64, plane_minb(N)) k_plane(PipeParams P, float2 *__restrict__ bufA, const float *__restrict__ vloc) {
+// Grid rows of the x phase, thread t of a 64-thread CTA: with two planes of
+// at most 32 rows, warp w takes plane w's rows (both planes at once);
+// otherwise thread t takes row t of each plane in turn.
+template <int NY, int PL>
+struct PlaneRows {
+  static constexpr bool both = PL == 2 && NY <= 32;
+  static constexpr int passes = both ? 1 : PL;
+  __device__ static int plane(int t, int pass) { return both ? (t >> 5) : pass; }
+  __device__ static int row(int t) { return both ? (t & 31) : t; }
+};
+
+template <int NX, int NY, int PL>
+__global__ void __launch_bounds__(64, plane_minb(NX > NY ? NX : NY))
+    k_plane(PipeParams P, float2 *__restrict__ bufA, const float *__restrict__ vloc) {
   using rf::out_pos;
+  using Rows = PlaneRows<NY, PL>;
   // PL = 2: the CTA takes planes i3 and i3 + 1; the y phases give warp w the
-  // columns of plane w (P1 <= 32), the x phase runs the two planes' rows in
-  // turn.  PL = 1: one plane, the columns on threads 0 .. P1 - 1.
+  // columns of plane w (P1 <= 32).  PL = 1: one plane, the columns on
+  // threads 0 .. P1 - 1.  NX = k1 (x, the sphere's P1 columns), NY = k2.
   const int i3b = blockIdx.x * PL;
   const int pl = blockIdx.y, p = P.pair0 + pl;
   if (p >= (P.npair_dev ? *P.npair_dev : P.npair)) return;
   const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
   const int npl_here = min(PL, P.k3 - i3b);   // planes this CTA owns (uniform)
-  extern __shared__ float2 T[];   // [PL][N][P1]
+  extern __shared__ float2 T[];   // [PL][NY][P1]
   const int t = threadIdx.x;
   const float2 zero = make_float2(0.f, 0.f);
   // column phases: plane and column of this thread
   const int cpl = (PL == 2) ? (t >> 5) : 0, col = (PL == 2) ? (t & 31) : t;
   const bool col_on = col < P1 && cpl < npl_here;
   float2 *A = bufA + ((long)pl * P.k3 + i3b + cpl) * P2 * P1;
-  float2 *Tc = T + (long)cpl * N * P1;
+  float2 *Tc = T + (long)cpl * NY * P1;
 
   // (1) y backward, thread = sphere column a of its plane
   if (col_on) {
-    float2 x[N];
+    float2 x[NY];
 #pragma unroll
-    for (int i2 = 0; i2 < N; ++i2) {
-      const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+    for (int i2 = 0; i2 < NY; ++i2) {
+      const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= NY - m2) ? i2 - NY + m2 : -1);
       float2 v = zero;
       if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) v = A[j2 * P1 + col];
       x[i2] = v;
     }
-    rf::fft<float, +1, N>(x);
-    rf::static_for<0, N>([&](auto ic) {
-      constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
+    rf::fft<float, +1, NY>(x);
+    rf::static_for<0, NY>([&](auto ic) {
+      constexpr int i2 = decltype(ic)::value, q = out_pos(NY, i2);
       Tc[i2 * P1 + col] = x[q];
     });
   }
   __syncthreads();
-  // (2) x backward, * V, x forward; thread = grid row i2, plane after plane
-  for (int rp = 0; rp < npl_here; ++rp) {
-    if (t < N) {
-      float2 x[N];
-      float2 *row = T + ((long)rp * N + t) * P1;
+  // (2) x backward, * V, x forward; thread = grid row r of plane rp
+  const int r = Rows::row(t);
+  for (int pass = 0; pass < Rows::passes; ++pass) {
+    const int rp = Rows::plane(t, pass);
+    if (r < NY && rp < npl_here) {
+      float2 x[NX];
+      float2 *row = T + ((long)rp * NY + r) * P1;
 #pragma unroll
-      for (int i1 = 0; i1 < N; ++i1) {
+      for (int i1 = 0; i1 < NX; ++i1) {
         float2 v = zero;
         if (i1 <= m1) v = row[i1 + m1];
-        else if (i1 >= N - m1) v = row[i1 - N + m1];
+        else if (i1 >= NX - m1) v = row[i1 - NX + m1];
         x[i1] = v;
       }
-      rf::fft<float, +1, N>(x);
-      const float *V = vloc + ((long)(i3b + rp) * N + t) * N;
-      float2 y[N];
-      rf::static_for<0, N>([&](auto ic) {
-        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+      rf::fft<float, +1, NX>(x);
+      const float *V = vloc + ((long)(i3b + rp) * NY + r) * NX;
+      float2 y[NX];
+      rf::static_for<0, NX>([&](auto ic) {
+        constexpr int i1 = decltype(ic)::value, q = out_pos(NX, i1);
         const float vv = V[i1];
         y[i1] = make_float2(x[q].x * vv, x[q].y * vv);
       });
-      rf::fft<float, -1, N>(y);
-      rf::static_for<0, N>([&](auto ic) {
-        constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+      rf::fft<float, -1, NX>(y);
+      rf::static_for<0, NX>([&](auto ic) {
+        constexpr int i1 = decltype(ic)::value, q = out_pos(NX, i1);
         if (i1 <= m1) row[i1 + m1] = y[q];
-        else if (i1 >= N - m1) row[i1 - N + m1] = y[q];
+        else if (i1 >= NX - m1) row[i1 - NX + m1] = y[q];
       });
     }
   }
   __syncthreads();
   // (3) y forward, thread = sphere column a of its plane; only rows inside the sphere are kept
   if (col_on) {
-    float2 x[N];
+    float2 x[NY];
 #pragma unroll
-    for (int i2 = 0; i2 < N; ++i2) x[i2] = Tc[i2 * P1 + col];
-    rf::fft<float, -1, N>(x);
-    rf::static_for<0, N>([&](auto ic) {
-      constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
-      const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+    for (int i2 = 0; i2 < NY; ++i2) x[i2] = Tc[i2 * P1 + col];
+    rf::fft<float, -1, NY>(x);
+    rf::static_for<0, NY>([&](auto ic) {
+      constexpr int i2 = decltype(ic)::value, q = out_pos(NY, i2);
+      const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= NY - m2) ? i2 - NY + m2 : -1);
       if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) A[j2 * P1 + col] = x[q];
     });
   }
@@ -383,62 +398,66 @@ int zcols_launch(const PipeParams &P, int npl, const float *cin, long ldc, float
 // owns one grid row).  The group's partial plane goes to part[group]; a
 // second kernel sums the groups in a fixed order, so the result is the same
 // from run to run.
-template <int N, int PL>
+template <int NX, int NY, int PL>
 __global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__restrict__ bufA,
                                                   const double *__restrict__ wocc, double *__restrict__ part,
                                                   int npl, int per_group) {
   using rf::out_pos;
+  using Rows = PlaneRows<NY, PL>;
   // PL = 2: planes i3 and i3 + 1, warp w taking plane w's columns in the y
-  // phase (P1 <= 32), the rows of the two planes in turn in the x phase.
+  // phase (P1 <= 32); the x phase as in k_plane.
   const int i3b = blockIdx.x * PL, grp = blockIdx.y;
   const int P1 = P.P1, P2 = P.P2, m1 = P.m1, m2 = P.m2;
   const int npl_here = min(PL, P.k3 - i3b);
-  extern __shared__ double accs[];            // [PL][N][N] FP64, then the [PL][N][P1] complex tiles
-  float2 *T = reinterpret_cast<float2 *>(accs + PL * N * N);
+  constexpr int NP = NX * NY;
+  extern __shared__ double accs[];            // [PL][NY][NX] FP64, then the [PL][NY][P1] complex tiles
+  float2 *T = reinterpret_cast<float2 *>(accs + PL * NP);
   const int t = threadIdx.x;
   const float2 zero = make_float2(0.f, 0.f);
   const int cpl = (PL == 2) ? (t >> 5) : 0, col = (PL == 2) ? (t & 31) : t;
   const bool col_on = col < P1 && cpl < npl_here;
-  float2 *Tc = T + (long)cpl * N * P1;
-  for (int i = t; i < PL * N * N; i += blockDim.x) accs[i] = 0.0;
+  float2 *Tc = T + (long)cpl * NY * P1;
+  for (int i = t; i < PL * NP; i += blockDim.x) accs[i] = 0.0;
   const int np = min(npl, (P.npair_dev ? *P.npair_dev : P.npair) - P.pair0);
   const int pl0 = grp * per_group, pl1 = min(np, pl0 + per_group);
+  const int r = Rows::row(t);
   for (int pl = pl0; pl < pl1; ++pl) {
     const int p = P.pair0 + pl;
     const float2 *A = bufA + ((long)pl * P.k3 + i3b + cpl) * P2 * P1;
     if (col_on) {
-      float2 x[N];
+      float2 x[NY];
 #pragma unroll
-      for (int i2 = 0; i2 < N; ++i2) {
-        const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= N - m2) ? i2 - N + m2 : -1);
+      for (int i2 = 0; i2 < NY; ++i2) {
+        const int j2 = (i2 <= m2) ? i2 + m2 : ((i2 >= NY - m2) ? i2 - NY + m2 : -1);
         float2 v = zero;
         if (j2 >= 0 && col >= P.row_lo[j2] && col <= P.row_hi[j2]) v = A[j2 * P1 + col];
         x[i2] = v;
       }
-      rf::fft<float, +1, N>(x);
-      rf::static_for<0, N>([&](auto ic) {
-        constexpr int i2 = decltype(ic)::value, q = out_pos(N, i2);
+      rf::fft<float, +1, NY>(x);
+      rf::static_for<0, NY>([&](auto ic) {
+        constexpr int i2 = decltype(ic)::value, q = out_pos(NY, i2);
         Tc[i2 * P1 + col] = x[q];
       });
     }
     __syncthreads();
     const int bA = P.pairs[2 * p], bB = P.pairs[2 * p + 1];
     const double fa = wocc[bA], fb = bB >= 0 ? wocc[bB] : 0.0;
-    for (int rp = 0; rp < npl_here; ++rp) {
-      if (t < N) {
-        float2 x[N];
-        const float2 *row = T + ((long)rp * N + t) * P1;
+    for (int pass = 0; pass < Rows::passes; ++pass) {
+      const int rp = Rows::plane(t, pass);
+      if (r < NY && rp < npl_here) {
+        float2 x[NX];
+        const float2 *row = T + ((long)rp * NY + r) * P1;
 #pragma unroll
-        for (int i1 = 0; i1 < N; ++i1) {
+        for (int i1 = 0; i1 < NX; ++i1) {
           float2 v = zero;
           if (i1 <= m1) v = row[i1 + m1];
-          else if (i1 >= N - m1) v = row[i1 - N + m1];
+          else if (i1 >= NX - m1) v = row[i1 - NX + m1];
           x[i1] = v;
         }
-        rf::fft<float, +1, N>(x);
-        double *a = accs + ((long)rp * N + t) * N;
-        rf::static_for<0, N>([&](auto ic) {
-          constexpr int i1 = decltype(ic)::value, q = out_pos(N, i1);
+        rf::fft<float, +1, NX>(x);
+        double *a = accs + ((long)rp * NY + r) * NX;
+        rf::static_for<0, NX>([&](auto ic) {
+          constexpr int i1 = decltype(ic)::value, q = out_pos(NX, i1);
           const double re = x[q].x, im = x[q].y;
           a[i1] += fa * re * re + fb * im * im;
         });
@@ -448,8 +467,8 @@ __global__ void __launch_bounds__(64) k_rho_plane(PipeParams P, const float2 *__
   }
   __syncthreads();
   for (int rp = 0; rp < npl_here; ++rp) {
-    double *dst = part + ((long)grp * P.k3 + i3b + rp) * N * N;
-    for (int i = t; i < N * N; i += blockDim.x) dst[i] = accs[(long)rp * N * N + i];
+    double *dst = part + ((long)grp * P.k3 + i3b + rp) * NP;
+    for (int i = t; i < NP; i += blockDim.x) dst[i] = accs[(long)rp * NP + i];
   }
 }
 
@@ -525,23 +544,23 @@ __global__ void __launch_bounds__(2 * N) k_rho_plane2(PipeParams P, const float2
   for (int i = t; i < N * N; i += 2 * N) dst[i] = accs[i];
 }
 
-template <int N>
+template <int NX, int NY>
 int rho_launch(const PipeParams &P, int npl, const float2 *bufA, const double *wocc, double *part, double *rho,
-                      int accumulate, cudaStream_t st) {
+               int accumulate, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_rho_plane<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_rho_plane<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 192 * 1024);
+    cudaFuncSetAttribute(k_rho_plane<NX, NY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_rho_plane<NX, NY, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 192 * 1024);
     attr = true;
   }
   const int per_group = (npl + RHO_GROUPS - 1) / RHO_GROUPS;
-  const size_t sm1 = sizeof(double) * (size_t)N * N + sizeof(float2) * (size_t)N * P.P1;
+  const size_t sm1 = sizeof(double) * (size_t)NX * NY + sizeof(float2) * (size_t)NY * P.P1;
   if (P.P1 <= 32 && plane_pairs_enabled() && 2 * sm1 <= 192 * 1024) {
     dim3 g((P.k3 + 1) / 2, RHO_GROUPS);
-    k_rho_plane<N, 2><<<g, 64, 2 * sm1, st>>>(P, bufA, wocc, part, npl, per_group);
+    k_rho_plane<NX, NY, 2><<<g, 64, 2 * sm1, st>>>(P, bufA, wocc, part, npl, per_group);
   } else {
     dim3 g(P.k3, RHO_GROUPS);
-    k_rho_plane<N, 1><<<g, 64, sm1, st>>>(P, bufA, wocc, part, npl, per_group);
+    k_rho_plane<NX, NY, 1><<<g, 64, sm1, st>>>(P, bufA, wocc, part, npl, per_group);
   }
   note_launch();
   const long n = (long)P.k1 * P.k2 * P.k3;
@@ -568,22 +587,22 @@ int rho2_launch(const PipeParams &P, int npl, const float2 *bufA, const double *
   return 0;
 }
 
-template <int N>
+template <int NX, int NY>
 int plane_launch(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_plane<N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-    cudaFuncSetAttribute(k_plane<N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_plane<NX, NY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaFuncSetAttribute(k_plane<NX, NY, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
     attr = true;
   }
   if (P.P1 <= 32 && plane_pairs_enabled()) {   // two planes a CTA: warp w takes plane w's columns
-    const size_t sm = sizeof(float2) * 2 * (size_t)N * P.P1;
+    const size_t sm = sizeof(float2) * 2 * (size_t)NY * P.P1;
     dim3 g((P.k3 + 1) / 2, npl);
-    k_plane<N, 2><<<g, 64, sm, st>>>(P, bufA, vloc);
+    k_plane<NX, NY, 2><<<g, 64, sm, st>>>(P, bufA, vloc);
   } else {
-    const size_t sm = sizeof(float2) * (size_t)N * P.P1;
+    const size_t sm = sizeof(float2) * (size_t)NY * P.P1;
     dim3 g(P.k3, npl);
-    k_plane<N, 1><<<g, 64, sm, st>>>(P, bufA, vloc);
+    k_plane<NX, NY, 1><<<g, 64, sm, st>>>(P, bufA, vloc);
   }
   note_launch();
   return 0;
@@ -604,11 +623,13 @@ int plane2_launch(const PipeParams &P, int npl, float2 *bufA, const float *vloc,
   return 0;
 }
 
-// Explicit instantiation of every launcher of one length.
-#define QX_PLANE_LENGTH(N)                                                                                      \
-  template int plane_launch<N>(const PipeParams &, int, float2 *, const float *, cudaStream_t);                 \
-  template int rho_launch<N>(const PipeParams &, int, const float2 *, const double *, double *, double *, int,   \
-                             cudaStream_t);                                                                     \
+// Explicit instantiation of the launchers of one k1 x k2 plane shape.
+#define QX_PLANE_GRID(NX, NY)                                                                                    \
+  template int plane_launch<NX, NY>(const PipeParams &, int, float2 *, const float *, cudaStream_t);             \
+  template int rho_launch<NX, NY>(const PipeParams &, int, const float2 *, const double *, double *, double *,   \
+                                  int, cudaStream_t);
+// ... and of the z-column launcher of one k3.
+#define QX_ZCOLS_LENGTH(N)                                                                                      \
   template int zcols_launch<N>(const PipeParams &, int, const float *, long, float2 *, const float2 *, float2 *, \
                                bool, cudaStream_t);
 // The same for the two-lanes-a-line kernels.

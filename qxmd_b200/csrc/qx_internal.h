@@ -106,8 +106,8 @@ void fnl_r_sum(const double *fpart, int npair, int natom, double *fnl, cudaStrea
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
 template <typename T> void set_fft_smem_limits(size_t bytes);
-// qx_fftplane.cu: fused y-x-y pass (FP32, k1 == k2 of a specialised length);
-// returns -1 when the grid is not covered.
+// qx_fftplane.cu: fused y-x-y pass (FP32, k1 x k2 planes of a specialised
+// shape, QX_PLANE_GRIDS); returns -1 when the grid is not covered.
 int launch_plane_f32(const PipeParams &P, int npl, float2 *bufA, const float *vloc, cudaStream_t st);
 // Density through the plane kernel: groups of pairs per z plane, partial
 // planes in part (RHO_GROUPS * kfft0 doubles) summed in a fixed order.

@@ -112,18 +112,11 @@ def test_hpsi_linearity_full_si64():
         assert oracle.dot(x[b], out[1][b]) == pytest.approx(oracle.dot(y[b], out[0][b]), rel=1e-10)
 
 
-@pytest.mark.parametrize("ecutdens,n", [(40.0, 21), (55.0, 25), (152.5, 42), (170.0, 45), (200.0, 48),
-                                          (217.5, 49), (235.0, 54), (295.0, 60), (760.0, 96)])
-def test_plane_pass_lengths(monkeypatch, ecutdens, n):
-    """The fused FP32 plane pass on the larger specialised lengths (Si8 cells
-    whose density cutoff gives an n^3 grid, wave cutoff ecutdens/4 so the
-    sphere spans half the grid) against the oracle, and against the separate
-    y/x passes and shared-memory z passes (QX_PLANE=0, QX_ZCOLS=0) on the
-    same input; the density pass (softchg) the same way.  96 runs the
-    two-threads-a-line kernels (plane, density and inverse z passes)."""
-    need_gpu()
-    s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), ecutdens / 4.0, ecutdens, 4, with_ewald=False)
-    assert tuple(s.gs.grid) == (n, n, n)
+def _plane_pass_vs_oracle(monkeypatch, s):
+    """H|psi> and softchg of 4 random bands of system s on the mixed path
+    with the fused plane and column kernels (QX_PLANE=1, QX_ZCOLS=1) and
+    with the separate y/x and shared-memory z passes (0), each against the
+    oracle and against each other."""
     c = cell.random_wavefunctions(s.gs.nplwex, 4)
     c /= np.sqrt(np.array([oracle.dot(x, x) for x in c]))[:, None]
     h = oracle.Ham(s, QX_NL_GSPACE)
@@ -145,6 +138,34 @@ def test_plane_pass_lengths(monkeypatch, ecutdens, n):
         assert relerr(rho[mode], rref) < TOL[QX_PREC_MIXED]
     assert relerr(out["1"], out["0"]) < TOL[QX_PREC_MIXED]
     assert relerr(rho["1"], rho["0"]) < TOL[QX_PREC_MIXED]
+
+
+@pytest.mark.parametrize("ecutdens,n", [(40.0, 21), (55.0, 25), (152.5, 42), (170.0, 45), (200.0, 48),
+                                          (217.5, 49), (235.0, 54), (295.0, 60), (760.0, 96)])
+def test_plane_pass_lengths(monkeypatch, ecutdens, n):
+    """The fused FP32 plane pass on the larger specialised lengths (Si8 cells
+    whose density cutoff gives an n^3 grid, wave cutoff ecutdens/4 so the
+    sphere spans half the grid) against the oracle and against the separate
+    passes, the density pass (softchg) the same way.  96 runs the
+    two-threads-a-line kernels (plane, density and inverse z passes)."""
+    need_gpu()
+    s = cell.build_system(cell.diamond_si((1, 1, 1), seed=1), ecutdens / 4.0, ecutdens, 4, with_ewald=False)
+    assert tuple(s.gs.grid) == (n, n, n)
+    _plane_pass_vs_oracle(monkeypatch, s)
+
+
+@pytest.mark.parametrize("index,grid", [(14, (24, 25, 25)), (5, (25, 24, 25)), (1, (25, 27, 27)),
+                                        (8, (27, 25, 25)), (2, (42, 21, 21)), (3, (45, 24, 24)),
+                                        (32, (45, 42, 21)), (43, (48, 45, 24)), (9, (49, 25, 25)),
+                                        (41, (54, 24, 24)), (6, (54, 25, 27)), (10, (54, 27, 27))])
+def test_plane_pass_rectangular(monkeypatch, index, grid):
+    """The plane kernels on k1 != k2 planes (x and y transforms of different
+    lengths; planes of at most 32 rows run both planes' x transforms at
+    once): one batch cell of each elongated shape, as above."""
+    need_gpu()
+    s = cell.batch_cell(index)
+    assert tuple(s.gs.grid) == grid
+    _plane_pass_vs_oracle(monkeypatch, s)
 
 
 @pytest.mark.parametrize("plan", ["2x3x4", "3x8", "4x6", "6x4", "8x3", "2x2x2x3", "3x2x2x2"])
