@@ -1,5 +1,6 @@
-// GEMMs of the band and projector contractions (CUDA-core kernel for FP32
-// with a column map, FP64 tensor-core kernel for FP64):
+// GEMMs of the band and projector contractions (CUDA-core kernels for the
+// small FP32 shapes and those with a column map, FP64 tensor-core kernel for
+// FP64):
 // S = C^T C (schmidt.f90:190-237), H_sub = C^T HC (engrad.f90:869-895),
 // <beta|psi> and its back-application (nlkbpp.f90:1678-1713), subgs3
 // (engrad.f90:1122-1142), C*U (eigen.f90:1482-1510) and C*L^-T
@@ -192,12 +193,14 @@ void gemm_reduce_f32(bool ta, bool tb, int M, int N, int nsplit, float alpha, co
   note_launch();
 }
 
-// Dispatch (gemm<T> below): FP32 without a column map goes to the tensor-core
-// kernel (qx_tcgemm.cu) when the operands meet its TMA rules; all FP64 work
-// goes to the DMMA kernel k_dgemm; the rest (FP32 with a column map or
-// operands outside the TMA rules) runs on the CUDA-core kernel above.  Split
-// K when the output has too few tiles to fill the GPU and the caller
-// provides a workspace of at least nsplit*M*N elements.
+// Dispatch (gemm<T> below): FP32 without a column map and above the size
+// threshold goes to the tensor-core kernel (qx_tcgemm.cu) when the operands
+// meet its TMA rules; all FP64 work goes to the DMMA kernel k_dgemm; the
+// rest of FP32 (small shapes, a column map, operands outside the TMA rules)
+// runs on the CUDA-core kernel k_sgemm below (A and B both transposed, not
+// used by the library, on k_gemm above).  Split K when the output has too
+// few tiles to fill the GPU and the caller provides a workspace of at least
+// nsplit*M*N elements.
 // ---------------------------------------------------------------------------
 // FP64 contractions on the FP64 tensor cores: mma.sync m8n8k4 (DMMA, 256
 // FMAs a warp instruction; the FP64 FMA pipe of a B200 measures about 10 %
@@ -500,6 +503,221 @@ static double tc_min_flops() {
   return e ? atof(e) : TC_MIN_FLOPS_DEFAULT;
 }
 
+// ---------------------------------------------------------------------------
+// FP32 contractions on the CUDA cores (the shapes below the tensor-core size
+// threshold, and those with a column map): 256 threads as 16 x 16, each an
+// MT x NT block of the (16 MT) x (16 NT) output tile, so that a band count
+// of 20-80 is not padded to a multiple of 64 (MT, NT in 2..5 picked per
+// shape).  k-blocks of SBK are staged in shared memory by 4-byte cp.async
+// (zero-filled outside the operands), SST deep, one barrier a k-block; the
+// row offsets of what a thread stages are computed once (B through the
+// column map).  Shared layout [k][row] for both operands (pitch rows + 1):
+// in a warp the A reads are two broadcasts and the B reads 16 consecutive
+// words.  Split-K partials and the epilogue as k_gemm's.
+constexpr int SBK = 16, SST = 3;
+
+__device__ __forceinline__ void cp_async4(float *sdst, const float *gsrc, bool live) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc), "r"(live ? 4 : 0) : "memory");
+}
+
+template <int MT, int NT>
+constexpr size_t sgemm_smem() {
+  return sizeof(float) * SST * (size_t)SBK * (16 * MT + 1 + 16 * NT + 1);
+}
+
+template <bool TA, bool TB, bool SPLIT, int MT, int NT>
+__global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha, const float *__restrict__ A, long lda,
+                                               const float *__restrict__ B, long ldb, float beta,
+                                               float *__restrict__ Cm, long ldc, int gamma,
+                                               const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
+                                               int kchunk, float *__restrict__ W) {
+  constexpr int TMM = 16 * MT, TNN = 16 * NT, PA = TMM + 1, PB = TNN + 1;
+  constexpr int SA = SBK * PA, SSZ = SA + SBK * PB;
+  extern __shared__ __align__(16) float ssm[];
+  const int Nact = ncol_dev ? min(N, *ncol_dev) : N;
+  const int m0 = blockIdx.x * TMM, n0 = blockIdx.y * TNN;
+  if (n0 >= Nact) return;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int kb = SPLIT ? blockIdx.z * kchunk : 0;
+  const int ke = SPLIT ? min(K, kb + kchunk) : K;
+  const int nk = (ke - kb + SBK - 1) / SBK;
+  // element e = tid + 256 i of a k-block: k-contiguous operands (A
+  // transposed, B not) take k = e % 16, row e / 16; the others row e % rows,
+  // k = e / rows
+  long aoff[MT], boff[NT];
+  unsigned alive = 0, blive = 0;
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    const int e = tid + 256 * i, r = TA ? e / SBK : e % TMM, gm = m0 + r;
+    if (gm < M) alive |= 1u << i;
+    aoff[i] = gm < M ? (TA ? (long)gm * lda : (long)gm) : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < NT; ++i) {
+    const int e = tid + 256 * i, r = TB ? e % TNN : e / SBK, gn = n0 + r;
+    if (gn < Nact) blive |= 1u << i;
+    const long cn = gn < Nact ? (colmap ? (long)colmap[gn] : (long)gn) : 0;
+    boff[i] = TB ? cn : cn * ldb;
+  }
+  auto stage = [&](int blk) {
+    float *S = ssm + (blk % SST) * SSZ;
+    const int k0 = kb + blk * SBK;
+#pragma unroll
+    for (int i = 0; i < MT; ++i) {
+      const int e = tid + 256 * i;
+      const int r = TA ? e / SBK : e % TMM, k = TA ? e % SBK : e / TMM;
+      const bool live = ((alive >> i) & 1) && k0 + k < ke;
+      const float *src = live ? (TA ? A + aoff[i] + k0 + k : A + aoff[i] + (long)(k0 + k) * lda) : A;
+      cp_async4(S + k * PA + r, src, live);
+    }
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      const int e = tid + 256 * i;
+      const int r = TB ? e % TNN : e / SBK, k = TB ? e / TNN : e % SBK;
+      const bool live = ((blive >> i) & 1) && k0 + k < ke;
+      const float *src = live ? (TB ? B + boff[i] + (long)(k0 + k) * ldb : B + boff[i] + k0 + k) : B;
+      cp_async4(S + SA + k * PB + r, src, live);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < SST - 1; ++s) {
+    if (s < nk) stage(s);
+    cp_async_commit();
+  }
+  float acc[MT][NT];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[i][j] = 0.f;
+  for (int it = 0; it < nk; ++it) {
+    cp_async_wait<SST - 2>();   // this thread's copies of block it are in
+    __syncthreads();            // everyone's are, and block it - 1 is consumed
+    if (it + SST - 1 < nk) stage(it + SST - 1);
+    cp_async_commit();
+    const float *As = ssm + (it % SST) * SSZ, *Bs = As + SA;
+#pragma unroll
+    for (int k = 0; k < SBK; ++k) {
+      float a[MT], b[NT];
+#pragma unroll
+      for (int i = 0; i < MT; ++i) a[i] = As[k * PA + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) b[j] = Bs[k * PB + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int i = 0; i < MT; ++i) {
+    const int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const int gn = n0 + tx + 16 * j;
+      if (gn >= Nact) continue;
+      if (SPLIT) {
+        W[((long)blockIdx.z * N + gn) * M + gm] = acc[i][j];
+        continue;
+      }
+      const long cn = colmap ? colmap[gn] : gn;
+      float v = acc[i][j];
+      if (gamma) {
+        const float a0 = TA ? A[(long)gm * lda] : A[gm];
+        const float b0 = TB ? B[cn] : B[cn * ldb];
+        v = 2.f * v - a0 * b0;
+        if (gamma == 2) {
+          const float a1 = TA ? A[(long)gm * lda + 1] : A[lda + gm];
+          const float b1 = TB ? B[ldb + cn] : B[cn * ldb + 1];
+          v -= 2.f * a1 * b1;
+        }
+      }
+      float *c = Cm + cn * ldc + gm;
+      *c = (beta == 0.f) ? alpha * v : alpha * v + beta * *c;
+    }
+  }
+}
+
+// Rows of a tile a thread-row covers for an extent of n: the smallest of
+// 2..5 (tiles of 32..80) that holds n, else 4 (64-row tiles).
+// QX_SGEMM=0 keeps the FP32 CUDA-core contractions on k_gemm (read at every
+// call).
+static bool sgemm_enabled() {
+  const char *e = getenv("QX_SGEMM");
+  return !(e && e[0] == '0');
+}
+
+static int sgemm_rows(int n) {
+  for (int t = 2; t <= 5; ++t)
+    if (16 * t >= n) return t;
+  return 4;
+}
+
+template <bool TA, bool TB, bool SPLIT, int MT, int NT>
+static void sgemm_go(dim3 g, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
+                     float beta, float *C, long ldc, int gamma, const int *colmap, const int *ncol_dev, int kchunk,
+                     float *W, cudaStream_t st) {
+  constexpr size_t sm = sgemm_smem<MT, NT>();
+  static_assert(sm <= 48 * 1024, "stages fit the default shared-memory limit");
+  k_sgemm<TA, TB, SPLIT, MT, NT><<<g, 256, sm, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap,
+                                                     ncol_dev, kchunk, W);
+  note_launch();
+}
+
+// One shape's launch: tile rows MT x NT from the extents (k-contiguous A:
+// both from the band-sized extents; otherwise 64-row tiles down M), K split
+// as k_gemm's, then the ordered reduction of the partials.
+template <bool TA, bool TB>
+static void sgemm_launch(int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
+                         float beta, float *C, long ldc, int gamma, const int *colmap, const int *ncol_dev, void *ws,
+                         size_t ws_bytes, cudaStream_t st) {
+  const int mt = TA ? sgemm_rows(M) : 4, nt = sgemm_rows(N);
+  dim3 g((M + 16 * mt - 1) / (16 * mt), (N + 16 * nt - 1) / (16 * nt));
+  const long tiles = (long)g.x * g.y;
+  int nsplit = 1, kchunk = K;
+  if (ws && tiles < 2 * 148 && K >= 4 * 256) {
+    nsplit = (int)std::min<long>((2 * 148 + tiles - 1) / tiles, (K + 255) / 256);
+    kchunk = ((K + nsplit - 1) / nsplit + SBK - 1) / SBK * SBK;
+    nsplit = (K + kchunk - 1) / kchunk;
+    if ((size_t)nsplit * M * N * sizeof(float) > ws_bytes) {
+      nsplit = (int)(ws_bytes / ((size_t)M * N * sizeof(float)));
+      if (nsplit < 2) nsplit = 1;
+      else {
+        kchunk = ((K + nsplit - 1) / nsplit + SBK - 1) / SBK * SBK;
+        nsplit = (K + kchunk - 1) / kchunk;
+      }
+    }
+  }
+  if (nsplit <= 1) kchunk = K;
+  g.z = nsplit;
+  float *W = (float *)ws;
+  const bool split = nsplit > 1;
+#define QX_SG(MT_, NT_)                                                                                              \
+  if (mt == MT_ && nt == NT_) {                                                                                      \
+    if (split) sgemm_go<TA, TB, true, MT_, NT_>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap,     \
+                                                ncol_dev, kchunk, W, st);                                            \
+    else sgemm_go<TA, TB, false, MT_, NT_>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, \
+                                           kchunk, W, st);                                                           \
+  }
+  if (TA) {
+    QX_SG(2, 2) else QX_SG(2, 3) else QX_SG(2, 4) else QX_SG(2, 5)
+    else QX_SG(3, 2) else QX_SG(3, 3) else QX_SG(3, 4) else QX_SG(3, 5)
+    else QX_SG(4, 2) else QX_SG(4, 3) else QX_SG(4, 4) else QX_SG(4, 5)
+    else QX_SG(5, 2) else QX_SG(5, 3) else QX_SG(5, 4) else QX_SG(5, 5)
+  } else {
+    QX_SG(4, 2) else QX_SG(4, 3) else QX_SG(4, 4) else QX_SG(4, 5)
+  }
+#undef QX_SG
+  if (split) {
+    const long mn = (long)M * N;
+    k_gemm_reduce<float, TA, TB><<<(int)((mn + 31) / 32), RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C,
+                                                                          ldc, gamma, colmap, ncol_dev, W, nullptr);
+    note_launch();
+  }
+}
+
 // FP32 contractions that ran on the CUDA-core kernel instead of the tensor
 // cores (a column map, a device column count or operands outside the TMA
 // rules; not the small ones sent there by tc_min_flops), counted for
@@ -544,6 +762,21 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
       r = launch_dgemm<false, false>(M, N, K, alpha, Ad, lda, Bd, ldb, beta, Cd, ldc, gamma, colmap, ncol_dev, ws,
                                      ws_bytes, st);
     if (r) return r;
+    if (rowscale) scale_rows<T>(M, N, C, ldc, rowscale, colmap, ncol_dev, st);
+    return 0;
+  }
+  if (sizeof(T) == sizeof(float) && !(ta && tb) && sgemm_enabled()) {
+    const float *Af = (const float *)A, *Bf = (const float *)B;
+    float *Cf = (float *)C;
+    if (ta)
+      sgemm_launch<true, false>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap, ncol_dev,
+                                ws, ws_bytes, st);
+    else if (tb)
+      sgemm_launch<false, true>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap, ncol_dev,
+                                ws, ws_bytes, st);
+    else
+      sgemm_launch<false, false>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap,
+                                 ncol_dev, ws, ws_bytes, st);
     if (rowscale) scale_rows<T>(M, N, C, ldc, rowscale, colmap, ncol_dev, st);
     return 0;
   }
