@@ -567,6 +567,12 @@ extern "C" int qx_create(qx_ctx **out, int precision, int k1, int k2, int k3, in
   FAIL(dalloc(c, &c->mat_t, ts * nb * nb));
   c->gws_bytes = sizeof(double) * (size_t)64 * 1024 * 1024 / 8;   // 64 MB
   FAIL(dalloc(c, &c->gws, c->gws_bytes));
+  // the split-K tile counters, zero before the first GEMM on the context's stream
+  if (cudaMemsetAsync(c->gws, 0, GEMM_COUNTER_BYTES, c->st) != cudaSuccess) {
+    set_error("qx_create: clearing the GEMM counters failed");
+    qx_destroy(c);
+    return QX_ERR_CUDA;
+  }
   FAIL(tcpad_reserve(c, 2L * nb));
   cudaMemset(c->psi, 0, blk);
   cudaMemset(c->hpsi, 0, blk);

@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
                                                const float *__restrict__ B, long ldb, float beta,
                                                float *__restrict__ Cm, long ldc, int gamma,
                                                const int *__restrict__ colmap, const int *__restrict__ ncol_dev,
-                                               int kchunk, float *__restrict__ W) {
+                                               int kchunk, float *__restrict__ W, int *__restrict__ cnt) {
   constexpr int TMM = 16 * MT, TNN = 16 * NT, PA = TMM + 1, PB = TNN + 1;
   constexpr int SA = SBK * PA, SSZ = SA + SBK * PB;
   extern __shared__ __align__(16) float ssm[];
@@ -610,6 +610,37 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
     }
   }
   cp_async_wait<0>();
+  if (SPLIT) {
+    // Split K: every CTA stores its partial tile (element e of thread t at
+    // W[((z tiles + tile) MT NT + e) 256 + t], coalesced), counts itself in
+    // for the tile, and the last to arrive sums the partials in z order and
+    // finishes the tile; it then clears the count for the next launch.  No
+    // CTA waits for another.
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    const long zs = (long)gridDim.x * gridDim.y * MT * NT * 256;
+    float *Wt = W + (long)tile * MT * NT * 256 + tid;
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) Wt[blockIdx.z * zs + (i * NT + j) * 256] = acc[i][j];
+    __threadfence();
+    __syncthreads();
+    __shared__ int last;
+    if (tid == 0) last = atomicAdd(cnt + tile, 1) == (int)gridDim.z - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) acc[i][j] = 0.f;
+    for (int z = 0; z < (int)gridDim.z; ++z)
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) acc[i][j] += __ldcg(Wt + z * zs + (i * NT + j) * 256);
+    if (tid == 0) cnt[tile] = 0;
+  }
 #pragma unroll
   for (int i = 0; i < MT; ++i) {
     const int gm = m0 + ty + 16 * i;
@@ -618,10 +649,6 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
     for (int j = 0; j < NT; ++j) {
       const int gn = n0 + tx + 16 * j;
       if (gn >= Nact) continue;
-      if (SPLIT) {
-        W[((long)blockIdx.z * N + gn) * M + gm] = acc[i][j];
-        continue;
-      }
       const long cn = colmap ? colmap[gn] : gn;
       float v = acc[i][j];
       if (gamma) {
@@ -640,8 +667,6 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
   }
 }
 
-// Rows of a tile a thread-row covers for an extent of n: the smallest of
-// 2..5 (tiles of 32..80) that holds n, else 4 (64-row tiles).
 // QX_SGEMM=0 keeps the FP32 CUDA-core contractions on k_gemm (read at every
 // call).
 static bool sgemm_enabled() {
@@ -649,6 +674,8 @@ static bool sgemm_enabled() {
   return !(e && e[0] == '0');
 }
 
+// Rows of a tile a thread-row covers for an extent of n: the smallest of
+// 2..5 (tiles of 32..80) that holds n, else 4 (64-row tiles).
 static int sgemm_rows(int n) {
   for (int t = 2; t <= 5; ++t)
     if (16 * t >= n) return t;
@@ -658,31 +685,33 @@ static int sgemm_rows(int n) {
 template <bool TA, bool TB, bool SPLIT, int MT, int NT>
 static void sgemm_go(dim3 g, int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
                      float beta, float *C, long ldc, int gamma, const int *colmap, const int *ncol_dev, int kchunk,
-                     float *W, cudaStream_t st) {
+                     float *W, int *cnt, cudaStream_t st) {
   constexpr size_t sm = sgemm_smem<MT, NT>();
   static_assert(sm <= 48 * 1024, "stages fit the default shared-memory limit");
   k_sgemm<TA, TB, SPLIT, MT, NT><<<g, 256, sm, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap,
-                                                     ncol_dev, kchunk, W);
+                                                     ncol_dev, kchunk, W, cnt);
   note_launch();
 }
 
 // One shape's launch: tile rows MT x NT from the extents (k-contiguous A:
 // both from the band-sized extents; otherwise 64-row tiles down M), K split
-// as k_gemm's, then the ordered reduction of the partials.
+// as k_gemm's, the partials summed by the last CTA of each tile (cnt: one
+// zeroed counter per tile).
 template <bool TA, bool TB>
 static void sgemm_launch(int M, int N, int K, float alpha, const float *A, long lda, const float *B, long ldb,
                          float beta, float *C, long ldc, int gamma, const int *colmap, const int *ncol_dev, void *ws,
-                         size_t ws_bytes, cudaStream_t st) {
+                         size_t ws_bytes, int *cnt, cudaStream_t st) {
   const int mt = TA ? sgemm_rows(M) : 4, nt = sgemm_rows(N);
   dim3 g((M + 16 * mt - 1) / (16 * mt), (N + 16 * nt - 1) / (16 * nt));
   const long tiles = (long)g.x * g.y;
+  const size_t part = sizeof(float) * (size_t)tiles * 256 * mt * nt;   // one split's partial tiles
   int nsplit = 1, kchunk = K;
-  if (ws && tiles < 2 * 148 && K >= 4 * 256) {
+  if (ws && cnt && tiles <= GEMM_TILE_COUNTERS && tiles < 2 * 148 && K >= 4 * 256) {
     nsplit = (int)std::min<long>((2 * 148 + tiles - 1) / tiles, (K + 255) / 256);
     kchunk = ((K + nsplit - 1) / nsplit + SBK - 1) / SBK * SBK;
     nsplit = (K + kchunk - 1) / kchunk;
-    if ((size_t)nsplit * M * N * sizeof(float) > ws_bytes) {
-      nsplit = (int)(ws_bytes / ((size_t)M * N * sizeof(float)));
+    if ((size_t)nsplit * part > ws_bytes) {
+      nsplit = (int)(ws_bytes / part);
       if (nsplit < 2) nsplit = 1;
       else {
         kchunk = ((K + nsplit - 1) / nsplit + SBK - 1) / SBK * SBK;
@@ -697,9 +726,9 @@ static void sgemm_launch(int M, int N, int K, float alpha, const float *A, long 
 #define QX_SG(MT_, NT_)                                                                                              \
   if (mt == MT_ && nt == NT_) {                                                                                      \
     if (split) sgemm_go<TA, TB, true, MT_, NT_>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap,     \
-                                                ncol_dev, kchunk, W, st);                                            \
+                                                ncol_dev, kchunk, W, cnt, st);                                       \
     else sgemm_go<TA, TB, false, MT_, NT_>(g, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, gamma, colmap, ncol_dev, \
-                                           kchunk, W, st);                                                           \
+                                           kchunk, W, nullptr, st);                                                  \
   }
   if (TA) {
     QX_SG(2, 2) else QX_SG(2, 3) else QX_SG(2, 4) else QX_SG(2, 5)
@@ -710,12 +739,6 @@ static void sgemm_launch(int M, int N, int K, float alpha, const float *A, long 
     QX_SG(4, 2) else QX_SG(4, 3) else QX_SG(4, 4) else QX_SG(4, 5)
   }
 #undef QX_SG
-  if (split) {
-    const long mn = (long)M * N;
-    k_gemm_reduce<float, TA, TB><<<(int)((mn + 31) / 32), RD_T, 0, st>>>(M, N, nsplit, alpha, A, lda, B, ldb, beta, C,
-                                                                          ldc, gamma, colmap, ncol_dev, W, nullptr);
-    note_launch();
-  }
 }
 
 // FP32 contractions that ran on the CUDA-core kernel instead of the tensor
@@ -731,6 +754,16 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
          long ldc, int gamma, const int *colmap, const int *ncol_dev, cudaStream_t st, void *ws, size_t ws_bytes,
          const T *rowscale, void *pad, size_t pad_bytes) {
   if (M <= 0 || N <= 0) return 0;
+  // the workspace opens with the per-tile counters of k_sgemm's split K
+  int *cnt = nullptr;
+  if (ws && ws_bytes > GEMM_COUNTER_BYTES) {
+    cnt = (int *)ws;
+    ws = (char *)ws + GEMM_COUNTER_BYTES;
+    ws_bytes -= GEMM_COUNTER_BYTES;
+  } else {
+    ws = nullptr;
+    ws_bytes = 0;
+  }
   // small FP32 contractions run on the CUDA-core kernel by choice (not counted)
   const bool small = sizeof(T) == sizeof(float) && 2.0 * (double)M * (double)N * (double)K < tc_min_flops();
   if (sizeof(T) == sizeof(float) && K > 0 && !small && (colmap || ncol_dev || !tc_enabled())) ++g_fp32_fallbacks;
@@ -770,13 +803,13 @@ int gemm(bool ta, bool tb, int M, int N, int K, T alpha, const T *A, long lda, c
     float *Cf = (float *)C;
     if (ta)
       sgemm_launch<true, false>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap, ncol_dev,
-                                ws, ws_bytes, st);
+                                ws, ws_bytes, cnt, st);
     else if (tb)
       sgemm_launch<false, true>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap, ncol_dev,
-                                ws, ws_bytes, st);
+                                ws, ws_bytes, cnt, st);
     else
       sgemm_launch<false, false>(M, N, K, (float)alpha, Af, lda, Bf, ldb, (float)beta, Cf, ldc, gamma, colmap,
-                                 ncol_dev, ws, ws_bytes, st);
+                                 ncol_dev, ws, ws_bytes, cnt, st);
     if (rowscale) scale_rows<T>(M, N, C, ldc, rowscale, colmap, ncol_dev, st);
     return 0;
   }

@@ -122,6 +122,11 @@ int launch_zcols_fwd_f32(const PipeParams &P, int npl, const float2 *bufA, float
 template <typename T> size_t fft_smem_need(const Plan &pl);
 int init_fft_roots();
 
+// The split-K workspace of gemm() opens with GEMM_COUNTER_BYTES of per-tile
+// arrival counters (zeroed when the workspace is allocated; each split
+// launch leaves them zero again); the partial sums follow.
+constexpr size_t GEMM_COUNTER_BYTES = 16384;
+constexpr long GEMM_TILE_COUNTERS = GEMM_COUNTER_BYTES / sizeof(int);
 // qx_gemm.cu: C(m,n) = alpha * op(A)(m,:) . op(B)(:,n) + beta * C(m,n), column-major.
 // TA: A stored K x M (A[m*lda + k]); TB: B stored N x K (B[k*ldb + n]).
 // gamma: 0 plain; 1 Gamma-point metric 2*sum - a0*b0; 2 KB projection
