@@ -810,6 +810,17 @@ static bool plane_enabled() {
   return !(e && e[0] == '0');
 }
 
+// Forward z pass one sphere column a thread (k_zcols_fwd) for columns of at
+// most 32 points, where it measured faster than the shared-memory pass (the
+// 48-cell batch, z lengths 21-27: 9365 -> 9735 cell-iter/s); at 54 points
+// (Si64) it measured 2.5 % slower.  QX_ZCOLS_FWD=0 / 1 forces either (read at
+// every call).
+static bool zcols_fwd_enabled(int k3) {
+  const char *e = getenv("QX_ZCOLS_FWD");
+  if (e && (e[0] == '0' || e[0] == '1')) return e[0] == '1';
+  return k3 <= 32;
+}
+
 template <typename T>
 int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin, long ldc, T *out, long ldo,
                       const double *dk, int accumulate, int nlmode, cudaStream_t st, cudaEvent_t before_unpack) {
@@ -822,9 +833,12 @@ int launch_hpsi_chunk(const Plan &pl, const PipeParams &P, int npl, const T *cin
   const bool zc = sizeof(T) == sizeof(float) &&
                   launch_zcols_inv_f32(P, npl, (const float *)cin, ldc, (float2 *)bf.bufA, st) == 0;
   if (!zc) { k_zinv<T><<<gz, QX_THREADS, smz, st>>>(P, cin, ldc, bf.bufA, g3); note_launch(); }
-  // the forward z pass stays on the shared-memory kernel: the column-wise
-  // one measured slower there (its scatter to the sphere is the cost)
-  auto zfwd = [&]() { k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch(); };
+  auto zfwd = [&]() {
+    if (sizeof(T) == sizeof(float) && zcols_fwd_enabled(P.k3) &&
+        launch_zcols_fwd_f32(P, npl, (const float2 *)bf.bufA, (float2 *)bf.zsph, st) == 0)
+      return;
+    k_zfwd<T><<<gz, QX_THREADS, smz, st>>>(P, bf.bufA, bf.zsph, g3); note_launch();
+  };
   dim3 gy(P.k3, npl);
   const size_t smy = fft_smem(P.L2, P.P1, cs);
   if (sizeof(T) == sizeof(float) && nlmode != 2 && pl.use_plane && plane_enabled() &&
