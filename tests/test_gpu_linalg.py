@@ -187,6 +187,41 @@ def test_rfft3(si8):
     assert np.all(by == 0.0)
 
 
+def _si8_at(ecutdens):
+    return cell.build_system(cell.diamond_si((1, 1, 1), seed=1), ecutdens / 4.0, ecutdens, 4, with_ewald=False)
+
+
+@pytest.mark.parametrize("make,grid", [
+    (lambda: _si8_at(32.5), (20, 20, 20)), (lambda: cell.batch_cell(42), (21, 21, 21)),
+    (lambda: cell.batch_cell(14), (24, 25, 25)), (lambda: cell.batch_cell(5), (25, 24, 25)),
+    (lambda: cell.batch_cell(1), (25, 27, 27)), (lambda: cell.batch_cell(47), (27, 27, 27)),
+    (lambda: _si8_at(75.0), (30, 30, 30)), (lambda: _si8_at(85.0), (32, 32, 32)),
+    (lambda: cell.batch_cell(6), (54, 25, 27))])
+def test_rfft3_register_lines(monkeypatch, make, grid):
+    """The FP64 full-grid transform with its z and y passes one line per
+    thread in registers (lengths up to 32) against numpy, both directions,
+    and against the shared-memory passes (QX_FULL_LINES=0)."""
+    need_gpu()
+    s = make()
+    assert tuple(s.gs.grid) == grid
+    k1, k2, k3 = grid
+    x = np.random.default_rng(5).standard_normal(s.gs.kfft0)
+    ref = np.fft.fftn(x.reshape(k3, k2, k1)).ravel() / s.gs.kfft0
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("QX_FULL_LINES", mode)
+        ctx = Context(s, QX_PREC_FP64, QX_NL_GSPACE, nband=4)
+        try:
+            fx, fy = ctx.rfft3_host(1, x, np.zeros_like(x))
+            bx, by = ctx.rfft3_host(2, fx, fy)
+        finally:
+            ctx.close()
+        assert relerr(fx + 1j * fy, ref) < 1e-13
+        assert relerr(bx, x) < 1e-13
+        out[mode] = fx + 1j * fy
+    assert relerr(out["1"], out["0"]) < 1e-13
+
+
 @pytest.mark.parametrize("prec,tol", [(QX_PREC_FP64, 1e-12), (QX_PREC_MIXED, 1e-5)])
 def test_tddft_overlap(si8, si8_psi, prec, tol):
     """tddft_fssh_cal_matrix (tddft_fssh.f90:1344-1414): aij = <psi_i(t)|psi_j(t+dt)>
