@@ -956,19 +956,20 @@ int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double s
   const int nlines = pl.xlines<T>();
   const int nch = (k2 + nlines - 1) / nlines;
   const FftLen &L1 = pl.L[0], &L2 = pl.L[1], &L3 = pl.L[2];
-  // FP64 z and y lines of at most 32 points: one line per thread in registers
+  // FP64 lines of at most 32 points: one line per thread in registers (the
+  // x pass applies the scale)
   auto lines = [&](int axis) {
     return sizeof(T) == sizeof(double) &&
-           launch_full_lines_f64((double2 *)g, k1, k2, k3, axis, sign, st) == 0;
+           launch_full_lines_f64((double2 *)g, k1, k2, k3, axis, sign, scale, st) == 0;
   };
   if (sign > 0) {
     if (!lines(2)) { k_full_z<T, +1><<<k2 * nxc, QX_THREADS, fft_smem(L3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L3, g3); note_launch(); }
     if (!lines(1)) { k_full_y<T, +1><<<k3 * nxc, QX_THREADS, fft_smem(L2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L2, g2); note_launch(); }
-    k_full_x<T, +1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch();
+    if (!lines(0)) { k_full_x<T, +1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch(); }
   } else {
     if (!lines(2)) { k_full_z<T, -1><<<k2 * nxc, QX_THREADS, fft_smem(L3, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L3, g3); note_launch(); }
     if (!lines(1)) { k_full_y<T, -1><<<k3 * nxc, QX_THREADS, fft_smem(L2, tx | 1, cs), st>>>(g, k1, k2, k3, tx, L2, g2); note_launch(); }
-    k_full_x<T, -1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch();
+    if (!lines(0)) { k_full_x<T, -1><<<k3 * nch, QX_THREADS, fft_smem(L1, nlines | 1, cs), st>>>(g, k1, k2, k3, nlines, L1, g1, scale); note_launch(); }
   }
   return 0;
 }

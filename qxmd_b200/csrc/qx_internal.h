@@ -105,9 +105,10 @@ int launch_fnl_r_chunk(const Plan &pl, const PipeParams &P, int npl, const T *ci
 void fnl_r_sum(const double *fpart, int npair, int natom, double *fnl, cudaStream_t st);
 template <typename T>
 int launch_full_fft(const Plan &pl, typename c2t<T>::type *g, int sign, double scale, cudaStream_t st);
-// qx_fftfull.cu: one z (axis 2) or y (axis 1) pass of the FP64 full-grid
-// transform with the lines in registers; -1 when the length has no kernel.
-int launch_full_lines_f64(double2 *g, int k1, int k2, int k3, int axis, int sign, cudaStream_t st);
+// qx_fftfull.cu: one z (axis 2), y (axis 1) or x (axis 0, times scale) pass
+// of the FP64 full-grid transform with the lines in registers; -1 when the
+// length has no kernel.
+int launch_full_lines_f64(double2 *g, int k1, int k2, int k3, int axis, int sign, double scale, cudaStream_t st);
 template <typename T> void set_fft_smem_limits(size_t bytes);
 // qx_fftplane.cu: fused y-x-y pass (FP32, k1 x k2 planes of a specialised
 // shape, QX_PLANE_GRIDS); returns -1 when the grid is not covered.
