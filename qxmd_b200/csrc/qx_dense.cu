@@ -1141,58 +1141,73 @@ __global__ void __launch_bounds__(TRR_W * 32, 1)
     const double vrow = (lane < NR) ? vof(r0 + lane) : 0.0;
     if (lane < NR) vsm[warp][lane] = vrow;
     __syncwarp();
-    {
-      double sc[NC];
+    // The product and the update for column k, compiled once for each first
+    // live column slot P = k / 32: the columns j <= k of slots below P are
+    // never read again (the product's entries j <= k are masked, the next
+    // columns gathered are > k), so their FMAs are left out.  P is a
+    // compile-time constant in each copy, so no branch sits inside the
+    // unrolled loops; the result is the same bit for bit.
+    auto product_update = [&](auto pc) {
+      constexpr int P = decltype(pc)::value;
+      {
+        double sc[NC];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) sc[c] = 0.0;
+        for (int c = 0; c < NC; ++c) sc[c] = 0.0;
+        if (rows_active) {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) {
+            const double vr = vsm[warp][r];
+#pragma unroll
+            for (int c = P; c < NC; ++c) sc[c] = fma(a[r][c], vr, sc[c]);
+          }
+        }
+#pragma unroll
+        for (int c = P; c < NC; ++c) part[warp][lane + 32 * c] = sc[c];
+      }
+      __syncthreads();                                                 // (2)
+      for (int j = 32 * P + tid; j < NCOL; j += TRR_W * 32) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < TRR_W; ++w) acc += part[w][j];
+        ps[j] = (j > k && j < n) ? t * acc : 0.0;
+      }
+      __syncthreads();                                                 // (3)
+      double kk = 0.0;
+#pragma unroll
+      for (int c = P; c < NC; ++c) kk = fma(vof(lane + 32 * c), ps[lane + 32 * c], kk);
+      const double K = 0.5 * t * warp_sum(kk);
+      // p of rows <= k is zero (ps below slot P is not rewritten in this copy)
+      const double prow = (r0 + lane > k) ? ps[min(r0 + lane, NCOL - 1)] : 0.0;
+      const double wrow = (lane < NR) ? fma(-K, vrow, prow) : 0.0;
+      if (lane < NR) wsm[warp][lane] = wrow;
+      __syncwarp();
+      // A -= v w^T, then A -= w v^T: each pass keeps one vector of the
+      // lane's columns live beside the block
       if (rows_active) {
+        double wc[NC];
+#pragma unroll
+        for (int c = P; c < NC; ++c) wc[c] = fma(-K, vof(lane + 32 * c), ps[lane + 32 * c]);
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-          const double vr = vsm[warp][r];
+          const double vi = vsm[warp][r];
 #pragma unroll
-          for (int c = 0; c < NC; ++c) sc[c] = fma(a[r][c], vr, sc[c]);
+          for (int c = P; c < NC; ++c) a[r][c] = fma(-vi, wc[c], a[r][c]);
+        }
+        double vc[NC];
+#pragma unroll
+        for (int c = P; c < NC; ++c) vc[c] = vof(lane + 32 * c);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          const double wi = wsm[warp][r];
+#pragma unroll
+          for (int c = P; c < NC; ++c) a[r][c] = fma(-wi, vc[c], a[r][c]);
         }
       }
-#pragma unroll
-      for (int c = 0; c < NC; ++c) part[warp][lane + 32 * c] = sc[c];
-    }
-    __syncthreads();                                                   // (2)
-    for (int j = tid; j < NCOL; j += TRR_W * 32) {
-      double acc = 0.0;
-#pragma unroll
-      for (int w = 0; w < TRR_W; ++w) acc += part[w][j];
-      ps[j] = (j > k && j < n) ? t * acc : 0.0;
-    }
-    __syncthreads();                                                   // (3)
-    double kk = 0.0;
-#pragma unroll
-    for (int c = 0; c < NC; ++c) kk = fma(vof(lane + 32 * c), ps[lane + 32 * c], kk);
-    const double K = 0.5 * t * warp_sum(kk);
-    const double wrow = (lane < NR) ? fma(-K, vrow, ps[min(r0 + lane, NCOL - 1)]) : 0.0;
-    if (lane < NR) wsm[warp][lane] = wrow;
-    __syncwarp();
-    // A -= v w^T, then A -= w v^T: each pass keeps one vector of the lane's
-    // columns live beside the block
-    if (rows_active) {
-      double wc[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) wc[c] = fma(-K, vof(lane + 32 * c), ps[lane + 32 * c]);
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const double vi = vsm[warp][r];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) a[r][c] = fma(-vi, wc[c], a[r][c]);
-      }
-      double vc[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) vc[c] = vof(lane + 32 * c);
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const double wi = wsm[warp][r];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) a[r][c] = fma(-wi, vc[c], a[r][c]);
-      }
-    }
+    };
+    const int pk = k >> 5;   // uniform: every thread takes the same copy
+    dense_static_for<0, NC>([&](auto pc) {
+      if (decltype(pc)::value == pk) product_update(pc);
+    });
     __syncwarp();   // vsm, wsm are rewritten in the next step
   }
   // the last 2 x 2 block
