@@ -1,19 +1,20 @@
-// Fused y-x-y pass of the FP32 H|psi> pipeline for grids with k1 == k2 == N,
-// one CTA per (band pair, z plane), one grid line per thread with the whole
-// line in registers (compile-time-length FFTs of qx_regfft.cuh):
+// Fused y-x-y pass of the FP32 H|psi> pipeline for k1 x k2 planes of the
+// specialised shapes (x length NX = k1, y length NY = k2), one CTA per (band
+// pair, z plane or two), one grid line per thread with the whole line in
+// registers (compile-time-length FFTs of qx_regfft.cuh):
 //   (1) backward y-FFT of each of the P1 sphere columns, read straight from
 //       the z-transformed plane in bufA (rows outside the sphere are zero);
 //   (2) per grid row: backward x-FFT (P1 non-zero inputs), times V_loc(r),
 //       forward x-FFT, keep the P1 sphere columns;
 //   (3) forward y-FFT of each column, the sphere rows written back to bufA.
-// Between the steps the plane lives in shared memory as N x P1 complex
+// Between the steps the plane lives in shared memory as NY x P1 complex
 // values.  This replaces k_ypass<+1>, k_xvx and k_ypass<-1> (hcnonloc's
 // c2r -> V_loc * psi -> r2c, engrad.f90:484-571) and removes the two round
 // trips of bufB through L2/HBM.
 //
-// This header holds the kernel templates and their per-length launchers; each
-// qx_fftplane_*.cu file instantiates a group of lengths (so the groups compile
-// in parallel), and qx_fftplane.cu dispatches on the grid length.
+// This header holds the kernel templates and their per-shape launchers; each
+// qx_fftplane_*.cu file instantiates a group of shapes and z lengths (so the
+// groups compile in parallel), and qx_fftplane.cu dispatches on the grid.
 #pragma once
 #include "qx_fftplane.h"
 #include "qx_regfft.cuh"
